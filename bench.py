@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the MiniFS iteration hot path on B200.
+
+One step = one iteration of the reference's main loop (main.cpp:201-291:
+Roe flux + residual, local time step, LU-SGS forward/backward sweeps with
+the update, node-based Green-Gauss gradient, residual norm) over the whole
+mesh.  Metric: cell-updates/s = cells x steps / device time.
+
+Workload (N=1): the 64^3 x 6 = 1,572,864-tet cube (interior jitter 0.15h,
+seed 1), Mach 0.5, alpha 2 deg, CFL 10, far field on all sides, freestream
+plus a 5% Gaussian density bump; FP64.  The working set (~1.2 GB) is far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With --gpus N > 1 (one process per GPU under torchrun) every rank runs its
+own replica of the workload (the path has no exchange step) and rank 0
+prints the aggregate.  --impl reference times the reference's own CPU code
+(oracle/_ref, all host cores) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s on 1 B200: FP64 vs mixed vs batched at equal residual drop"
+UNIT = "cell-updates/s"
+
+
+def workload(n: int) -> dict:
+    return dict(name=f"cube{n}x6_M0.5_a2_cfl10_fp64", n=n, jitter=0.15, seed=1, mach=0.5,
+                alpha=2.0, cfl=10.0, bump_amp=0.05, bump_sigma=0.1)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mfgpu", choices=["mfgpu", "reference"])
+    ap.add_argument("--size", type=int, default=64, help="hexes per cube edge (64 = 1.57M tets)")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per iteration (each input array element counted once per
+# kernel that needs it, each output once)
+# ---------------------------------------------------------------------------
+
+def algorithmic_bytes(C, G, F, N, K):
+    n = C + G
+    S = 2 * F - G
+    csr = 4 * (C + 1) + 4 * S
+    return {
+        # flux + res, time step + CellIsMG + limit, Diag: one fused gather
+        "face_gather": F * (32 + 8) + F * 24 + 40 * n + 24 * n + 8 * C + csr +
+                       40 * C + 8 * C + 8 * C,
+        "sweep_fwd": F * 40 + csr + 40 * n + 40 * C + 8 * C + 40 * C,
+        # backward sweep with the update fused: + the new state
+        "sweep_bwd_update": F * 40 + csr + 40 * n + 40 * C + 8 * C + 40 * C + 40 * C,
+        "node_values": 40 * n + 12 * K + 8 * K + 8 * N + 40 * N,
+        "grad_faces": 40 * N + F * (12 + 32 + 8) + 8 * C + 120 * n,
+        "norm": 0,
+    }
+
+
+KERNEL_OF_PHASE = {"face_gather": "k_face_gather", "sweep_fwd": "k_sweep_fwd",
+                   "sweep_bwd_update": "k_sweep_bwd", "node_values": "k_node_values",
+                   "grad_faces": "k_grad_faces", "norm": "k_norm_final"}
+
+
+def read_traffic(kernel: str, workload_name: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and \
+                parts[1] == workload_name:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own code (oracle/_ref), else the C oracle
+# ---------------------------------------------------------------------------
+
+def cpu_reference_run(mesh, wl, iters, threads=None):
+    from oracle import refrun
+    flow = dict(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"], cfl_end=wl["cfl"],
+                n_steps=iters, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
+                bump_x0=0.5, bump_y0=0.5, bump_z0=0.5)
+    threads = threads or os.cpu_count()
+    if refrun.available(tdtree=True):
+        r = refrun.run(mesh, flow, tdtree=True, threads=threads, light=True, dump=False)
+        kind, desc = "reference", f"reference TDTree build (OpenMP, {threads} threads)"
+    elif refrun.available():
+        r = refrun.run(mesh, flow, light=True, dump=False)
+        threads, kind, desc = 1, "reference", "reference serial build (1 thread)"
+    else:
+        return None
+    return dict(iter_times=list(r["iter_times"]), threads=threads, kind=kind, desc=desc)
+
+
+def cpu_port_run(pg, params, iters):
+    from oracle import oracle_py
+    o = oracle_py.OracleSolver(pg.arrays, params.as_dict(), pg.q0,
+                               (pg.n_node, pg.n_face, pg.n_cell, pg.n_bface))
+    times = []
+    for _ in range(iters):
+        t = time.perf_counter()
+        o.step()
+        times.append(time.perf_counter() - t)
+    return dict(iter_times=times, threads=1, kind="port", desc="C restatement (1 thread)")
+
+
+def cpu_baseline(mesh, pg, params, wl, iters=2):
+    r = cpu_reference_run(mesh, wl, iters)
+    if r is None:
+        r = cpu_port_run(pg, params, iters)
+    t = sum(r["iter_times"])
+    return {"value": pg.n_cell * len(r["iter_times"]) / t, "unit": UNIT, "cores": r["threads"],
+            "kind": r["kind"],
+            "sample": f"{wl['name']}, {len(r['iter_times'])} full iterations after setup, "
+                      f"{r['desc']}, {t:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+
+def build_case(wl):
+    from minifs_b200 import grid as gr, meshgen
+    mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
+    params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+    pg = gr.prepare(mesh, params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
+    return mesh, params, pg
+
+
+def run_reference_arm(args, rank, world):
+    wl = workload(args.size)
+    if rank != 0:
+        return
+    from minifs_b200 import meshgen
+    mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
+    total = args.warmup + args.steps
+    r = cpu_reference_run(mesh, wl, total)
+    if r is None:
+        from minifs_b200 import grid as gr
+        params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+        pg = gr.prepare(mesh, params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
+        r = cpu_port_run(pg, params, total)
+    timed = r["iter_times"][args.warmup:]
+    t = sum(timed)
+    value = mesh.n_cell * len(timed) / t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / len(timed), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "cells": mesh.n_cell, "parallelism": "cpu"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"],
+                             "kind": r["kind"],
+                             "sample": f"{wl['name']}: {args.warmup} warm-up + {args.steps} "
+                                       f"timed full iterations, {r['desc']}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from minifs_b200 import _lib
+    from minifs_b200.solver import Solver
+
+    wl = workload(args.size)
+    mesh, params, pg = build_case(wl)
+    s = Solver(pg, params, device=local)
+    # a dedicated (capturable) stream shared by the library and the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    s.set_stream(stream.cuda_stream)
+    info = s.info()
+    C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
+    K = int(pg.arrays["nnpc"].sum())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up (also builds the CUDA graphs)
+    s.calculate_gradient()
+    s.iterate(max(args.warmup, 3), norms=False)
+    barrier()
+
+    launches0 = _lib.kernel_launches()
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        s.iterate(args.steps, norms=False)
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+    launches = _lib.kernel_launches() - launches0
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * C * args.steps / (ms / 1e3)
+    clocks = clk.summary()
+    norms = s.residual_norm()
+
+    # phase breakdown with CUDA events on the same stream (same fused kernels)
+    phase_iters = max(3, min(args.steps, 10))
+    phases = s.profile_phases(phase_iters)
+    alg = algorithmic_bytes(C, G, F, N, K)
+    peak, peak_kind = measured_peak()
+    nl = {"face_gather": 1, "sweep_fwd": info["fw_levels"], "sweep_bwd_update": info["bw_levels"],
+          "node_values": 1, "grad_faces": 1, "norm": 1}
+    phase_out = {}
+    for ph, tot in phases.items():
+        per_it = tot / phase_iters
+        phase_out[ph] = {"ms_per_iter": per_it, "launches_per_iter": nl[ph],
+                         "alg_bytes": alg[ph],
+                         "gbs": (alg[ph] / (per_it / 1e3) / 1e9) if per_it > 0 else None}
+    dom = max(phases, key=lambda k: phases[k])
+    dom_ms_launch = phases[dom] / phase_iters / nl[dom]
+    dom_bytes_launch = alg[dom] / nl[dom]
+    achieved = dom_bytes_launch / (dom_ms_launch / 1e3) / 1e9
+    traffic = read_traffic(KERNEL_OF_PHASE[dom], wl["name"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": KERNEL_OF_PHASE[dom],
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "alg_bytes_per_launch": dom_bytes_launch, "ms_per_launch": dom_ms_launch}
+    flux_grad_ms = sum(phases[p] for p in ("face_gather", "node_values", "grad_faces")) / \
+        phase_iters
+    flux_grad_bytes = alg["face_gather"] + alg["node_values"] + alg["grad_faces"]
+
+    # end to end through the C ABI with host buffers (pinned), every step:
+    # host state in, one iteration, host state and residual out
+    qh = torch.empty(5 * pg.n, dtype=torch.float64, pin_memory=True).numpy()
+    qo = torch.empty(5 * pg.n, dtype=torch.float64, pin_memory=True).numpy()
+    rh = torch.empty(5 * C, dtype=torch.float64, pin_memory=True).numpy()
+    qh[:] = s.download("q")
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        s.iterate_host(1, qh, qo, rh)
+        qh, qo = qo, qh
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * C * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": 8 * 5 * pg.n, "d2h_bytes_per_step": 8 * 5 * pg.n + 8 * 5 * C,
+           "steps": args.e2e_steps, "api": "mfg_iterate_host (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(mesh, pg, params, wl)
+        except Exception as e:  # reported, never silently replaced
+            cpu = {"error": str(e)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": wl["name"], "cells": C, "faces": F, "nodes": N,
+                       "ghosts": G, "precision": "fp64 (bit-faithful)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "l2": "no flush: working set "
+                             f"{info['device_bytes'] / 2**20:.0f} MiB > 126 MB L2",
+                       "lusgs_levels": {"forward": info["fw_levels"],
+                                        "backward": info["bw_levels"]}},
+            "roofline": roofline,
+            "flux_plus_gradient": {"gbs": flux_grad_bytes / (flux_grad_ms / 1e3) / 1e9,
+                                   "frac": flux_grad_bytes / (flux_grad_ms / 1e3) / 1e9 / peak},
+            "phases": phase_out,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "residual_norm": [float(x) for x in norms],
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,226 @@
+/*
+ * mfgpu -- B200 (sm_100a) implementation of the MiniFS iteration hot path.
+ *
+ * C ABI: plain pointers and sizes, an opaque context, int status codes.
+ * Each entry point below names the reference routine it replaces
+ * (paths relative to the MiniFS project root).
+ *
+ * Array conventions follow the reference's PolyGrid after PreprocessGrid:
+ *   - C = n_cell, G = n_bface, F = n_face, N = n_node, n = C + G;
+ *   - faces [0, G) are boundary faces; the ghost cell of boundary face k is
+ *     C + k (SpecifyBC, src/Kernels/load_grid.cpp:893-901);
+ *   - flow fields are SoA blocks: q = [rho | u | v | w | p], each block n
+ *     long; res is 5 blocks of C; dqdx/dqdy/dqdz and DQ are 5 blocks of n.
+ *   - floating point is IEEE double; indices are int32 (number_type.h:26-39).
+ *
+ * Calls on one context are not reentrant (the reference is single-threaded,
+ * main.cpp:201-291).  All device work is issued on the context's stream;
+ * entry points that hand data to the host synchronise that stream.
+ */
+#ifndef MFGPU_H
+#define MFGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define MFG_OK 0
+#define MFG_ERR_INVALID (-1)     /* bad argument, size or field id */
+#define MFG_ERR_CUDA (-2)        /* CUDA runtime error (see mfg_last_cuda_error) */
+#define MFG_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define MFG_ERR_TIMEOUT (-4)     /* a bounded device-side wait gave up */
+#define MFG_ERR_NONFINITE (-5)   /* NaN/Inf found in residual or state */
+#define MFG_ERR_UNSUPPORTED (-6) /* LU-SGS order inconsistent with layers, etc. */
+#define MFG_ERR_BADMESH (-7)     /* degenerate volume, bad connectivity */
+#define MFG_ERR_NODEVICE (-8)    /* no CUDA device / wrong architecture */
+
+/* Boundary-condition codes (src/Base/constant.h:47-51). */
+#define MFG_BC_WALL 3
+#define MFG_BC_SYMM 4
+#define MFG_BC_FAR_FIELD 6
+#define MFG_BC_FAR_FIELD_MOD 61
+#define MFG_BC_INTERFACE 10
+
+/* Field ids for mfg_download / mfg_upload. */
+#define MFG_FIELD_Q 0    /* [5n] rho,u,v,w,p (download/upload) */
+#define MFG_FIELD_RES 1  /* [5C] residual (download) */
+#define MFG_FIELD_DT 2   /* [C] local time step (download) */
+#define MFG_FIELD_DQ 3   /* [5n] LU-SGS increment (download) */
+#define MFG_FIELD_DQDX 4 /* [5n] gradient x (download) */
+#define MFG_FIELD_DQDY 5 /* [5n] gradient y (download) */
+#define MFG_FIELD_DQDZ 6 /* [5n] gradient z (download) */
+#define MFG_FIELD_DIAG 7 /* [C] LU-SGS diagonal of the last sweep (download) */
+
+/* Precision modes. */
+#define MFG_PREC_FP64 0  /* the drop-in: every operation in FP64, bit-faithful */
+#define MFG_PREC_MIXED 1 /* FP32 Roe flux, gradient, LU-SGS off-diagonal terms */
+
+/* Solver parameters: the globals of src/Base/para_field_global.cpp.
+ * Fill the inputs (mach ... ratio_dtmax) and call mfg_params_derive to set
+ * the dependent values with the formulas of para_field_global.cpp:150-209. */
+typedef struct mfg_params {
+  /* inputs */
+  double mach, alpha, beita, re, T, gam, gascon;
+  double cfl_start, cfl_end;
+  int32_t cfl_nstep;
+  double lhs_omga, epsa_r, ratio_dtmax;
+  /* derived */
+  double amu, ainf, uqq, u_s, v_s, w_s, p_s, rho_s, p_bar, gamm1;
+  double p_stag, e_stag, p_min, p_max, rho_min, rho_max, p_break, e_stag_max;
+  double cfl_min, cfl_ratio, alf_l;
+} mfg_params;
+
+/* Grid as the reference holds it after PreprocessGrid (load_grid.cpp:405-540).
+ * Node-weight arrays are those of ComputeWeight3D_Node and FindNodeSYMM
+ * (grid_polyhedra_auxiliary_functions.cpp:831-1049, :2060-2140). */
+typedef struct mfg_mesh {
+  int32_t n_node, n_face, n_cell, n_bface;
+  const int32_t *f2c;    /* [2F]; ghost of boundary face k = C + k */
+  const int32_t *nnpf;   /* [F] nodes per face */
+  const int32_t *f2n;    /* [sum nnpf] */
+  const int32_t *bctype; /* [G] BC type of each boundary face */
+  const double *xfn, *yfn, *zfn, *area, *xfc, *yfc, *zfc; /* [F] */
+  const double *xcc, *ycc, *zcc, *vol;                   /* [n] */
+  const double *wnode;   /* WeightNodeDist [N] */
+  const int32_t *nmark;  /* Nmark [N] */
+  const double *wbface;  /* WeightNodeBFace2C, f2n layout of faces [0, G) */
+  const int32_t *nnpc;   /* nNPC [C] */
+  const int32_t *c2n;    /* C2N [sum nnpc] */
+  const double *wc2n;    /* WeightNodeC2N [sum nnpc] */
+  const int32_t *nodesymm;                            /* [N] */
+  const double *xfn_n_symm, *yfn_n_symm, *zfn_n_symm; /* [N] */
+  const int32_t *lusgs_order; /* LUSGSCellOrder [C], NULL = identity */
+  const int32_t *lusgs_layer; /* LUSGSLayer [n], NULL = identity */
+} mfg_mesh;
+
+typedef struct mfg_ctx mfg_ctx;
+
+/* Statistics of a context (level sets, memory). */
+typedef struct mfg_info {
+  int32_t n_cell, n_face, n_node, n_bface;
+  int32_t fw_levels, bw_levels;     /* LU-SGS level-set counts */
+  int32_t max_level_cells;          /* widest level */
+  int32_t precision;
+  int64_t device_bytes;             /* device memory held by the context */
+  int32_t sweep_mode;               /* 0 = one launch per level, 1 = persistent */
+  int32_t graph_ready;
+} mfg_info;
+
+/* ---- parameters -------------------------------------------------------- */
+/* Reference defaults (para_field_global.cpp:37-221), then derived values. */
+void mfg_params_default(mfg_params *p);
+/* para_field_global.cpp:150-209 evaluated at run time. */
+int mfg_params_derive(mfg_params *p);
+
+/* ---- context ----------------------------------------------------------- */
+/* Uploads the grid and the initial state q0 [5n] (ghost states included) to
+ * `device` and builds the CSR gathers and LU-SGS level sets.  Replaces the
+ * lazy allocations of ZeroResiduals / ComputeTimeStep / ForwardLUSGS
+ * (cal_flux.cpp:57-63, compute_timestep.cpp:77-84, forward_lusgs.cpp:112-117)
+ * and AllocAndCalQuantityGradient's storage (cal_gradient.cpp:50-78); the
+ * gradient itself is computed by the first mfg_calculate_gradient. */
+int mfg_create(const mfg_mesh *mesh, const mfg_params *params, const double *q0,
+               int32_t device, int32_t precision, mfg_ctx **out);
+int mfg_destroy(mfg_ctx *ctx);
+/* Issue all further work on this cudaStream_t (NULL = the context's own). */
+int mfg_set_stream(mfg_ctx *ctx, void *cuda_stream);
+int mfg_set_params(mfg_ctx *ctx, const mfg_params *params);
+int mfg_info_get(mfg_ctx *ctx, mfg_info *info);
+/* Sweep strategy: 0 = one kernel per level, 1 = persistent kernel with a
+ * bounded device-wide barrier between levels. */
+int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode);
+
+/* ---- the iteration path (reference routine replaced in brackets) -------- */
+/* [ZeroResiduals, cal_flux.cpp:54-72] */
+int mfg_zero_residuals(mfg_ctx *ctx);
+/* [InviscidFlux, cal_flux.cpp:84-192: SetQlQrWithQ + RoeFlux_noprec + LoadFlux]
+ * res += sum of first-order Roe face fluxes (cell-centric gather, no atomics). */
+int mfg_inviscid_flux(mfg_ctx *ctx);
+/* [ComputeTimeStep, compute_timestep.cpp:66-121: TimeStepNormal_new +
+ * CellIsMG + LimitTimeStep]; iter_done is the reference's global counter. */
+int mfg_compute_timestep(mfg_ctx *ctx, int32_t iter_done);
+/* [ForwardLUSGS, forward_lusgs.cpp:67-162: Diag, CalDiagLUSGS, SolveLUSGS3D
+ * forward/backward sweeps, UpdateFlowField3D_CFL3d] */
+int mfg_forward_lusgs(mfg_ctx *ctx);
+/* [CalculateGradient, cal_gradient.cpp:87-167: CompNodeVar3D_dist +
+ * CompGradientQ_Gauss_Node for rho,u,v,w,p] */
+int mfg_calculate_gradient(mfg_ctx *ctx);
+/* The whole main-loop body (main.cpp:201-291) n times, fused kernels in a
+ * CUDA graph.  norms (optional, host) receives 5 residual L2 norms per
+ * iteration (main.cpp:294-317 evaluated every iteration). */
+int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms);
+/* End-to-end form with host buffers: copies q_in [5n] (host) in, runs
+ * n_iter iterations, copies the state to q_out [5n] and the residual to
+ * res_out [5C] (either may be NULL).  Pinned host memory is fastest. */
+int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const double *q_in,
+                     double *q_out, double *res_out, double *norms);
+/* Phases of one fused iteration, for mfg_profile_phases. */
+#define MFG_NPHASES 6 /* face gather (flux+dt+Diag), forward sweep, backward sweep +
+                         update, node values, gradient face sums, norm reduction */
+/* Same work as mfg_iterate without the graph, with CUDA events recorded on
+ * the context's stream between phases; phase_ms[MFG_NPHASES] receives the
+ * summed device time of each phase over the n_iter iterations. */
+int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *phase_ms);
+/* [main.cpp:294-317] L2 norm of each residual component. */
+int mfg_residual_norm(mfg_ctx *ctx, double out[5]);
+/* The running extrema dt_max / dt_min (para_field_global.cpp:220-221,
+ * updated in LimitTimeStep, compute_timestep.cpp:914-918). */
+int mfg_get_dt_extrema(mfg_ctx *ctx, double *dt_max, double *dt_min);
+int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min);
+
+/* ---- data movement ----------------------------------------------------- */
+int mfg_download(mfg_ctx *ctx, int32_t field, double *host);
+int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host);
+int mfg_sync(mfg_ctx *ctx);
+
+/* ---- diagnostics ------------------------------------------------------- */
+const char *mfg_error_string(int32_t code);
+const char *mfg_last_cuda_error(void);
+/* Number of kernels this library launched (all contexts), for accounting. */
+int64_t mfg_kernel_launches(void);
+
+/* ---- host preprocessing (restatements of the reference's setup) -------- */
+/* Raw grid as read from a FlowStar binary file (ReadMFlowGrid_binary,
+ * load_grid.cpp:129-273): boundary faces first, f2c[2k+1] = -patch id. */
+typedef struct mfg_raw_grid {
+  int32_t n_node, n_face, n_cell, n_bface;
+  const double *x, *y, *z;
+  const int32_t *nnpf, *f2n;
+  int32_t *f2c; /* rewritten in place by mfg_prep_specify_bc */
+} mfg_raw_grid;
+
+/* [SpecifyBC, load_grid.cpp:804-902]: bctype[k] = patch_types[patch(k) - 1],
+ * f2c[2k+1] = C + k. */
+int mfg_prep_specify_bc(mfg_raw_grid *g, int32_t n_patch, const int32_t *patch_types,
+                        int32_t *bctype);
+/* [PolyGrid::ComputeMetrics, grid_polyhedra.cpp:1071-1118]: outputs sized
+ * [F] for face arrays and [n] for cell arrays. */
+int mfg_prep_metrics(const mfg_raw_grid *g, double *xfn, double *yfn, double *zfn, double *area,
+                     double *xfc, double *yfc, double *zfc, double *xcc, double *ycc,
+                     double *zcc, double *vol);
+/* [AllocAndInitFlowfield + SetGhostVariables, load_grid.cpp:571-601,
+ * :953-1212] with an optional Gaussian density bump at the cell centroids
+ * rho = rho_s*(1 + amp*exp(-|x - x0|^2 / (2 sigma^2))) applied in between. */
+int mfg_prep_init_flow(const mfg_raw_grid *g, const mfg_params *p, const int32_t *bctype,
+                       const double *xfn, const double *yfn, const double *zfn,
+                       const double *xcc, const double *ycc, const double *zcc,
+                       double bump_amp, double bump_sigma, double bump_x0, double bump_y0,
+                       double bump_z0, double *q);
+/* Sizes for mfg_prep_node_weights: *n_c2n = sum over cells of distinct nodes. */
+int mfg_prep_c2n_size(const mfg_raw_grid *g, int64_t *n_c2n);
+/* [CalnNPC/CalC2N + ComputeWeight3D_Node + FindNodeSYMM]. */
+int mfg_prep_node_weights(const mfg_raw_grid *g, const int32_t *bctype, const double *xfn,
+                          const double *yfn, const double *zfn, const double *xfc,
+                          const double *yfc, const double *zfc, const double *xcc,
+                          const double *ycc, const double *zcc, double *wnode, int32_t *nmark,
+                          double *wbface, int32_t *nnpc, int32_t *c2n, double *wc2n,
+                          int32_t *nodesymm, double *xfn_n_symm, double *yfn_n_symm,
+                          double *zfn_n_symm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFGPU_H */

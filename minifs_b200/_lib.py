@@ -1,0 +1,154 @@
+"""ctypes binding of ``libmfgpu.so`` (declarations in include/mfgpu.h).
+
+Loading fails loudly when the library is missing: there is no fallback
+implementation of the hot path.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libmfgpu.so")
+
+i32p = ct.POINTER(ct.c_int32)
+f64p = ct.POINTER(ct.c_double)
+
+MFG_OK = 0
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory",
+          -4: "device wait timed out", -5: "non-finite value", -6: "unsupported configuration",
+          -7: "bad mesh", -8: "no usable CUDA device"}
+
+FIELD = {"q": 0, "res": 1, "dt": 2, "dq": 3, "dqdx": 4, "dqdy": 5, "dqdz": 6, "diag": 7}
+PREC = {"fp64": 0, "mixed": 1}
+PHASES = ("face_gather", "sweep_fwd", "sweep_bwd_update", "node_values", "grad_faces", "norm")
+
+PARAM_INPUTS = ("mach", "alpha", "beita", "re", "T", "gam", "gascon", "cfl_start", "cfl_end")
+PARAM_FIELDS = (
+    [(k, ct.c_double) for k in PARAM_INPUTS] + [("cfl_nstep", ct.c_int32)] +
+    [(k, ct.c_double) for k in ("lhs_omga", "epsa_r", "ratio_dtmax", "amu", "ainf", "uqq",
+                                "u_s", "v_s", "w_s", "p_s", "rho_s", "p_bar", "gamm1", "p_stag",
+                                "e_stag", "p_min", "p_max", "rho_min", "rho_max", "p_break",
+                                "e_stag_max", "cfl_min", "cfl_ratio", "alf_l")])
+
+
+class Params(ct.Structure):
+    _fields_ = PARAM_FIELDS
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+MESH_I32 = ("f2c", "nnpf", "f2n", "bctype")
+MESH_F64_FACE = ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc")
+MESH_F64_CELL = ("xcc", "ycc", "zcc", "vol")
+
+
+class Mesh(ct.Structure):
+    _fields_ = ([("n_node", ct.c_int32), ("n_face", ct.c_int32), ("n_cell", ct.c_int32),
+                 ("n_bface", ct.c_int32)] +
+                [(k, i32p) for k in MESH_I32] +
+                [(k, f64p) for k in MESH_F64_FACE + MESH_F64_CELL] +
+                [("wnode", f64p), ("nmark", i32p), ("wbface", f64p), ("nnpc", i32p),
+                 ("c2n", i32p), ("wc2n", f64p), ("nodesymm", i32p), ("xfn_n_symm", f64p),
+                 ("yfn_n_symm", f64p), ("zfn_n_symm", f64p), ("lusgs_order", i32p),
+                 ("lusgs_layer", i32p)])
+
+
+class Info(ct.Structure):
+    _fields_ = [("n_cell", ct.c_int32), ("n_face", ct.c_int32), ("n_node", ct.c_int32),
+                ("n_bface", ct.c_int32), ("fw_levels", ct.c_int32), ("bw_levels", ct.c_int32),
+                ("max_level_cells", ct.c_int32), ("precision", ct.c_int32),
+                ("device_bytes", ct.c_int64), ("sweep_mode", ct.c_int32),
+                ("graph_ready", ct.c_int32)]
+
+
+class RawGrid(ct.Structure):
+    _fields_ = [("n_node", ct.c_int32), ("n_face", ct.c_int32), ("n_cell", ct.c_int32),
+                ("n_bface", ct.c_int32), ("x", f64p), ("y", f64p), ("z", f64p),
+                ("nnpf", i32p), ("f2n", i32p), ("f2c", i32p)]
+
+
+class MfgError(RuntimeError):
+    def __init__(self, func: str, code: int, detail: str = ""):
+        msg = f"{func} failed: {ERRORS.get(code, code)}"
+        if detail:
+            msg += f" ({detail})"
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+
+
+def load(build_if_missing: bool = True):
+    """Load libmfgpu.so, building it in-tree with nvcc if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if not build_if_missing:
+            raise FileNotFoundError(f"{LIB_PATH} is not built (python -m minifs_b200.build)")
+        from . import build as _build
+        _build.build()
+    lib = ct.CDLL(LIB_PATH)
+    ctxp = ct.c_void_p
+    sig = {
+        "mfg_params_default": (None, [ct.POINTER(Params)]),
+        "mfg_params_derive": (ct.c_int, [ct.POINTER(Params)]),
+        "mfg_create": (ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Params), f64p, ct.c_int32,
+                                  ct.c_int32, ct.POINTER(ctxp)]),
+        "mfg_destroy": (ct.c_int, [ctxp]),
+        "mfg_set_stream": (ct.c_int, [ctxp, ct.c_void_p]),
+        "mfg_set_params": (ct.c_int, [ctxp, ct.POINTER(Params)]),
+        "mfg_info_get": (ct.c_int, [ctxp, ct.POINTER(Info)]),
+        "mfg_set_sweep_mode": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_zero_residuals": (ct.c_int, [ctxp]),
+        "mfg_inviscid_flux": (ct.c_int, [ctxp]),
+        "mfg_compute_timestep": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_forward_lusgs": (ct.c_int, [ctxp]),
+        "mfg_calculate_gradient": (ct.c_int, [ctxp]),
+        "mfg_iterate": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
+        "mfg_iterate_host": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p, f64p, f64p, f64p]),
+        "mfg_residual_norm": (ct.c_int, [ctxp, f64p]),
+        "mfg_profile_phases": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
+        "mfg_get_dt_extrema": (ct.c_int, [ctxp, f64p, f64p]),
+        "mfg_set_dt_extrema": (ct.c_int, [ctxp, ct.c_double, ct.c_double]),
+        "mfg_download": (ct.c_int, [ctxp, ct.c_int32, f64p]),
+        "mfg_upload": (ct.c_int, [ctxp, ct.c_int32, f64p]),
+        "mfg_sync": (ct.c_int, [ctxp]),
+        "mfg_error_string": (ct.c_char_p, [ct.c_int32]),
+        "mfg_last_cuda_error": (ct.c_char_p, []),
+        "mfg_kernel_launches": (ct.c_int64, []),
+        "mfg_prep_specify_bc": (ct.c_int, [ct.POINTER(RawGrid), ct.c_int32, i32p, i32p]),
+        "mfg_prep_metrics": (ct.c_int, [ct.POINTER(RawGrid)] + [f64p] * 11),
+        "mfg_prep_init_flow": (ct.c_int, [ct.POINTER(RawGrid), ct.POINTER(Params), i32p] +
+                               [f64p] * 6 + [ct.c_double] * 5 + [f64p]),
+        "mfg_prep_c2n_size": (ct.c_int, [ct.POINTER(RawGrid), ct.POINTER(ct.c_int64)]),
+        "mfg_prep_node_weights": (ct.c_int, [ct.POINTER(RawGrid), i32p] + [f64p] * 9 +
+                                  [f64p, i32p, f64p, i32p, i32p, f64p, i32p, f64p, f64p, f64p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(func: str, code: int) -> None:
+    if code != MFG_OK:
+        detail = ""
+        if code == -2 and _lib is not None:
+            detail = _lib.mfg_last_cuda_error().decode(errors="replace")
+        raise MfgError(func, code, detail)
+
+
+def ptr(a: np.ndarray, kind=f64p):
+    return a.ctypes.data_as(kind)
+
+
+def kernel_launches() -> int:
+    return int(load().mfg_kernel_launches())

@@ -1,0 +1,67 @@
+"""Build the mfgpu shared library in-tree (``minifs_b200/_lib/libmfgpu.so``).
+
+``nvcc`` cross-compiles for sm_100a only; no GPU is needed to build.  The
+device code is compiled with ``--fmad=false`` and the host code with
+``-ffp-contract=off`` so that every floating-point operation rounds as in the
+reference's plain x86-64 build (no fused multiply-adds anywhere).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libmfgpu.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+SOURCES = ["mfg_device.cu", "mfg_host.cpp"]
+DEPS = SOURCES + ["mfg_kernels.cuh"]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise FileNotFoundError("nvcc not found")
+
+
+def host_cxx() -> str:
+    # the system driver (the one the reference's build uses)
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise FileNotFoundError("g++ not found")
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, s) for s in DEPS] + [os.path.join(INCLUDE, "mfgpu.h")]
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not needs_build():
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc(), "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-lineinfo", "--fmad=false", "-ccbin", host_cxx(),
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-O3", "-shared",
+           "-I" + INCLUDE, "-I" + CSRC, "-o", tmp] + \
+          [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

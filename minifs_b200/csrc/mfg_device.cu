@@ -1,0 +1,1343 @@
+// mfgpu: the MiniFS iteration hot path on B200 (sm_100a), behind the C ABI
+// of include/mfgpu.h.
+//
+// Layout in HBM (C cells, G ghosts, n = C + G, S = sum of faces per cell):
+//   q8[2][n][8]     two state buffers (the backward sweep writes the update
+//                   into the other one; ghosts are frozen and held by both)
+//   dq8[n][8]       LU-SGS increments (ghost rows stay zero)
+//   res[5][C], dt[C], diag[C]            SoA, as the reference
+//   dqdx/dqdy/dqdz[5][n]                 SoA, as the reference
+//   qn8[N][8]       node values of the gradient
+//   slots[S]        (cell, face) records in ascending face order per cell
+//   fw_*/bw_*       LU-SGS level sets: cells sorted by (level, index) and
+//                   their lower / upper neighbour records in that order
+//   node lists      per node, its contributions in the reference's order
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mfg_kernels.cuh"
+#include "mfgpu.h"
+
+using namespace mfg;
+
+namespace {
+
+thread_local std::string g_cuda_error;
+std::atomic<long long> g_launches{0};
+
+constexpr int kBlock = 256;
+constexpr int kNormBlocks = 1184;  // 8 x 148 SMs, fixed so the norm reduction order is fixed
+
+#define MFG_CUDA(call)                                                            \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      g_cuda_error = std::string(#call) + ": " + cudaGetErrorString(e_);          \
+      return MFG_ERR_CUDA;                                                        \
+    }                                                                             \
+  } while (0)
+
+inline int grid_for(int64_t n, int block = kBlock) {
+  return (int)std::max<int64_t>(1, (n + block - 1) / block);
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+// Scatter SoA q (5 blocks of n) into both state buffers and derive per-cell
+// quantities.
+__global__ void k_upload_q(const double *__restrict__ soa, double *__restrict__ qa,
+                           double *__restrict__ qb, int64_t n, Params P) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double q[Q_STRIDE];
+  for (int k = 0; k < 5; k++) q[k] = soa[k * n + i];
+  cell_props(q, P);
+  store_q(qa, i, q);
+  if (qb) store_q(qb, i, q);
+}
+
+__global__ void k_download_rec(const double *__restrict__ rec, double *__restrict__ soa,
+                               int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = 0; k < 5; k++) soa[k * n + i] = rec[i * Q_STRIDE + k];
+}
+
+// Per-cell face gather: Roe flux into the residual, local time step with
+// CellIsMG and LimitTimeStep, and the LU-SGS diagonal.  One thread per cell,
+// faces in ascending order (see the file header for why that is exact).
+template <bool FLUX, bool DT, bool DIAG>
+__global__ void __launch_bounds__(kBlock)
+k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+              const double *__restrict__ q8, const double *__restrict__ vol,
+              double *__restrict__ res, int res_zero, double *__restrict__ dt,
+              double *__restrict__ diag, const double *__restrict__ cfl_tab,
+              const int32_t *__restrict__ iter_counter, double cfl_arg, Params P,
+              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < C;
+  double qc[Q_STRIDE];
+  double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double dtc = 0.0;
+  if (live) {
+    load_q(q8, c, qc);
+    if (FLUX && !res_zero)
+      for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
+    const int32_t s0 = __ldg(cptr + c), s1 = __ldg(cptr + c + 1);
+    double dtl = kBig;
+    int det = 1;
+    for (int32_t s = s0; s < s1; s++) {
+      const SlotRec sr = slots[s];
+      if (FLUX || DT) {
+        double qn[Q_STRIDE];
+        load_q(q8, sr.nb, qn);
+        if (FLUX) {
+          double f[5];
+          if (sr.flags & SLOT_IS_C2) {
+            roe_flux(qn, qc, sr.nx, sr.ny, sr.nz, sr.area, P, f);
+            for (int k = 0; k < 5; k++) r[k] += f[k];
+          } else {
+            roe_flux(qc, qn, sr.nx, sr.ny, sr.nz, sr.area, P, f);
+            for (int k = 0; k < 5; k++) r[k] -= f[k];
+          }
+        }
+        if (DT) {
+          double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
+          vn = fabs(vn);
+          const double eigv = vn + qc[Q_A];
+          dtl = smin(dtl, sr.dn / eigv);
+          // CellIsMG: |p2-p1| and p2+p1 are symmetric in the two sides.
+          const double dp = fabs(qn[4] - qc[4]) / (qn[4] + qc[4] + P.p_bar + P.p_bar);
+          if (dp > 0.1) det = 0;
+        }
+      }
+    }
+    if (DT) {
+      const double cfl = cfl_tab ? cfl_tab[*iter_counter] : cfl_arg;
+      const double cfl_min = 0.5 * cfl;
+      dtc = dtl * local_cfl(qc[4], det, cfl, cfl_min, P);
+      dt[c] = dtc;
+    }
+    if (DIAG) {
+      const double dtv = DT ? dtc : dt[c];
+      double d = vol[c] / dtv;
+      for (int32_t s = s0; s < s1; s++) {
+        const SlotRec sr = slots[s];
+        double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
+        vn = fabs(vn);
+        const double eig = vn + qc[Q_A];
+        d += 0.5 * sr.area * eig * P.lhs_omga;
+      }
+      diag[c] = d;
+    }
+    if (FLUX)
+      for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
+  }
+  if (DT) {
+    // running extrema (compute_timestep.cpp:914-918); dt >= 0 so the bit
+    // patterns order like the values
+    unsigned long long mx = live ? dbits(dtc) : 0ull;
+    unsigned long long mn = live ? dbits(dtc) : ~0ull;
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMax(dt_ext + 0, mx);
+      atomicMin(dt_ext + 1, mn);
+    }
+  }
+  if (FLUX && norm_part) {
+    // per-block partial sums of res^2, reduced in a fixed order
+    __shared__ double sh[kBlock / 32][5];
+    double s2[5];
+    for (int k = 0; k < 5; k++) s2[k] = live ? r[k] * r[k] : 0.0;
+    for (int o = 16; o > 0; o >>= 1)
+      for (int k = 0; k < 5; k++) s2[k] += __shfl_down_sync(0xffffffffu, s2[k], o);
+    if ((threadIdx.x & 31) == 0)
+      for (int k = 0; k < 5; k++) sh[threadIdx.x >> 5][k] = s2[k];
+    __syncthreads();
+    if (threadIdx.x < 5) {
+      double acc = 0.0;
+      for (int wgi = 0; wgi < kBlock / 32; wgi++) acc += sh[wgi][threadIdx.x];
+      norm_part[(int64_t)blockIdx.x * 5 + threadIdx.x] = acc;
+    }
+  }
+}
+
+// LimitTimeStep's ratio clamp (compute_timestep.cpp:929-944).
+__global__ void k_dt_clamp(int32_t C, double *__restrict__ dt,
+                           const unsigned long long *__restrict__ dt_ext, double ratio_dtmax) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt_max = __longlong_as_double((long long)dt_ext[0]);
+  const double dt_min = __longlong_as_double((long long)dt_ext[1]);
+  const double ratio_max = dt_max / dt_min;
+  if (!(ratio_max > ratio_dtmax) || c >= C) return;
+  const double lim = ratio_dtmax * dt_min;
+  if (dt[c] > lim) dt[c] = lim;
+}
+
+// Forward (lower) sweep of one level: cells [l0, l1) of the level order.
+// In the fused path the ratio clamp of LimitTimeStep is applied here: a cell
+// whose dt exceeds the limit gets the limited dt and its Diag rebuilt.
+__global__ void __launch_bounds__(kBlock)
+k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
+            const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
+            const int32_t *__restrict__ nbs, const double *__restrict__ q8,
+            double *__restrict__ dq8, const double *__restrict__ res, int32_t C,
+            double *__restrict__ diag, int32_t first_cell, Params P, int clamp_check,
+            double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
+            const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+            const double *__restrict__ vol) {
+  const int32_t i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= l1) return;
+  const int32_t c = cells[i];
+  double d[5];
+  for (int k = 0; k < 5; k++) d[k] = res[(int64_t)k * C + c];
+  const int32_t s1 = sptr[i + 1];
+  for (int32_t s = sptr[i]; s < s1; s++) {
+    const SweepRec r = recs[s];
+    const int32_t nb = nbs[s];
+    double qn[Q_STRIDE], dn[5], f[5];
+    load_q(q8, nb, qn);
+    load_dq_cg(dq8, nb, dn);
+    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
+    for (int k = 0; k < 5; k++) d[k] -= r.w * f[k];
+  }
+  double dg = diag[c];
+  if (clamp_check) {
+    const double dt_max = __longlong_as_double((long long)dt_ext[0]);
+    const double dt_min = __longlong_as_double((long long)dt_ext[1]);
+    if (dt_max / dt_min > P.ratio_dtmax) {
+      const double lim = P.ratio_dtmax * dt_min;
+      if (dt[c] > lim) {
+        dt[c] = lim;
+        double qc[Q_STRIDE];
+        load_q(q8, c, qc);
+        dg = vol[c] / lim;
+        for (int32_t s = cptr[c]; s < cptr[c + 1]; s++) {
+          const SlotRec sr = slots[s];
+          double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
+          vn = fabs(vn);
+          dg += 0.5 * sr.area * (vn + qc[Q_A]) * P.lhs_omga;
+        }
+        diag[c] = dg;
+      }
+    }
+  }
+  for (int k = 0; k < 5; k++) d[k] /= dg;
+  if (c != first_cell) {
+    double qc[Q_STRIDE];
+    load_q(q8, c, qc);
+    dq_limit(qc, d, P);
+  }
+  store_dq(dq8, c, d);
+}
+
+// Backward (upper) sweep of one level, fused with the state update: the new
+// state of the cell goes to the other buffer, so later levels of this sweep
+// still read the old state (the reference updates after the sweep).
+__global__ void __launch_bounds__(kBlock)
+k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
+            const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
+            const int32_t *__restrict__ nbs, const double *__restrict__ q8,
+            double *__restrict__ q8_new, double *__restrict__ dq8,
+            const double *__restrict__ diag, Params P) {
+  const int32_t i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= l1) return;
+  const int32_t c = cells[i];
+  double d[5], fs[5] = {0., 0., 0., 0., 0.};
+  load_dq_cg(dq8, c, d);
+  const int32_t s1 = sptr[i + 1];
+  for (int32_t s = sptr[i]; s < s1; s++) {
+    const SweepRec r = recs[s];
+    const int32_t nb = nbs[s];
+    double qn[Q_STRIDE], dn[5], f[5];
+    load_q(q8, nb, qn);
+    load_dq_cg(dq8, nb, dn);
+    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
+    for (int k = 0; k < 5; k++) fs[k] += r.w * f[k];
+  }
+  const double tmp = 2.0 * diag[c];
+  for (int k = 0; k < 5; k++) d[k] -= fs[k] / tmp;
+  double qc[Q_STRIDE];
+  load_q(q8, c, qc);
+  dq_limit(qc, d, P);
+  store_dq(dq8, c, d);
+  update_cell(qc, d, P);
+  cell_props(qc, P);
+  store_q(q8_new, c, qc);
+}
+
+// Node values of all five variables (CompNodeVar3D_dist, cal_gradient.cpp
+// :1922-2372): boundary-marked nodes average their boundary-face states,
+// the others their cells, each in the reference's accumulation order; then
+// the symmetry-plane projection of the velocity.
+__global__ void __launch_bounds__(kBlock)
+k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
+              const int32_t *__restrict__ nsrc, const double *__restrict__ nw,
+              const int32_t *__restrict__ ninfo, const double *__restrict__ wnode,
+              const double *__restrict__ nsym, const int32_t *__restrict__ bface_c1,
+              const double *__restrict__ q8, double *__restrict__ qn8) {
+  const int32_t nd = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nd >= N) return;
+  const int32_t info = ninfo[nd];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const int32_t e1 = nptr[nd + 1];
+  if (info & 1) {
+    for (int32_t e = nptr[nd]; e < e1; e++) {
+      const int32_t k = nsrc[e];
+      const double w = nw[e];
+      double qa[Q_STRIDE], qb[Q_STRIDE];
+      load_q(q8, bface_c1[k], qa);
+      load_q(q8, (int64_t)C + k, qb);
+      for (int v = 0; v < 5; v++) {
+        double facq = qa[v] + qb[v];
+        facq *= 0.5;
+        acc[v] += facq * w;
+      }
+    }
+  } else {
+    for (int32_t e = nptr[nd]; e < e1; e++) {
+      double qa[Q_STRIDE];
+      load_q(q8, nsrc[e], qa);
+      const double w = nw[e];
+      for (int v = 0; v < 5; v++) acc[v] += qa[v] * w;
+    }
+  }
+  const double den = wnode[nd] + kTiny;
+  for (int v = 0; v < 5; v++) acc[v] /= den;
+  if (info & 2) {
+    const double xs = nsym[3 * nd], ys = nsym[3 * nd + 1], zs = nsym[3 * nd + 2];
+    const double un = acc[1], vn_ = acc[2], wn = acc[3];
+    const double vn = un * xs + vn_ * ys + wn * zs;
+    acc[1] = un - vn * xs;
+    acc[2] = vn_ - vn * ys;
+    acc[3] = wn - vn * zs;
+  }
+  double *o = qn8 + (int64_t)nd * Q_STRIDE;
+  reinterpret_cast<double2 *>(o)[0] = make_double2(acc[0], acc[1]);
+  reinterpret_cast<double2 *>(o)[1] = make_double2(acc[2], acc[3]);
+  reinterpret_cast<double2 *>(o)[2] = make_double2(acc[4], 0.0);
+}
+
+// Green-Gauss face sums per cell (CompGradientQ_Gauss_Node face loops,
+// cal_gradient.cpp:1740-1897), divided by the volume.
+__global__ void __launch_bounds__(kBlock)
+k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
+             const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+             const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
+             const double *__restrict__ q8, const double *__restrict__ vol,
+             double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  double gx[5] = {0., 0., 0., 0., 0.}, gy[5] = {0., 0., 0., 0., 0.},
+         gz[5] = {0., 0., 0., 0., 0.};
+  double qc[Q_STRIDE];
+  load_q(q8, c, qc);
+  const int32_t s1 = cptr[c + 1];
+  for (int32_t s = cptr[c]; s < s1; s++) {
+    const SlotRec sr = slots[s];
+    double qs[5];
+    if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
+      double qg[Q_STRIDE];
+      load_q(q8, sr.nb, qg);
+      for (int v = 0; v < 5; v++) qs[v] = 0.5 * (qc[v] + qg[v]);
+    } else {
+      for (int v = 0; v < 5; v++) qs[v] = 0.0;
+      const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+      for (int32_t j = j0; j < j1; j++) {
+        const double2 *p = reinterpret_cast<const double2 *>(qn8 + (int64_t)fnodes[j] * Q_STRIDE);
+        const double2 a = __ldg(p), b = __ldg(p + 1), e = __ldg(p + 2);
+        qs[0] += a.x;
+        qs[1] += a.y;
+        qs[2] += b.x;
+        qs[3] += b.y;
+        qs[4] += e.x;
+      }
+      const double cnt = (double)(j1 - j0);
+      for (int v = 0; v < 5; v++) qs[v] /= cnt;
+    }
+    const bool minus = (sr.flags & SLOT_IS_C2) != 0;
+    for (int v = 0; v < 5; v++) {
+      const double qsum = qs[v] * sr.area;
+      const double tx = qsum * sr.nx, ty = qsum * sr.ny, tz = qsum * sr.nz;
+      if (minus) {
+        gx[v] -= tx;
+        gy[v] -= ty;
+        gz[v] -= tz;
+      } else {
+        gx[v] += tx;
+        gy[v] += ty;
+        gz[v] += tz;
+      }
+    }
+  }
+  const double vc = vol[c];
+  for (int v = 0; v < 5; v++) {
+    dqdx[v * n + c] = gx[v] / vc;
+    dqdy[v * n + c] = gy[v] / vc;
+    dqdz[v * n + c] = gz[v] / vc;
+  }
+}
+
+// Residual norm from res (main.cpp:294-317) as fixed-order block partials.
+__global__ void k_norm_partial(int32_t C, const double *__restrict__ res,
+                               double *__restrict__ part) {
+  __shared__ double sh[kBlock / 32][5];
+  double s2[5] = {0., 0., 0., 0., 0.};
+  for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x)
+    for (int k = 0; k < 5; k++) {
+      const double r = res[(int64_t)k * C + c];
+      s2[k] += r * r;
+    }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 5; k++) s2[k] += __shfl_down_sync(0xffffffffu, s2[k], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 5; k++) sh[threadIdx.x >> 5][k] = s2[k];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double acc = 0.0;
+    for (int w = 0; w < kBlock / 32; w++) acc += sh[w][threadIdx.x];
+    part[(int64_t)blockIdx.x * 5 + threadIdx.x] = acc;
+  }
+}
+
+// Final reduction of the partials; also advances the fused-loop counter.
+__global__ void k_norm_final(int32_t nparts, const double *__restrict__ part,
+                             double *__restrict__ out, int32_t *__restrict__ iter_counter,
+                             double *__restrict__ hist) {
+  __shared__ double sh[5][32];
+  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+  if (k < 5) {
+    double acc = 0.0;
+    for (int32_t b = lane; b < nparts; b += 32) acc += part[(int64_t)b * 5 + k];
+    sh[k][lane] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double acc = 0.0;
+    for (int l = 0; l < 32; l++) acc += sh[threadIdx.x][l];
+    const double v = sqrt(acc);
+    out[threadIdx.x] = v;
+    if (hist) hist[(int64_t)(*iter_counter) * 5 + threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && iter_counter) *iter_counter += 1;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct mfg_ctx {
+  int device = 0;
+  int precision = MFG_PREC_FP64;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  int32_t C = 0, G = 0, F = 0, N = 0;
+  int64_t n = 0, S = 0;
+  mfg_params hp{};
+  Params P{};
+  int first_cell = 0;
+  bool res_zero = true;
+  int cur = 0;
+  int sweep_mode = 0;
+  // device arrays
+  double *q8[2] = {nullptr, nullptr};
+  double *dq8 = nullptr, *res = nullptr, *dt = nullptr, *diag = nullptr;
+  double *dqdx = nullptr, *dqdy = nullptr, *dqdz = nullptr, *qn8 = nullptr;
+  double *vol = nullptr, *staging = nullptr;
+  int32_t *cptr = nullptr;
+  SlotRec *slots = nullptr;
+  int32_t *fnptr = nullptr, *fnodes = nullptr;
+  int32_t *nptr = nullptr, *nsrc = nullptr, *ninfo = nullptr, *bface_c1 = nullptr;
+  double *nw = nullptr, *wnode = nullptr, *nsym = nullptr;
+  int32_t *fw_cells = nullptr, *fw_sptr = nullptr, *fw_nb = nullptr;
+  SweepRec *fw_recs = nullptr;
+  int32_t *bw_cells = nullptr, *bw_sptr = nullptr, *bw_nb = nullptr;
+  SweepRec *bw_recs = nullptr;
+  std::vector<int32_t> fw_lptr, bw_lptr;
+  unsigned long long *dt_ext = nullptr;
+  double *norm_part = nullptr, *norm_out = nullptr, *norm_hist = nullptr, *cfl_tab = nullptr;
+  int32_t *iter_counter = nullptr;
+  int32_t hist_cap = 0, cfl_cap = 0;
+  double *h_pinned = nullptr;  // small pinned scratch for scalars
+  std::vector<void *> allocs;
+  int64_t device_bytes = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int64_t graph_nodes = 0;
+  int max_level_cells = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(mfg_ctx *ctx, T **p, size_t count) {
+  size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+  cudaError_t e = cudaMalloc((void **)p, bytes);
+  if (e != cudaSuccess) {
+    g_cuda_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return MFG_ERR_NOMEM;
+  }
+  ctx->allocs.push_back((void *)*p);
+  ctx->device_bytes += (int64_t)bytes;
+  return MFG_OK;
+}
+
+template <typename T>
+int dupload(mfg_ctx *ctx, T **p, const std::vector<T> &h) {
+  int rc = dalloc(ctx, p, h.size());
+  if (rc) return rc;
+  if (!h.empty()) MFG_CUDA(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return MFG_OK;
+}
+
+Params make_params(const mfg_params &p) {
+  Params P;
+  P.gam = p.gam;
+  P.gamm1 = p.gamm1;
+  P.p_bar = p.p_bar;
+  P.alf_l = p.alf_l;
+  P.lhs_omga = p.lhs_omga;
+  const double gam1 = p.gam - 1.;
+  P.peff = p.gam * p.p_bar / gam1;  // forward_lusgs.cpp:1295
+  P.rho_min = p.rho_min;
+  P.rho_max = p.rho_max;
+  P.p_min = p.p_min;
+  P.p_max = p.p_max;
+  P.p_break = p.p_break;
+  P.ratio_dtmax = p.ratio_dtmax;
+  return P;
+}
+
+inline void count_launch(int64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+int check_kernel() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_cuda_error = std::string("kernel launch: ") + cudaGetErrorString(e);
+    return MFG_ERR_CUDA;
+  }
+  return MFG_OK;
+}
+
+// host: CSR of faces per cell, ascending (CalnFPC + CalC2F order).
+void build_c2f(const mfg_mesh *m, std::vector<int32_t> &ptr, std::vector<int32_t> &c2f) {
+  const int32_t C = m->n_cell;
+  ptr.assign(C + 1, 0);
+  for (int32_t f = 0; f < m->n_face; f++) {
+    ptr[m->f2c[2 * f] + 1]++;
+    if (f >= m->n_bface) ptr[m->f2c[2 * f + 1] + 1]++;
+  }
+  for (int32_t c = 0; c < C; c++) ptr[c + 1] += ptr[c];
+  c2f.resize(ptr[C]);
+  std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+  for (int32_t f = 0; f < m->n_face; f++) {
+    c2f[fill[m->f2c[2 * f]]++] = f;
+    if (f >= m->n_bface) c2f[fill[m->f2c[2 * f + 1]]++] = f;
+  }
+}
+
+int validate_mesh(const mfg_mesh *m) {
+  if (!m || m->n_cell <= 0 || m->n_face <= 0 || m->n_node <= 0 || m->n_bface < 0 ||
+      m->n_bface > m->n_face)
+    return MFG_ERR_INVALID;
+  if (!m->f2c || !m->nnpf || !m->f2n || (!m->bctype && m->n_bface) || !m->xfn || !m->yfn ||
+      !m->zfn || !m->area || !m->xfc || !m->yfc || !m->zfc || !m->xcc || !m->ycc || !m->zcc ||
+      !m->vol || !m->wnode || !m->nmark || !m->wbface || !m->nnpc || !m->c2n || !m->wc2n ||
+      !m->nodesymm || !m->xfn_n_symm || !m->yfn_n_symm || !m->zfn_n_symm)
+    return MFG_ERR_INVALID;
+  const int64_t n = (int64_t)m->n_cell + m->n_bface;
+  for (int32_t f = 0; f < m->n_face; f++) {
+    const int32_t c1 = m->f2c[2 * f], c2 = m->f2c[2 * f + 1];
+    if (c1 < 0 || c1 >= m->n_cell) return MFG_ERR_BADMESH;
+    if (f < m->n_bface) {
+      if (c2 != m->n_cell + f) return MFG_ERR_BADMESH;
+    } else if (c2 < 0 || c2 >= m->n_cell || c2 == c1) {
+      return MFG_ERR_BADMESH;
+    }
+    if (m->nnpf[f] <= 0) return MFG_ERR_BADMESH;
+  }
+  (void)n;
+  return MFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mfg_error_string(int32_t code) {
+  switch (code) {
+    case MFG_OK: return "ok";
+    case MFG_ERR_INVALID: return "invalid argument";
+    case MFG_ERR_CUDA: return "CUDA error";
+    case MFG_ERR_NOMEM: return "out of memory";
+    case MFG_ERR_TIMEOUT: return "device wait timed out";
+    case MFG_ERR_NONFINITE: return "non-finite value";
+    case MFG_ERR_UNSUPPORTED: return "unsupported configuration";
+    case MFG_ERR_BADMESH: return "bad mesh";
+    case MFG_ERR_NODEVICE: return "no usable CUDA device";
+    default: return "unknown error";
+  }
+}
+
+const char *mfg_last_cuda_error(void) { return g_cuda_error.c_str(); }
+
+int64_t mfg_kernel_launches(void) { return g_launches.load(); }
+
+static void free_ctx(mfg_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  for (int k = 0; k < 2; k++)
+    if (ctx->graph[k]) cudaGraphExecDestroy(ctx->graph[k]);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+int mfg_destroy(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  free_ctx(ctx);
+  return MFG_OK;
+}
+
+static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32_t> &cptr,
+                        const std::vector<int32_t> &c2f) {
+  const int32_t C = m->n_cell;
+  const int64_t n = ctx->n;
+  std::vector<int32_t> order(C), pos(C);
+  for (int32_t i = 0; i < C; i++) order[i] = m->lusgs_order ? m->lusgs_order[i] : i;
+  std::vector<char> seen(C, 0);
+  for (int32_t i = 0; i < C; i++) {
+    if (order[i] < 0 || order[i] >= C || seen[order[i]]) return MFG_ERR_INVALID;
+    seen[order[i]] = 1;
+    pos[order[i]] = i;
+  }
+  auto layer = [&](int64_t c) -> int64_t { return m->lusgs_layer ? m->lusgs_layer[c] : c; };
+  ctx->first_cell = order[0];
+  // forward: neighbour used iff layer[nb] <= layer[c] (forward_lusgs.cpp:838)
+  std::vector<int32_t> lvl(C, 0);
+  std::vector<int32_t> fw_cnt(C, 0);
+  for (int32_t i = 0; i < C; i++) {
+    const int32_t c = order[i];
+    if (i == 0) continue;  // the first cell only divides by Diag (:803-804)
+    int32_t l = 0;
+    for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+      const int32_t f = c2f[j];
+      const int32_t nb = (m->f2c[2 * f] == c) ? m->f2c[2 * f + 1] : m->f2c[2 * f];
+      if (layer(nb) > layer(c)) continue;
+      fw_cnt[c]++;
+      if (nb >= C) continue;  // ghost: DQ stays zero, no dependency
+      if (pos[nb] > pos[c]) return MFG_ERR_UNSUPPORTED;
+      l = std::max(l, lvl[nb] + 1);
+    }
+    lvl[c] = l;
+  }
+  std::vector<int32_t> blvl(C, 0), bw_cnt(C, 0);
+  for (int32_t i = C - 1; i >= 0; i--) {
+    const int32_t c = order[i];
+    int32_t l = 0;
+    for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+      const int32_t f = c2f[j];
+      const int32_t nb = (m->f2c[2 * f] == c) ? m->f2c[2 * f + 1] : m->f2c[2 * f];
+      if (layer(nb) < layer(c)) continue;
+      bw_cnt[c]++;
+      if (nb >= C) continue;
+      if (pos[nb] < pos[c]) return MFG_ERR_UNSUPPORTED;
+      l = std::max(l, blvl[nb] + 1);
+    }
+    blvl[c] = l;
+  }
+  auto make = [&](const std::vector<int32_t> &lv, const std::vector<int32_t> &cnt, bool fwd,
+                  std::vector<int32_t> &lptr, int32_t **d_cells, int32_t **d_sptr,
+                  SweepRec **d_recs, int32_t **d_nb) -> int {
+    int32_t L = 0;
+    for (int32_t c = 0; c < C; c++) L = std::max(L, lv[c] + 1);
+    lptr.assign(L + 1, 0);
+    for (int32_t c = 0; c < C; c++) lptr[lv[c] + 1]++;
+    for (int32_t l = 0; l < L; l++) {
+      ctx->max_level_cells = std::max(ctx->max_level_cells, lptr[l + 1]);
+      lptr[l + 1] += lptr[l];
+    }
+    std::vector<int32_t> cells(C), fill(lptr.begin(), lptr.end() - 1);
+    for (int32_t c = 0; c < C; c++) cells[fill[lv[c]]++] = c;  // ascending index per level
+    std::vector<int32_t> sptr(C + 1, 0);
+    for (int32_t i = 0; i < C; i++) sptr[i + 1] = sptr[i] + cnt[cells[i]];
+    std::vector<SweepRec> recs(sptr[C]);
+    std::vector<int32_t> nbs(sptr[C]);
+    for (int32_t i = 0; i < C; i++) {
+      const int32_t c = cells[i];
+      int32_t s = sptr[i];
+      if (fwd && c == order[0]) continue;
+      for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+        const int32_t f = c2f[j];
+        const bool is_c1 = m->f2c[2 * f] == c;
+        const int32_t nb = is_c1 ? m->f2c[2 * f + 1] : m->f2c[2 * f];
+        if (fwd ? (layer(nb) > layer(c)) : (layer(nb) < layer(c))) continue;
+        SweepRec r;
+        r.nx = is_c1 ? m->xfn[f] : -m->xfn[f];
+        r.ny = is_c1 ? m->yfn[f] : -m->yfn[f];
+        r.nz = is_c1 ? m->zfn[f] : -m->zfn[f];
+        r.w = fwd ? 0.5 * m->area[f] : m->area[f];
+        recs[s] = r;
+        nbs[s] = nb;
+        s++;
+      }
+    }
+    int rc;
+    if ((rc = dupload(ctx, d_cells, cells))) return rc;
+    if ((rc = dupload(ctx, d_sptr, sptr))) return rc;
+    if ((rc = dupload(ctx, d_recs, recs))) return rc;
+    if ((rc = dupload(ctx, d_nb, nbs))) return rc;
+    return MFG_OK;
+  };
+  (void)n;
+  int rc = make(lvl, fw_cnt, true, ctx->fw_lptr, &ctx->fw_cells, &ctx->fw_sptr, &ctx->fw_recs,
+                &ctx->fw_nb);
+  if (rc) return rc;
+  return make(blvl, bw_cnt, false, ctx->bw_lptr, &ctx->bw_cells, &ctx->bw_sptr, &ctx->bw_recs,
+              &ctx->bw_nb);
+}
+
+// Node contribution lists that replay CompNodeVar3D_dist's loops
+// (cal_gradient.cpp:2041-2125 boundary passes, :2261-2279 cell pass).
+static int build_node_lists(mfg_ctx *ctx, const mfg_mesh *m) {
+  const int32_t N = m->n_node, G = m->n_bface, C = m->n_cell;
+  std::vector<int64_t> fptr(m->n_face + 1, 0);
+  for (int32_t f = 0; f < m->n_face; f++) fptr[f + 1] = fptr[f] + m->nnpf[f];
+  std::vector<int32_t> cnt(N, 0);
+  auto bpass = [&](int pass, auto &&emit) {
+    for (int32_t i = 0; i < G; i++) {
+      const int type = m->bctype[i];
+      if (pass == 0 && type != MFG_BC_WALL) continue;
+      if (pass == 1 && type != MFG_BC_FAR_FIELD) continue;
+      if (pass == 2 && (type == MFG_BC_WALL || type == MFG_BC_SYMM ||
+                        type == MFG_BC_FAR_FIELD || type == MFG_BC_INTERFACE))
+        continue;
+      for (int32_t j = 0; j < m->nnpf[i]; j++) {
+        const int32_t p1 = m->f2n[fptr[i] + j];
+        if (pass == 1 && m->nmark[p1] == MFG_BC_WALL) continue;
+        if (pass == 2 && (m->nmark[p1] == MFG_BC_WALL || m->nmark[p1] == MFG_BC_FAR_FIELD))
+          continue;
+        emit(p1, i, m->wbface[fptr[i] + j]);
+      }
+    }
+  };
+  auto cpass = [&](auto &&emit) {
+    int64_t k = 0;
+    for (int32_t i = 0; i < C; i++)
+      for (int32_t j = 0; j < m->nnpc[i]; j++, k++) {
+        const int32_t p1 = m->c2n[k];
+        if (m->nmark[p1] != 0) continue;
+        emit(p1, i, m->wc2n[k]);
+      }
+  };
+  // A boundary pass only touches marked nodes and the cell pass only
+  // unmarked ones (the weights loops mark every node the face passes reach),
+  // so each node has entries of one kind.
+  std::vector<char> kind(N, 0);
+  for (int pass = 0; pass < 3; pass++)
+    bpass(pass, [&](int32_t p1, int32_t, double) { cnt[p1]++; kind[p1] |= 1; });
+  cpass([&](int32_t p1, int32_t, double) { cnt[p1]++; kind[p1] |= 2; });
+  std::vector<int32_t> ptr(N + 1, 0);
+  for (int32_t i = 0; i < N; i++) {
+    if (kind[i] == 3) return MFG_ERR_UNSUPPORTED;
+    ptr[i + 1] = ptr[i] + cnt[i];
+  }
+  std::vector<int32_t> src(ptr[N]), fill(ptr.begin(), ptr.end() - 1);
+  std::vector<double> w(ptr[N]);
+  for (int pass = 0; pass < 3; pass++)
+    bpass(pass, [&](int32_t p1, int32_t face, double wr) {
+      src[fill[p1]] = face;
+      w[fill[p1]++] = wr;
+    });
+  cpass([&](int32_t p1, int32_t cell, double wr) {
+    src[fill[p1]] = cell;
+    w[fill[p1]++] = wr;
+  });
+  std::vector<int32_t> info(N, 0);
+  std::vector<double> nsym(3 * (size_t)N, 0.0), wnode(m->wnode, m->wnode + N);
+  for (int32_t i = 0; i < N; i++) {
+    if (m->nmark[i] != 0) info[i] |= 1;
+    if (m->nodesymm[i] == 1) {
+      info[i] |= 2;
+      nsym[3 * i] = m->xfn_n_symm[i];
+      nsym[3 * i + 1] = m->yfn_n_symm[i];
+      nsym[3 * i + 2] = m->zfn_n_symm[i];
+    }
+  }
+  std::vector<int32_t> bc1(std::max(G, 1), 0);
+  for (int32_t k = 0; k < G; k++) bc1[k] = m->f2c[2 * k];
+  int rc;
+  if ((rc = dupload(ctx, &ctx->nptr, ptr))) return rc;
+  if ((rc = dupload(ctx, &ctx->nsrc, src))) return rc;
+  if ((rc = dupload(ctx, &ctx->nw, w))) return rc;
+  if ((rc = dupload(ctx, &ctx->ninfo, info))) return rc;
+  if ((rc = dupload(ctx, &ctx->nsym, nsym))) return rc;
+  if ((rc = dupload(ctx, &ctx->wnode, wnode))) return rc;
+  if ((rc = dupload(ctx, &ctx->bface_c1, bc1))) return rc;
+  std::vector<int32_t> fnp(m->n_face + 1), fns(fptr[m->n_face]);
+  for (int32_t f = 0; f <= m->n_face; f++) fnp[f] = (int32_t)fptr[f];
+  std::memcpy(fns.data(), m->f2n, sizeof(int32_t) * fns.size());
+  if ((rc = dupload(ctx, &ctx->fnptr, fnp))) return rc;
+  if ((rc = dupload(ctx, &ctx->fnodes, fns))) return rc;
+  return MFG_OK;
+}
+
+int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, int32_t device,
+               int32_t precision, mfg_ctx **out) {
+  if (!out || !params || !q0) return MFG_ERR_INVALID;
+  *out = nullptr;
+  int rc = validate_mesh(m);
+  if (rc) return rc;
+  if (precision != MFG_PREC_FP64) return MFG_ERR_UNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) {
+    g_cuda_error = "no CUDA device";
+    return MFG_ERR_NODEVICE;
+  }
+  mfg_ctx *ctx = new mfg_ctx();
+  ctx->device = device;
+  ctx->precision = precision;
+  auto fail = [&](int code) {
+    free_ctx(ctx);
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return fail(MFG_ERR_NODEVICE);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10)
+    return fail(MFG_ERR_NODEVICE);
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(MFG_ERR_CUDA);
+  ctx->stream = ctx->own_stream;
+  ctx->C = m->n_cell;
+  ctx->G = m->n_bface;
+  ctx->F = m->n_face;
+  ctx->N = m->n_node;
+  ctx->n = (int64_t)m->n_cell + m->n_bface;
+  ctx->hp = *params;
+  ctx->P = make_params(*params);
+  const int32_t C = ctx->C;
+  const int64_t n = ctx->n;
+
+  std::vector<int32_t> cptr, c2f;
+  build_c2f(m, cptr, c2f);
+  ctx->S = cptr[C];
+  std::vector<SlotRec> slots(ctx->S);
+  for (int32_t c = 0; c < C; c++) {
+    for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+      const int32_t f = c2f[j];
+      SlotRec s;
+      const bool is_c1 = m->f2c[2 * f] == c;
+      s.nx = m->xfn[f];
+      s.ny = m->yfn[f];
+      s.nz = m->zfn[f];
+      s.area = m->area[f];
+      // compute_timestep.cpp:762, the same expression for either side
+      s.dn = std::fabs((m->xfc[f] - m->xcc[c]) * m->xfn[f] + (m->yfc[f] - m->ycc[c]) * m->yfn[f] +
+                       (m->zfc[f] - m->zcc[c]) * m->zfn[f]);
+      s.nb = is_c1 ? m->f2c[2 * f + 1] : m->f2c[2 * f];
+      s.face = f;
+      s.flags = 0;
+      if (!is_c1) s.flags |= SLOT_IS_C2;
+      if (f < m->n_bface) {
+        s.flags |= SLOT_BOUNDARY;
+        const int t = m->bctype[f];
+        if (t == MFG_BC_INTERFACE || t == MFG_BC_SYMM) s.flags |= SLOT_NODE_AVG;
+      }
+      s.pad = 0;
+      slots[j] = s;
+    }
+  }
+  if ((rc = dupload(ctx, &ctx->cptr, cptr))) return fail(rc);
+  if ((rc = dupload(ctx, &ctx->slots, slots))) return fail(rc);
+  slots.clear();
+  slots.shrink_to_fit();
+  std::vector<double> volv(m->vol, m->vol + n);
+  if ((rc = dupload(ctx, &ctx->vol, volv))) return fail(rc);
+  if ((rc = build_levels(ctx, m, cptr, c2f))) return fail(rc);
+  if ((rc = build_node_lists(ctx, m))) return fail(rc);
+
+  for (int k = 0; k < 2; k++)
+    if ((rc = dalloc(ctx, &ctx->q8[k], (size_t)n * Q_STRIDE))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dq8, (size_t)n * Q_STRIDE))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->res, (size_t)5 * C))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dt, (size_t)C))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->diag, (size_t)C))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dqdx, (size_t)5 * n))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dqdy, (size_t)5 * n))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dqdz, (size_t)5 * n))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->qn8, (size_t)ctx->N * Q_STRIDE))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->staging, (size_t)5 * n))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dt_ext, 2))) return fail(rc);
+  const int nparts = std::max(grid_for(C), kNormBlocks);
+  if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->norm_out, 5))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return fail(rc);
+  if (cudaMallocHost((void **)&ctx->h_pinned, 64 * sizeof(double)) != cudaSuccess)
+    return fail(MFG_ERR_NOMEM);
+
+  cudaStream_t st = ctx->stream;
+  if (cudaMemsetAsync(ctx->dq8, 0, sizeof(double) * n * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->res, 0, sizeof(double) * 5 * C, st) ||
+      cudaMemsetAsync(ctx->dt, 0, sizeof(double) * C, st) ||
+      cudaMemsetAsync(ctx->diag, 0, sizeof(double) * C, st) ||
+      cudaMemsetAsync(ctx->dqdx, 0, sizeof(double) * 5 * n, st) ||
+      cudaMemsetAsync(ctx->dqdy, 0, sizeof(double) * 5 * n, st) ||
+      cudaMemsetAsync(ctx->dqdz, 0, sizeof(double) * 5 * n, st) ||
+      cudaMemsetAsync(ctx->qn8, 0, sizeof(double) * ctx->N * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st))
+    return fail(MFG_ERR_CUDA);
+  if ((rc = mfg_set_dt_extrema(ctx, 0.0, kBig))) return fail(rc);  // para_field_global.cpp:220-221
+  if ((rc = mfg_upload(ctx, MFG_FIELD_Q, q0))) return fail(rc);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail(MFG_ERR_CUDA);
+  *out = ctx;
+  return MFG_OK;
+}
+
+int mfg_set_stream(mfg_ctx *ctx, void *s) {
+  if (!ctx) return MFG_ERR_INVALID;
+  ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+  return MFG_OK;
+}
+
+int mfg_set_params(mfg_ctx *ctx, const mfg_params *p) {
+  if (!ctx || !p) return MFG_ERR_INVALID;
+  ctx->hp = *p;
+  ctx->P = make_params(*p);
+  for (int k = 0; k < 2; k++)
+    if (ctx->graph[k]) {
+      cudaGraphExecDestroy(ctx->graph[k]);
+      ctx->graph[k] = nullptr;
+    }
+  return MFG_OK;
+}
+
+int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode) {
+  if (!ctx || mode != 0) return mode == 1 ? MFG_ERR_UNSUPPORTED : MFG_ERR_INVALID;
+  ctx->sweep_mode = mode;
+  return MFG_OK;
+}
+
+int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
+  if (!ctx || !info) return MFG_ERR_INVALID;
+  info->n_cell = ctx->C;
+  info->n_face = ctx->F;
+  info->n_node = ctx->N;
+  info->n_bface = ctx->G;
+  info->fw_levels = (int32_t)ctx->fw_lptr.size() - 1;
+  info->bw_levels = (int32_t)ctx->bw_lptr.size() - 1;
+  info->max_level_cells = ctx->max_level_cells;
+  info->precision = ctx->precision;
+  info->device_bytes = ctx->device_bytes;
+  info->sweep_mode = ctx->sweep_mode;
+  info->graph_ready = ctx->graph[0] != nullptr;
+  return MFG_OK;
+}
+
+int mfg_zero_residuals(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  ctx->res_zero = true;  // the next flux gather writes instead of accumulating
+  return MFG_OK;
+}
+
+static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
+                       bool use_table) {
+  cudaStream_t st = ctx->stream;
+  const int g = grid_for(ctx->C);
+  const double *q = ctx->q8[ctx->cur];
+  const double *tab = use_table ? ctx->cfl_tab : nullptr;
+  double *np = flux ? ctx->norm_part : nullptr;
+#define MFG_FACE(F, D, G)                                                                    \
+  k_face_gather<F, D, G><<<g, kBlock, 0, st>>>(ctx->C, ctx->cptr, ctx->slots, q, ctx->vol,   \
+                                                ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,    \
+                                                ctx->diag, tab, ctx->iter_counter, cfl,      \
+                                                ctx->P, ctx->dt_ext, np)
+  if (flux && dtp && diag) MFG_FACE(true, true, true);
+  else if (flux && !dtp && !diag) MFG_FACE(true, false, false);
+  else if (!flux && dtp && !diag) MFG_FACE(false, true, false);
+  else if (!flux && !dtp && diag) MFG_FACE(false, false, true);
+  else return MFG_ERR_INVALID;
+#undef MFG_FACE
+  count_launch();
+  if (flux) ctx->res_zero = false;
+  return check_kernel();
+}
+
+int mfg_inviscid_flux(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  return launch_face(ctx, true, false, false, 0.0, false);
+}
+
+// LimitTimeStep's CFL (compute_timestep.cpp:865-873), evaluated with glibc.
+static double cfl_for(const mfg_params &p, int32_t iter_done) {
+  if (iter_done > p.cfl_nstep) return p.cfl_end;
+  return p.cfl_start * pow(p.cfl_ratio, (double)iter_done / p.cfl_nstep);
+}
+
+int mfg_compute_timestep(mfg_ctx *ctx, int32_t iter_done) {
+  if (!ctx) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  const double cfl = cfl_for(ctx->hp, iter_done);
+  ctx->hp.cfl_min = 0.5 * cfl;
+  int rc = launch_face(ctx, false, true, false, cfl, false);
+  if (rc) return rc;
+  k_dt_clamp<<<grid_for(ctx->C), kBlock, 0, ctx->stream>>>(ctx->C, ctx->dt, ctx->dt_ext,
+                                                           ctx->P.ratio_dtmax);
+  count_launch();
+  return check_kernel();
+}
+
+static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
+  cudaStream_t st = ctx->stream;
+  const double *q = ctx->q8[ctx->cur];
+  double *qn = ctx->q8[ctx->cur ^ 1];
+  const int Lf = (int)ctx->fw_lptr.size() - 1, Lb = (int)ctx->bw_lptr.size() - 1;
+  for (int l = 0; l < Lf; l++) {
+    const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
+    k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
+        a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dq8, ctx->res,
+        ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt, ctx->dt_ext,
+        ctx->cptr, ctx->slots, ctx->vol);
+  }
+  for (int l = 0; l < Lb; l++) {
+    const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
+    k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
+                                                    ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dq8,
+                                                    ctx->diag, ctx->P);
+  }
+  count_launch(Lf + Lb);
+  return check_kernel();
+}
+
+int mfg_forward_lusgs(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  int rc = launch_face(ctx, false, false, true, 0.0, false);
+  if (rc) return rc;
+  rc = launch_sweeps(ctx, false);
+  if (rc) return rc;
+  ctx->cur ^= 1;
+  return MFG_OK;
+}
+
+static int launch_gradient(mfg_ctx *ctx) {
+  cudaStream_t st = ctx->stream;
+  const double *q = ctx->q8[ctx->cur];
+  k_node_values<<<grid_for(ctx->N), kBlock, 0, st>>>(ctx->N, ctx->C, ctx->nptr, ctx->nsrc,
+                                                     ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
+                                                     ctx->bface_c1, q, ctx->qn8);
+  k_grad_faces<<<grid_for(ctx->C), kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,
+                                                    ctx->fnptr, ctx->fnodes, ctx->qn8, q,
+                                                    ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
+  count_launch(2);
+  return check_kernel();
+}
+
+int mfg_calculate_gradient(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  return launch_gradient(ctx);
+}
+
+// One fused iteration: flux + dt + Diag in one gather, level sweeps with the
+// update, gradient, residual norm.  Reads the CFL from cfl_tab[counter].
+static int launch_iteration(mfg_ctx *ctx) {
+  int rc = launch_face(ctx, true, true, true, 0.0, true);
+  if (rc) return rc;
+  rc = launch_sweeps(ctx, true);
+  if (rc) return rc;
+  ctx->cur ^= 1;
+  rc = launch_gradient(ctx);
+  if (rc) return rc;
+  const int nparts = grid_for(ctx->C);
+  k_norm_final<<<1, 160, 0, ctx->stream>>>(nparts, ctx->norm_part, ctx->norm_out,
+                                           ctx->iter_counter, ctx->norm_hist);
+  count_launch();
+  return check_kernel();
+}
+
+static int ensure_graphs(mfg_ctx *ctx) {
+  if (ctx->graph[0] && ctx->graph[1]) return MFG_OK;
+  const int start = ctx->cur;
+  for (int k = 0; k < 2; k++) {
+    const int par = start ^ k;
+    ctx->cur = par;
+    ctx->res_zero = true;  // each captured iteration starts with ZeroResiduals
+    cudaGraph_t g = nullptr;
+    MFG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const long long before = g_launches.load();
+    int rc = launch_iteration(ctx);
+    const long long nodes = g_launches.load() - before;
+    g_launches.fetch_sub(nodes);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      ctx->cur = start;
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      g_cuda_error = std::string("capture: ") + cudaGetErrorString(e);
+      ctx->cur = start;
+      return MFG_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&ctx->graph[par], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      g_cuda_error = std::string("instantiate: ") + cudaGetErrorString(e);
+      ctx->cur = start;
+      return MFG_ERR_CUDA;
+    }
+    ctx->graph_nodes = nodes;
+  }
+  ctx->cur = start;
+  return MFG_OK;
+}
+
+int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) {
+  if (!ctx || n_iter < 0) return MFG_ERR_INVALID;
+  if (n_iter == 0) return MFG_OK;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (n_iter > ctx->hist_cap) {
+    // grow the per-iteration tables; graphs hold their pointers, so rebuild
+    for (int k = 0; k < 2; k++)
+      if (ctx->graph[k]) {
+        cudaGraphExecDestroy(ctx->graph[k]);
+        ctx->graph[k] = nullptr;
+      }
+    const int32_t cap = std::max(n_iter, 256);
+    int rc;
+    if ((rc = dalloc(ctx, &ctx->norm_hist, (size_t)5 * cap))) return rc;
+    if ((rc = dalloc(ctx, &ctx->cfl_tab, (size_t)cap))) return rc;
+    ctx->hist_cap = cap;
+  }
+  std::vector<double> tab(n_iter);
+  for (int32_t i = 0; i < n_iter; i++) tab[i] = cfl_for(ctx->hp, iter_done + i);
+  ctx->hp.cfl_min = 0.5 * tab[n_iter - 1];
+  MFG_CUDA(cudaMemcpyAsync(ctx->cfl_tab, tab.data(), sizeof(double) * n_iter,
+                           cudaMemcpyHostToDevice, st));
+  MFG_CUDA(cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st));
+  ctx->res_zero = true;  // ZeroResiduals at the top of each iteration
+  int rc = ensure_graphs(ctx);
+  if (rc) return rc;
+  for (int32_t i = 0; i < n_iter; i++) {
+    MFG_CUDA(cudaGraphLaunch(ctx->graph[ctx->cur], st));
+    count_launch(ctx->graph_nodes);
+    ctx->cur ^= 1;
+  }
+  ctx->res_zero = false;
+  if (norms) {
+    MFG_CUDA(cudaMemcpyAsync(norms, ctx->norm_hist, sizeof(double) * 5 * n_iter,
+                             cudaMemcpyDeviceToHost, st));
+    MFG_CUDA(cudaStreamSynchronize(st));
+  }
+  MFG_CUDA(cudaGetLastError());
+  return MFG_OK;
+}
+
+int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *phase_ms) {
+  if (!ctx || n_iter <= 0 || !phase_ms) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (n_iter > ctx->hist_cap) {
+    for (int k = 0; k < 2; k++)
+      if (ctx->graph[k]) {
+        cudaGraphExecDestroy(ctx->graph[k]);
+        ctx->graph[k] = nullptr;
+      }
+    const int32_t cap = std::max(n_iter, 256);
+    int rc;
+    if ((rc = dalloc(ctx, &ctx->norm_hist, (size_t)5 * cap))) return rc;
+    if ((rc = dalloc(ctx, &ctx->cfl_tab, (size_t)cap))) return rc;
+    ctx->hist_cap = cap;
+  }
+  std::vector<double> tab(n_iter);
+  for (int32_t i = 0; i < n_iter; i++) tab[i] = cfl_for(ctx->hp, iter_done + i);
+  MFG_CUDA(cudaMemcpyAsync(ctx->cfl_tab, tab.data(), sizeof(double) * n_iter,
+                           cudaMemcpyHostToDevice, st));
+  MFG_CUDA(cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st));
+  cudaEvent_t ev[MFG_NPHASES + 1];
+  for (auto &e : ev) MFG_CUDA(cudaEventCreate(&e));
+  for (int k = 0; k < MFG_NPHASES; k++) phase_ms[k] = 0.0;
+  int rc = MFG_OK;
+  const int Lf = (int)ctx->fw_lptr.size() - 1, Lb = (int)ctx->bw_lptr.size() - 1;
+  for (int32_t it = 0; it < n_iter && rc == MFG_OK; it++) {
+    ctx->res_zero = true;
+    const double *q = ctx->q8[ctx->cur];
+    double *qn = ctx->q8[ctx->cur ^ 1];
+    cudaEventRecord(ev[0], st);
+    rc = launch_face(ctx, true, true, true, 0.0, true);
+    cudaEventRecord(ev[1], st);
+    for (int l = 0; l < Lf && rc == MFG_OK; l++) {
+      const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
+      k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
+          a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dq8, ctx->res,
+          ctx->C, ctx->diag, ctx->first_cell, ctx->P, 1, ctx->dt, ctx->dt_ext, ctx->cptr,
+          ctx->slots, ctx->vol);
+    }
+    cudaEventRecord(ev[2], st);
+    for (int l = 0; l < Lb; l++) {
+      const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
+      k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
+                                                      ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dq8,
+                                                      ctx->diag, ctx->P);
+    }
+    count_launch(Lf + Lb);
+    cudaEventRecord(ev[3], st);
+    ctx->cur ^= 1;
+    const double *q2 = ctx->q8[ctx->cur];
+    k_node_values<<<grid_for(ctx->N), kBlock, 0, st>>>(ctx->N, ctx->C, ctx->nptr, ctx->nsrc,
+                                                       ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
+                                                       ctx->bface_c1, q2, ctx->qn8);
+    cudaEventRecord(ev[4], st);
+    k_grad_faces<<<grid_for(ctx->C), kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,
+                                                      ctx->fnptr, ctx->fnodes, ctx->qn8, q2,
+                                                      ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
+    cudaEventRecord(ev[5], st);
+    k_norm_final<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, ctx->norm_out,
+                                    ctx->iter_counter, ctx->norm_hist);
+    cudaEventRecord(ev[6], st);
+    count_launch(3);
+    if (rc == MFG_OK) rc = check_kernel();
+    if (cudaEventSynchronize(ev[6]) != cudaSuccess) rc = MFG_ERR_CUDA;
+    for (int k = 0; k < MFG_NPHASES && rc == MFG_OK; k++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      phase_ms[k] += ms;
+    }
+  }
+  ctx->res_zero = false;
+  for (auto &e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
+int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const double *q_in,
+                     double *q_out, double *res_out, double *norms) {
+  if (!ctx) return MFG_ERR_INVALID;
+  int rc;
+  if (q_in && (rc = mfg_upload(ctx, MFG_FIELD_Q, q_in))) return rc;
+  if ((rc = mfg_iterate(ctx, n_iter, iter_done, norms))) return rc;
+  if (q_out && (rc = mfg_download(ctx, MFG_FIELD_Q, q_out))) return rc;
+  if (res_out && (rc = mfg_download(ctx, MFG_FIELD_RES, res_out))) return rc;
+  return MFG_OK;
+}
+
+int mfg_residual_norm(mfg_ctx *ctx, double out[5]) {
+  if (!ctx || !out) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (ctx->res_zero) {
+    for (int k = 0; k < 5; k++) out[k] = 0.0;
+    return MFG_OK;
+  }
+  k_norm_partial<<<kNormBlocks, kBlock, 0, st>>>(ctx->C, ctx->res, ctx->norm_part);
+  k_norm_final<<<1, 160, 0, st>>>(kNormBlocks, ctx->norm_part, ctx->norm_out, nullptr, nullptr);
+  count_launch(2);
+  MFG_CUDA(cudaGetLastError());
+  MFG_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->norm_out, 5 * sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
+  MFG_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < 5; k++) out[k] = ctx->h_pinned[k];
+  return MFG_OK;
+}
+
+int mfg_get_dt_extrema(mfg_ctx *ctx, double *dt_max, double *dt_min) {
+  if (!ctx || !dt_max || !dt_min) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  MFG_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->dt_ext, 2 * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  *dt_max = ctx->h_pinned[0];
+  *dt_min = ctx->h_pinned[1];
+  return MFG_OK;
+}
+
+int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min) {
+  if (!ctx || !(dt_max >= 0.0) || !(dt_min >= 0.0)) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->h_pinned[0] = dt_max;
+  ctx->h_pinned[1] = dt_min;
+  MFG_CUDA(cudaMemcpyAsync(ctx->dt_ext, ctx->h_pinned, 2 * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MFG_OK;
+}
+
+int mfg_sync(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MFG_OK;
+}
+
+int mfg_download(mfg_ctx *ctx, int32_t field, double *host) {
+  if (!ctx || !host) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n, C = ctx->C;
+  const double *src = nullptr;
+  size_t count = 0;
+  switch (field) {
+    case MFG_FIELD_Q:
+    case MFG_FIELD_DQ: {
+      const double *rec = field == MFG_FIELD_Q ? ctx->q8[ctx->cur] : ctx->dq8;
+      k_download_rec<<<grid_for(n), kBlock, 0, st>>>(rec, ctx->staging, n);
+      count_launch();
+      MFG_CUDA(cudaGetLastError());
+      src = ctx->staging;
+      count = 5 * n;
+      break;
+    }
+    case MFG_FIELD_RES:
+      if (ctx->res_zero) MFG_CUDA(cudaMemsetAsync(ctx->res, 0, sizeof(double) * 5 * C, st));
+      src = ctx->res;
+      count = 5 * C;
+      break;
+    case MFG_FIELD_DT: src = ctx->dt; count = C; break;
+    case MFG_FIELD_DIAG: src = ctx->diag; count = C; break;
+    case MFG_FIELD_DQDX: src = ctx->dqdx; count = 5 * n; break;
+    case MFG_FIELD_DQDY: src = ctx->dqdy; count = 5 * n; break;
+    case MFG_FIELD_DQDZ: src = ctx->dqdz; count = 5 * n; break;
+    default: return MFG_ERR_INVALID;
+  }
+  MFG_CUDA(cudaMemcpyAsync(host, src, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+  MFG_CUDA(cudaStreamSynchronize(st));
+  return MFG_OK;
+}
+
+int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
+  if (!ctx || !host) return MFG_ERR_INVALID;
+  if (field != MFG_FIELD_Q) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  MFG_CUDA(cudaMemcpyAsync(ctx->staging, host, sizeof(double) * 5 * n, cudaMemcpyHostToDevice,
+                           st));
+  k_upload_q<<<grid_for(n), kBlock, 0, st>>>(ctx->staging, ctx->q8[ctx->cur],
+                                            ctx->q8[ctx->cur ^ 1], n, ctx->P);
+  count_launch();
+  MFG_CUDA(cudaGetLastError());
+  return MFG_OK;
+}
+
+}  // extern "C"

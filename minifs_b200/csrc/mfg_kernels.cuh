@@ -1,0 +1,294 @@
+// Device code of the mfgpu hot path (sm_100a, FP64).
+//
+// Bit-faithfulness rules, kept throughout:
+//  * every arithmetic expression has the operand order of the reference
+//    routine it restates (cited per function); the file is compiled with
+//    --fmad=false so no multiply-add is contracted;
+//  * per-cell sums run over the cell's faces in ascending face order, the
+//    order in which the reference's face loops scatter into that cell, so
+//    gathers reproduce the scatter sums exactly and no atomics are needed;
+//  * per-cell values that the reference recomputes at every face from the
+//    same operands (sound speed, total enthalpy, conserved energy) are
+//    computed once per cell with the same expression, which yields the same
+//    bits.
+#pragma once
+
+#include <cstdint>
+
+namespace mfg {
+
+constexpr double kTiny = 1.e-40;  // number_type.h:29
+constexpr double kBig = 1.e40;    // number_type.h:28
+
+// Per-cell state record, 64 bytes: the five primitive variables of the
+// reference's SoA arrays plus three derived per-cell quantities.
+enum : int {
+  Q_RHO = 0, Q_U, Q_V, Q_W, Q_P,
+  Q_A,   // sqrt(gam*(p+p_bar)/rho): compute_timestep.cpp:763-768, forward_lusgs.cpp:566-570, :1291-1293
+  Q_HT,  // total enthalpy et + p + p_bar: cal_flux.cpp:688-693
+  Q_E,   // p/gam1 + 0.5*rho*|v|^2: forward_lusgs.cpp:1285-1289
+  Q_STRIDE = 8
+};
+
+// One (cell, face) slot in ascending face order of the cell: the face normal
+// as stored (pointing out of the face's first cell), the face area, the
+// distance of the face centroid to this cell's centroid along the normal
+// (compute_timestep.cpp:762), the other cell, and flags.
+struct __align__(16) SlotRec {
+  double nx, ny, nz, area, dn;
+  int32_t nb;     // neighbour cell (ghost C+k for boundary face k)
+  int32_t face;   // face index
+  int32_t flags;  // SLOT_*
+  int32_t pad;
+};
+enum : int32_t { SLOT_IS_C2 = 1, SLOT_BOUNDARY = 2, SLOT_NODE_AVG = 4 };
+
+// LU-SGS sweep record: normal oriented out of the swept cell and the
+// multiplier of the flux (0.5*area forward, area backward).
+struct __align__(16) SweepRec {
+  double nx, ny, nz, w;
+};
+
+struct Params {
+  double gam, gamm1, p_bar, alf_l, lhs_omga, peff;
+  double rho_min, rho_max, p_min, p_max, p_break, ratio_dtmax;
+};
+
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ void load_q(const double *__restrict__ q8, int64_t c, double *q) {
+  const double2 *p = reinterpret_cast<const double2 *>(q8 + c * Q_STRIDE);
+  double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2), e = __ldg(p + 3);
+  q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y;
+  q[4] = d.x; q[5] = d.y; q[6] = e.x; q[7] = e.y;
+}
+
+__device__ __forceinline__ void store_q(double *__restrict__ q8, int64_t c, const double *q) {
+  double2 *p = reinterpret_cast<double2 *>(q8 + c * Q_STRIDE);
+  p[0] = make_double2(q[0], q[1]);
+  p[1] = make_double2(q[2], q[3]);
+  p[2] = make_double2(q[4], q[5]);
+  p[3] = make_double2(q[6], q[7]);
+}
+
+// Loads that must observe writes of earlier levels of the same sweep in a
+// persistent kernel: bypass the non-coherent path.
+__device__ __forceinline__ void load_dq_cg(const double *dq8, int64_t c, double *d) {
+  const double2 *p = reinterpret_cast<const double2 *>(dq8 + c * Q_STRIDE);
+  double2 a = __ldcg(p), b = __ldcg(p + 1), e = __ldcg(p + 2);
+  d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y; d[4] = e.x;
+}
+
+__device__ __forceinline__ void store_dq(double *dq8, int64_t c, const double *d) {
+  double2 *p = reinterpret_cast<double2 *>(dq8 + c * Q_STRIDE);
+  __stcg(p, make_double2(d[0], d[1]));
+  __stcg(p + 1, make_double2(d[2], d[3]));
+  __stcg(p + 2, make_double2(d[4], 0.0));
+}
+
+// Derived per-cell quantities from the primitive variables.
+__device__ __forceinline__ void cell_props(double *q, const Params &P) {
+  const double rho = q[0], u = q[1], v = q[2], w = q[3], p = q[4];
+  // compute_timestep.cpp:763 c2tmp = gam * (p[c1] + p_bar) / rho[c1]; eigv = vn + sqrt(c2tmp)
+  q[Q_A] = sqrt(P.gam * (p + P.p_bar) / rho);
+  // cal_flux.cpp:688-693
+  const double et = (p + P.p_bar) / P.gamm1 + 0.5 * rho * (u * u + v * v + w * w);
+  q[Q_HT] = et + p + P.p_bar;
+  // forward_lusgs.cpp:1285-1289 (gam1 = gam - 1. equals gamm1 = gam - 1.0)
+  const double rv2 = 0.5 * rho * (u * u + v * v + w * w);
+  q[Q_E] = p / P.gamm1 + rv2;
+}
+
+// RoeFlux_noprec serial body (cal_flux.cpp:676-834) for one face with
+// first-order face states ql = q[c1], qr = q[c2]; includes the 0.5*area
+// factor.  ht_l / ht_r come precomputed from the cell records.
+__device__ __forceinline__ void roe_flux(const double *ql, const double *qr, double areax,
+                                         double areay, double areaz, double area,
+                                         const Params &P, double *flux) {
+  const double ht_l = ql[Q_HT], ht_r = qr[Q_HT];
+  const double vn_l = areax * ql[1] + areay * ql[2] + areaz * ql[3];
+  const double vn_r = areax * qr[1] + areay * qr[2] + areaz * qr[3];
+  double tmp0 = vn_l * ql[0];
+  double tmp1 = vn_r * qr[0];
+  double f0 = tmp0 + tmp1;
+  double f1 = tmp0 * ql[1] + areax * ql[4] + tmp1 * qr[1] + areax * qr[4];
+  double f2 = tmp0 * ql[2] + areay * ql[4] + tmp1 * qr[2] + areay * qr[4];
+  double f3 = tmp0 * ql[3] + areaz * ql[4] + tmp1 * qr[3] + areaz * qr[4];
+  double f4 = ht_l * vn_l + ht_r * vn_r;
+
+  tmp0 = sqrt(qr[0] / ql[0]);
+  tmp1 = 1.0 / (1.0 + tmp0);
+  const double rho_a = sqrt(qr[0] * ql[0]);
+  const double u_a = (ql[1] + qr[1] * tmp0) * tmp1;
+  const double v_a = (ql[2] + qr[2] * tmp0) * tmp1;
+  const double w_a = (ql[3] + qr[3] * tmp0) * tmp1;
+  const double vn_a = u_a * areax + v_a * areay + w_a * areaz;
+  const double h_a = (ht_l / ql[0] + ht_r / qr[0] * tmp0) * tmp1;
+
+  const double q2 = 0.5 * (u_a * u_a + v_a * v_a + w_a * w_a);
+  double c2_a = P.gamm1 * (h_a - q2);
+  c2_a = fabs(c2_a);
+  const double c_a = sqrt(c2_a);
+
+  double eigv1 = fabs(vn_a);
+  double eigv2 = fabs(vn_a + c_a);
+  double eigv3 = fabs(vn_a - c_a);
+
+  const double spectral = fabs(u_a) + fabs(v_a) + fabs(w_a) + c_a;
+  const double epsaa = P.alf_l * spectral;
+  const double epsbb = 0.25 / smax(epsaa, kTiny);
+  const double epscc = 2.0 * epsaa;
+  if (eigv1 < epscc) eigv1 = eigv1 * eigv1 * epsbb + epsaa;
+  if (eigv2 < epscc) eigv2 = eigv2 * eigv2 * epsbb + epsaa;
+  if (eigv3 < epscc) eigv3 = eigv3 * eigv3 * epsbb + epsaa;
+
+  const double drho = qr[0] - ql[0];
+  const double du = qr[1] - ql[1];
+  const double dv = qr[2] - ql[2];
+  const double dw = qr[3] - ql[3];
+  const double dp = qr[4] - ql[4];
+  const double dvn = vn_r - vn_l;
+  const double dq2 = u_a * du + v_a * dv + w_a * dw;
+
+  tmp0 = dp / c2_a;
+  tmp1 = rho_a * dvn / c_a;
+  const double alpha1 = (drho - tmp0) * eigv1;
+  const double alpha2 = 0.5 * (tmp0 + tmp1) * eigv2;
+  const double alpha3 = 0.5 * (tmp0 - tmp1) * eigv3;
+
+  tmp0 = alpha1 + alpha2 + alpha3;
+  tmp1 = eigv1 * rho_a;
+  const double tmp2 = -tmp1 * dvn + (alpha2 - alpha3) * c_a;
+  f0 -= tmp0;
+  f1 -= tmp0 * u_a + tmp1 * du + tmp2 * areax;
+  f2 -= tmp0 * v_a + tmp1 * dv + tmp2 * areay;
+  f3 -= tmp0 * w_a + tmp1 * dw + tmp2 * areaz;
+  f4 -= alpha1 * q2 + (alpha2 + alpha3) * h_a + tmp1 * dq2 + tmp2 * vn_a;
+
+  const double half = 0.5 * area;
+  flux[0] = f0 * half;
+  flux[1] = f1 * half;
+  flux[2] = f2 * half;
+  flux[3] = f3 * half;
+  flux[4] = f4 * half;
+}
+
+// FluxLUSGS3D (forward_lusgs.cpp:1271-1324) with the neighbour's sound speed
+// and conserved energy taken from its record (same expressions).
+__device__ __forceinline__ void flux_lusgs(const double *q, const double *DQ, double nx, double ny,
+                                           double nz, const Params &P, double *flux) {
+  const double gam1 = P.gamm1;
+  double Q0 = q[0], Q1 = q[0] * q[1], Q2 = q[0] * q[2], Q3 = q[0] * q[3];
+  double Q4 = q[Q_E];
+  double p = q[4];
+  double v_n = q[1] * nx + q[2] * ny + q[3] * nz;
+  double eig = fabs(v_n) + q[Q_A];
+  eig *= P.lhs_omga;
+  const double peff = P.peff;
+  double f1 = -Q1 * v_n - p * nx;
+  double f2 = -Q2 * v_n - p * ny;
+  double f3 = -Q3 * v_n - p * nz;
+  double f4 = -(Q4 + p + peff) * v_n;
+  Q0 += DQ[0];
+  Q1 += DQ[1];
+  Q2 += DQ[2];
+  Q3 += DQ[3];
+  Q4 += DQ[4];
+  const double rv2 = 0.5 * (Q1 * Q1 + Q2 * Q2 + Q3 * Q3) / Q0;
+  p = gam1 * (Q4 - rv2);
+  double f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
+  v_n *= q[0];
+  v_n += f0;
+  v_n /= Q0;
+  f1 += Q1 * v_n + p * nx;
+  f2 += Q2 * v_n + p * ny;
+  f3 += Q3 * v_n + p * nz;
+  f4 += (Q4 + p + peff) * v_n;
+  flux[0] = f0 - eig * DQ[0];
+  flux[1] = f1 - eig * DQ[1];
+  flux[2] = f2 - eig * DQ[2];
+  flux[3] = f3 - eig * DQ[3];
+  flux[4] = f4 - eig * DQ[4];
+}
+
+// DQ_limit == 2 positivity limiter (forward_lusgs.cpp:939-973, :1184-1218).
+__device__ __forceinline__ void dq_limit(const double *q, double *d, const Params &P) {
+  const double vv = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+#pragma unroll
+  for (int stage = 0; stage < 3; stage++) {
+    double dp = d[4] + 0.5 * d[0] * vv - (d[1] * q[1] + d[2] * q[2] + d[3] * q[3]);
+    dp *= P.gamm1;
+    if ((q[0] + d[0]) < P.rho_min || (q[0] + d[0]) > P.rho_max || (q[4] + dp) < P.p_min ||
+        (q[4] + dp) > P.p_max) {
+      if (stage < 2) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) d[k] *= 0.1;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 5; k++) d[k] = 0.0;
+      }
+    }
+  }
+}
+
+// UpdateFlowField3D_CFL3d (forward_lusgs.cpp:1335-1488) for one cell; q is
+// updated in place (primitive part).
+__device__ __forceinline__ void update_cell(double *q, const double *DQ, const Params &P) {
+  const double gam1 = P.gamm1;
+  const double p00 = P.p_bar;
+  const double alpq = -0.2;
+  const double phiq = 1. / 0.5;
+  const double betq = 1.0 + alpq * phiq;
+  double rhot = q[0];
+  double ru = rhot * q[1];
+  double rv = rhot * q[2];
+  double rw = rhot * q[3];
+  double re = q[4] / gam1 + 0.5 * rhot * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  rhot += DQ[0];
+  ru += DQ[1];
+  rv += DQ[2];
+  rw += DQ[3];
+  re += DQ[4];
+  const double rhotr = 1. / (rhot + kTiny);
+  const double u = ru * rhotr, v = rv * rhotr, w = rw * rhotr;
+  double rho_del = DQ[0];
+  const double rho_rat = rho_del / q[0];
+  if (rho_rat < alpq) rho_del /= betq + fabs(rho_rat) * phiq;
+  double rho = q[0] + rho_del;
+  rho = smax(rho, P.rho_min);
+  rho = smin(rho, P.rho_max);
+  const double ptmp = gam1 * (re - 0.5 * (u * u + v * v + w * w) * rho);
+  double p_del = ptmp - q[4];
+  const double p_rat = p_del / (q[4] + p00);
+  if (p_rat < alpq) p_del /= betq + fabs(p_rat) * phiq;
+  double p = q[4] + p_del;
+  p = smax(p, P.p_min);
+  p = smin(p, P.p_max);
+  q[0] = rho;
+  q[1] = u;
+  q[2] = v;
+  q[3] = w;
+  q[4] = p;
+}
+
+// LimitTimeStep's local CFL (compute_timestep.cpp:881-906).
+__device__ __forceinline__ double local_cfl(double p, int det, double cfl, double cfl_min,
+                                            const Params &P) {
+  double cfl_tmp;
+  if (p > P.p_break)
+    cfl_tmp = cfl;
+  else if (p < P.p_min)
+    cfl_tmp = cfl_min;
+  else
+    cfl_tmp = (p - P.p_min) / (P.p_break - P.p_min) * (cfl - cfl_min) + cfl_min;
+  if (!det) cfl_tmp = cfl_min;
+  return cfl_tmp;
+}
+
+// Order-preserving bit pattern of a non-negative double for atomic max/min.
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return static_cast<unsigned long long>(__double_as_longlong(x));
+}
+
+}  // namespace mfg

@@ -199,6 +199,7 @@ int main(int argc, char **argv) {
              *write_mesh = nullptr;
   std::set<int> dump_iters;
   bool dump_all_iters = false;
+  bool light = false;  // timings and norms only
   for (int a = 1; a < argc; a++) {
     std::string k = argv[a];
     auto need = [&](void) -> const char * {
@@ -210,6 +211,7 @@ int main(int argc, char **argv) {
     else if (k == "--params") params = need();
     else if (k == "--out") out = need();
     else if (k == "--write-mesh") write_mesh = need();
+    else if (k == "--light") light = true;
     else if (k == "--dump-iters") {
       std::string v = need();
       if (v == "all") dump_all_iters = true;
@@ -291,15 +293,19 @@ int main(int argc, char **argv) {
   FindNodeSYMM(grid);
   AllocAndCalQuantityGradient(grid);
   double t_pre = now_s() - t0;
-  dump_preprocessing(D, grid);
-  dump_state(D, grid, "init.");
-  dump_grad(D, grid, "init.");
+  if (!light) {
+    dump_preprocessing(D, grid);
+    dump_state(D, grid, "init.");
+    dump_grad(D, grid, "init.");
+  }
+  std::vector<double> iter_times;
 
   const int nc = grid->GetNTCell();
   const long long n = (long long)nc + grid->GetNBFace();
   std::vector<double> norms;
   std::vector<double> diag(nc);
   double t_loop = 0.0, t_phase[4] = {0, 0, 0, 0};  // inviscid, lusgs, gradient, timestep
+  double loop_before = 0.0;
   for (IntType inner_iter = 0; inner_iter < n_steps; ++inner_iter) {
     const bool dump_it = out && (dump_all_iters || dump_iters.count(inner_iter));
     const std::string pfx = "it" + std::to_string(inner_iter) + ".";
@@ -341,6 +347,8 @@ int main(int argc, char **argv) {
     t_phase[1] += t_b - t_a;
     t_phase[2] += t_c - t_b;
     t_loop += t_c - t_a;
+    iter_times.push_back(t_loop - loop_before);
+    loop_before = t_loop;
     // residual norm exactly as main.cpp:294-317 (on the residual of this step)
     const RealFlow *res = grid->GetRes();
     for (int j = 0; j < 5; j++) {
@@ -357,11 +365,14 @@ int main(int argc, char **argv) {
     }
   }
   D.d("norms", norms.data(), (long long)norms.size());
+  D.d("iter_times", iter_times.data(), (long long)iter_times.size());
   double ext[2] = {dt_max, dt_min};
   D.d("final.dt_extrema", ext, 2);
-  D.d("final.res", grid->GetRes(), 5LL * nc);
-  dump_state(D, grid, "final.");
-  dump_grad(D, grid, "final.");
+  if (!light) {
+    D.d("final.res", grid->GetRes(), 5LL * nc);
+    dump_state(D, grid, "final.");
+    dump_grad(D, grid, "final.");
+  }
   double tim[8] = {t_loop, t_pre, t_decouple, t_phase[0], t_phase[1], t_phase[2], t_phase[3],
                    (double)n_steps};
   D.d("timing", tim, 8);

@@ -61,7 +61,7 @@ def write_params(path: str, params: dict) -> None:
 
 def run(mesh, params: dict, *, tdtree: bool = False, dump_iters="0", threads: int | None = None,
         write_mesh: bool = False, workdir: str | None = None, dump: bool = True,
-        timeout: float | None = None) -> dict:
+        timeout: float | None = None, light: bool = False) -> dict:
     """Run the reference on ``mesh`` (a ``meshgen.RawMesh``) and return the dump.
 
     The returned dict also carries ``"summary"`` (the JSON line the harness
@@ -82,8 +82,10 @@ def run(mesh, params: dict, *, tdtree: bool = False, dump_iters="0", threads: in
     meshgen.write_bc(mesh, bcp)
     write_params(par, params)
     cmd = [exe, "--mesh", mfl, "--bc", bcp, "--params", par]
-    if dump:
-        cmd += ["--out", out, "--dump-iters", str(dump_iters)]
+    if dump or light:
+        cmd += ["--out", out, "--dump-iters", str(dump_iters) if dump else "-1"]
+    if light:
+        cmd += ["--light"]
     ren = os.path.join(tmp, "renumbered.mfl")
     if write_mesh:
         cmd += ["--write-mesh", ren]
@@ -99,7 +101,7 @@ def run(mesh, params: dict, *, tdtree: bool = False, dump_iters="0", threads: in
         line = line.strip()
         if line.startswith("{") and line.endswith("}"):
             summary = json.loads(line)
-    res = read_dump(out) if dump else {}
+    res = read_dump(out) if (dump or light) else {}
     res["summary"] = summary
     res["stdout"] = proc.stdout
     if write_mesh:
