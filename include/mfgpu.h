@@ -166,6 +166,29 @@ int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const doub
 int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *phase_ms);
 /* [main.cpp:294-317] L2 norm of each residual component. */
 int mfg_residual_norm(mfg_ctx *ctx, double out[5]);
+
+/* Allocation-free residual norm (no counterpart in the reference: an extra
+ * entry point of this library).  For callers that must not allocate device
+ * memory -- code that holds only device pointers and no mfgpu context
+ * (creating one allocates), or an application whose device memory budget is
+ * owned by another allocator.  res: device pointer to the residual, 5 SoA
+ * blocks of n_cell doubles; norms: device pointer receiving 5 doubles (the
+ * L2 norm of each component).  Runs on `stream` (a cudaStream_t, NULL = the
+ * default stream) on the current device; allocates nothing (no cudaMalloc,
+ * cudaFree or allocating library call).
+ *   - The block partial sums go to a file-scope __device__ array sized for
+ *     MFG_NORM_STATIC_MAX_CELLS cells (2.5 MiB); every device that loads the
+ *     library holds it until the process exits.  Larger n_cell is rejected
+ *     with MFG_ERR_INVALID (message in mfg_last_cuda_error).
+ *   - The first call on a device resolves the array's device address
+ *     (cudaGetSymbolAddress, once per device); make that first call before
+ *     any stream capture.
+ *   - All calls on a device share the one array: calls that overlap on the
+ *     GPU (different streams, no ordering between them) race and may return
+ *     wrong norms.  Every partial read is written by the same call first, so
+ *     no clearing is needed between calls. */
+#define MFG_NORM_STATIC_MAX_CELLS (1 << 24)
+int mfg_residual_norm_static(const double *res, int32_t n_cell, double *norms, void *stream);
 /* The running extrema dt_max / dt_min (para_field_global.cpp:220-221,
  * updated in LimitTimeStep, compute_timestep.cpp:914-918). */
 int mfg_get_dt_extrema(mfg_ctx *ctx, double *dt_max, double *dt_min);

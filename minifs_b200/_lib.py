@@ -114,6 +114,8 @@ def load(build_if_missing: bool = True):
         "mfg_iterate_host": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p, f64p, f64p, f64p]),
         "mfg_residual_norm": (ct.c_int, [ctxp, f64p]),
         "mfg_profile_phases": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
+        "mfg_residual_norm_static": (ct.c_int, [ct.c_void_p, ct.c_int32, ct.c_void_p,
+                                                ct.c_void_p]),
         "mfg_get_dt_extrema": (ct.c_int, [ctxp, f64p, f64p]),
         "mfg_set_dt_extrema": (ct.c_int, [ctxp, ct.c_double, ct.c_double]),
         "mfg_download": (ct.c_int, [ctxp, ct.c_int32, f64p]),

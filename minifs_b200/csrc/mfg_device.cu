@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1341,3 +1342,67 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual norm.
+//
+// For callers that may not allocate device memory themselves: code that
+// only holds device pointers (no mfgpu context, whose creation allocates),
+// or a host application whose device memory budget is owned by another
+// allocator, where an extra cudaMalloc/cudaFree would fail or fragment it.
+// The per-block partial sums live in a fixed file-scope device array instead
+// of a context buffer.  The array stays resident on every device that loads
+// this library until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kStaticNormBlocks = MFG_NORM_STATIC_MAX_CELLS / kBlock;
+static_assert(MFG_NORM_STATIC_MAX_CELLS % kBlock == 0, "whole blocks");
+
+// One partial (5 doubles) per 256-cell block: 65536 x 5 x 8 B = 2.5 MiB.
+__device__ __align__(256) double g_norm_scratch[kStaticNormBlocks * 5];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_dev[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" int mfg_residual_norm_static(const double *res, int32_t n_cell, double *norms,
+                                        void *stream) {
+  if (!res || !norms || n_cell < 0) return MFG_ERR_INVALID;
+  if (n_cell > MFG_NORM_STATIC_MAX_CELLS) {
+    g_cuda_error = "mfg_residual_norm_static: n_cell " + std::to_string(n_cell) +
+                   " exceeds the static scratch limit of " +
+                   std::to_string(MFG_NORM_STATIC_MAX_CELLS) + " cells";
+    return MFG_ERR_INVALID;
+  }
+  int dev = 0;
+  MFG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return MFG_ERR_INVALID;
+  double *scratch = nullptr;
+  {
+    // Host code cannot use the symbol itself (it names a host-side shadow),
+    // so resolve its device address once per device, with it current.
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_dev[dev]) {
+      void *p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
+      if (e != cudaSuccess) {
+        g_cuda_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        return MFG_ERR_CUDA;
+      }
+      g_scratch_dev[dev] = static_cast<double *>(p);
+    }
+    scratch = g_scratch_dev[dev];
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nblocks = grid_for(n_cell);  // <= kStaticNormBlocks by the check above
+  // every partial that k_norm_final reads is written first, so nothing in
+  // the scratch needs clearing between calls
+  k_norm_partial<<<nblocks, kBlock, 0, st>>>(n_cell, res, scratch);
+  k_norm_final<<<1, 160, 0, st>>>(nblocks, scratch, norms, nullptr, nullptr);
+  count_launch(2);
+  MFG_CUDA(cudaGetLastError());
+  return MFG_OK;
+}
