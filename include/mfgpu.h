@@ -129,9 +129,19 @@ int mfg_destroy(mfg_ctx *ctx);
 int mfg_set_stream(mfg_ctx *ctx, void *cuda_stream);
 int mfg_set_params(mfg_ctx *ctx, const mfg_params *params);
 int mfg_info_get(mfg_ctx *ctx, mfg_info *info);
-/* Sweep strategy: 0 = one kernel per level, 1 = persistent kernel with a
- * bounded device-wide barrier between levels. */
+/* Sweep strategy: 0 = one kernel per LU-SGS level; 1 (default when the
+ * device supports cooperative launch) = one persistent kernel per sweep: the
+ * LU-SGS order is cut into one contiguous chunk per resident block, a block
+ * walks its chunk level by level, and a cell that depends on another chunk
+ * waits, with a bounded spin, for that neighbour's ready flag.  Both modes
+ * give identical results. */
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode);
+/* Failure-detection self-test of the bounded waits: runs a forward sweep
+ * whose first chunk is withheld, so the cells that depend on it wait for
+ * flags that are never set; each wait gives up after spin_cycles SM cycles.
+ * Returns MFG_ERR_TIMEOUT and leaves the context's state unchanged and
+ * usable (MFG_ERR_UNSUPPORTED when the grid has a single chunk). */
+int mfg_selftest_sweep_timeout(mfg_ctx *ctx, int64_t spin_cycles);
 
 /* ---- the iteration path (reference routine replaced in brackets) -------- */
 /* [ZeroResiduals, cal_flux.cpp:54-72] */

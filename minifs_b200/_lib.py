@@ -105,6 +105,7 @@ def load(build_if_missing: bool = True):
         "mfg_set_params": (ct.c_int, [ctxp, ct.POINTER(Params)]),
         "mfg_info_get": (ct.c_int, [ctxp, ct.POINTER(Info)]),
         "mfg_set_sweep_mode": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_selftest_sweep_timeout": (ct.c_int, [ctxp, ct.c_int64]),
         "mfg_zero_residuals": (ct.c_int, [ctxp]),
         "mfg_inviscid_flux": (ct.c_int, [ctxp]),
         "mfg_compute_timestep": (ct.c_int, [ctxp, ct.c_int32]),

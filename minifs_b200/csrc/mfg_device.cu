@@ -73,6 +73,12 @@ __global__ void k_download_rec(const double *__restrict__ rec, double *__restric
   for (int k = 0; k < 5; k++) soa[k * n + i] = rec[i * Q_STRIDE + k];
 }
 
+// Interior rows of an increment array set to the "not yet written" sentinel.
+__global__ void k_arm_sentinel(int32_t C, double *__restrict__ dq8) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < C) store_sentinel(dq8, c);
+}
+
 // Per-cell face gather: Roe flux into the residual, local time step with
 // CellIsMG and LimitTimeStep, and the LU-SGS diagonal.  One thread per cell,
 // faces in ascending order (see the file header for why that is exact).
@@ -188,14 +194,43 @@ __global__ void k_dt_clamp(int32_t C, double *__restrict__ dt,
 }
 
 // Forward (lower) sweep of one level: cells [l0, l1) of the level order.
-// In the fused path the ratio clamp of LimitTimeStep is applied here: a cell
-// whose dt exceeds the limit gets the limited dt and its Diag rebuilt.
+// Increments of the forward sweep go to dqf, those of the backward sweep to
+// dqb (the final DQ); each sweep re-arms the other array's row of its cell
+// with the sentinel (see mfg_kernels.cuh), the protocol the persistent
+// sweeps rely on.  In the fused path the ratio clamp of LimitTimeStep is
+// applied here: a cell whose dt exceeds the limit gets the limited dt and
+// its Diag rebuilt.
+__device__ __forceinline__ void clamp_diag(int32_t c, const double *qc, double &dg,
+                                           const Params &P, double *__restrict__ dt,
+                                           const unsigned long long *__restrict__ dt_ext,
+                                           const int32_t *__restrict__ cptr,
+                                           const SlotRec *__restrict__ slots,
+                                           const double *__restrict__ vol,
+                                           double *__restrict__ diag) {
+  const double dt_max = __longlong_as_double((long long)dt_ext[0]);
+  const double dt_min = __longlong_as_double((long long)dt_ext[1]);
+  if (dt_max / dt_min > P.ratio_dtmax) {
+    const double lim = P.ratio_dtmax * dt_min;
+    if (dt[c] > lim) {
+      dt[c] = lim;
+      dg = vol[c] / lim;
+      for (int32_t s = cptr[c]; s < cptr[c + 1]; s++) {
+        const SlotRec sr = slots[s];
+        double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
+        vn = fabs(vn);
+        dg += 0.5 * sr.area * (vn + qc[Q_A]) * P.lhs_omga;
+      }
+      diag[c] = dg;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kBlock)
 k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
             const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
             const int32_t *__restrict__ nbs, const double *__restrict__ q8,
-            double *__restrict__ dq8, const double *__restrict__ res, int32_t C,
-            double *__restrict__ diag, int32_t first_cell, Params P, int clamp_check,
+            double *__restrict__ dqf, double *__restrict__ dqb, const double *__restrict__ res,
+            int32_t C, double *__restrict__ diag, int32_t first_cell, Params P, int clamp_check,
             double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
             const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
             const double *__restrict__ vol) {
@@ -210,38 +245,18 @@ k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
     const int32_t nb = nbs[s];
     double qn[Q_STRIDE], dn[5], f[5];
     load_q(q8, nb, qn);
-    load_dq_cg(dq8, nb, dn);
+    load_dq_cg(dqf, nb, dn);
     flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
     for (int k = 0; k < 5; k++) d[k] -= r.w * f[k];
   }
   double dg = diag[c];
-  if (clamp_check) {
-    const double dt_max = __longlong_as_double((long long)dt_ext[0]);
-    const double dt_min = __longlong_as_double((long long)dt_ext[1]);
-    if (dt_max / dt_min > P.ratio_dtmax) {
-      const double lim = P.ratio_dtmax * dt_min;
-      if (dt[c] > lim) {
-        dt[c] = lim;
-        double qc[Q_STRIDE];
-        load_q(q8, c, qc);
-        dg = vol[c] / lim;
-        for (int32_t s = cptr[c]; s < cptr[c + 1]; s++) {
-          const SlotRec sr = slots[s];
-          double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
-          vn = fabs(vn);
-          dg += 0.5 * sr.area * (vn + qc[Q_A]) * P.lhs_omga;
-        }
-        diag[c] = dg;
-      }
-    }
-  }
+  double qc[Q_STRIDE];
+  load_q(q8, c, qc);
+  if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext, cptr, slots, vol, diag);
   for (int k = 0; k < 5; k++) d[k] /= dg;
-  if (c != first_cell) {
-    double qc[Q_STRIDE];
-    load_q(q8, c, qc);
-    dq_limit(qc, d, P);
-  }
-  store_dq(dq8, c, d);
+  if (c != first_cell) dq_limit(qc, d, P);
+  store_dq(dqf, c, d);
+  store_sentinel(dqb, c);
 }
 
 // Backward (upper) sweep of one level, fused with the state update: the new
@@ -251,20 +266,20 @@ __global__ void __launch_bounds__(kBlock)
 k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
             const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
             const int32_t *__restrict__ nbs, const double *__restrict__ q8,
-            double *__restrict__ q8_new, double *__restrict__ dq8,
+            double *__restrict__ q8_new, double *__restrict__ dqf, double *__restrict__ dqb,
             const double *__restrict__ diag, Params P) {
   const int32_t i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= l1) return;
   const int32_t c = cells[i];
   double d[5], fs[5] = {0., 0., 0., 0., 0.};
-  load_dq_cg(dq8, c, d);
+  load_dq_cg(dqf, c, d);
   const int32_t s1 = sptr[i + 1];
   for (int32_t s = sptr[i]; s < s1; s++) {
     const SweepRec r = recs[s];
     const int32_t nb = nbs[s];
     double qn[Q_STRIDE], dn[5], f[5];
     load_q(q8, nb, qn);
-    load_dq_cg(dq8, nb, dn);
+    load_dq_cg(dqb, nb, dn);
     flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
     for (int k = 0; k < 5; k++) fs[k] += r.w * f[k];
   }
@@ -273,10 +288,183 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
   double qc[Q_STRIDE];
   load_q(q8, c, qc);
   dq_limit(qc, d, P);
-  store_dq(dq8, c, d);
+  store_dq(dqb, c, d);
+  store_sentinel(dqf, c);
   update_cell(qc, d, P);
   cell_props(qc, P);
   store_q(q8_new, c, qc);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent chunked sweeps.  Cells are split into chunks, one per resident
+// block (cooperative launch), so that every LU-SGS level is shared evenly by
+// the chunks and most dependencies stay inside a chunk (a cell joins the
+// chunk of most of the cells it depends on).  A block walks the levels of its
+// chunk in increasing order, all its threads sharing one level, with
+// __syncthreads between levels: a dependency inside the chunk is then
+// resolved through the SM's own L1.  A dependency on another chunk is
+// resolved by polling the neighbour's increment in L2 until it is no longer
+// the sentinel (bounded wait).  Progress: a cell waits only for cells of
+// lower levels, each block visits its levels in increasing order, and every
+// block is resident, so by induction over the levels every cell completes.
+// ---------------------------------------------------------------------------
+// Threads per persistent block and resident blocks per SM (tuning).
+#ifndef MFG_PERSIST_BLOCK
+#define MFG_PERSIST_BLOCK 64
+#endif
+#ifndef MFG_PERSIST_MINB
+#define MFG_PERSIST_MINB 6
+#endif
+constexpr int kPersistBlock = MFG_PERSIST_BLOCK;
+constexpr int kPre = 4;                  // neighbour records held in registers
+constexpr uint32_t kMark = 0x80000000u;  // high bit of a neighbour: in another chunk
+constexpr int kMinChunk = 64;            // no chunk smaller than this many cells
+
+// Per chunk position: the cell, its first record and its record count.
+struct __align__(16) ChunkCell {
+  int32_t cell, s0, ns, pad;
+};
+
+// acc (-/+)= w * FluxLUSGS3D(q[nb], DQ[nb], n) over records [s0, s0+ns) in
+// order, DQ[nb] read from src (same chunk: written before the last
+// __syncthreads; other chunk: waited for in L2).
+template <bool FWD>
+__device__ __forceinline__ void sweep_gather(int32_t s0, int32_t ns,
+                                             const SweepRec *__restrict__ recs,
+                                             const int32_t *__restrict__ nbs,
+                                             const double *__restrict__ q8, const double *src,
+                                             int *err, long long spin, const Params &P,
+                                             double *acc) {
+  SweepRec r[kPre];
+  uint32_t nb[kPre];
+  double qn[kPre][Q_STRIDE];
+#pragma unroll
+  for (int j = 0; j < kPre; j++)
+    if (j < ns) {
+      r[j] = recs[s0 + j];
+      nb[j] = (uint32_t)nbs[s0 + j];
+      load_q(q8, nb[j] & ~kMark, qn[j]);
+    }
+#pragma unroll
+  for (int j = 0; j < kPre; j++)
+    if (j < ns) {
+      double dn[5], f[5];
+      const double *rec = src + (int64_t)(nb[j] & ~kMark) * Q_STRIDE;
+      if (nb[j] & kMark) {
+        wait_rec(rec, dn, err, spin);
+      } else {
+        const double2 *pp = reinterpret_cast<const double2 *>(rec);
+        const double2 x = pp[0], y = pp[1], z = pp[2];
+        dn[0] = x.x; dn[1] = x.y; dn[2] = y.x; dn[3] = y.y; dn[4] = z.x;
+      }
+      flux_lusgs(qn[j], dn, r[j].nx, r[j].ny, r[j].nz, P, f);
+      for (int k = 0; k < 5; k++) {
+        if (FWD)
+          acc[k] -= r[j].w * f[k];
+        else
+          acc[k] += r[j].w * f[k];
+      }
+    }
+  for (int32_t s = s0 + kPre; s < s0 + ns; s++) {
+    const SweepRec rr = recs[s];
+    const uint32_t b = (uint32_t)nbs[s];
+    double qq[Q_STRIDE], dn[5], f[5];
+    load_q(q8, b & ~kMark, qq);
+    const double *rec = src + (int64_t)(b & ~kMark) * Q_STRIDE;
+    if (b & kMark) {
+      wait_rec(rec, dn, err, spin);
+    } else {
+      const double2 *pp = reinterpret_cast<const double2 *>(rec);
+      const double2 x = pp[0], y = pp[1], z = pp[2];
+      dn[0] = x.x; dn[1] = x.y; dn[2] = y.x; dn[3] = y.y; dn[4] = z.x;
+    }
+    flux_lusgs(qq, dn, rr.nx, rr.ny, rr.nz, P, f);
+    for (int k = 0; k < 5; k++) {
+      if (FWD)
+        acc[k] -= rr.w * f[k];
+      else
+        acc[k] += rr.w * f[k];
+    }
+  }
+}
+
+// chunk_skip > 0 withholds the first chunk_skip chunks (failure-detection
+// self-test only: the cells that depend on them wait until the bound runs out).
+__global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
+k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
+                  const ChunkCell *__restrict__ ccells, const SweepRec *__restrict__ recs,
+                  const int32_t *__restrict__ nbs, const double *__restrict__ q8, double *dqf,
+                  double *__restrict__ dqb, const double *__restrict__ res, int32_t C,
+                  double *__restrict__ diag, int32_t first_cell, Params P, int clamp_check,
+                  double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
+                  const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+                  const double *__restrict__ vol, int *err, long long spin,
+                  int32_t chunk_skip) {
+  if ((int32_t)blockIdx.x < chunk_skip) return;
+  const int32_t sg1 = seg_begin[blockIdx.x + 1];
+  for (int32_t sg = seg_begin[blockIdx.x]; sg < sg1; sg++) {
+    const int32_t a = segs[sg], b = segs[sg + 1];
+    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+      const ChunkCell cc = ccells[i];
+      const int32_t c = cc.cell;
+      double d[5];
+      for (int k = 0; k < 5; k++) d[k] = res[(int64_t)k * C + c];
+      double dg = diag[c];
+      double qc[Q_STRIDE];
+      load_q(q8, c, qc);
+      sweep_gather<true>(cc.s0, cc.ns, recs, nbs, q8, dqf, err, spin, P, d);
+      if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext, cptr, slots, vol, diag);
+      for (int k = 0; k < 5; k++) d[k] /= dg;
+      if (c != first_cell) dq_limit(qc, d, P);
+      store_dq(dqf, c, d);
+      store_sentinel(dqb, c);  // armed for the backward sweep
+    }
+    __syncthreads();
+  }
+}
+
+// Backward sweep.  The state update of a cell is not needed by any later
+// level, so it runs after the block has swept its whole chunk.
+__global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
+k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
+                  const ChunkCell *__restrict__ ccells, const SweepRec *__restrict__ recs,
+                  const int32_t *__restrict__ nbs, const double *__restrict__ q8,
+                  double *__restrict__ q8_new, double *__restrict__ dqf, double *dqb,
+                  const double *__restrict__ diag, Params P, int *err, long long spin) {
+  const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
+  for (int32_t sg = sg0; sg < sg1; sg++) {
+    const int32_t a = segs[sg], b = segs[sg + 1];
+    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+      const ChunkCell cc = ccells[i];
+      const int32_t c = cc.cell;
+      double d[5], fs[5] = {0., 0., 0., 0., 0.};
+      load_dq_cg(dqf, c, d);  // this cell's forward value (previous kernel)
+      double qc[Q_STRIDE];
+      load_q(q8, c, qc);
+      const double tmp = 2.0 * diag[c];
+      sweep_gather<false>(cc.s0, cc.ns, recs, nbs, q8, dqb, err, spin, P, fs);
+      for (int k = 0; k < 5; k++) d[k] -= fs[k] / tmp;
+      dq_limit(qc, d, P);
+      store_dq(dqb, c, d);
+      store_sentinel(dqf, c);  // armed for the next forward sweep
+    }
+    __syncthreads();
+  }
+  // UpdateFlowField3D_CFL3d for the chunk's cells (their DQ is final now)
+  if (sg1 > sg0) {
+    const int32_t a = segs[sg0], b = segs[sg1];
+    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+      const int32_t c = ccells[i].cell;
+      double d[5], qc[Q_STRIDE];
+      const double2 *pp = reinterpret_cast<const double2 *>(dqb + (int64_t)c * Q_STRIDE);
+      const double2 x = pp[0], y = pp[1], z = pp[2];
+      d[0] = x.x; d[1] = x.y; d[2] = y.x; d[3] = y.y; d[4] = z.x;
+      load_q(q8, c, qc);
+      update_cell(qc, d, P);
+      cell_props(qc, P);
+      store_q(q8_new, c, qc);
+    }
+  }
 }
 
 // Node values of all five variables (CompNodeVar3D_dist, cal_gradient.cpp
@@ -442,9 +630,11 @@ __global__ void k_norm_final(int32_t nparts, const double *__restrict__ part,
 // context
 // ---------------------------------------------------------------------------
 
-struct DevBuf {
-  void *p = nullptr;
-  size_t bytes = 0;
+struct ChunkSweep {
+  int32_t *seg_begin = nullptr, *segs = nullptr, *nbs = nullptr;
+  ChunkCell *cells = nullptr;
+  SweepRec *recs = nullptr;
+  int32_t nseg = 0;
 };
 
 struct mfg_ctx {
@@ -474,6 +664,13 @@ struct mfg_ctx {
   int32_t *bw_cells = nullptr, *bw_sptr = nullptr, *bw_nb = nullptr;
   SweepRec *bw_recs = nullptr;
   std::vector<int32_t> fw_lptr, bw_lptr;
+  // persistent sweeps: chunked level order, ready flags, error word
+  ChunkSweep fwc, bwc;
+  int32_t nchunks = 0;
+  bool chunk0_exported = false;
+  double *dqf = nullptr;  // forward-sweep increments (dq8 holds the backward ones = DQ)
+  int *sweep_err = nullptr;
+  int persist_grid = 0;
   unsigned long long *dt_ext = nullptr;
   double *norm_part = nullptr, *norm_out = nullptr, *norm_hist = nullptr, *cfl_tab = nullptr;
   int32_t *iter_counter = nullptr;
@@ -702,11 +899,100 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
         s++;
       }
     }
+    // Chunks for the persistent sweeps, one per resident block.  Level by
+    // level, a cell joins the chunk that most of its dependencies are in,
+    // unless that chunk already holds its share of the level; the remaining
+    // cells fill the chunks in order.  Every level is thereby spread evenly
+    // over the chunks while dependency chains mostly stay in one chunk.
+    const int32_t P = ctx->nchunks;
+    std::vector<int32_t> assign(C, -1), load(P), pending, chunk_cnt(P, 0);
+    for (int32_t l = 0; l < L; l++) {
+      const int32_t a0 = lptr[l], a1 = lptr[l + 1];
+      const int32_t quota = (a1 - a0 + P - 1) / P;
+      std::fill(load.begin(), load.end(), 0);
+      pending.clear();
+      for (int32_t i = a0; i < a1; i++) {
+        int32_t best = -1, bestn = 0;
+        for (int32_t s0 = sptr[i]; s0 < sptr[i + 1]; s0++) {
+          if (nbs[s0] >= C) continue;
+          const int32_t ch = assign[nbs[s0]];
+          int32_t votes = 0;
+          for (int32_t t = sptr[i]; t < sptr[i + 1]; t++)
+            if (nbs[t] < C && assign[nbs[t]] == ch) votes++;
+          if (votes > bestn) {
+            best = ch;
+            bestn = votes;
+          }
+        }
+        if (best >= 0 && load[best] < quota) {
+          assign[cells[i]] = best;
+          load[best]++;
+        } else {
+          pending.push_back(cells[i]);
+        }
+      }
+      int32_t pp = 0;
+      for (int32_t c : pending) {
+        while (load[pp] >= quota) pp++;
+        assign[c] = pp;
+        load[pp]++;
+      }
+    }
+    // chunk-major, level-sorted cell lists (the level order is already sorted)
+    for (int32_t c = 0; c < C; c++) chunk_cnt[assign[c]]++;
+    std::vector<int32_t> chunk_ptr(P + 1, 0);
+    for (int32_t p = 0; p < P; p++) chunk_ptr[p + 1] = chunk_ptr[p] + chunk_cnt[p];
+    std::vector<int32_t> slot_of(C), cfill(chunk_ptr.begin(), chunk_ptr.end() - 1);
+    std::vector<int32_t> ccells(C);
+    for (int32_t i = 0; i < C; i++) {
+      const int32_t c = cells[i];
+      slot_of[i] = cfill[assign[c]]++;
+      ccells[slot_of[i]] = c;
+    }
+    std::vector<int32_t> gpos(C);
+    for (int32_t i = 0; i < C; i++) gpos[cells[i]] = i;
+    std::vector<int32_t> csptr(C + 1, 0), segs, seg_begin;
+    for (int32_t k = 0; k < C; k++) {
+      const int32_t gi = gpos[ccells[k]];
+      csptr[k + 1] = csptr[k] + (sptr[gi + 1] - sptr[gi]);
+    }
+    std::vector<int32_t> cnbs(csptr[C]);
+    std::vector<SweepRec> crecs(csptr[C]);
+    bool chunk0_exported = false;
+    for (int32_t p = 0; p < P; p++) {
+      seg_begin.push_back((int32_t)segs.size());
+      for (int32_t k = chunk_ptr[p]; k < chunk_ptr[p + 1]; k++) {
+        const int32_t c = ccells[k];
+        if (k == chunk_ptr[p] || lv[c] != lv[ccells[k - 1]]) segs.push_back(k);
+        const int32_t gi = gpos[c];
+        int32_t o = csptr[k];
+        for (int32_t s0 = sptr[gi]; s0 < sptr[gi + 1]; s0++, o++) {
+          const int32_t nb = nbs[s0];
+          const bool cross = nb < C && assign[nb] != p;
+          if (cross && assign[nb] == 0) chunk0_exported = true;
+          cnbs[o] = cross ? (int32_t)((uint32_t)nb | kMark) : nb;
+          crecs[o] = recs[s0];
+        }
+      }
+    }
+    seg_begin.push_back((int32_t)segs.size());
+    segs.push_back(C);
+    if (fwd) ctx->chunk0_exported = chunk0_exported;
     int rc;
     if ((rc = dupload(ctx, d_cells, cells))) return rc;
     if ((rc = dupload(ctx, d_sptr, sptr))) return rc;
     if ((rc = dupload(ctx, d_recs, recs))) return rc;
     if ((rc = dupload(ctx, d_nb, nbs))) return rc;
+    ChunkSweep &cs = fwd ? ctx->fwc : ctx->bwc;
+    cs.nseg = (int32_t)segs.size() - 1;
+    if ((rc = dupload(ctx, &cs.seg_begin, seg_begin))) return rc;
+    if ((rc = dupload(ctx, &cs.segs, segs))) return rc;
+    std::vector<ChunkCell> packed(C);
+    for (int32_t k = 0; k < C; k++)
+      packed[k] = ChunkCell{ccells[k], csptr[k], csptr[k + 1] - csptr[k], 0};
+    if ((rc = dupload(ctx, &cs.cells, packed))) return rc;
+    if ((rc = dupload(ctx, &cs.recs, crecs))) return rc;
+    if ((rc = dupload(ctx, &cs.nbs, cnbs))) return rc;
     return MFG_OK;
   };
   (void)n;
@@ -873,6 +1159,21 @@ int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, in
   slots.shrink_to_fit();
   std::vector<double> volv(m->vol, m->vol + n);
   if ((rc = dupload(ctx, &ctx->vol, volv))) return fail(rc);
+  {
+    // persistent sweeps need every block resident: one chunk per block, at
+    // most as many blocks as the occupancy of the heavier kernel allows
+    int bf = 0, bb = 0, coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_sweep_fwd_chunk, kPersistBlock,
+                                                      0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_sweep_bwd_chunk, kPersistBlock,
+                                                      0) != cudaSuccess)
+      return fail(MFG_ERR_CUDA);
+    const int per_sm = std::min(bf, bb);
+    ctx->persist_grid = coop ? per_sm * prop.multiProcessorCount : 0;
+    ctx->nchunks = std::max(1, std::min(ctx->persist_grid, (C + kMinChunk - 1) / kMinChunk));
+    ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
+  }
   if ((rc = build_levels(ctx, m, cptr, c2f))) return fail(rc);
   if ((rc = build_node_lists(ctx, m))) return fail(rc);
 
@@ -892,6 +1193,8 @@ int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, in
   if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->norm_out, 5))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dqf, (size_t)n * Q_STRIDE))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->sweep_err, 1))) return fail(rc);
   if (cudaMallocHost((void **)&ctx->h_pinned, 64 * sizeof(double)) != cudaSuccess)
     return fail(MFG_ERR_NOMEM);
 
@@ -904,8 +1207,13 @@ int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, in
       cudaMemsetAsync(ctx->dqdy, 0, sizeof(double) * 5 * n, st) ||
       cudaMemsetAsync(ctx->dqdz, 0, sizeof(double) * 5 * n, st) ||
       cudaMemsetAsync(ctx->qn8, 0, sizeof(double) * ctx->N * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->dqf, 0, sizeof(double) * n * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->sweep_err, 0, sizeof(int), st) ||
       cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st))
     return fail(MFG_ERR_CUDA);
+  k_arm_sentinel<<<grid_for(C), kBlock, 0, st>>>(C, ctx->dqf);  // ready for a forward sweep
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess) return fail(MFG_ERR_CUDA);
   if ((rc = mfg_set_dt_extrema(ctx, 0.0, kBig))) return fail(rc);  // para_field_global.cpp:220-221
   if ((rc = mfg_upload(ctx, MFG_FIELD_Q, q0))) return fail(rc);
   if (cudaStreamSynchronize(st) != cudaSuccess) return fail(MFG_ERR_CUDA);
@@ -932,8 +1240,14 @@ int mfg_set_params(mfg_ctx *ctx, const mfg_params *p) {
 }
 
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode) {
-  if (!ctx || mode != 0) return mode == 1 ? MFG_ERR_UNSUPPORTED : MFG_ERR_INVALID;
+  if (!ctx || (mode != 0 && mode != 1)) return MFG_ERR_INVALID;
+  if (mode == 1 && ctx->persist_grid <= 0) return MFG_ERR_UNSUPPORTED;
   ctx->sweep_mode = mode;
+  for (int k = 0; k < 2; k++)
+    if (ctx->graph[k]) {
+      cudaGraphExecDestroy(ctx->graph[k]);
+      ctx->graph[k] = nullptr;
+    }
   return MFG_OK;
 }
 
@@ -1007,7 +1321,68 @@ int mfg_compute_timestep(mfg_ctx *ctx, int32_t iter_done) {
   return check_kernel();
 }
 
+static int launch_coop(const void *fn, int blocks, cudaStream_t st, void **args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kPersistBlock);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  MFG_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+  count_launch();
+  return MFG_OK;
+}
+
+static int launch_fwd_persist(mfg_ctx *ctx, bool clamp_check, int32_t chunk_skip,
+                              long long spin) {
+  const double *q = ctx->q8[ctx->cur];
+  int32_t C = ctx->C, first = ctx->first_cell, skip = chunk_skip;
+  int clamp = clamp_check ? 1 : 0;
+  Params P = ctx->P;
+  ChunkSweep &w = ctx->fwc;
+  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, (void *)&q,
+                  &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P, &clamp, &ctx->dt,
+                  &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol, &ctx->sweep_err, &spin, &skip};
+  return launch_coop((const void *)k_sweep_fwd_chunk, ctx->nchunks, ctx->stream, args);
+}
+
+static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
+  const double *q = ctx->q8[ctx->cur];
+  double *qn = ctx->q8[ctx->cur ^ 1];
+  Params P = ctx->P;
+  ChunkSweep &w = ctx->bwc;
+  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, (void *)&q, &qn,
+                  &ctx->dqf, &ctx->dq8, &ctx->diag, &P, &ctx->sweep_err, &spin};
+  return launch_coop((const void *)k_sweep_bwd_chunk, ctx->nchunks, ctx->stream, args);
+}
+
+// Reads the sweeps' error word; on a timeout, re-arms the flags so that the
+// context stays usable, and reports MFG_ERR_TIMEOUT.  Synchronises.
+static int check_sweep_error(mfg_ctx *ctx) {
+  if (ctx->sweep_mode != 1) return MFG_OK;
+  int *h = reinterpret_cast<int *>(ctx->h_pinned + 32);
+  MFG_CUDA(cudaMemcpyAsync(h, ctx->sweep_err, sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (*h == 0) return MFG_OK;
+  k_arm_sentinel<<<grid_for(ctx->C), kBlock, 0, ctx->stream>>>(ctx->C, ctx->dqf);
+  count_launch();
+  MFG_CUDA(cudaMemsetAsync(ctx->sweep_err, 0, sizeof(int), ctx->stream));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  g_cuda_error = "an LU-SGS sweep gave up waiting for a neighbour (results invalid)";
+  return MFG_ERR_TIMEOUT;
+}
+
 static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
+  if (ctx->sweep_mode == 1) {
+    int rc = launch_fwd_persist(ctx, clamp_check, 0, kSpinCycles);
+    if (rc) return rc;
+    return launch_bwd_persist(ctx, kSpinCycles);
+  }
   cudaStream_t st = ctx->stream;
   const double *q = ctx->q8[ctx->cur];
   double *qn = ctx->q8[ctx->cur ^ 1];
@@ -1015,15 +1390,15 @@ static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
   for (int l = 0; l < Lf; l++) {
     const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
     k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
-        a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dq8, ctx->res,
-        ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt, ctx->dt_ext,
-        ctx->cptr, ctx->slots, ctx->vol);
+        a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
+        ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt,
+        ctx->dt_ext, ctx->cptr, ctx->slots, ctx->vol);
   }
   for (int l = 0; l < Lb; l++) {
     const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
     k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
-                                                    ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dq8,
-                                                    ctx->diag, ctx->P);
+                                                    ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dqf,
+                                                    ctx->dq8, ctx->diag, ctx->P);
   }
   count_launch(Lf + Lb);
   return check_kernel();
@@ -1037,7 +1412,37 @@ int mfg_forward_lusgs(mfg_ctx *ctx) {
   rc = launch_sweeps(ctx, false);
   if (rc) return rc;
   ctx->cur ^= 1;
-  return MFG_OK;
+  return check_sweep_error(ctx);
+}
+
+// Failure-detection self-test: a forward sweep whose first chunk is never
+// run, so the cells that depend on it wait for flags nobody sets.  The
+// bounded waits give up after spin_cycles; the call must return
+// MFG_ERR_TIMEOUT and leave the context usable.  State is not changed.
+int mfg_selftest_sweep_timeout(mfg_ctx *ctx, int64_t spin_cycles) {
+  if (!ctx || spin_cycles <= 0) return MFG_ERR_INVALID;
+  if (ctx->sweep_mode != 1 || ctx->nchunks < 2 || !ctx->chunk0_exported)
+    return MFG_ERR_UNSUPPORTED;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  // keep DQ intact: the test sweep writes only cells of later levels, so
+  // save and restore the whole increment array around it
+  double *save = nullptr;
+  int rc = dalloc(ctx, &save, (size_t)ctx->n * Q_STRIDE);
+  if (rc) return rc;
+  MFG_CUDA(cudaMemcpyAsync(save, ctx->dq8, sizeof(double) * ctx->n * Q_STRIDE,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
+  rc = launch_fwd_persist(ctx, false, 1, (long long)spin_cycles);
+  const int rc2 = check_sweep_error(ctx);
+  cudaMemcpyAsync(ctx->dq8, save, sizeof(double) * ctx->n * Q_STRIDE, cudaMemcpyDeviceToDevice,
+                  ctx->stream);
+  k_arm_sentinel<<<grid_for(ctx->C), kBlock, 0, ctx->stream>>>(ctx->C, ctx->dqf);
+  count_launch();
+  cudaStreamSynchronize(ctx->stream);
+  ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)save));
+  ctx->device_bytes -= (int64_t)sizeof(double) * ctx->n * Q_STRIDE;
+  cudaFree(save);
+  if (rc) return rc;
+  return rc2;
 }
 
 static int launch_gradient(mfg_ctx *ctx) {
@@ -1152,7 +1557,7 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
     MFG_CUDA(cudaStreamSynchronize(st));
   }
   MFG_CUDA(cudaGetLastError());
-  return MFG_OK;
+  return check_sweep_error(ctx);
 }
 
 int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *phase_ms) {
@@ -1188,21 +1593,27 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
     cudaEventRecord(ev[0], st);
     rc = launch_face(ctx, true, true, true, 0.0, true);
     cudaEventRecord(ev[1], st);
-    for (int l = 0; l < Lf && rc == MFG_OK; l++) {
-      const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
-      k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
-          a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dq8, ctx->res,
-          ctx->C, ctx->diag, ctx->first_cell, ctx->P, 1, ctx->dt, ctx->dt_ext, ctx->cptr,
-          ctx->slots, ctx->vol);
+    if (ctx->sweep_mode == 1) {
+      if (rc == MFG_OK) rc = launch_fwd_persist(ctx, true, 0, kSpinCycles);
+      cudaEventRecord(ev[2], st);
+      if (rc == MFG_OK) rc = launch_bwd_persist(ctx, kSpinCycles);
+    } else {
+      for (int l = 0; l < Lf && rc == MFG_OK; l++) {
+        const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
+        k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
+            a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
+            ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, 1, ctx->dt, ctx->dt_ext,
+            ctx->cptr, ctx->slots, ctx->vol);
+      }
+      cudaEventRecord(ev[2], st);
+      for (int l = 0; l < Lb; l++) {
+        const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
+        k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
+                                                        ctx->bw_recs, ctx->bw_nb, q, qn,
+                                                        ctx->dqf, ctx->dq8, ctx->diag, ctx->P);
+      }
+      count_launch(Lf + Lb);
     }
-    cudaEventRecord(ev[2], st);
-    for (int l = 0; l < Lb; l++) {
-      const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
-      k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
-                                                      ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dq8,
-                                                      ctx->diag, ctx->P);
-    }
-    count_launch(Lf + Lb);
     cudaEventRecord(ev[3], st);
     ctx->cur ^= 1;
     const double *q2 = ctx->q8[ctx->cur];
@@ -1228,7 +1639,8 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
   }
   ctx->res_zero = false;
   for (auto &e : ev) cudaEventDestroy(e);
-  return rc;
+  if (rc) return rc;
+  return check_sweep_error(ctx);
 }
 
 int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const double *q_in,

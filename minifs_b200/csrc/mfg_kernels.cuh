@@ -80,11 +80,13 @@ __device__ __forceinline__ void load_dq_cg(const double *dq8, int64_t c, double 
   d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y; d[4] = e.x;
 }
 
+// Plain (write-through) stores: readers in the same block see them after
+// __syncthreads, readers on other SMs through L2 after the release flag.
 __device__ __forceinline__ void store_dq(double *dq8, int64_t c, const double *d) {
   double2 *p = reinterpret_cast<double2 *>(dq8 + c * Q_STRIDE);
-  __stcg(p, make_double2(d[0], d[1]));
-  __stcg(p + 1, make_double2(d[2], d[3]));
-  __stcg(p + 2, make_double2(d[4], 0.0));
+  p[0] = make_double2(d[0], d[1]);
+  p[1] = make_double2(d[2], d[3]);
+  p[2] = make_double2(d[4], 0.0);
 }
 
 // Derived per-cell quantities from the primitive variables.
@@ -289,6 +291,73 @@ __device__ __forceinline__ double local_cfl(double p, int det, double cfl, doubl
 // Order-preserving bit pattern of a non-negative double for atomic max/min.
 __device__ __forceinline__ unsigned long long dbits(double x) {
   return static_cast<unsigned long long>(__double_as_longlong(x));
+}
+
+// ---- readiness of LU-SGS increments -----------------------------------------
+// The forward and backward increments live in separate arrays whose interior
+// rows hold this signalling-NaN pattern until written.  IEEE arithmetic only
+// produces quiet NaNs, so a computed increment never equals it, and every
+// 8-byte word is written and read atomically: a reader may use a record as
+// soon as none of its five words is the sentinel, with no flag or fence.
+constexpr unsigned long long kSentinelBits = 0x7FF40000DEADBEEFull;
+
+__device__ __forceinline__ bool is_sentinel(double x) {
+  return (unsigned long long)__double_as_longlong(x) == kSentinelBits;
+}
+
+// Five words of a record straight from L2 (the point of coherence), never a
+// stale L1 line; asm volatile keeps the loads inside a polling loop.
+__device__ __forceinline__ void load_rec5_l2(const double *rec, double *d) {
+  double a0, a1, b0, b1, e0;
+  asm volatile("ld.global.cg.v2.f64 {%0, %1}, [%2];" : "=d"(a0), "=d"(a1) : "l"(rec) : "memory");
+  asm volatile("ld.global.cg.v2.f64 {%0, %1}, [%2];" : "=d"(b0), "=d"(b1) : "l"(rec + 2) : "memory");
+  asm volatile("ld.global.cg.f64 %0, [%1];" : "=d"(e0) : "l"(rec + 4) : "memory");
+  d[0] = a0; d[1] = a1; d[2] = b0; d[3] = b1; d[4] = e0;
+}
+
+__device__ __forceinline__ bool rec5_ready(const double *d) {
+  return !(is_sentinel(d[0]) || is_sentinel(d[1]) || is_sentinel(d[2]) || is_sentinel(d[3]) ||
+           is_sentinel(d[4]));
+}
+
+__device__ __forceinline__ int ld_relaxed(const int *p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Cycles a lane may wait for one neighbour (~2 s at 1.9 GHz) before it gives
+// up, records the failure in *err and lets the sweep run to its end.
+constexpr long long kSpinCycles = 4000000000LL;
+
+// Bounded wait for a neighbour increment produced on another SM: poll the
+// record in L2 until none of its words is the sentinel.  Returns false when
+// it gave up (or another lane did); d then holds whatever was read.
+__device__ __forceinline__ bool wait_rec(const double *rec, double *d, int *err,
+                                         long long max_cycles) {
+  load_rec5_l2(rec, d);
+  if (rec5_ready(d)) return true;
+  const long long t0 = clock64();
+  int polls = 0;
+  for (;;) {
+    if (polls > 64) __nanosleep(64);
+    ++polls;
+    load_rec5_l2(rec, d);
+    if (rec5_ready(d)) return true;
+    if (ld_relaxed(err)) return false;  // another lane gave up: finish quickly
+    if (clock64() - t0 > max_cycles) {
+      atomicExch(err, 1);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void store_sentinel(double *dq8, int64_t c) {
+  const double s = __longlong_as_double((long long)kSentinelBits);
+  double2 *p = reinterpret_cast<double2 *>(dq8 + c * Q_STRIDE);
+  p[0] = make_double2(s, s);
+  p[1] = make_double2(s, s);
+  p[2] = make_double2(s, 0.0);
 }
 
 }  // namespace mfg

@@ -113,6 +113,14 @@ class Solver:
         self.iter_done += n
         return dict(zip(_lib.PHASES, out.tolist()))
 
+    def set_sweep_mode(self, mode: int):
+        """0 = one kernel per LU-SGS level, 1 = persistent dataflow sweeps."""
+        self._call("mfg_set_sweep_mode", int(mode))
+
+    def selftest_sweep_timeout(self, spin_cycles: int = 2_000_000) -> int:
+        """Run the bounded-wait self-test; returns the status code."""
+        return int(self.lib.mfg_selftest_sweep_timeout(self._ctx, int(spin_cycles)))
+
     def set_stream(self, stream_handle: int):
         """Issue the context's work on this cudaStream_t (e.g. torch's)."""
         _lib.check("mfg_set_stream", self.lib.mfg_set_stream(self._ctx, ct.c_void_p(stream_handle)))

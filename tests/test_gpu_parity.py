@@ -153,3 +153,34 @@ def test_upload_download_round_trip_and_errors():
     s.zero_residuals()
     assert not s.download("res").any()
     s.close()
+
+
+@pytest.mark.parametrize("name", ["cube4", "tdtree8"])
+def test_sweep_modes_identical(name):
+    """Per-level launches and the persistent dataflow sweeps give the same bits."""
+    d, a, _ = _pair(name)
+    _, b, _ = _pair(name)
+    assert a.info()["sweep_mode"] == 1, "persistent sweeps should be the default on B200"
+    b.set_sweep_mode(0)
+    for s in (a, b):
+        s.calculate_gradient()
+        s.iterate(4)
+        s.step()
+    for f in ("q", "dq", "diag", "res", "dqdx"):
+        assert_bitwise(a.download(f), b.download(f), f"sweep modes {f}")
+
+
+def test_bounded_wait_reports_timeout_and_context_survives():
+    """Failure detection without a fault: a sweep whose first level is withheld
+    must give up waiting, report MFG_ERR_TIMEOUT, and leave a usable context."""
+    d, s, o = _pair("ramp5")
+    s.calculate_gradient()
+    o.calculate_gradient()
+    s.iterate(2)
+    o.iterate(2)
+    before = s.download("dq")
+    assert s.selftest_sweep_timeout(2_000_000) == -4
+    assert_bitwise(s.download("dq"), before, "state untouched by the self-test")
+    s.iterate(3)
+    o.iterate(3)
+    assert_bitwise(s.download("q"), o.q, "iterations after the self-test")
