@@ -77,9 +77,12 @@ def algorithmic_bytes(C, G, F, N, K):
     }
 
 
-KERNEL_OF_PHASE = {"face_gather": "k_face_gather", "sweep_fwd": "k_sweep_fwd",
-                   "sweep_bwd_update": "k_sweep_bwd", "node_values": "k_node_values",
-                   "grad_faces": "k_grad_faces", "norm": "k_norm_final"}
+def kernel_of_phase(phase: str, sweep_mode: int) -> str:
+    persistent = {"sweep_fwd": "k_sweep_fwd_chunk", "sweep_bwd_update": "k_sweep_bwd_chunk"}
+    per_level = {"sweep_fwd": "k_sweep_fwd", "sweep_bwd_update": "k_sweep_bwd"}
+    other = {"face_gather": "k_face_gather", "node_values": "k_node_values",
+             "grad_faces": "k_grad_faces", "norm": "k_norm_final"}
+    return (persistent if sweep_mode == 1 else per_level).get(phase, other.get(phase, phase))
 
 
 def read_traffic(kernel: str, workload_name: str):
@@ -317,7 +320,9 @@ def main():
     phases = s.profile_phases(phase_iters)
     alg = algorithmic_bytes(C, G, F, N, K)
     peak, peak_kind = measured_peak()
-    nl = {"face_gather": 1, "sweep_fwd": info["fw_levels"], "sweep_bwd_update": info["bw_levels"],
+    per_level = info["sweep_mode"] == 0
+    nl = {"face_gather": 1, "sweep_fwd": info["fw_levels"] if per_level else 1,
+          "sweep_bwd_update": info["bw_levels"] if per_level else 1,
           "node_values": 1, "grad_faces": 1, "norm": 1}
     phase_out = {}
     for ph, tot in phases.items():
@@ -329,9 +334,10 @@ def main():
     dom_ms_launch = phases[dom] / phase_iters / nl[dom]
     dom_bytes_launch = alg[dom] / nl[dom]
     achieved = dom_bytes_launch / (dom_ms_launch / 1e3) / 1e9
-    traffic = read_traffic(KERNEL_OF_PHASE[dom], wl["name"])
+    dom_kernel = kernel_of_phase(dom, info["sweep_mode"])
+    traffic = read_traffic(dom_kernel, wl["name"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": KERNEL_OF_PHASE[dom],
+                "frac": achieved / peak, "traffic": traffic, "kernel": dom_kernel,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "alg_bytes_per_launch": dom_bytes_launch, "ms_per_launch": dom_ms_launch}
     flux_grad_ms = sum(phases[p] for p in ("face_gather", "node_values", "grad_faces")) / \
@@ -381,7 +387,9 @@ def main():
                        "l2": "no flush: working set "
                              f"{info['device_bytes'] / 2**20:.0f} MiB > 126 MB L2",
                        "lusgs_levels": {"forward": info["fw_levels"],
-                                        "backward": info["bw_levels"]}},
+                                        "backward": info["bw_levels"]},
+                       "sweeps": "persistent chunked" if info["sweep_mode"] == 1 else
+                                 "one launch per level"},
             "roofline": roofline,
             "flux_plus_gradient": {"gbs": flux_grad_bytes / (flux_grad_ms / 1e3) / 1e9,
                                    "frac": flux_grad_bytes / (flux_grad_ms / 1e3) / 1e9 / peak},
