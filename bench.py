@@ -12,6 +12,12 @@ plus a 5% Gaussian density bump; FP64.  The working set (~1.2 GB) is far
 larger than the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py --form batched [--ncase 64]
+
+--form batched: 64 cube cases with n^3 x 6 tets, n uniform in [8, 48], Mach
+U(0.3, 0.8), alpha U(-5, 5) deg, jitter U(0, 0.2)h, all in one context (one
+launch per kernel covers every case), against the same cases run one after
+another in their own contexts.
 
 With --gpus N > 1 (one process per GPU under torchrun) every rank runs its
 own replica of the workload (the path has no exchange step) and rank 0
@@ -52,6 +58,10 @@ def parse():
     ap.add_argument("--size", type=int, default=64, help="hexes per cube edge (64 = 1.57M tets)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "batched"],
+                    help="fp64: the single-grid workload; batched: 64 uneven cases in one "
+                         "context against the same cases run one after another")
+    ap.add_argument("--ncase", type=int, default=64)
     return ap.parse_args()
 
 
@@ -253,36 +263,37 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        run_reference_arm(args, rank, world)
-        return
+def batched_workload(ncase=64, seed=2024):
+    """64 cube cases, n uniform in [8, 48] hexes per edge (n^3 x 6 tets), Mach
+    U(0.3, 0.8), alpha U(-5, 5) deg, jitter U(0, 0.2)h, CFL 10."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for k in range(ncase):
+        cases.append(dict(n=int(rng.integers(8, 49)), mach=float(rng.uniform(0.3, 0.8)),
+                          alpha=float(rng.uniform(-5.0, 5.0)),
+                          jitter=float(rng.uniform(0.0, 0.2)), seed=1000 + k, cfl=10.0,
+                          bump_amp=0.05, bump_sigma=0.1))
+    return dict(name=f"batched{ncase}_cube_n8-48_fp64", cases=cases)
+
+
+def build_batched(bw):
+    from minifs_b200 import grid as gr, meshgen
+    grids, params = [], []
+    for c in bw["cases"]:
+        m = meshgen.cube_mesh(c["n"], jitter=c["jitter"], seed=c["seed"])
+        p = gr.make_params(mach=c["mach"], alpha=c["alpha"], cfl_start=c["cfl"])
+        grids.append(gr.prepare(m, p, bump_amp=c["bump_amp"], bump_sigma=c["bump_sigma"]))
+        params.append(p)
+    return grids, params
+
+
+def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
+    """Timed fused iterations of a context, its phase breakdown, roofline and
+    the end-to-end host-buffer run.  counts = (C, G, F, N, K, n)."""
     import torch
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-
     from minifs_b200 import _lib
-    from minifs_b200.solver import Solver
-
-    wl = workload(args.size)
-    mesh, params, pg = build_case(wl)
-    s = Solver(pg, params, device=local)
-    # a dedicated (capturable) stream shared by the library and the events
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    s.set_stream(stream.cuda_stream)
+    C, G, F, N, K, n = counts
     info = s.info()
-    C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
-    K = int(pg.arrays["nnpc"].sum())
 
     def barrier():
         torch.cuda.synchronize()
@@ -290,11 +301,17 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(ms):
+        if dist is None:
+            return ms
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     # warm-up (also builds the CUDA graphs)
     s.calculate_gradient()
     s.iterate(max(args.warmup, 3), norms=False)
     barrier()
-
     launches0 = _lib.kernel_launches()
     with ClockSampler(local) as clk:
         barrier()
@@ -306,14 +323,9 @@ def main():
         ev1.synchronize()
         barrier()
     launches = _lib.kernel_launches() - launches0
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * C * args.steps / (ms / 1e3)
-    clocks = clk.summary()
-    norms = s.residual_norm()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    out = {"ms": ms, "value": world * C * args.steps / (ms / 1e3), "launches": int(launches),
+           "clocks": clk.summary(), "info": info}
 
     # phase breakdown with CUDA events on the same stream (same fused kernels)
     phase_iters = max(3, min(args.steps, 10))
@@ -335,19 +347,21 @@ def main():
     dom_bytes_launch = alg[dom] / nl[dom]
     achieved = dom_bytes_launch / (dom_ms_launch / 1e3) / 1e9
     dom_kernel = kernel_of_phase(dom, info["sweep_mode"])
-    traffic = read_traffic(dom_kernel, wl["name"])
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": dom_kernel,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "alg_bytes_per_launch": dom_bytes_launch, "ms_per_launch": dom_ms_launch}
-    flux_grad_ms = sum(phases[p] for p in ("face_gather", "node_values", "grad_faces")) / \
-        phase_iters
-    flux_grad_bytes = alg["face_gather"] + alg["node_values"] + alg["grad_faces"]
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "traffic": None, "kernel": dom_kernel,
+                       "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                       "alg_bytes_per_launch": dom_bytes_launch,
+                       "ms_per_launch": dom_ms_launch}
+    fg_ms = sum(phases[p] for p in ("face_gather", "node_values", "grad_faces")) / phase_iters
+    fg_bytes = alg["face_gather"] + alg["node_values"] + alg["grad_faces"]
+    out["flux_plus_gradient"] = {"gbs": fg_bytes / (fg_ms / 1e3) / 1e9,
+                                 "frac": fg_bytes / (fg_ms / 1e3) / 1e9 / peak}
+    out["phases"] = phase_out
 
     # end to end through the C ABI with host buffers (pinned), every step:
     # host state in, one iteration, host state and residual out
-    qh = torch.empty(5 * pg.n, dtype=torch.float64, pin_memory=True).numpy()
-    qo = torch.empty(5 * pg.n, dtype=torch.float64, pin_memory=True).numpy()
+    qh = torch.empty(5 * n, dtype=torch.float64, pin_memory=True).numpy()
+    qo = torch.empty(5 * n, dtype=torch.float64, pin_memory=True).numpy()
     rh = torch.empty(5 * C, dtype=torch.float64, pin_memory=True).numpy()
     qh[:] = s.download("q")
     barrier()
@@ -359,30 +373,68 @@ def main():
         qh, qo = qo, qh
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * C * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": 8 * 5 * pg.n, "d2h_bytes_per_step": 8 * 5 * pg.n + 8 * 5 * C,
-           "steps": args.e2e_steps, "api": "mfg_iterate_host (C ABI, pinned host buffers)"}
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    out["e2e"] = {"value": world * C * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+                  "h2d_bytes_per_step": 8 * 5 * n, "d2h_bytes_per_step": 8 * 5 * n + 8 * 5 * C,
+                  "steps": args.e2e_steps,
+                  "api": "mfg_iterate_host (C ABI, pinned host buffers)"}
+    return out
 
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    # a dedicated (capturable) stream shared by the library and the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    if args.form == "batched":
+        run_batched(args, rank, world, local, stream, dist)
+    else:
+        run_single(args, rank, world, local, stream, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_single(args, rank, world, local, stream, dist):
+    from minifs_b200.solver import Solver
+    wl = workload(args.size)
+    mesh, params, pg = build_case(wl)
+    s = Solver(pg, params, device=local)
+    s.set_stream(stream.cuda_stream)
+    C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
+    K = int(pg.arrays["nnpc"].sum())
+    r = measure(s, (C, G, F, N, K, pg.n), args, stream, dist, world, local)
+    r["roofline"]["traffic"] = read_traffic(r["roofline"]["kernel"], wl["name"])
+    norms = s.residual_norm()
+    info = r["info"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_baseline(mesh, pg, params, wl)
         except Exception as e:  # reported, never silently replaced
             cpu = {"error": str(e)[:200]}
-
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": wl["name"], "cells": C, "faces": F, "nodes": N,
-                       "ghosts": G, "precision": "fp64 (bit-faithful)",
+            "config": {"workload": wl["name"], "form": "fp64", "cells": C, "faces": F,
+                       "nodes": N, "ghosts": G, "precision": "fp64 (bit-faithful)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single",
                        "l2": "no flush: working set "
                              f"{info['device_bytes'] / 2**20:.0f} MiB > 126 MB L2",
@@ -390,21 +442,86 @@ def main():
                                         "backward": info["bw_levels"]},
                        "sweeps": "persistent chunked" if info["sweep_mode"] == 1 else
                                  "one launch per level"},
-            "roofline": roofline,
-            "flux_plus_gradient": {"gbs": flux_grad_bytes / (flux_grad_ms / 1e3) / 1e9,
-                                   "frac": flux_grad_bytes / (flux_grad_ms / 1e3) / 1e9 / peak},
-            "phases": phase_out,
+            "roofline": r["roofline"],
+            "flux_plus_gradient": r["flux_plus_gradient"],
+            "phases": r["phases"],
             "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": int(launches),
-            "clocks": clocks,
+            "e2e": r["e2e"],
+            "gpu_launches": r["launches"],
+            "clocks": r["clocks"],
             "residual_norm": [float(x) for x in norms],
         }
         print(json.dumps(line), flush=True)
     s.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+
+
+def run_batched(args, rank, world, local, stream, dist):
+    """64 uneven cases in one context against the same cases run one after
+    another, each in its own context (sequential per-case launches)."""
+    import torch
+    from minifs_b200.solver import BatchSolver, Solver
+    bw = batched_workload(args.ncase)
+    grids, params = build_batched(bw)
+    counts = [0] * 6
+    for pg in grids:
+        for i, v in enumerate((pg.n_cell, pg.n_bface, pg.n_face, pg.n_node,
+                               int(pg.arrays["nnpc"].sum()), pg.n)):
+            counts[i] += v
+    # sequential per-case launches: each case alone, timed on the device
+    seq_ms, seq_cells = 0.0, 0
+    for pg, p in zip(grids, params):
+        s = Solver(pg, p, device=local)
+        s.set_stream(stream.cuda_stream)
+        s.calculate_gradient()
+        s.iterate(max(args.warmup, 3), norms=False)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.iterate(args.steps, norms=False)
+        e1.record(stream)
+        e1.synchronize()
+        seq_ms += e0.elapsed_time(e1)
+        seq_cells += pg.n_cell
+        s.close()
+    b = BatchSolver(grids, params, device=local)
+    b.set_stream(stream.cuda_stream)
+    r = measure(b, tuple(counts), args, stream, dist, world, local)
+    norms = b.residual_norm()
+    info = r["info"]
+    seq_value = world * seq_cells * args.steps / (seq_ms / 1e3)
+    if rank == 0:
+        ns = [c["n"] for c in bw["cases"]]
+        line = {
+            "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": bw["name"], "form": "batched", "ncase": len(ns),
+                       "n_min": min(ns), "n_max": max(ns), "cells": counts[0],
+                       "faces": counts[2], "precision": "fp64 (bit-faithful per case)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "l2": "no flush: working set "
+                             f"{info['device_bytes'] / 2**20:.0f} MiB > 126 MB L2",
+                       "lusgs_levels": {"forward": info["fw_levels"],
+                                        "backward": info["bw_levels"]},
+                       "sweeps": "persistent chunked" if info["sweep_mode"] == 1 else
+                                 "one launch per level"},
+            "sequential": {"value": seq_value, "unit": UNIT, "ms_per_step": seq_ms / args.steps,
+                           "how": "each case in its own context, graph-captured fused "
+                                  "iterations, cases one after another; device time summed"},
+            "batched_over_sequential": r["value"] / seq_value,
+            "roofline": r["roofline"],
+            "flux_plus_gradient": r["flux_plus_gradient"],
+            "phases": r["phases"],
+            "cpu_baseline": None,
+            "e2e": r["e2e"],
+            "gpu_launches": r["launches"],
+            "clocks": r["clocks"],
+            "residual_norm_max": [float(x) for x in norms.max(axis=0)],
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
 
 
 if __name__ == "__main__":

@@ -107,6 +107,7 @@ typedef struct mfg_info {
   int64_t device_bytes;             /* device memory held by the context */
   int32_t sweep_mode;               /* 0 = one launch per level, 1 = persistent */
   int32_t graph_ready;
+  int32_t ncase;                    /* independent cases in the context (1 unless batched) */
 } mfg_info;
 
 /* ---- parameters -------------------------------------------------------- */
@@ -124,6 +125,27 @@ int mfg_params_derive(mfg_params *p);
  * gradient itself is computed by the first mfg_calculate_gradient. */
 int mfg_create(const mfg_mesh *mesh, const mfg_params *params, const double *q0,
                int32_t device, int32_t precision, mfg_ctx **out);
+/* Batched cases: ncase independent grids (each a complete mfg_mesh with its
+ * own mfg_params and initial state q0s[k] [5 n_k]) solved together in one
+ * context, so that every launch and every level of the LU-SGS sweeps covers
+ * all cases at once -- the reference's whole main loop run once per case
+ * (main.cpp:170-291), as many cases as fit the device.  The context holds the
+ * union grid: the cells of case 0, 1, ..., then the ghosts of case 0, 1, ...
+ * (mfg_batch_layout gives the offsets); downloads and uploads use that order.
+ * Each case computes exactly what it would alone: same bits, its own CFL
+ * ramp, its own dt_max/dt_min, its own first cell of the LU-SGS order.
+ * Meshes must use the identity LU-SGS order (lusgs_order = lusgs_layer =
+ * NULL); mfg_set_params is not available on a batch. */
+int mfg_create_batch(int32_t ncase, const mfg_mesh *meshes, const mfg_params *params,
+                     const double *const *q0s, int32_t device, int32_t precision,
+                     mfg_ctx **out);
+/* cell0[k] = first cell of case k in the union, bface0[k] = its first
+ * boundary face (its ghosts start at n_cell + bface0[k]); both [ncase + 1]. */
+int mfg_batch_layout(mfg_ctx *ctx, int32_t *cell0, int32_t *bface0);
+/* dt_max, dt_min of every case: ext[2k], ext[2k + 1]. */
+int mfg_batch_dt_extrema(mfg_ctx *ctx, double *ext);
+/* Residual L2 norms per case: out[5k + v]. */
+int mfg_batch_residual_norm(mfg_ctx *ctx, double *out);
 int mfg_destroy(mfg_ctx *ctx);
 /* Issue all further work on this cudaStream_t (NULL = the context's own). */
 int mfg_set_stream(mfg_ctx *ctx, void *cuda_stream);
@@ -160,7 +182,8 @@ int mfg_forward_lusgs(mfg_ctx *ctx);
 int mfg_calculate_gradient(mfg_ctx *ctx);
 /* The whole main-loop body (main.cpp:201-291) n times, fused kernels in a
  * CUDA graph.  norms (optional, host) receives 5 residual L2 norms per
- * iteration (main.cpp:294-317 evaluated every iteration). */
+ * iteration (main.cpp:294-317 evaluated every iteration); for a batch
+ * norms[(i * ncase + k) * 5 + v]. */
 int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms);
 /* End-to-end form with host buffers: copies q_in [5n] (host) in, runs
  * n_iter iterations, copies the state to q_out [5n] and the residual to
@@ -200,7 +223,8 @@ int mfg_residual_norm(mfg_ctx *ctx, double out[5]);
 #define MFG_NORM_STATIC_MAX_CELLS (1 << 24)
 int mfg_residual_norm_static(const double *res, int32_t n_cell, double *norms, void *stream);
 /* The running extrema dt_max / dt_min (para_field_global.cpp:220-221,
- * updated in LimitTimeStep, compute_timestep.cpp:914-918). */
+ * updated in LimitTimeStep, compute_timestep.cpp:914-918).  For a batch, get
+ * returns case 0's and set sets every case's. */
 int mfg_get_dt_extrema(mfg_ctx *ctx, double *dt_max, double *dt_min);
 int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min);
 

@@ -62,7 +62,7 @@ class Info(ct.Structure):
                 ("n_bface", ct.c_int32), ("fw_levels", ct.c_int32), ("bw_levels", ct.c_int32),
                 ("max_level_cells", ct.c_int32), ("precision", ct.c_int32),
                 ("device_bytes", ct.c_int64), ("sweep_mode", ct.c_int32),
-                ("graph_ready", ct.c_int32)]
+                ("graph_ready", ct.c_int32), ("ncase", ct.c_int32)]
 
 
 class RawGrid(ct.Structure):
@@ -100,6 +100,12 @@ def load(build_if_missing: bool = True):
         "mfg_params_derive": (ct.c_int, [ct.POINTER(Params)]),
         "mfg_create": (ct.c_int, [ct.POINTER(Mesh), ct.POINTER(Params), f64p, ct.c_int32,
                                   ct.c_int32, ct.POINTER(ctxp)]),
+        "mfg_create_batch": (ct.c_int, [ct.c_int32, ct.POINTER(Mesh), ct.POINTER(Params),
+                                        ct.POINTER(f64p), ct.c_int32, ct.c_int32,
+                                        ct.POINTER(ctxp)]),
+        "mfg_batch_layout": (ct.c_int, [ctxp, i32p, i32p]),
+        "mfg_batch_dt_extrema": (ct.c_int, [ctxp, f64p]),
+        "mfg_batch_residual_norm": (ct.c_int, [ctxp, f64p]),
         "mfg_destroy": (ct.c_int, [ctxp]),
         "mfg_set_stream": (ct.c_int, [ctxp, ct.c_void_p]),
         "mfg_set_params": (ct.c_int, [ctxp, ct.POINTER(Params)]),

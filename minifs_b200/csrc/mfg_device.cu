@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +36,7 @@ std::atomic<long long> g_launches{0};
 
 constexpr int kBlock = 256;
 constexpr int kNormBlocks = 1184;  // 8 x 148 SMs, fixed so the norm reduction order is fixed
+constexpr int kSegBlocks = 32;     // blocks per case of the batched norm reduction
 
 #define MFG_CUDA(call)                                                            \
   do {                                                                            \
@@ -56,12 +58,12 @@ inline int grid_for(int64_t n, int block = kBlock) {
 // Scatter SoA q (5 blocks of n) into both state buffers and derive per-cell
 // quantities.
 __global__ void k_upload_q(const double *__restrict__ soa, double *__restrict__ qa,
-                           double *__restrict__ qb, int64_t n, Params P) {
+                           double *__restrict__ qb, int64_t n, Params P0, Cases cs) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double q[Q_STRIDE];
   for (int k = 0; k < 5; k++) q[k] = soa[k * n + i];
-  cell_props(q, P);
+  cell_props(q, params_of(P0, cs, i));
   store_q(qa, i, q);
   if (qb) store_q(qb, i, q);
 }
@@ -88,10 +90,12 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
               const double *__restrict__ q8, const double *__restrict__ vol,
               double *__restrict__ res, int res_zero, double *__restrict__ dt,
               double *__restrict__ diag, const double *__restrict__ cfl_tab,
-              const int32_t *__restrict__ iter_counter, double cfl_arg, Params P,
-              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part) {
+              const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
+              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < C;
+  const int32_t cse = live ? case_of(cs, c) : 0;
+  const Params P = live ? params_of(P0, cs, c) : P0;
   double qc[Q_STRIDE];
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   double dtc = 0.0;
@@ -129,7 +133,8 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
       }
     }
     if (DT) {
-      const double cfl = cfl_tab ? cfl_tab[*iter_counter] : cfl_arg;
+      const double cfl =
+          cfl_tab ? cfl_tab[(int64_t)(*iter_counter) * max(cs.ncase, 1) + cse] : cfl_arg;
       const double cfl_min = 0.5 * cfl;
       dtc = dtl * local_cfl(qc[4], det, cfl, cfl_min, P);
       dt[c] = dtc;
@@ -154,13 +159,21 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
     // patterns order like the values
     unsigned long long mx = live ? dbits(dtc) : 0ull;
     unsigned long long mn = live ? dbits(dtc) : ~0ull;
-    for (int o = 16; o > 0; o >>= 1) {
-      mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-      atomicMax(dt_ext + 0, mx);
-      atomicMin(dt_ext + 1, mn);
+    // one atomic pair per warp when the warp's cells share a case (the
+    // extrema are per case), else one per cell
+    const int32_t c0 = __shfl_sync(0xffffffffu, cse, 0);
+    if (__all_sync(0xffffffffu, !live || cse == c0)) {
+      for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        atomicMax(dt_ext + 2 * c0, mx);
+        atomicMin(dt_ext + 2 * c0 + 1, mn);
+      }
+    } else if (live) {
+      atomicMax(dt_ext + 2 * cse, mx);
+      atomicMin(dt_ext + 2 * cse + 1, mn);
     }
   }
   if (FLUX && norm_part) {
@@ -181,14 +194,17 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
   }
 }
 
-// LimitTimeStep's ratio clamp (compute_timestep.cpp:929-944).
+// LimitTimeStep's ratio clamp (compute_timestep.cpp:929-944), per case.
 __global__ void k_dt_clamp(int32_t C, double *__restrict__ dt,
-                           const unsigned long long *__restrict__ dt_ext, double ratio_dtmax) {
+                           const unsigned long long *__restrict__ dt_ext, Params P0, Cases cs) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  const double dt_max = __longlong_as_double((long long)dt_ext[0]);
-  const double dt_min = __longlong_as_double((long long)dt_ext[1]);
+  if (c >= C) return;
+  const int32_t cse = case_of(cs, c);
+  const double ratio_dtmax = params_of(P0, cs, c).ratio_dtmax;
+  const double dt_max = __longlong_as_double((long long)dt_ext[2 * cse]);
+  const double dt_min = __longlong_as_double((long long)dt_ext[2 * cse + 1]);
   const double ratio_max = dt_max / dt_min;
-  if (!(ratio_max > ratio_dtmax) || c >= C) return;
+  if (!(ratio_max > ratio_dtmax)) return;
   const double lim = ratio_dtmax * dt_min;
   if (dt[c] > lim) dt[c] = lim;
 }
@@ -230,13 +246,16 @@ k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
             const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
             const int32_t *__restrict__ nbs, const double *__restrict__ q8,
             double *__restrict__ dqf, double *__restrict__ dqb, const double *__restrict__ res,
-            int32_t C, double *__restrict__ diag, int32_t first_cell, Params P, int clamp_check,
+            int32_t C, double *__restrict__ diag, int32_t first_cell, Params P0, int clamp_check,
             double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
             const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
-            const double *__restrict__ vol) {
+            const double *__restrict__ vol, Cases cs) {
   const int32_t i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= l1) return;
   const int32_t c = cells[i];
+  const int32_t cse = case_of(cs, c);
+  const Params P = params_of(P0, cs, c);
+  const int32_t first = cs.P ? cs.first[cse] : first_cell;
   double d[5];
   for (int k = 0; k < 5; k++) d[k] = res[(int64_t)k * C + c];
   const int32_t s1 = sptr[i + 1];
@@ -252,9 +271,9 @@ k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
   double dg = diag[c];
   double qc[Q_STRIDE];
   load_q(q8, c, qc);
-  if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext, cptr, slots, vol, diag);
+  if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext + 2 * cse, cptr, slots, vol, diag);
   for (int k = 0; k < 5; k++) d[k] /= dg;
-  if (c != first_cell) dq_limit(qc, d, P);
+  if (c != first) dq_limit(qc, d, P);
   store_dq(dqf, c, d);
   store_sentinel(dqb, c);
 }
@@ -267,10 +286,11 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
             const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
             const int32_t *__restrict__ nbs, const double *__restrict__ q8,
             double *__restrict__ q8_new, double *__restrict__ dqf, double *__restrict__ dqb,
-            const double *__restrict__ diag, Params P) {
+            const double *__restrict__ diag, Params P0, Cases cs) {
   const int32_t i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= l1) return;
   const int32_t c = cells[i];
+  const Params P = params_of(P0, cs, c);
   double d[5], fs[5] = {0., 0., 0., 0., 0.};
   load_dq_cg(dqf, c, d);
   const int32_t s1 = sptr[i + 1];
@@ -395,11 +415,11 @@ k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
                   const ChunkCell *__restrict__ ccells, const SweepRec *__restrict__ recs,
                   const int32_t *__restrict__ nbs, const double *__restrict__ q8, double *dqf,
                   double *__restrict__ dqb, const double *__restrict__ res, int32_t C,
-                  double *__restrict__ diag, int32_t first_cell, Params P, int clamp_check,
+                  double *__restrict__ diag, int32_t first_cell, Params P0, int clamp_check,
                   double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
                   const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
                   const double *__restrict__ vol, int *err, long long spin,
-                  int32_t chunk_skip) {
+                  int32_t chunk_skip, Cases cs) {
   if ((int32_t)blockIdx.x < chunk_skip) return;
   const int32_t sg1 = seg_begin[blockIdx.x + 1];
   for (int32_t sg = seg_begin[blockIdx.x]; sg < sg1; sg++) {
@@ -407,15 +427,17 @@ k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
     for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
       const ChunkCell cc = ccells[i];
       const int32_t c = cc.cell;
+      const int32_t cse = case_of(cs, c);
+      const Params P = params_of(P0, cs, c);
       double d[5];
       for (int k = 0; k < 5; k++) d[k] = res[(int64_t)k * C + c];
       double dg = diag[c];
       double qc[Q_STRIDE];
       load_q(q8, c, qc);
       sweep_gather<true>(cc.s0, cc.ns, recs, nbs, q8, dqf, err, spin, P, d);
-      if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext, cptr, slots, vol, diag);
+      if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext + 2 * cse, cptr, slots, vol, diag);
       for (int k = 0; k < 5; k++) d[k] /= dg;
-      if (c != first_cell) dq_limit(qc, d, P);
+      if (c != (cs.P ? cs.first[cse] : first_cell)) dq_limit(qc, d, P);
       store_dq(dqf, c, d);
       store_sentinel(dqb, c);  // armed for the backward sweep
     }
@@ -430,13 +452,15 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
                   const ChunkCell *__restrict__ ccells, const SweepRec *__restrict__ recs,
                   const int32_t *__restrict__ nbs, const double *__restrict__ q8,
                   double *__restrict__ q8_new, double *__restrict__ dqf, double *dqb,
-                  const double *__restrict__ diag, Params P, int *err, long long spin) {
+                  const double *__restrict__ diag, Params P0, int *err, long long spin,
+                  Cases cs) {
   const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
   for (int32_t sg = sg0; sg < sg1; sg++) {
     const int32_t a = segs[sg], b = segs[sg + 1];
     for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
       const ChunkCell cc = ccells[i];
       const int32_t c = cc.cell;
+      const Params P = params_of(P0, cs, c);
       double d[5], fs[5] = {0., 0., 0., 0., 0.};
       load_dq_cg(dqf, c, d);  // this cell's forward value (previous kernel)
       double qc[Q_STRIDE];
@@ -460,6 +484,7 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
       const double2 x = pp[0], y = pp[1], z = pp[2];
       d[0] = x.x; d[1] = x.y; d[2] = y.x; d[3] = y.y; d[4] = z.x;
       load_q(q8, c, qc);
+      const Params P = params_of(P0, cs, c);
       update_cell(qc, d, P);
       cell_props(qc, P);
       store_q(q8_new, c, qc);
@@ -624,6 +649,46 @@ __global__ void k_norm_final(int32_t nparts, const double *__restrict__ part,
   if (threadIdx.x == 0 && iter_counter) *iter_counter += 1;
 }
 
+// Batched cases: residual norms per case.  Block (x, k) reduces cells
+// [cell0[k], cell0[k+1]) with stride gridDim.x * blockDim.x; fixed order.
+__global__ void k_norm_seg_partial(int32_t C, const double *__restrict__ res,
+                                   const int32_t *__restrict__ cell0, double *__restrict__ part) {
+  __shared__ double sh[kBlock / 32][5];
+  const int32_t k = blockIdx.y;
+  double s2[5] = {0., 0., 0., 0., 0.};
+  for (int32_t c = cell0[k] + blockIdx.x * blockDim.x + threadIdx.x; c < cell0[k + 1];
+       c += gridDim.x * blockDim.x)
+    for (int v = 0; v < 5; v++) {
+      const double r = res[(int64_t)v * C + c];
+      s2[v] += r * r;
+    }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int v = 0; v < 5; v++) s2[v] += __shfl_down_sync(0xffffffffu, s2[v], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int v = 0; v < 5; v++) sh[threadIdx.x >> 5][v] = s2[v];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double acc = 0.0;
+    for (int w = 0; w < kBlock / 32; w++) acc += sh[w][threadIdx.x];
+    part[((int64_t)k * gridDim.x + blockIdx.x) * 5 + threadIdx.x] = acc;
+  }
+}
+
+__global__ void k_norm_seg_final(int32_t nparts, const double *__restrict__ part,
+                                 double *__restrict__ out, const int32_t *__restrict__ iter_counter,
+                                 double *__restrict__ hist) {
+  const int32_t k = blockIdx.x;
+  if (threadIdx.x < 5) {
+    double acc = 0.0;
+    for (int32_t b = 0; b < nparts; b++) acc += part[((int64_t)k * nparts + b) * 5 + threadIdx.x];
+    const double v = sqrt(acc);
+    out[k * 5 + threadIdx.x] = v;
+    if (hist) hist[((int64_t)(*iter_counter) * gridDim.x + k) * 5 + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_counter_inc(int32_t *__restrict__ counter) { *counter += 1; }
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -675,6 +740,14 @@ struct mfg_ctx {
   double *norm_part = nullptr, *norm_out = nullptr, *norm_hist = nullptr, *cfl_tab = nullptr;
   int32_t *iter_counter = nullptr;
   int32_t hist_cap = 0, cfl_cap = 0;
+  // batched cases (ncase == 1: a single grid, kernels use P)
+  int32_t ncase = 1;
+  std::vector<mfg_params> hps;          // per-case host parameters
+  std::vector<int32_t> case_cell0;      // first cell of each case [ncase+1]
+  std::vector<int32_t> case_bface0;     // first boundary face (= ghost - C) [ncase+1]
+  Params *ptab = nullptr;               // per-case device parameters
+  int32_t *case_of_d = nullptr, *case_first_d = nullptr, *case_cell0_d = nullptr;
+  double *seg_part = nullptr;
   double *h_pinned = nullptr;  // small pinned scratch for scalars
   std::vector<void *> allocs;
   int64_t device_bytes = 0;
@@ -725,6 +798,11 @@ Params make_params(const mfg_params &p) {
 }
 
 inline void count_launch(int64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+Cases cases_of(const mfg_ctx *ctx) {
+  if (ctx->ncase <= 1) return Cases{nullptr, nullptr, nullptr, 1};
+  return Cases{ctx->ptab, ctx->case_of_d, ctx->case_first_d, ctx->ncase};
+}
 
 int check_kernel() {
   cudaError_t e = cudaGetLastError();
@@ -1088,8 +1166,16 @@ static int build_node_lists(mfg_ctx *ctx, const mfg_mesh *m) {
   return MFG_OK;
 }
 
-int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, int32_t device,
-               int32_t precision, mfg_ctx **out) {
+// Case layout of a context: offsets of each case's cells and boundary faces
+// in the concatenated grid, the case of every cell and ghost, and the first
+// cell of each case's LU-SGS order.
+struct CaseLayout {
+  int32_t ncase = 1;
+  std::vector<int32_t> cell0, bface0, of, first;
+};
+
+static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLayout &cl,
+                       const double *q0, int32_t device, int32_t precision, mfg_ctx **out) {
   if (!out || !params || !q0) return MFG_ERR_INVALID;
   *out = nullptr;
   int rc = validate_mesh(m);
@@ -1121,8 +1207,24 @@ int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, in
   ctx->n = (int64_t)m->n_cell + m->n_bface;
   ctx->hp = *params;
   ctx->P = make_params(*params);
+  ctx->ncase = cl.ncase;
+  ctx->hps.assign(params, params + cl.ncase);
   const int32_t C = ctx->C;
   const int64_t n = ctx->n;
+  if (cl.ncase > 1) {
+    ctx->case_cell0 = cl.cell0;
+    ctx->case_bface0 = cl.bface0;
+    std::vector<Params> pt(cl.ncase);
+    for (int32_t k = 0; k < cl.ncase; k++) pt[k] = make_params(params[k]);
+    if ((rc = dupload(ctx, &ctx->ptab, pt))) return fail(rc);
+    if ((rc = dupload(ctx, &ctx->case_of_d, cl.of))) return fail(rc);
+    if ((rc = dupload(ctx, &ctx->case_first_d, cl.first))) return fail(rc);
+    if ((rc = dupload(ctx, &ctx->case_cell0_d, cl.cell0))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->seg_part, (size_t)5 * kSegBlocks * cl.ncase))) return fail(rc);
+  } else {
+    ctx->case_cell0 = {0, C};
+    ctx->case_bface0 = {0, ctx->G};
+  }
 
   std::vector<int32_t> cptr, c2f;
   build_c2f(m, cptr, c2f);
@@ -1188,14 +1290,15 @@ int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, in
   if ((rc = dalloc(ctx, &ctx->dqdz, (size_t)5 * n))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->qn8, (size_t)ctx->N * Q_STRIDE))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->staging, (size_t)5 * n))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dt_ext, 2))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->dt_ext, (size_t)2 * cl.ncase))) return fail(rc);
   const int nparts = std::max(grid_for(C), kNormBlocks);
   if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->norm_out, 5))) return fail(rc);
+  if ((rc = dalloc(ctx, &ctx->norm_out, (size_t)5 * cl.ncase))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->dqf, (size_t)n * Q_STRIDE))) return fail(rc);
   if ((rc = dalloc(ctx, &ctx->sweep_err, 1))) return fail(rc);
-  if (cudaMallocHost((void **)&ctx->h_pinned, 64 * sizeof(double)) != cudaSuccess)
+  if (cudaMallocHost((void **)&ctx->h_pinned, (64 + 5 * (size_t)cl.ncase) * sizeof(double)) !=
+      cudaSuccess)
     return fail(MFG_ERR_NOMEM);
 
   cudaStream_t st = ctx->stream;
@@ -1221,6 +1324,143 @@ int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, in
   return MFG_OK;
 }
 
+int mfg_create(const mfg_mesh *m, const mfg_params *params, const double *q0, int32_t device,
+               int32_t precision, mfg_ctx **out) {
+  CaseLayout cl;
+  return create_impl(m, params, cl, q0, device, precision, out);
+}
+
+// Concatenation of independent grids into one: cells of case 0, 1, ...; then
+// the boundary faces of all cases (so that faces [0, G) stay the boundary
+// faces and the ghost of union boundary face K is C + K), then the interior
+// faces of all cases; nodes likewise.  No face joins two cases, so every
+// gather, level set and sweep of the union computes each case exactly as it
+// would alone.
+int mfg_create_batch(int32_t ncase, const mfg_mesh *ms, const mfg_params *params,
+                     const double *const *q0s, int32_t device, int32_t precision,
+                     mfg_ctx **out) {
+  if (!out || ncase <= 0 || !ms || !params || !q0s) return MFG_ERR_INVALID;
+  if (ncase == 1) return mfg_create(&ms[0], &params[0], q0s[0], device, precision, out);
+  CaseLayout cl;
+  cl.ncase = ncase;
+  cl.cell0.assign(ncase + 1, 0);
+  cl.bface0.assign(ncase + 1, 0);
+  std::vector<int64_t> node0(ncase + 1, 0), iface0(ncase + 1, 0), fnode0(ncase + 1, 0),
+      bnode0(ncase + 1, 0), c2n0(ncase + 1, 0);
+  for (int32_t k = 0; k < ncase; k++) {
+    const mfg_mesh &m = ms[k];
+    int rc = validate_mesh(&m);
+    if (rc) return rc;
+    if (m.lusgs_order || m.lusgs_layer) return MFG_ERR_UNSUPPORTED;
+    cl.cell0[k + 1] = cl.cell0[k] + m.n_cell;
+    cl.bface0[k + 1] = cl.bface0[k] + m.n_bface;
+    node0[k + 1] = node0[k] + m.n_node;
+    iface0[k + 1] = iface0[k] + (m.n_face - m.n_bface);
+    int64_t sb = 0, sf = 0, sc = 0;
+    for (int32_t f = 0; f < m.n_face; f++) (f < m.n_bface ? sb : sf) += m.nnpf[f];
+    for (int32_t c = 0; c < m.n_cell; c++) sc += m.nnpc[c];
+    bnode0[k + 1] = bnode0[k] + sb;
+    fnode0[k + 1] = fnode0[k] + sf;
+    c2n0[k + 1] = c2n0[k] + sc;
+  }
+  const int64_t C = cl.cell0[ncase], G = cl.bface0[ncase], N = node0[ncase];
+  const int64_t F = G + iface0[ncase], n = C + G;
+  if (n > INT32_MAX || F > INT32_MAX || bnode0[ncase] + fnode0[ncase] > INT32_MAX ||
+      c2n0[ncase] > INT32_MAX)
+    return MFG_ERR_INVALID;
+  std::vector<int32_t> f2c(2 * F), nnpf(F), f2n(bnode0[ncase] + fnode0[ncase]), bct(G);
+  std::vector<double> fa[7], ca[4], na[5];
+  for (auto &v : fa) v.resize(F);
+  for (auto &v : ca) v.resize(n);
+  for (auto &v : na) v.resize(N);
+  std::vector<int32_t> nmark(N), nsym(N), nnpc(C), c2n(c2n0[ncase]);
+  std::vector<double> wbface(bnode0[ncase]), wc2n(c2n0[ncase]);
+  std::vector<double> q0((size_t)5 * n);
+  cl.of.resize(n);
+  cl.first.resize(ncase);
+  for (int32_t k = 0; k < ncase; k++) {
+    const mfg_mesh &m = ms[k];
+    const int64_t cb = cl.cell0[k], gb = cl.bface0[k], nb = node0[k];
+    const int64_t mc = m.n_cell, mg = m.n_bface, mn = (int64_t)m.n_cell + m.n_bface;
+    auto cell_map = [&](int64_t c) -> int64_t { return c < mc ? cb + c : C + gb + (c - mc); };
+    auto face_map = [&](int64_t f) -> int64_t {
+      return f < mg ? gb + f : G + iface0[k] + (f - mg);
+    };
+    const double *fsrc[7] = {m.xfn, m.yfn, m.zfn, m.area, m.xfc, m.yfc, m.zfc};
+    int64_t pb = bnode0[k], pi = bnode0[ncase] + fnode0[k], off = 0;
+    for (int32_t f = 0; f < m.n_face; f++) {
+      const int64_t g = face_map(f);
+      f2c[2 * g] = (int32_t)cell_map(m.f2c[2 * f]);
+      f2c[2 * g + 1] = (int32_t)cell_map(m.f2c[2 * f + 1]);
+      nnpf[g] = m.nnpf[f];
+      for (int j = 0; j < 7; j++) fa[j][g] = fsrc[j][f];
+      for (int32_t j = 0; j < m.nnpf[f]; j++) {
+        const int64_t dst = (f < m.n_bface ? pb : pi) + j;
+        f2n[dst] = (int32_t)(nb + m.f2n[off + j]);
+        if (f < m.n_bface) wbface[dst] = m.wbface[off + j];
+      }
+      (f < m.n_bface ? pb : pi) += m.nnpf[f];
+      off += m.nnpf[f];
+      if (f < m.n_bface) bct[gb + f] = m.bctype[f];
+    }
+    const double *csrc[4] = {m.xcc, m.ycc, m.zcc, m.vol};
+    for (int64_t c = 0; c < mn; c++) {
+      const int64_t g = cell_map(c);
+      for (int j = 0; j < 4; j++) ca[j][g] = csrc[j][c];
+      cl.of[g] = k;
+      for (int v = 0; v < 5; v++) q0[(size_t)v * n + g] = q0s[k][(size_t)v * mn + c];
+    }
+    const double *nsrc[5] = {m.wnode, m.xfn_n_symm, m.yfn_n_symm, m.zfn_n_symm, nullptr};
+    for (int64_t p = 0; p < m.n_node; p++) {
+      for (int j = 0; j < 4; j++) na[j][nb + p] = nsrc[j][p];
+      nmark[nb + p] = m.nmark[p];
+      nsym[nb + p] = m.nodesymm[p];
+    }
+    for (int64_t c = 0, o = 0; c < mc; c++) {
+      nnpc[cb + c] = m.nnpc[c];
+      for (int32_t j = 0; j < m.nnpc[c]; j++, o++) {
+        c2n[c2n0[k] + o] = (int32_t)(nb + m.c2n[o]);
+        wc2n[c2n0[k] + o] = m.wc2n[o];
+      }
+    }
+    cl.first[k] = (int32_t)cb;  // identity LU-SGS order
+  }
+  // boundary-face node lists must precede interior ones in f2n order: the
+  // union keeps face order, and faces [0, G) are the boundary faces of all
+  // cases in case order, whose node lists were written at [0, sum bnode)
+  mfg_mesh u = {};
+  u.n_node = (int32_t)N;
+  u.n_face = (int32_t)F;
+  u.n_cell = (int32_t)C;
+  u.n_bface = (int32_t)G;
+  u.f2c = f2c.data();
+  u.nnpf = nnpf.data();
+  u.f2n = f2n.data();
+  u.bctype = bct.data();
+  u.xfn = fa[0].data();
+  u.yfn = fa[1].data();
+  u.zfn = fa[2].data();
+  u.area = fa[3].data();
+  u.xfc = fa[4].data();
+  u.yfc = fa[5].data();
+  u.zfc = fa[6].data();
+  u.xcc = ca[0].data();
+  u.ycc = ca[1].data();
+  u.zcc = ca[2].data();
+  u.vol = ca[3].data();
+  u.wnode = na[0].data();
+  u.nmark = nmark.data();
+  u.wbface = wbface.data();
+  u.nnpc = nnpc.data();
+  u.c2n = c2n.data();
+  u.wc2n = wc2n.data();
+  u.nodesymm = nsym.data();
+  u.xfn_n_symm = na[1].data();
+  u.yfn_n_symm = na[2].data();
+  u.zfn_n_symm = na[3].data();
+  return create_impl(&u, params, cl, q0.data(), device, precision, out);
+}
+
 int mfg_set_stream(mfg_ctx *ctx, void *s) {
   if (!ctx) return MFG_ERR_INVALID;
   ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
@@ -1229,7 +1469,9 @@ int mfg_set_stream(mfg_ctx *ctx, void *s) {
 
 int mfg_set_params(mfg_ctx *ctx, const mfg_params *p) {
   if (!ctx || !p) return MFG_ERR_INVALID;
+  if (ctx->ncase > 1) return MFG_ERR_UNSUPPORTED;  // a batch fixes its cases at creation
   ctx->hp = *p;
+  ctx->hps[0] = *p;
   ctx->P = make_params(*p);
   for (int k = 0; k < 2; k++)
     if (ctx->graph[k]) {
@@ -1264,6 +1506,26 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
   info->device_bytes = ctx->device_bytes;
   info->sweep_mode = ctx->sweep_mode;
   info->graph_ready = ctx->graph[0] != nullptr;
+  info->ncase = ctx->ncase;
+  return MFG_OK;
+}
+
+int mfg_batch_layout(mfg_ctx *ctx, int32_t *cell0, int32_t *bface0) {
+  if (!ctx || !cell0 || !bface0) return MFG_ERR_INVALID;
+  for (int32_t k = 0; k <= ctx->ncase; k++) {
+    cell0[k] = ctx->case_cell0[k];
+    bface0[k] = ctx->case_bface0[k];
+  }
+  return MFG_OK;
+}
+
+int mfg_batch_dt_extrema(mfg_ctx *ctx, double *ext) {
+  if (!ctx || !ext) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  MFG_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->dt_ext, 2 * sizeof(double) * ctx->ncase,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(ext, ctx->h_pinned, 2 * sizeof(double) * ctx->ncase);
   return MFG_OK;
 }
 
@@ -1279,12 +1541,13 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
   const int g = grid_for(ctx->C);
   const double *q = ctx->q8[ctx->cur];
   const double *tab = use_table ? ctx->cfl_tab : nullptr;
-  double *np = flux ? ctx->norm_part : nullptr;
+  double *np = (flux && ctx->ncase == 1) ? ctx->norm_part : nullptr;
+  const Cases cs = cases_of(ctx);
 #define MFG_FACE(F, D, G)                                                                    \
   k_face_gather<F, D, G><<<g, kBlock, 0, st>>>(ctx->C, ctx->cptr, ctx->slots, q, ctx->vol,   \
                                                 ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,    \
                                                 ctx->diag, tab, ctx->iter_counter, cfl,      \
-                                                ctx->P, ctx->dt_ext, np)
+                                                ctx->P, ctx->dt_ext, np, cs)
   if (flux && dtp && diag) MFG_FACE(true, true, true);
   else if (flux && !dtp && !diag) MFG_FACE(true, false, false);
   else if (!flux && dtp && !diag) MFG_FACE(false, true, false);
@@ -1308,15 +1571,24 @@ static double cfl_for(const mfg_params &p, int32_t iter_done) {
   return p.cfl_start * pow(p.cfl_ratio, (double)iter_done / p.cfl_nstep);
 }
 
+static int fill_cfl_table(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done);
+
 int mfg_compute_timestep(mfg_ctx *ctx, int32_t iter_done) {
   if (!ctx) return MFG_ERR_INVALID;
   MFG_CUDA(cudaSetDevice(ctx->device));
   const double cfl = cfl_for(ctx->hp, iter_done);
   ctx->hp.cfl_min = 0.5 * cfl;
-  int rc = launch_face(ctx, false, true, false, cfl, false);
+  int rc;
+  if (ctx->ncase > 1) {
+    // one CFL per case (their ramps differ): through the CFL table, slot 0
+    if ((rc = fill_cfl_table(ctx, 1, iter_done))) return rc;
+    rc = launch_face(ctx, false, true, false, cfl, true);
+  } else {
+    rc = launch_face(ctx, false, true, false, cfl, false);
+  }
   if (rc) return rc;
-  k_dt_clamp<<<grid_for(ctx->C), kBlock, 0, ctx->stream>>>(ctx->C, ctx->dt, ctx->dt_ext,
-                                                           ctx->P.ratio_dtmax);
+  k_dt_clamp<<<grid_for(ctx->C), kBlock, 0, ctx->stream>>>(ctx->C, ctx->dt, ctx->dt_ext, ctx->P,
+                                                           cases_of(ctx));
   count_launch();
   return check_kernel();
 }
@@ -1343,10 +1615,12 @@ static int launch_fwd_persist(mfg_ctx *ctx, bool clamp_check, int32_t chunk_skip
   int32_t C = ctx->C, first = ctx->first_cell, skip = chunk_skip;
   int clamp = clamp_check ? 1 : 0;
   Params P = ctx->P;
+  Cases cs = cases_of(ctx);
   ChunkSweep &w = ctx->fwc;
   void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, (void *)&q,
                   &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P, &clamp, &ctx->dt,
-                  &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol, &ctx->sweep_err, &spin, &skip};
+                  &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol, &ctx->sweep_err, &spin, &skip,
+                  &cs};
   return launch_coop((const void *)k_sweep_fwd_chunk, ctx->nchunks, ctx->stream, args);
 }
 
@@ -1354,9 +1628,10 @@ static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
   const double *q = ctx->q8[ctx->cur];
   double *qn = ctx->q8[ctx->cur ^ 1];
   Params P = ctx->P;
+  Cases cs = cases_of(ctx);
   ChunkSweep &w = ctx->bwc;
   void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, (void *)&q, &qn,
-                  &ctx->dqf, &ctx->dq8, &ctx->diag, &P, &ctx->sweep_err, &spin};
+                  &ctx->dqf, &ctx->dq8, &ctx->diag, &P, &ctx->sweep_err, &spin, &cs};
   return launch_coop((const void *)k_sweep_bwd_chunk, ctx->nchunks, ctx->stream, args);
 }
 
@@ -1392,13 +1667,13 @@ static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
     k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
         a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
         ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt,
-        ctx->dt_ext, ctx->cptr, ctx->slots, ctx->vol);
+        ctx->dt_ext, ctx->cptr, ctx->slots, ctx->vol, cases_of(ctx));
   }
   for (int l = 0; l < Lb; l++) {
     const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
     k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
                                                     ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dqf,
-                                                    ctx->dq8, ctx->diag, ctx->P);
+                                                    ctx->dq8, ctx->diag, ctx->P, cases_of(ctx));
   }
   count_launch(Lf + Lb);
   return check_kernel();
@@ -1464,6 +1739,63 @@ int mfg_calculate_gradient(mfg_ctx *ctx) {
   return launch_gradient(ctx);
 }
 
+// End of a fused iteration: the residual norm into norm_hist[counter] and the
+// counter advanced.  One grid reduces the flux gather's block partials; a
+// batch reduces each case's cell range.
+static int launch_norm_tail(mfg_ctx *ctx, cudaStream_t st) {
+  if (ctx->ncase == 1) {
+    k_norm_final<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, ctx->norm_out,
+                                    ctx->iter_counter, ctx->norm_hist);
+    count_launch();
+  } else {
+    k_norm_seg_partial<<<dim3(kSegBlocks, ctx->ncase), kBlock, 0, st>>>(
+        ctx->C, ctx->res, ctx->case_cell0_d, ctx->seg_part);
+    k_norm_seg_final<<<ctx->ncase, 32, 0, st>>>(kSegBlocks, ctx->seg_part, ctx->norm_out,
+                                                ctx->iter_counter, ctx->norm_hist);
+    k_counter_inc<<<1, 1, 0, st>>>(ctx->iter_counter);
+    count_launch(3);
+  }
+  return check_kernel();
+}
+
+// Per-iteration tables of a fused run: CFL [n_iter][ncase] and norms
+// [n_iter][ncase][5].  Captured graphs hold their pointers, so growing them
+// drops the graphs.
+static int ensure_tables(mfg_ctx *ctx, int32_t n_iter) {
+  if (n_iter <= ctx->hist_cap) return MFG_OK;
+  for (int k = 0; k < 2; k++)
+    if (ctx->graph[k]) {
+      cudaGraphExecDestroy(ctx->graph[k]);
+      ctx->graph[k] = nullptr;
+    }
+  const int32_t cap = std::max(n_iter, 256);
+  int rc;
+  if ((rc = dalloc(ctx, &ctx->norm_hist, (size_t)5 * cap * ctx->ncase))) return rc;
+  if ((rc = dalloc(ctx, &ctx->cfl_tab, (size_t)cap * ctx->ncase))) return rc;
+  ctx->hist_cap = cap;
+  return MFG_OK;
+}
+
+// CFL of iterations iter_done .. iter_done + n_iter - 1 of every case (each
+// case ramps with its own cfl_start/cfl_end/cfl_nstep) into cfl_tab, and the
+// fused-loop counter reset.
+static int fill_cfl_table(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done) {
+  int rc = ensure_tables(ctx, n_iter);
+  if (rc) return rc;
+  const int32_t K = ctx->ncase;
+  std::vector<double> tab((size_t)n_iter * K);
+  for (int32_t i = 0; i < n_iter; i++)
+    for (int32_t k = 0; k < K; k++) tab[(size_t)i * K + k] = cfl_for(ctx->hps[k], iter_done + i);
+  ctx->hp.cfl_min = 0.5 * cfl_for(ctx->hp, iter_done + n_iter - 1);
+  for (int32_t k = 0; k < K; k++) ctx->hps[k].cfl_min = 0.5 * tab[(size_t)(n_iter - 1) * K + k];
+  // the copy must finish before tab goes out of scope
+  MFG_CUDA(cudaMemcpyAsync(ctx->cfl_tab, tab.data(), sizeof(double) * tab.size(),
+                           cudaMemcpyHostToDevice, ctx->stream));
+  MFG_CUDA(cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), ctx->stream));
+  MFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MFG_OK;
+}
+
 // One fused iteration: flux + dt + Diag in one gather, level sweeps with the
 // update, gradient, residual norm.  Reads the CFL from cfl_tab[counter].
 static int launch_iteration(mfg_ctx *ctx) {
@@ -1474,11 +1806,7 @@ static int launch_iteration(mfg_ctx *ctx) {
   ctx->cur ^= 1;
   rc = launch_gradient(ctx);
   if (rc) return rc;
-  const int nparts = grid_for(ctx->C);
-  k_norm_final<<<1, 160, 0, ctx->stream>>>(nparts, ctx->norm_part, ctx->norm_out,
-                                           ctx->iter_counter, ctx->norm_hist);
-  count_launch();
-  return check_kernel();
+  return launch_norm_tail(ctx, ctx->stream);
 }
 
 static int ensure_graphs(mfg_ctx *ctx) {
@@ -1523,27 +1851,10 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
   if (n_iter == 0) return MFG_OK;
   MFG_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  if (n_iter > ctx->hist_cap) {
-    // grow the per-iteration tables; graphs hold their pointers, so rebuild
-    for (int k = 0; k < 2; k++)
-      if (ctx->graph[k]) {
-        cudaGraphExecDestroy(ctx->graph[k]);
-        ctx->graph[k] = nullptr;
-      }
-    const int32_t cap = std::max(n_iter, 256);
-    int rc;
-    if ((rc = dalloc(ctx, &ctx->norm_hist, (size_t)5 * cap))) return rc;
-    if ((rc = dalloc(ctx, &ctx->cfl_tab, (size_t)cap))) return rc;
-    ctx->hist_cap = cap;
-  }
-  std::vector<double> tab(n_iter);
-  for (int32_t i = 0; i < n_iter; i++) tab[i] = cfl_for(ctx->hp, iter_done + i);
-  ctx->hp.cfl_min = 0.5 * tab[n_iter - 1];
-  MFG_CUDA(cudaMemcpyAsync(ctx->cfl_tab, tab.data(), sizeof(double) * n_iter,
-                           cudaMemcpyHostToDevice, st));
-  MFG_CUDA(cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st));
+  int rc = fill_cfl_table(ctx, n_iter, iter_done);
+  if (rc) return rc;
   ctx->res_zero = true;  // ZeroResiduals at the top of each iteration
-  int rc = ensure_graphs(ctx);
+  rc = ensure_graphs(ctx);
   if (rc) return rc;
   for (int32_t i = 0; i < n_iter; i++) {
     MFG_CUDA(cudaGraphLaunch(ctx->graph[ctx->cur], st));
@@ -1552,7 +1863,7 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
   }
   ctx->res_zero = false;
   if (norms) {
-    MFG_CUDA(cudaMemcpyAsync(norms, ctx->norm_hist, sizeof(double) * 5 * n_iter,
+    MFG_CUDA(cudaMemcpyAsync(norms, ctx->norm_hist, sizeof(double) * 5 * n_iter * ctx->ncase,
                              cudaMemcpyDeviceToHost, st));
     MFG_CUDA(cudaStreamSynchronize(st));
   }
@@ -1564,23 +1875,10 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
   if (!ctx || n_iter <= 0 || !phase_ms) return MFG_ERR_INVALID;
   MFG_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  if (n_iter > ctx->hist_cap) {
-    for (int k = 0; k < 2; k++)
-      if (ctx->graph[k]) {
-        cudaGraphExecDestroy(ctx->graph[k]);
-        ctx->graph[k] = nullptr;
-      }
-    const int32_t cap = std::max(n_iter, 256);
-    int rc;
-    if ((rc = dalloc(ctx, &ctx->norm_hist, (size_t)5 * cap))) return rc;
-    if ((rc = dalloc(ctx, &ctx->cfl_tab, (size_t)cap))) return rc;
-    ctx->hist_cap = cap;
+  {
+    int rc = fill_cfl_table(ctx, n_iter, iter_done);
+    if (rc) return rc;
   }
-  std::vector<double> tab(n_iter);
-  for (int32_t i = 0; i < n_iter; i++) tab[i] = cfl_for(ctx->hp, iter_done + i);
-  MFG_CUDA(cudaMemcpyAsync(ctx->cfl_tab, tab.data(), sizeof(double) * n_iter,
-                           cudaMemcpyHostToDevice, st));
-  MFG_CUDA(cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st));
   cudaEvent_t ev[MFG_NPHASES + 1];
   for (auto &e : ev) MFG_CUDA(cudaEventCreate(&e));
   for (int k = 0; k < MFG_NPHASES; k++) phase_ms[k] = 0.0;
@@ -1603,14 +1901,15 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
         k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
             a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
             ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, 1, ctx->dt, ctx->dt_ext,
-            ctx->cptr, ctx->slots, ctx->vol);
+            ctx->cptr, ctx->slots, ctx->vol, cases_of(ctx));
       }
       cudaEventRecord(ev[2], st);
       for (int l = 0; l < Lb; l++) {
         const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
         k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
                                                         ctx->bw_recs, ctx->bw_nb, q, qn,
-                                                        ctx->dqf, ctx->dq8, ctx->diag, ctx->P);
+                                                        ctx->dqf, ctx->dq8, ctx->diag, ctx->P,
+                                                        cases_of(ctx));
       }
       count_launch(Lf + Lb);
     }
@@ -1625,10 +1924,10 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
                                                       ctx->fnptr, ctx->fnodes, ctx->qn8, q2,
                                                       ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
     cudaEventRecord(ev[5], st);
-    k_norm_final<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, ctx->norm_out,
-                                    ctx->iter_counter, ctx->norm_hist);
+    const int rn = launch_norm_tail(ctx, st);
     cudaEventRecord(ev[6], st);
-    count_launch(3);
+    count_launch(2);
+    if (rc == MFG_OK) rc = rn;
     if (rc == MFG_OK) rc = check_kernel();
     if (cudaEventSynchronize(ev[6]) != cudaSuccess) rc = MFG_ERR_CUDA;
     for (int k = 0; k < MFG_NPHASES && rc == MFG_OK; k++) {
@@ -1673,6 +1972,28 @@ int mfg_residual_norm(mfg_ctx *ctx, double out[5]) {
   return MFG_OK;
 }
 
+int mfg_batch_residual_norm(mfg_ctx *ctx, double *out) {
+  if (!ctx || !out) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  if (ctx->ncase == 1) return mfg_residual_norm(ctx, out);
+  cudaStream_t st = ctx->stream;
+  const size_t nb = sizeof(double) * 5 * ctx->ncase;
+  if (ctx->res_zero) {
+    std::memset(out, 0, nb);
+    return MFG_OK;
+  }
+  k_norm_seg_partial<<<dim3(kSegBlocks, ctx->ncase), kBlock, 0, st>>>(
+      ctx->C, ctx->res, ctx->case_cell0_d, ctx->seg_part);
+  k_norm_seg_final<<<ctx->ncase, 32, 0, st>>>(kSegBlocks, ctx->seg_part, ctx->norm_out, nullptr,
+                                              nullptr);
+  count_launch(2);
+  MFG_CUDA(cudaGetLastError());
+  MFG_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->norm_out, nb, cudaMemcpyDeviceToHost, st));
+  MFG_CUDA(cudaStreamSynchronize(st));
+  std::memcpy(out, ctx->h_pinned, nb);
+  return MFG_OK;
+}
+
 int mfg_get_dt_extrema(mfg_ctx *ctx, double *dt_max, double *dt_min) {
   if (!ctx || !dt_max || !dt_min) return MFG_ERR_INVALID;
   MFG_CUDA(cudaSetDevice(ctx->device));
@@ -1688,9 +2009,11 @@ int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min) {
   if (!ctx || !(dt_max >= 0.0) || !(dt_min >= 0.0)) return MFG_ERR_INVALID;
   MFG_CUDA(cudaSetDevice(ctx->device));
   MFG_CUDA(cudaStreamSynchronize(ctx->stream));
-  ctx->h_pinned[0] = dt_max;
-  ctx->h_pinned[1] = dt_min;
-  MFG_CUDA(cudaMemcpyAsync(ctx->dt_ext, ctx->h_pinned, 2 * sizeof(double),
+  for (int32_t k = 0; k < ctx->ncase; k++) {
+    ctx->h_pinned[2 * k] = dt_max;
+    ctx->h_pinned[2 * k + 1] = dt_min;
+  }
+  MFG_CUDA(cudaMemcpyAsync(ctx->dt_ext, ctx->h_pinned, 2 * sizeof(double) * ctx->ncase,
                            cudaMemcpyHostToDevice, ctx->stream));
   MFG_CUDA(cudaStreamSynchronize(ctx->stream));
   return MFG_OK;
@@ -1747,7 +2070,7 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
   MFG_CUDA(cudaMemcpyAsync(ctx->staging, host, sizeof(double) * 5 * n, cudaMemcpyHostToDevice,
                            st));
   k_upload_q<<<grid_for(n), kBlock, 0, st>>>(ctx->staging, ctx->q8[ctx->cur],
-                                            ctx->q8[ctx->cur ^ 1], n, ctx->P);
+                                            ctx->q8[ctx->cur ^ 1], n, ctx->P, cases_of(ctx));
   count_launch();
   MFG_CUDA(cudaGetLastError());
   return MFG_OK;

@@ -54,6 +54,24 @@ struct Params {
   double rho_min, rho_max, p_min, p_max, p_break, ratio_dtmax;
 };
 
+// Batched cases: several independent grids concatenated into one (cells,
+// then ghosts, each in case order).  Kernels read the case of a cell and that
+// case's parameters; with P == nullptr there is a single case whose
+// parameters come as a kernel argument.
+struct Cases {
+  const Params *P;        // [ncase]
+  const int32_t *of;      // case of each cell and ghost [n]
+  const int32_t *first;   // first cell of each case's LU-SGS order [ncase]
+  int32_t ncase;
+};
+
+__device__ __forceinline__ int32_t case_of(const Cases &cs, int64_t c) {
+  return cs.P ? cs.of[c] : 0;
+}
+__device__ __forceinline__ Params params_of(const Params &P0, const Cases &cs, int64_t c) {
+  return cs.P ? cs.P[cs.of[c]] : P0;
+}
+
 __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 

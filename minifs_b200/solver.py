@@ -158,7 +158,106 @@ class Solver:
         return {k: getattr(inf, k) for k, _ in inf._fields_}
 
 
-# Reference-named entry points (src/Kernels/*.h), operating on a Solver.
+class BatchSolver(Solver):
+    """Independent cases solved together in one context (``mfg_create_batch``):
+    one launch per kernel and per LU-SGS level covers every case.  Each case
+    gets the bits it would get alone; fields come back per case."""
+
+    def __init__(self, grids, params, device: int = 0, precision: str = "fp64"):
+        self.lib = _lib.load()
+        self.grids = list(grids)
+        self.params_list = list(params)
+        if len(self.grids) != len(self.params_list) or not self.grids:
+            raise ValueError("one Params per grid, at least one case")
+        self.ncase = len(self.grids)
+        self.iter_done = 0
+        meshes, keeps, q0s = [], [], []
+        for g in self.grids:
+            m, keep = mesh_struct(g)
+            meshes.append(m)
+            keeps.append(keep)
+            q0s.append(np.ascontiguousarray(g.q0, np.float64))
+        marr = (_lib.Mesh * self.ncase)(*meshes)
+        parr = (_lib.Params * self.ncase)(*self.params_list)
+        qarr = (_lib.f64p * self.ncase)(*[_lib.ptr(q) for q in q0s])
+        self._ctx = ct.c_void_p()
+        _lib.check("mfg_create_batch",
+                   self.lib.mfg_create_batch(self.ncase, marr, parr, qarr, int(device),
+                                             _lib.PREC[precision], ct.byref(self._ctx)))
+        del keeps
+        self.cell0 = np.zeros(self.ncase + 1, np.int32)
+        self.bface0 = np.zeros(self.ncase + 1, np.int32)
+        self._call("mfg_batch_layout", _lib.ptr(self.cell0, _lib.i32p),
+                   _lib.ptr(self.bface0, _lib.i32p))
+        self.n_cell = int(self.cell0[-1])
+        self.n = self.n_cell + int(self.bface0[-1])
+
+    def iterate(self, n: int, norms: bool = True) -> np.ndarray | None:
+        """``n`` fused iterations of every case; norms shape ``[n, ncase, 5]``."""
+        out = np.zeros(5 * n * self.ncase) if norms else None
+        self._call("mfg_iterate", int(n), int(self.iter_done),
+                   _lib.ptr(out) if norms else None)
+        self.iter_done += n
+        return out.reshape(n, self.ncase, 5) if norms else None
+
+    def residual_norm(self) -> np.ndarray:
+        out = np.zeros(5 * self.ncase)
+        self._call("mfg_batch_residual_norm", _lib.ptr(out))
+        return out.reshape(self.ncase, 5)
+
+    @property
+    def dt_extrema(self):
+        out = np.zeros(2 * self.ncase)
+        self._call("mfg_batch_dt_extrema", _lib.ptr(out))
+        return [(out[2 * k], out[2 * k + 1]) for k in range(self.ncase)]
+
+    def download(self, field: str) -> np.ndarray:
+        """The union array (cells of all cases, then ghosts of all cases)."""
+        C, n = self.n_cell, self.n
+        size = {"q": 5 * n, "res": 5 * C, "dt": C, "dq": 5 * n, "dqdx": 5 * n, "dqdy": 5 * n,
+                "dqdz": 5 * n, "diag": C}[field]
+        out = np.empty(size)
+        self._call("mfg_download", _lib.FIELD[field], _lib.ptr(out))
+        return out
+
+    def split(self, field: str, arr: np.ndarray) -> list:
+        """Per-case arrays, each in the single-case layout of its grid."""
+        C, n = self.n_cell, self.n
+        per_cell = field in ("res", "dt", "diag")
+        nv = 1 if field in ("dt", "diag") else 5
+        stride = C if per_cell else n
+        out = []
+        for k in range(self.ncase):
+            a, b = int(self.cell0[k]), int(self.cell0[k + 1])
+            ga, gb = C + int(self.bface0[k]), C + int(self.bface0[k + 1])
+            parts = []
+            for v in range(nv):
+                base = v * stride
+                parts.append(arr[base + a:base + b])
+                if not per_cell:
+                    parts.append(arr[base + ga:base + gb])
+            out.append(np.concatenate(parts))
+        return out
+
+    def download_cases(self, field: str) -> list:
+        return self.split(field, self.download(field))
+
+    def upload_cases(self, qs):
+        """Set the state of every case (each [5 n_k] in its own layout)."""
+        C, n = self.n_cell, self.n
+        q = np.empty(5 * n)
+        for k, qk in enumerate(qs):
+            a, b = int(self.cell0[k]), int(self.cell0[k + 1])
+            ga, gb = C + int(self.bface0[k]), C + int(self.bface0[k + 1])
+            nk = (b - a) + (gb - ga)
+            qk = np.asarray(qk, np.float64).reshape(5, nk)
+            for v in range(5):
+                q[v * n + a:v * n + b] = qk[v, :b - a]
+                q[v * n + ga:v * n + gb] = qk[v, b - a:]
+        self.upload_q(q)
+
+
+# Reference-named entry points (src/Kernels/*.h), operating on a Solver.# Reference-named entry points (src/Kernels/*.h), operating on a Solver.
 
 def ZeroResiduals(s: Solver):  # cal_flux.h:24
     s.zero_residuals()
