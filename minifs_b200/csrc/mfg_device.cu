@@ -336,149 +336,359 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
 #define MFG_PERSIST_MINB 6
 #endif
 constexpr int kPersistBlock = MFG_PERSIST_BLOCK;
-constexpr int kPre = 4;                  // neighbour records held in registers
-constexpr uint32_t kMark = 0x80000000u;  // high bit of a neighbour: in another chunk
-constexpr int kMinChunk = 64;            // no chunk smaller than this many cells
+constexpr uint32_t kMark = 0x80000000u;    // neighbour flag: in another chunk (wait in L2)
+constexpr uint32_t kInRing = 0x40000000u;  // neighbour flag: increment in the block's ring
+constexpr uint32_t kIdMask = 0x3FFFFFFFu;  // neighbour id bits
+constexpr int kMinChunk = 64;              // no chunk smaller than this many cells
+// Increments of the last kRing positions of a chunk stay in shared memory, so
+// that a dependency inside the chunk is read on the SM instead of from L2.
+#ifndef MFG_SWEEP_RING
+#define MFG_SWEEP_RING 128
+#endif
+constexpr int kRing = MFG_SWEEP_RING;
+static_assert((kRing & (kRing - 1)) == 0, "ring size must be a power of two");
 
-// Per chunk position: the cell, its first record and its record count.
-struct __align__(16) ChunkCell {
-  int32_t cell, s0, ns, pad;
+// Position-major sweep tables.  Position p (chunk-major, level-sorted) holds
+// one cell; its records sit at [p * W, p * W + ns), so every index a thread
+// needs for a future level follows from the position alone and can be loaded
+// levels ahead.  W = 4 (tetrahedra) or 8 (any cell with at most 8 lower or
+// upper neighbours).
+struct __align__(8) PosCell {
+  int32_t cell, ns;
 };
 
-// acc (-/+)= w * FluxLUSGS3D(q[nb], DQ[nb], n) over records [s0, s0+ns) in
-// order, DQ[nb] read from src (same chunk: written before the last
-// __syncthreads; other chunk: waited for in L2).
-template <bool FWD>
-__device__ __forceinline__ void sweep_gather(int32_t s0, int32_t ns,
-                                             const SweepRec *__restrict__ recs,
-                                             const int32_t *__restrict__ nbs,
-                                             const double *__restrict__ q8, const double *src,
-                                             int *err, long long spin, const Params &P,
-                                             double *acc) {
-  SweepRec r[kPre];
-  uint32_t nb[kPre];
-  double qn[kPre][Q_STRIDE];
+// A cell is swept by a group of W lanes: lane j computes the flux of the
+// cell's record j, lane l owns the components k = l, l + W, ... < 5 of the
+// increment (the ordered sum over the records and the division), and lane 0
+// applies the limiter to the whole increment and stores it.  The operations
+// and their order per component are those of the one-thread form, so the
+// results are the same bits, while a level costs one flux and one division
+// of latency.
+
+// Segment starts of a chunk kept in shared memory (longer chunks read the
+// rest from global memory).
+constexpr int kSegCache = 512;
+// Cases whose LimitTimeStep clamp state is kept in shared memory.
+constexpr int kCaseCache = 128;
+
+// What a lane knows about its group's position on a future level: the
+// position, its ring slot, the cell, the record count, this lane's neighbour
+// (flags kMark / kInRing) and that neighbour's ring slot; cell < 0 = none.
+struct LaneRegs {
+  int32_t p, slot, cell, ns;
+  uint32_t nb;
+  int32_t nslot;
+};
+
+// Everything a group reads for one cell that no sweep writes, staged into
+// shared memory by cp.async one level ahead: neighbour states and records
+// (lane j), the cell's state and Diag (lane 0), and res (forward) or the
+// cell's forward increment (backward), component k by lane k % W.
+template <int W>
+struct __align__(16) Stage {
+  double qn[W][Q_STRIDE];
+  SweepRec rec[W];
+  double qc[Q_STRIDE];
+  double in5[5];
+  double diag;
+  double pad[2];
+};
+
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int W>
+__device__ __forceinline__ void fetch_lane(const int32_t *s_segs, const int32_t *__restrict__ segs,
+                                           int32_t sg0, int32_t sg, int32_t sg1, int32_t pbase,
+                                           int32_t pos_in_level, int32_t lane,
+                                           const PosCell *__restrict__ pcs,
+                                           const int32_t *__restrict__ pnb,
+                                           const int32_t *__restrict__ pslot, LaneRegs &o) {
+  o.cell = -1;
+  o.ns = 0;
+  o.nb = 0;
+  o.nslot = 0;
+  if (sg >= sg1) return;
+  const int32_t i = sg - sg0;
+  const int32_t a = i < kSegCache ? s_segs[i] : segs[sg];
+  const int32_t b = i + 1 <= kSegCache ? s_segs[i + 1] : segs[sg + 1];
+  const int32_t p = a + pos_in_level;
+  if (p >= b) return;
+  const PosCell x = pcs[p];
+  o.p = p;
+  o.slot = (p - pbase) & (kRing - 1);
+  o.cell = x.cell;
+  o.ns = x.ns;
+  o.nb = (uint32_t)pnb[(int64_t)p * W + lane];  // padding reads 0
+  o.nslot = pslot[(int64_t)p * W + lane];
+}
+
+template <int W, bool FWD>
+__device__ __forceinline__ void stage_copy(const LaneRegs &o, int32_t lane, Stage<W> &st,
+                                           const double *q8, const SweepRec *prec,
+                                           const double *res, const double *diag,
+                                           const double *dqf, int32_t C) {
+  if (o.cell < 0) return;
+  if (lane < o.ns) {
+    const double *qs = q8 + (int64_t)(o.nb & kIdMask) * Q_STRIDE;
 #pragma unroll
-  for (int j = 0; j < kPre; j++)
-    if (j < ns) {
-      r[j] = recs[s0 + j];
-      nb[j] = (uint32_t)nbs[s0 + j];
-      load_q(q8, nb[j] & ~kMark, qn[j]);
-    }
+    for (int i = 0; i < 4; i++) cp_async16(&st.qn[lane][2 * i], qs + 2 * i);
+    const double *rs = reinterpret_cast<const double *>(prec + (int64_t)o.p * W + lane);
+    double *rd = reinterpret_cast<double *>(&st.rec[lane]);
+    cp_async16(rd, rs);
+    cp_async16(rd + 2, rs + 2);
+  }
+  if (lane == 0) {
+    const double *qs = q8 + (int64_t)o.cell * Q_STRIDE;
 #pragma unroll
-  for (int j = 0; j < kPre; j++)
-    if (j < ns) {
-      double dn[5], f[5];
-      const double *rec = src + (int64_t)(nb[j] & ~kMark) * Q_STRIDE;
-      if (nb[j] & kMark) {
-        wait_rec(rec, dn, err, spin);
-      } else {
-        const double2 *pp = reinterpret_cast<const double2 *>(rec);
-        const double2 x = pp[0], y = pp[1], z = pp[2];
-        dn[0] = x.x; dn[1] = x.y; dn[2] = y.x; dn[3] = y.y; dn[4] = z.x;
-      }
-      flux_lusgs(qn[j], dn, r[j].nx, r[j].ny, r[j].nz, P, f);
-      for (int k = 0; k < 5; k++) {
-        if (FWD)
-          acc[k] -= r[j].w * f[k];
-        else
-          acc[k] += r[j].w * f[k];
-      }
-    }
-  for (int32_t s = s0 + kPre; s < s0 + ns; s++) {
-    const SweepRec rr = recs[s];
-    const uint32_t b = (uint32_t)nbs[s];
-    double qq[Q_STRIDE], dn[5], f[5];
-    load_q(q8, b & ~kMark, qq);
-    const double *rec = src + (int64_t)(b & ~kMark) * Q_STRIDE;
-    if (b & kMark) {
-      wait_rec(rec, dn, err, spin);
+    for (int i = 0; i < 4; i++) cp_async16(&st.qc[2 * i], qs + 2 * i);
+    cp_async8(&st.diag, diag + o.cell);
+  }
+  for (int k = lane; k < 5; k += W)
+    cp_async8(&st.in5[k], FWD ? res + (int64_t)k * C + o.cell : dqf + (int64_t)o.cell * Q_STRIDE + k);
+}
+
+// Diag of a cell whose dt LimitTimeStep clamps to lim (compute_timestep.cpp
+// :929-944, then Diag = vol / dt + the face sum of CalDiagLUSGS,
+// forward_lusgs.cpp:96 and :175-260, with that dt).
+__device__ __forceinline__ double clamped_diag(int32_t c, const double *qc, const Params &P,
+                                               double lim, const int32_t *__restrict__ cptr,
+                                               const SlotRec *__restrict__ slots,
+                                               const double *__restrict__ vol) {
+  double dg = vol[c] / lim;
+  for (int32_t s = cptr[c]; s < cptr[c + 1]; s++) {
+    const SlotRec sr = slots[s];
+    double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
+    vn = fabs(vn);
+    dg += 0.5 * sr.area * (vn + qc[Q_A]) * P.lhs_omga;
+  }
+  return dg;
+}
+
+// Per-case clamp state: lim > 0 when dt_max / dt_min exceeds ratio_dtmax.
+__device__ __forceinline__ double clamp_limit(const Params &P,
+                                              const unsigned long long *__restrict__ ext) {
+  const double dt_max = __longlong_as_double((long long)ext[0]);
+  const double dt_min = __longlong_as_double((long long)ext[1]);
+  return (dt_max / dt_min > P.ratio_dtmax) ? P.ratio_dtmax * dt_min : -1.0;
+}
+
+// One cell of one sweep level on a lane group, from its stage (the group's
+// lanes only wait for one another: a cell is stored as soon as its own
+// inputs are in).  sh: the group's scratch (W * 5 + 5 doubles); ring: the
+// block's increments of its last kRing positions.  FWD: DQ* = (res - sum_j
+// 0.5 area_j F_j) / Diag, limited except for the first cell (SolveLUSGS3D
+// forward, forward_lusgs.cpp:799-870); backward: DQ = DQ* - (sum_j area_j
+// F_j) / (2 Diag), limited (:871-940).
+template <int W, bool FWD>
+__device__ __forceinline__ void sweep_cell(
+    const LaneRegs &o, int32_t lane, const Stage<W> &st, double *sh, double *ring,
+    const double *src, double *dst, double *rearm, int32_t first_cell, const Params &P0,
+    const double *s_lim, int clamp_check, double *__restrict__ dt, double *__restrict__ diag,
+    const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
+    const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err,
+    long long spin, const Cases &cs) {
+  if (o.cell < 0) return;  // the whole group
+  const unsigned gmask = ((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1));
+  const int32_t c = o.cell;
+  const int32_t cse = case_of(cs, c);
+  const Params P = params_of(P0, cs, c);
+  // lane j < ns: w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j)
+  if (lane < o.ns) {
+    const uint32_t b = o.nb;
+    double dn[5], f[5], qn[Q_STRIDE];
+    if (b & kInRing) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) dn[k] = ring[o.nslot * 5 + k];
+    } else if (b & kMark) {
+      wait_rec(src + (int64_t)(b & kIdMask) * Q_STRIDE, dn, err, spin);
     } else {
-      const double2 *pp = reinterpret_cast<const double2 *>(rec);
+      const double2 *pp = reinterpret_cast<const double2 *>(src + (int64_t)b * Q_STRIDE);
       const double2 x = pp[0], y = pp[1], z = pp[2];
       dn[0] = x.x; dn[1] = x.y; dn[2] = y.x; dn[3] = y.y; dn[4] = z.x;
     }
-    flux_lusgs(qq, dn, rr.nx, rr.ny, rr.nz, P, f);
-    for (int k = 0; k < 5; k++) {
-      if (FWD)
-        acc[k] -= rr.w * f[k];
-      else
-        acc[k] += rr.w * f[k];
+#pragma unroll
+    for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[lane][k];
+    const SweepRec r = st.rec[lane];
+    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
+#pragma unroll
+    for (int k = 0; k < 5; k++) sh[lane * 5 + k] = r.w * f[k];
+  }
+  // LimitTimeStep's clamp (fused forward sweep only): every component lane
+  // reads dt[c] before lane 0 may write it below
+  double dg = st.diag, lim = -1.0;
+  bool clamped = false;
+  if (FWD && clamp_check && lane < 5) {
+    lim = (cse < kCaseCache) ? s_lim[cse] : clamp_limit(P, dt_ext + 2 * cse);
+    if (lim > 0.0 && dt[c] > lim) {
+      double qc[Q_STRIDE];
+#pragma unroll
+      for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
+      dg = clamped_diag(c, qc, P, lim, cptr, slots, vol);
+      clamped = true;
     }
   }
+  __syncwarp(gmask);
+  // lane l: components l, l + W, ...; records summed in order
+  for (int k = lane; k < 5; k += W) {
+    double acc = FWD ? st.in5[k] : 0.0;
+    for (int32_t j = 0; j < o.ns; j++) {
+      if (FWD)
+        acc -= sh[j * 5 + k];
+      else
+        acc += sh[j * 5 + k];
+    }
+    if (FWD) {
+      acc /= dg;
+    } else {
+      const double tmp = 2.0 * st.diag;
+      acc = st.in5[k] - acc / tmp;
+    }
+    sh[W * 5 + k] = acc;
+  }
+  __syncwarp(gmask);
+  if (lane == 0) {
+    if (FWD && clamped) {
+      dt[c] = lim;
+      diag[c] = dg;
+    }
+    double d[5], qc[Q_STRIDE];
+#pragma unroll
+    for (int k = 0; k < 5; k++) d[k] = sh[W * 5 + k];
+#pragma unroll
+    for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
+    if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit(qc, d, P);
+    store_dq(dst, c, d);
+    store_sentinel(rearm, c);  // armed for the other sweep
+#pragma unroll
+    for (int k = 0; k < 5; k++) ring[o.slot * 5 + k] = d[k];
+  }
+  __syncwarp(gmask);  // sh is free for the group's next cell
 }
 
-// chunk_skip > 0 withholds the first chunk_skip chunks (failure-detection
-// self-test only: the cells that depend on them wait until the bound runs out).
+// One persistent sweep: block b walks chunk b level by level.  Indices of a
+// group's first position of each level are loaded two levels ahead and its
+// read-only data staged into shared memory one level ahead (cp.async), so a
+// level's critical path holds the increments it depends on and one cell's
+// arithmetic.  A level wider than the block's groups takes further passes,
+// staged and waited for on the spot.
+template <int W, bool FWD>
+__device__ __forceinline__ void sweep_chunk(
+    const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
+    const PosCell *__restrict__ pcs, const SweepRec *__restrict__ prec,
+    const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
+    const double *__restrict__ q8, const double *src, double *dst, double *rearm,
+    const double *__restrict__ res, const double *__restrict__ dqf_own, int32_t C,
+    double *__restrict__ diag, int32_t first_cell, const Params &P0, int clamp_check,
+    double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
+    const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+    const double *__restrict__ vol, int *err, long long spin, const Cases &cs) {
+  constexpr int kGroups = kPersistBlock / W;
+  __shared__ Stage<W> stg[3][kGroups];
+  __shared__ double shm[kGroups][W * 5 + 5];
+  __shared__ double ring[kRing * 5];
+  __shared__ int32_t s_segs[kSegCache + 1];
+  __shared__ double s_lim[FWD ? kCaseCache : 1];
+  const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
+  const int32_t lane = threadIdx.x & (W - 1);
+  const int32_t grp = threadIdx.x / W;
+  for (int32_t i = threadIdx.x; i <= sg1 - sg0 && i <= kSegCache; i += blockDim.x)
+    s_segs[i] = segs[sg0 + i];
+  if (FWD && clamp_check)
+    for (int32_t k = threadIdx.x; k < cs.ncase && k < kCaseCache; k += blockDim.x)
+      s_lim[k] = clamp_limit(cs.P ? cs.P[k] : P0, dt_ext + 2 * k);
+  __syncthreads();
+  const unsigned gmask = ((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1));
+  double *sh = shm[grp];
+  const int32_t pbase = sg1 > sg0 ? s_segs[0] : 0;
+  LaneRegs cur, nxt, far;
+  fetch_lane<W>(s_segs, segs, sg0, sg0, sg1, pbase, grp, lane, pcs, pnb, pslot, cur);
+  fetch_lane<W>(s_segs, segs, sg0, sg0 + 1, sg1, pbase, grp, lane, pcs, pnb, pslot, nxt);
+  stage_copy<W, FWD>(cur, lane, stg[0][grp], q8, prec, res, diag, dqf_own, C);
+  cp_async_commit();
+  for (int32_t sg = sg0; sg < sg1; sg++) {
+    const int par = (sg - sg0) & 1;
+    fetch_lane<W>(s_segs, segs, sg0, sg + 2, sg1, pbase, grp, lane, pcs, pnb, pslot, far);
+    stage_copy<W, FWD>(nxt, lane, stg[par ^ 1][grp], q8, prec, res, diag, dqf_own, C);
+    cp_async_commit();
+    cp_async_wait<1>();  // this level's stage
+    __syncwarp(gmask);
+    sweep_cell<W, FWD>(cur, lane, stg[par][grp], sh, ring, src, dst, rearm, first_cell, P0,
+                       s_lim, clamp_check, dt, diag, dt_ext, cptr, slots, vol, err, spin, cs);
+    const int32_t i = sg - sg0;
+    const int32_t a = i < kSegCache ? s_segs[i] : segs[sg];
+    const int32_t b = i + 1 <= kSegCache ? s_segs[i + 1] : segs[sg + 1];
+    for (int32_t base = a + kGroups; base < b; base += kGroups) {  // uniform over the block
+      LaneRegs e;
+      fetch_lane<W>(s_segs, segs, sg0, sg, sg1, pbase, base - a + grp, lane, pcs, pnb, pslot, e);
+      stage_copy<W, FWD>(e, lane, stg[2][grp], q8, prec, res, diag, dqf_own, C);
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncwarp(gmask);
+      sweep_cell<W, FWD>(e, lane, stg[2][grp], sh, ring, src, dst, rearm, first_cell, P0, s_lim,
+                         clamp_check, dt, diag, dt_ext, cptr, slots, vol, err, spin, cs);
+    }
+    __syncthreads();
+    cur = nxt;
+    nxt = far;
+  }
+  cp_async_wait<0>();
+}
+
+// Forward sweep.  chunk_skip > 0 withholds the first chunk_skip chunks
+// (failure-detection self-test only: the cells that depend on them wait
+// until the bound runs out).
+template <int W>
 __global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
 k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
-                  const ChunkCell *__restrict__ ccells, const SweepRec *__restrict__ recs,
-                  const int32_t *__restrict__ nbs, const double *__restrict__ q8, double *dqf,
-                  double *__restrict__ dqb, const double *__restrict__ res, int32_t C,
-                  double *__restrict__ diag, int32_t first_cell, Params P0, int clamp_check,
-                  double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
+                  const PosCell *__restrict__ pcs, const SweepRec *__restrict__ prec,
+                  const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
+                  const double *__restrict__ q8, double *dqf, double *__restrict__ dqb,
+                  const double *__restrict__ res, int32_t C, double *__restrict__ diag,
+                  int32_t first_cell, Params P0, int clamp_check, double *__restrict__ dt,
+                  const unsigned long long *__restrict__ dt_ext,
                   const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
                   const double *__restrict__ vol, int *err, long long spin,
                   int32_t chunk_skip, Cases cs) {
   if ((int32_t)blockIdx.x < chunk_skip) return;
-  const int32_t sg1 = seg_begin[blockIdx.x + 1];
-  for (int32_t sg = seg_begin[blockIdx.x]; sg < sg1; sg++) {
-    const int32_t a = segs[sg], b = segs[sg + 1];
-    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-      const ChunkCell cc = ccells[i];
-      const int32_t c = cc.cell;
-      const int32_t cse = case_of(cs, c);
-      const Params P = params_of(P0, cs, c);
-      double d[5];
-      for (int k = 0; k < 5; k++) d[k] = res[(int64_t)k * C + c];
-      double dg = diag[c];
-      double qc[Q_STRIDE];
-      load_q(q8, c, qc);
-      sweep_gather<true>(cc.s0, cc.ns, recs, nbs, q8, dqf, err, spin, P, d);
-      if (clamp_check) clamp_diag(c, qc, dg, P, dt, dt_ext + 2 * cse, cptr, slots, vol, diag);
-      for (int k = 0; k < 5; k++) d[k] /= dg;
-      if (c != (cs.P ? cs.first[cse] : first_cell)) dq_limit(qc, d, P);
-      store_dq(dqf, c, d);
-      store_sentinel(dqb, c);  // armed for the backward sweep
-    }
-    __syncthreads();
-  }
+  sweep_chunk<W, true>(seg_begin, segs, pcs, prec, pnb, pslot, q8, dqf, dqf, dqb, res, nullptr, C,
+                       diag, first_cell, P0, clamp_check, dt, dt_ext, cptr, slots, vol, err,
+                       spin, cs);
 }
 
 // Backward sweep.  The state update of a cell is not needed by any later
 // level, so it runs after the block has swept its whole chunk.
+template <int W>
 __global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
 k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
-                  const ChunkCell *__restrict__ ccells, const SweepRec *__restrict__ recs,
-                  const int32_t *__restrict__ nbs, const double *__restrict__ q8,
-                  double *__restrict__ q8_new, double *__restrict__ dqf, double *dqb,
-                  const double *__restrict__ diag, Params P0, int *err, long long spin,
-                  Cases cs) {
+                  const PosCell *__restrict__ pcs, const SweepRec *__restrict__ prec,
+                  const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
+                  const double *__restrict__ q8, double *__restrict__ q8_new,
+                  double *__restrict__ dqf, double *dqb, const double *__restrict__ diag,
+                  Params P0, int *err, long long spin, Cases cs) {
   const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
-  for (int32_t sg = sg0; sg < sg1; sg++) {
-    const int32_t a = segs[sg], b = segs[sg + 1];
-    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-      const ChunkCell cc = ccells[i];
-      const int32_t c = cc.cell;
-      const Params P = params_of(P0, cs, c);
-      double d[5], fs[5] = {0., 0., 0., 0., 0.};
-      load_dq_cg(dqf, c, d);  // this cell's forward value (previous kernel)
-      double qc[Q_STRIDE];
-      load_q(q8, c, qc);
-      const double tmp = 2.0 * diag[c];
-      sweep_gather<false>(cc.s0, cc.ns, recs, nbs, q8, dqb, err, spin, P, fs);
-      for (int k = 0; k < 5; k++) d[k] -= fs[k] / tmp;
-      dq_limit(qc, d, P);
-      store_dq(dqb, c, d);
-      store_sentinel(dqf, c);  // armed for the next forward sweep
-    }
-    __syncthreads();
-  }
-  // UpdateFlowField3D_CFL3d for the chunk's cells (their DQ is final now)
+  sweep_chunk<W, false>(seg_begin, segs, pcs, prec, pnb, pslot, q8, dqb, dqb, dqf, nullptr, dqf,
+                        0, const_cast<double *>(diag), 0, P0, 0, nullptr, nullptr, nullptr,
+                        nullptr, nullptr, err, spin, cs);
+  __syncthreads();  // the chunk's increments are final
+  // UpdateFlowField3D_CFL3d for the chunk's cells
   if (sg1 > sg0) {
     const int32_t a = segs[sg0], b = segs[sg1];
     for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-      const int32_t c = ccells[i].cell;
+      const int32_t c = pcs[i].cell;
       double d[5], qc[Q_STRIDE];
       const double2 *pp = reinterpret_cast<const double2 *>(dqb + (int64_t)c * Q_STRIDE);
       const double2 x = pp[0], y = pp[1], z = pp[2];
@@ -696,8 +906,8 @@ __global__ void k_counter_inc(int32_t *__restrict__ counter) { *counter += 1; }
 // ---------------------------------------------------------------------------
 
 struct ChunkSweep {
-  int32_t *seg_begin = nullptr, *segs = nullptr, *nbs = nullptr;
-  ChunkCell *cells = nullptr;
+  int32_t *seg_begin = nullptr, *segs = nullptr, *nbs = nullptr, *nslots = nullptr;
+  PosCell *cells = nullptr;
   SweepRec *recs = nullptr;
   int32_t nseg = 0;
 };
@@ -736,6 +946,9 @@ struct mfg_ctx {
   double *dqf = nullptr;  // forward-sweep increments (dq8 holds the backward ones = DQ)
   int *sweep_err = nullptr;
   int persist_grid = 0;
+  int sweep_w = 0;               // records per position of the persistent sweeps (4 or 8)
+  int persist_per_sm[2] = {0, 0};  // resident blocks per SM for W = 4, 8
+  int n_sm = 0;
   unsigned long long *dt_ext = nullptr;
   double *norm_part = nullptr, *norm_out = nullptr, *norm_hist = nullptr, *cfl_tab = nullptr;
   int32_t *iter_counter = nullptr;
@@ -941,6 +1154,18 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     }
     blvl[c] = l;
   }
+  // persistent sweeps: records per position and chunk count
+  {
+    int32_t maxns = 0;
+    for (int32_t c = 0; c < C; c++) maxns = std::max(maxns, std::max(fw_cnt[c], bw_cnt[c]));
+    ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
+    if (n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
+    const int per_sm = ctx->sweep_w ? ctx->persist_per_sm[ctx->sweep_w == 4 ? 0 : 1] : 0;
+    ctx->persist_grid = per_sm * ctx->n_sm;
+    ctx->nchunks = std::max(1, std::min(ctx->persist_grid, (C + kMinChunk - 1) / kMinChunk));
+    ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
+  }
+  const int W = std::max(ctx->sweep_w, 1);
   auto make = [&](const std::vector<int32_t> &lv, const std::vector<int32_t> &cnt, bool fwd,
                   std::vector<int32_t> &lptr, int32_t **d_cells, int32_t **d_sptr,
                   SweepRec **d_recs, int32_t **d_nb) -> int {
@@ -1029,26 +1254,42 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     }
     std::vector<int32_t> gpos(C);
     for (int32_t i = 0; i < C; i++) gpos[cells[i]] = i;
-    std::vector<int32_t> csptr(C + 1, 0), segs, seg_begin;
-    for (int32_t k = 0; k < C; k++) {
-      const int32_t gi = gpos[ccells[k]];
-      csptr[k + 1] = csptr[k] + (sptr[gi + 1] - sptr[gi]);
-    }
-    std::vector<int32_t> cnbs(csptr[C]);
-    std::vector<SweepRec> crecs(csptr[C]);
+    std::vector<int32_t> segs, seg_begin;
+    // position-major: the records of position k at [k * W, k * W + ns)
+    std::vector<int32_t> cnbs((size_t)C * W, 0);
+    std::vector<SweepRec> crecs((size_t)C * W, SweepRec{0.0, 0.0, 0.0, 0.0});
+    std::vector<int32_t> cslot((size_t)C * W, 0), posof(C);
+    for (int32_t k = 0; k < C; k++) posof[ccells[k]] = k;
+    std::vector<PosCell> packed(C);
     bool chunk0_exported = false;
     for (int32_t p = 0; p < P; p++) {
       seg_begin.push_back((int32_t)segs.size());
+      int32_t seg_end = chunk_ptr[p];
       for (int32_t k = chunk_ptr[p]; k < chunk_ptr[p + 1]; k++) {
         const int32_t c = ccells[k];
-        if (k == chunk_ptr[p] || lv[c] != lv[ccells[k - 1]]) segs.push_back(k);
+        if (k == chunk_ptr[p] || lv[c] != lv[ccells[k - 1]]) {
+          segs.push_back(k);
+          seg_end = k;
+          while (seg_end < chunk_ptr[p + 1] && lv[ccells[seg_end]] == lv[c]) seg_end++;
+        }
         const int32_t gi = gpos[c];
-        int32_t o = csptr[k];
+        packed[k] = PosCell{c, sptr[gi + 1] - sptr[gi]};
+        if (!ctx->sweep_w) continue;  // no persistent sweeps for this grid
+        int64_t o = (int64_t)k * W;
         for (int32_t s0 = sptr[gi]; s0 < sptr[gi + 1]; s0++, o++) {
           const int32_t nb = nbs[s0];
           const bool cross = nb < C && assign[nb] != p;
           if (cross && assign[nb] == 0) chunk0_exported = true;
-          cnbs[o] = cross ? (int32_t)((uint32_t)nb | kMark) : nb;
+          uint32_t e = (uint32_t)nb;
+          if (cross) {
+            e |= kMark;
+          } else if (nb < C && posof[nb] >= seg_end - kRing) {
+            // still in the ring when this level reads it: overwritten only by
+            // position posof[nb] + kRing, which lies in a later level
+            e |= kInRing;
+            cslot[o] = (posof[nb] - chunk_ptr[p]) & (kRing - 1);
+          }
+          cnbs[o] = (int32_t)e;
           crecs[o] = recs[s0];
         }
       }
@@ -1065,12 +1306,10 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     cs.nseg = (int32_t)segs.size() - 1;
     if ((rc = dupload(ctx, &cs.seg_begin, seg_begin))) return rc;
     if ((rc = dupload(ctx, &cs.segs, segs))) return rc;
-    std::vector<ChunkCell> packed(C);
-    for (int32_t k = 0; k < C; k++)
-      packed[k] = ChunkCell{ccells[k], csptr[k], csptr[k + 1] - csptr[k], 0};
     if ((rc = dupload(ctx, &cs.cells, packed))) return rc;
     if ((rc = dupload(ctx, &cs.recs, crecs))) return rc;
     if ((rc = dupload(ctx, &cs.nbs, cnbs))) return rc;
+    if ((rc = dupload(ctx, &cs.nslots, cslot))) return rc;
     return MFG_OK;
   };
   (void)n;
@@ -1264,17 +1503,21 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   {
     // persistent sweeps need every block resident: one chunk per block, at
     // most as many blocks as the occupancy of the heavier kernel allows
-    int bf = 0, bb = 0, coop = 0;
+    int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_sweep_fwd_chunk, kPersistBlock,
-                                                      0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bb, k_sweep_bwd_chunk, kPersistBlock,
-                                                      0) != cudaSuccess)
+    int b[4] = {0, 0, 0, 0};
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[0], k_sweep_fwd_chunk<4>,
+                                                      kPersistBlock, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[1], k_sweep_bwd_chunk<4>,
+                                                      kPersistBlock, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_sweep_fwd_chunk<8>,
+                                                      kPersistBlock, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[3], k_sweep_bwd_chunk<8>,
+                                                      kPersistBlock, 0) != cudaSuccess)
       return fail(MFG_ERR_CUDA);
-    const int per_sm = std::min(bf, bb);
-    ctx->persist_grid = coop ? per_sm * prop.multiProcessorCount : 0;
-    ctx->nchunks = std::max(1, std::min(ctx->persist_grid, (C + kMinChunk - 1) / kMinChunk));
-    ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
+    ctx->persist_per_sm[0] = coop ? std::min(b[0], b[1]) : 0;
+    ctx->persist_per_sm[1] = coop ? std::min(b[2], b[3]) : 0;
+    ctx->n_sm = prop.multiProcessorCount;
   }
   if ((rc = build_levels(ctx, m, cptr, c2f))) return fail(rc);
   if ((rc = build_node_lists(ctx, m))) return fail(rc);
@@ -1617,11 +1860,13 @@ static int launch_fwd_persist(mfg_ctx *ctx, bool clamp_check, int32_t chunk_skip
   Params P = ctx->P;
   Cases cs = cases_of(ctx);
   ChunkSweep &w = ctx->fwc;
-  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, (void *)&q,
+  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, &w.nslots, (void *)&q,
                   &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P, &clamp, &ctx->dt,
                   &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol, &ctx->sweep_err, &spin, &skip,
                   &cs};
-  return launch_coop((const void *)k_sweep_fwd_chunk, ctx->nchunks, ctx->stream, args);
+  const void *fn = ctx->sweep_w == 8 ? (const void *)k_sweep_fwd_chunk<8>
+                                      : (const void *)k_sweep_fwd_chunk<4>;
+  return launch_coop(fn, ctx->nchunks, ctx->stream, args);
 }
 
 static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
@@ -1630,9 +1875,11 @@ static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
   Params P = ctx->P;
   Cases cs = cases_of(ctx);
   ChunkSweep &w = ctx->bwc;
-  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, (void *)&q, &qn,
+  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, &w.nslots, (void *)&q, &qn,
                   &ctx->dqf, &ctx->dq8, &ctx->diag, &P, &ctx->sweep_err, &spin, &cs};
-  return launch_coop((const void *)k_sweep_bwd_chunk, ctx->nchunks, ctx->stream, args);
+  const void *fn = ctx->sweep_w == 8 ? (const void *)k_sweep_bwd_chunk<8>
+                                      : (const void *)k_sweep_bwd_chunk<4>;
+  return launch_coop(fn, ctx->nchunks, ctx->stream, args);
 }
 
 // Reads the sweeps' error word; on a timeout, re-arms the flags so that the

@@ -248,6 +248,8 @@ __device__ __forceinline__ void dq_limit(const double *q, double *d, const Param
 #pragma unroll
         for (int k = 0; k < 5; k++) d[k] = 0.0;
       }
+    } else {
+      break;  // d unchanged: the later stages repeat this test and pass too
     }
   }
 }
