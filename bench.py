@@ -58,9 +58,14 @@ def parse():
     ap.add_argument("--size", type=int, default=64, help="hexes per cube edge (64 = 1.57M tets)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="fp64", choices=["fp64", "batched"],
+    ap.add_argument("--form", default="fp64", choices=["fp64", "batched", "mixed"],
                     help="fp64: the single-grid workload; batched: 64 uneven cases in one "
-                         "context against the same cases run one after another")
+                         "context against the same cases run one after another; mixed: the "
+                         "mixed-precision form against FP64 on the 128^3 x 6 cube")
+    ap.add_argument("--mixed-size", type=int, default=128)
+    ap.add_argument("--converge", type=int, default=0,
+                    help="mixed form: also iterate both forms to a 1e-6 residual drop "
+                         "(at most this many iterations) and time it")
     ap.add_argument("--ncase", type=int, default=64)
     return ap.parse_args()
 
@@ -402,6 +407,8 @@ def main():
     torch.cuda.set_stream(stream)
     if args.form == "batched":
         run_batched(args, rank, world, local, stream, dist)
+    elif args.form == "mixed":
+        run_mixed(args, rank, world, local, stream, dist)
     else:
         run_single(args, rank, world, local, stream, dist)
     if dist is not None:
@@ -453,6 +460,113 @@ def run_single(args, rank, world, local, stream, dist):
         }
         print(json.dumps(line), flush=True)
     s.close()
+
+
+def mixed_workload(n: int) -> dict:
+    """Cube n^3 x 6 tets, jitter 0.1h, Mach 0.8, alpha 1.25 deg, CFL 20,
+    far field on all sides, 5% density bump."""
+    return dict(name=f"cube{n}x6_M0.8_a1.25_cfl20", n=n, jitter=0.1, seed=1, mach=0.8,
+                alpha=1.25, cfl=20.0, bump_amp=0.05, bump_sigma=0.1)
+
+
+def to_drop(s, stream, target, max_iter, chunk=100):
+    """Iterate until the rho residual norm falls below target x its first
+    value; returns (iterations, device ms, drop reached)."""
+    import torch
+    first, it, ms, drop = None, 0, 0.0, 1.0
+    while it < max_iter:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nrm = s.iterate(chunk)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        if first is None:
+            first = nrm[0, 0]
+        hit = np.nonzero(nrm[:, 0] <= target * first)[0]
+        if hit.size:
+            it += int(hit[0]) + 1
+            drop = float(nrm[hit[0], 0] / first)
+            break
+        it += chunk
+        drop = float(nrm[-1, 0] / first)
+    return it, ms, drop
+
+
+def run_mixed(args, rank, world, local, stream, dist):
+    """FP64 and mixed forms on the same grid: throughput of each, the mixed
+    state's error against FP64 after the same iterations, and (--converge)
+    the iterations and time each needs for a 1e-6 residual drop."""
+    from minifs_b200 import grid as gr, meshgen
+    from minifs_b200.solver import Solver
+    wl = mixed_workload(args.mixed_size)
+    mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
+    params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+    pg = gr.prepare(mesh, params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
+    C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
+    K = int(pg.arrays["nnpc"].sum())
+    res = {}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        s = Solver(pg, params, device=local, precision=prec)
+        s.set_stream(stream.cuda_stream)
+        r = measure(s, (C, G, F, N, K, pg.n), args, stream, dist, world, local)
+        states[prec] = s.download("q")
+        r["residual_norm"] = [float(x) for x in s.residual_norm()]
+        if args.converge:
+            s2 = Solver(pg, params, device=local, precision=prec)
+            s2.set_stream(stream.cuda_stream)
+            s2.calculate_gradient()
+            it, ms, drop = to_drop(s2, stream, 1e-6, args.converge)
+            r["to_drop_1e-6"] = {"iterations": it, "ms": ms, "drop": drop,
+                                 "cell_updates_per_s": C * it / (ms / 1e3)}
+            states[prec + "_conv"] = s2.download("q")
+            s2.close()
+        res[prec] = r
+        s.close()
+    n = pg.n
+
+    from minifs_b200.compare import state_rel_err
+
+    def rel_err(a, b):
+        return state_rel_err(a, b, n, params.p_bar)
+    # same number of iterations in both forms: the warm-up, the timed steps
+    # and the phase-profile iterations of measure()
+    err_same_iters = rel_err(states["mixed"], states["fp64"])
+    err_conv = rel_err(states["mixed_conv"], states["fp64_conv"]) if args.converge else None
+    if rank == 0:
+        m, d = res["mixed"], res["fp64"]
+        info = m["info"]
+        line = {
+            "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "form": "mixed", "cells": C, "faces": F,
+                       "precision": "mixed: FP32 Roe averages/dissipation, LU-SGS off-diagonal "
+                                    "products and gradient; FP64 central flux, residual, "
+                                    "Diag, norm, update",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "l2": "no flush: working set "
+                             f"{info['device_bytes'] / 2**20:.0f} MiB > 126 MB L2",
+                       "lusgs_levels": {"forward": info["fw_levels"],
+                                        "backward": info["bw_levels"]}},
+            "fp64": {"value": d["value"], "ms_per_step": d["ms"] / args.steps,
+                     "phases": d["phases"], "to_drop_1e-6": d.get("to_drop_1e-6")},
+            "mixed_over_fp64": m["value"] / d["value"],
+            "state_rel_err_vs_fp64": {"same_iterations": err_same_iters,
+                                      "at_1e-6_drop": err_conv},
+            "roofline": m["roofline"],
+            "flux_plus_gradient": m["flux_plus_gradient"],
+            "phases": m["phases"],
+            "to_drop_1e-6": m.get("to_drop_1e-6"),
+            "cpu_baseline": None,
+            "e2e": m["e2e"],
+            "gpu_launches": m["launches"],
+            "clocks": m["clocks"],
+        }
+        print(json.dumps(line), flush=True)
 
 
 def run_batched(args, rank, world, local, stream, dist):

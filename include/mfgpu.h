@@ -108,6 +108,9 @@ typedef struct mfg_info {
   int32_t sweep_mode;               /* 0 = one launch per level, 1 = persistent */
   int32_t graph_ready;
   int32_t ncase;                    /* independent cases in the context (1 unless batched) */
+  int32_t sweep_chunks;             /* persistent sweeps: chunks (= resident blocks) */
+  int32_t sweep_lanes;              /* persistent sweeps: lanes per cell */
+  int32_t sweep_records;            /* persistent sweeps: record slots per cell (4 or 8) */
 } mfg_info;
 
 /* ---- parameters -------------------------------------------------------- */
@@ -158,6 +161,16 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info);
  * waits, with a bounded spin, for that neighbour's ready flag.  Both modes
  * give identical results. */
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode);
+/* Persistent sweeps: lanes per cell, either the record slots per cell W
+ * (shortest latency per cell) or W / 2 (twice the cells per pass over a
+ * wide level).  Results are identical either way. */
+int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes);
+/* Times n_trial fused iterations with each lane count on this context's own
+ * grid and keeps the faster (ms_out[2], optional, receives the ms per
+ * iteration of W and W / 2 lanes).  The state and the dt extrema are
+ * restored afterwards; res, dt, Diag, DQ and the gradient hold the last
+ * trial iteration's values.  iter_done: the CFL ramp position to time at. */
+int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double *ms_out);
 /* Failure-detection self-test of the bounded waits: runs a forward sweep
  * whose first chunk is withheld, so the cells that depend on it wait for
  * flags that are never set; each wait gives up after spin_cycles SM cycles.

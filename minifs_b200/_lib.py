@@ -62,7 +62,9 @@ class Info(ct.Structure):
                 ("n_bface", ct.c_int32), ("fw_levels", ct.c_int32), ("bw_levels", ct.c_int32),
                 ("max_level_cells", ct.c_int32), ("precision", ct.c_int32),
                 ("device_bytes", ct.c_int64), ("sweep_mode", ct.c_int32),
-                ("graph_ready", ct.c_int32), ("ncase", ct.c_int32)]
+                ("graph_ready", ct.c_int32), ("ncase", ct.c_int32),
+                ("sweep_chunks", ct.c_int32), ("sweep_lanes", ct.c_int32),
+                ("sweep_records", ct.c_int32)]
 
 
 class RawGrid(ct.Structure):
@@ -111,6 +113,8 @@ def load(build_if_missing: bool = True):
         "mfg_set_params": (ct.c_int, [ctxp, ct.POINTER(Params)]),
         "mfg_info_get": (ct.c_int, [ctxp, ct.POINTER(Info)]),
         "mfg_set_sweep_mode": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_set_sweep_lanes": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_autotune_sweeps": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
         "mfg_selftest_sweep_timeout": (ct.c_int, [ctxp, ct.c_int64]),
         "mfg_zero_residuals": (ct.c_int, [ctxp]),
         "mfg_inviscid_flux": (ct.c_int, [ctxp]),

@@ -1,0 +1,21 @@
+"""Comparison of flow states between the FP64 and the mixed-precision forms."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def state_rel_err(a, b, n, p_bar):
+    """Error of state a against state b (SoA rho, u, v, w, p over n cells and
+    ghosts) on physical scales: density against density, the velocity vector
+    against the speed, the gauge pressure against the absolute pressure
+    p + p_bar.  (v and the gauge p are near zero in these flows, so their
+    own magnitudes are no scale.)  Largest over the three, in the L2 and the
+    max norm."""
+    blk = [a[k * n:(k + 1) * n] - b[k * n:(k + 1) * n] for k in range(5)]
+    ref = [b[k * n:(k + 1) * n] for k in range(5)]
+    vel_d = np.sqrt(blk[1] ** 2 + blk[2] ** 2 + blk[3] ** 2)
+    vel = np.sqrt(ref[1] ** 2 + ref[2] ** 2 + ref[3] ** 2)
+    pairs = [(blk[0], ref[0]), (vel_d, vel), (blk[4], ref[4] + p_bar)]
+    l2 = max(float(np.linalg.norm(d) / np.linalg.norm(r)) for d, r in pairs)
+    mx = max(float(np.max(np.abs(d)) / np.max(np.abs(r))) for d, r in pairs)
+    return {"l2": l2, "max_norm": mx}

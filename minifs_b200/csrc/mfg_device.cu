@@ -58,7 +58,8 @@ inline int grid_for(int64_t n, int block = kBlock) {
 // Scatter SoA q (5 blocks of n) into both state buffers and derive per-cell
 // quantities.
 __global__ void k_upload_q(const double *__restrict__ soa, double *__restrict__ qa,
-                           double *__restrict__ qb, int64_t n, Params P0, Cases cs) {
+                           double *__restrict__ qb, float *__restrict__ q4a,
+                           float *__restrict__ q4b, int64_t n, Params P0, Cases cs) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double q[Q_STRIDE];
@@ -66,6 +67,8 @@ __global__ void k_upload_q(const double *__restrict__ soa, double *__restrict__ 
   cell_props(q, params_of(P0, cs, i));
   store_q(qa, i, q);
   if (qb) store_q(qb, i, q);
+  if (q4a) store_q4(q4a, i, q);
+  if (q4b) store_q4(q4b, i, q);
 }
 
 __global__ void k_download_rec(const double *__restrict__ rec, double *__restrict__ soa,
@@ -81,11 +84,57 @@ __global__ void k_arm_sentinel(int32_t C, double *__restrict__ dq8) {
   if (c < C) store_sentinel(dq8, c);
 }
 
+// End of a face gather, one cell per thread: the running dt extrema
+// (compute_timestep.cpp:914-918) and the block partial sums of res^2 for the
+// residual norm, reduced in a fixed order.
+template <bool FLUX, bool DT>
+__device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double dtc,
+                                                const double *r,
+                                                unsigned long long *__restrict__ dt_ext,
+                                                double *__restrict__ norm_part) {
+  if (DT) {
+    // dt >= 0, so the bit patterns order like the values
+    unsigned long long mx = live ? dbits(dtc) : 0ull;
+    unsigned long long mn = live ? dbits(dtc) : ~0ull;
+    // one atomic pair per warp when the warp's cells share a case (the
+    // extrema are per case), else one per cell
+    const int32_t c0 = __shfl_sync(0xffffffffu, cse, 0);
+    if (__all_sync(0xffffffffu, !live || cse == c0)) {
+      for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        atomicMax(dt_ext + 2 * c0, mx);
+        atomicMin(dt_ext + 2 * c0 + 1, mn);
+      }
+    } else if (live) {
+      atomicMax(dt_ext + 2 * cse, mx);
+      atomicMin(dt_ext + 2 * cse + 1, mn);
+    }
+  }
+  if (FLUX && norm_part) {
+    __shared__ double sh[kBlock / 32][5];
+    double s2[5];
+    for (int k = 0; k < 5; k++) s2[k] = live ? r[k] * r[k] : 0.0;
+    for (int o = 16; o > 0; o >>= 1)
+      for (int k = 0; k < 5; k++) s2[k] += __shfl_down_sync(0xffffffffu, s2[k], o);
+    if ((threadIdx.x & 31) == 0)
+      for (int k = 0; k < 5; k++) sh[threadIdx.x >> 5][k] = s2[k];
+    __syncthreads();
+    if (threadIdx.x < 5) {
+      double acc = 0.0;
+      for (int wgi = 0; wgi < kBlock / 32; wgi++) acc += sh[wgi][threadIdx.x];
+      norm_part[(int64_t)blockIdx.x * 5 + threadIdx.x] = acc;
+    }
+  }
+}
+
 // Per-cell face gather: Roe flux into the residual, local time step with
 // CellIsMG and LimitTimeStep, and the LU-SGS diagonal.  One thread per cell,
 // faces in ascending order (see the file header for why that is exact).
 template <bool FLUX, bool DT, bool DIAG>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 2)
 k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
               const double *__restrict__ q8, const double *__restrict__ vol,
               double *__restrict__ res, int res_zero, double *__restrict__ dt,
@@ -154,44 +203,83 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
     if (FLUX)
       for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
   }
-  if (DT) {
-    // running extrema (compute_timestep.cpp:914-918); dt >= 0 so the bit
-    // patterns order like the values
-    unsigned long long mx = live ? dbits(dtc) : 0ull;
-    unsigned long long mn = live ? dbits(dtc) : ~0ull;
-    // one atomic pair per warp when the warp's cells share a case (the
-    // extrema are per case), else one per cell
-    const int32_t c0 = __shfl_sync(0xffffffffu, cse, 0);
-    if (__all_sync(0xffffffffu, !live || cse == c0)) {
-      for (int o = 16; o > 0; o >>= 1) {
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
+}
+
+// Mixed form of the face gather: the Roe flux in the mixed form above; the
+// local time step and its CellIsMG switch (a discrete decision, kept in FP64
+// so that both forms take it alike), the Diag terms and all sums in FP64 in
+// the same face order.
+template <bool FLUX, bool DT, bool DIAG>
+__global__ void __launch_bounds__(kBlock, 2)
+k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+                 const double *__restrict__ q8, const double *__restrict__ vol,
+                 double *__restrict__ res, int res_zero, double *__restrict__ dt,
+                 double *__restrict__ diag, const double *__restrict__ cfl_tab,
+                 const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
+                 unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part,
+                 Cases cs) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < C;
+  const int32_t cse = live ? case_of(cs, c) : 0;
+  const Params P = live ? params_of(P0, cs, c) : P0;
+  const FluxP<float> F = flux_params<float>(P);
+  double qd[Q_STRIDE];
+  double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double dtc = 0.0;
+  if (live) {
+    load_q(q8, c, qd);
+    if (FLUX && !res_zero)
+      for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
+    const int32_t s0 = __ldg(cptr + c), s1 = __ldg(cptr + c + 1);
+    double dtl = kBig;
+    int det = 1;
+    for (int32_t s = s0; s < s1; s++) {
+      const SlotRec sr = slots[s];
+      if (FLUX || DT) {
+        double qn[Q_STRIDE];
+        load_q(q8, sr.nb, qn);
+        if (FLUX) {
+          double f[5];
+          if (sr.flags & SLOT_IS_C2) {
+            roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, F, f);
+            for (int k = 0; k < 5; k++) r[k] += f[k];
+          } else {
+            roe_flux_mx(qd, qn, sr.nx, sr.ny, sr.nz, sr.area, P, F, f);
+            for (int k = 0; k < 5; k++) r[k] -= f[k];
+          }
+        }
+        if (DT) {  // as in k_face_gather
+          double vn = qd[1] * sr.nx + qd[2] * sr.ny + qd[3] * sr.nz;
+          vn = fabs(vn);
+          const double eigv = vn + qd[Q_A];
+          dtl = smin(dtl, sr.dn / eigv);
+          const double dp = fabs(qn[4] - qd[4]) / (qn[4] + qd[4] + P.p_bar + P.p_bar);
+          if (dp > 0.1) det = 0;
+        }
       }
-      if ((threadIdx.x & 31) == 0) {
-        atomicMax(dt_ext + 2 * c0, mx);
-        atomicMin(dt_ext + 2 * c0 + 1, mn);
+    }
+    if (DT) {
+      const double cfl =
+          cfl_tab ? cfl_tab[(int64_t)(*iter_counter) * max(cs.ncase, 1) + cse] : cfl_arg;
+      dtc = dtl * local_cfl(qd[4], det, cfl, 0.5 * cfl, P);
+      dt[c] = dtc;
+    }
+    if (DIAG) {
+      const double dtv = DT ? dtc : dt[c];
+      double d = vol[c] / dtv;
+      for (int32_t s = s0; s < s1; s++) {
+        const SlotRec sr = slots[s];
+        double vn = qd[1] * sr.nx + qd[2] * sr.ny + qd[3] * sr.nz;
+        vn = fabs(vn);
+        d += 0.5 * sr.area * (vn + qd[Q_A]) * P.lhs_omga;
       }
-    } else if (live) {
-      atomicMax(dt_ext + 2 * cse, mx);
-      atomicMin(dt_ext + 2 * cse + 1, mn);
+      diag[c] = d;
     }
+    if (FLUX)
+      for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
   }
-  if (FLUX && norm_part) {
-    // per-block partial sums of res^2, reduced in a fixed order
-    __shared__ double sh[kBlock / 32][5];
-    double s2[5];
-    for (int k = 0; k < 5; k++) s2[k] = live ? r[k] * r[k] : 0.0;
-    for (int o = 16; o > 0; o >>= 1)
-      for (int k = 0; k < 5; k++) s2[k] += __shfl_down_sync(0xffffffffu, s2[k], o);
-    if ((threadIdx.x & 31) == 0)
-      for (int k = 0; k < 5; k++) sh[threadIdx.x >> 5][k] = s2[k];
-    __syncthreads();
-    if (threadIdx.x < 5) {
-      double acc = 0.0;
-      for (int wgi = 0; wgi < kBlock / 32; wgi++) acc += sh[wgi][threadIdx.x];
-      norm_part[(int64_t)blockIdx.x * 5 + threadIdx.x] = acc;
-    }
-  }
+  gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
 }
 
 // LimitTimeStep's ratio clamp (compute_timestep.cpp:929-944), per case.
@@ -357,13 +445,14 @@ struct __align__(8) PosCell {
   int32_t cell, ns;
 };
 
-// A cell is swept by a group of W lanes: lane j computes the flux of the
-// cell's record j, lane l owns the components k = l, l + W, ... < 5 of the
-// increment (the ordered sum over the records and the division), and lane 0
-// applies the limiter to the whole increment and stores it.  The operations
-// and their order per component are those of the one-thread form, so the
-// results are the same bits, while a level costs one flux and one division
-// of latency.
+// A cell is swept by a group of L lanes (L = W or W / 2, chosen per context):
+// lane l computes the fluxes of the cell's records j = l, l + L, ..., owns the
+// components k = l, l + L, ... < 5 of the increment (the ordered sum over the
+// records and the division), and lane 0 applies the limiter to the whole
+// increment and stores it.  The operations and their order per component are
+// those of the one-thread form, so the results are the same bits.  Wider
+// groups shorten a cell's latency; narrower ones let a block take more cells
+// of a wide level per pass.
 
 // Segment starts of a chunk kept in shared memory (longer chunks read the
 // rest from global memory).
@@ -372,22 +461,35 @@ constexpr int kSegCache = 512;
 constexpr int kCaseCache = 128;
 
 // What a lane knows about its group's position on a future level: the
-// position, its ring slot, the cell, the record count, this lane's neighbour
-// (flags kMark / kInRing) and that neighbour's ring slot; cell < 0 = none.
+// position, its ring slot, the cell, the record count, this lane's
+// neighbours (flags kMark / kInRing) and their ring slots; cell < 0 = none.
+template <int R>
 struct LaneRegs {
   int32_t p, slot, cell, ns;
-  uint32_t nb;
-  int32_t nslot;
+  uint32_t nb[R];
+  int32_t nslot[R];
 };
 
 // Everything a group reads for one cell that no sweep writes, staged into
-// shared memory by cp.async one level ahead: neighbour states and records
-// (lane j), the cell's state and Diag (lane 0), and res (forward) or the
-// cell's forward increment (backward), component k by lane k % W.
-template <int W>
+// shared memory by cp.async one item ahead: neighbour states and records
+// (by the lane of the record), the cell's state and Diag (lane 0), and res
+// (forward) or the cell's forward increment (backward), component k by the
+// lane that owns it.  The mixed form (MX) stages the single-precision
+// neighbour records.
+template <bool MX>
+struct SweepTypes {
+  using Q = double;
+  using Rec = SweepRec;
+};
+template <>
+struct SweepTypes<true> {
+  using Q = float;
+  using Rec = SweepRecF;
+};
+template <int W, bool MX>
 struct __align__(16) Stage {
-  double qn[W][Q_STRIDE];
-  SweepRec rec[W];
+  typename SweepTypes<MX>::Q qn[W][Q_STRIDE];
+  typename SweepTypes<MX>::Rec rec[W];
   double qc[Q_STRIDE];
   double in5[5];
   double diag;
@@ -410,17 +512,21 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int W>
+template <int W, int L>
 __device__ __forceinline__ void fetch_lane(const int32_t *s_segs, const int32_t *__restrict__ segs,
                                            int32_t sg0, int32_t sg, int32_t sg1, int32_t pbase,
                                            int32_t pos_in_level, int32_t lane,
                                            const PosCell *__restrict__ pcs,
                                            const int32_t *__restrict__ pnb,
-                                           const int32_t *__restrict__ pslot, LaneRegs &o) {
+                                           const int32_t *__restrict__ pslot,
+                                           LaneRegs<W / L> &o) {
   o.cell = -1;
   o.ns = 0;
-  o.nb = 0;
-  o.nslot = 0;
+#pragma unroll
+  for (int r = 0; r < W / L; r++) {
+    o.nb[r] = 0;
+    o.nslot[r] = 0;
+  }
   if (sg >= sg1) return;
   const int32_t i = sg - sg0;
   const int32_t a = i < kSegCache ? s_segs[i] : segs[sg];
@@ -432,24 +538,38 @@ __device__ __forceinline__ void fetch_lane(const int32_t *s_segs, const int32_t 
   o.slot = (p - pbase) & (kRing - 1);
   o.cell = x.cell;
   o.ns = x.ns;
-  o.nb = (uint32_t)pnb[(int64_t)p * W + lane];  // padding reads 0
-  o.nslot = pslot[(int64_t)p * W + lane];
+#pragma unroll
+  for (int r = 0; r < W / L; r++) {  // padding reads 0
+    o.nb[r] = (uint32_t)pnb[(int64_t)p * W + lane + L * r];
+    o.nslot[r] = pslot[(int64_t)p * W + lane + L * r];
+  }
 }
 
-template <int W, bool FWD>
-__device__ __forceinline__ void stage_copy(const LaneRegs &o, int32_t lane, Stage<W> &st,
-                                           const double *q8, const SweepRec *prec,
+template <int W, int L, bool FWD, bool MX>
+__device__ __forceinline__ void stage_copy(const LaneRegs<W / L> &o, int32_t lane,
+                                           Stage<W, MX> &st, const double *q8,
+                                           const typename SweepTypes<MX>::Q *qnb,
+                                           const typename SweepTypes<MX>::Rec *prec,
                                            const double *res, const double *diag,
                                            const double *dqf, int32_t C) {
   if (o.cell < 0) return;
-  if (lane < o.ns) {
-    const double *qs = q8 + (int64_t)(o.nb & kIdMask) * Q_STRIDE;
+  // 16-byte pieces of the neighbour record (64 B FP64, 32 B FP32) and of the
+  // sweep record (32 B, 16 B)
+  constexpr int kQ = sizeof(st.qn[0]) / 16, kR = sizeof(st.rec[0]) / 16;
 #pragma unroll
-    for (int i = 0; i < 4; i++) cp_async16(&st.qn[lane][2 * i], qs + 2 * i);
-    const double *rs = reinterpret_cast<const double *>(prec + (int64_t)o.p * W + lane);
-    double *rd = reinterpret_cast<double *>(&st.rec[lane]);
-    cp_async16(rd, rs);
-    cp_async16(rd + 2, rs + 2);
+  for (int r = 0; r < W / L; r++) {
+    const int j = lane + L * r;
+    if (j < o.ns) {
+      const char *qs =
+          reinterpret_cast<const char *>(qnb + (int64_t)(o.nb[r] & kIdMask) * Q_STRIDE);
+      char *qd = reinterpret_cast<char *>(&st.qn[j][0]);
+#pragma unroll
+      for (int i = 0; i < kQ; i++) cp_async16(qd + 16 * i, qs + 16 * i);
+      const char *rs = reinterpret_cast<const char *>(prec + (int64_t)o.p * W + j);
+      char *rd = reinterpret_cast<char *>(&st.rec[j]);
+#pragma unroll
+      for (int i = 0; i < kR; i++) cp_async16(rd + 16 * i, rs + 16 * i);
+    }
   }
   if (lane == 0) {
     const double *qs = q8 + (int64_t)o.cell * Q_STRIDE;
@@ -457,7 +577,7 @@ __device__ __forceinline__ void stage_copy(const LaneRegs &o, int32_t lane, Stag
     for (int i = 0; i < 4; i++) cp_async16(&st.qc[2 * i], qs + 2 * i);
     cp_async8(&st.diag, diag + o.cell);
   }
-  for (int k = lane; k < 5; k += W)
+  for (int k = lane; k < 5; k += L)
     cp_async8(&st.in5[k], FWD ? res + (int64_t)k * C + o.cell : dqf + (int64_t)o.cell * Q_STRIDE + k);
 }
 
@@ -493,39 +613,57 @@ __device__ __forceinline__ double clamp_limit(const Params &P,
 // 0.5 area_j F_j) / Diag, limited except for the first cell (SolveLUSGS3D
 // forward, forward_lusgs.cpp:799-870); backward: DQ = DQ* - (sum_j area_j
 // F_j) / (2 Diag), limited (:871-940).
-template <int W, bool FWD>
+template <int W, int L, bool FWD, bool MX>
 __device__ __forceinline__ void sweep_cell(
-    const LaneRegs &o, int32_t lane, const Stage<W> &st, double *sh, double *ring,
+    const LaneRegs<W / L> &o, int32_t lane, const Stage<W, MX> &st, double *sh, double *ring,
+    const double (*pre)[5],
     const double *src, double *dst, double *rearm, int32_t first_cell, const Params &P0,
     const double *s_lim, int clamp_check, double *__restrict__ dt, double *__restrict__ diag,
     const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
     const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err,
     long long spin, const Cases &cs) {
   if (o.cell < 0) return;  // the whole group
-  const unsigned gmask = ((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1));
+  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
   const int32_t c = o.cell;
   const int32_t cse = case_of(cs, c);
   const Params P = params_of(P0, cs, c);
-  // lane j < ns: w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j)
-  if (lane < o.ns) {
-    const uint32_t b = o.nb;
-    double dn[5], f[5], qn[Q_STRIDE];
-    if (b & kInRing) {
+  // record j = lane + L r < ns: w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j)
 #pragma unroll
-      for (int k = 0; k < 5; k++) dn[k] = ring[o.nslot * 5 + k];
-    } else if (b & kMark) {
-      wait_rec(src + (int64_t)(b & kIdMask) * Q_STRIDE, dn, err, spin);
-    } else {
-      const double2 *pp = reinterpret_cast<const double2 *>(src + (int64_t)b * Q_STRIDE);
-      const double2 x = pp[0], y = pp[1], z = pp[2];
-      dn[0] = x.x; dn[1] = x.y; dn[2] = y.x; dn[3] = y.y; dn[4] = z.x;
+  for (int r = 0; r < W / L; r++) {
+    const int j = lane + L * r;
+    if (j < o.ns) {
+      const uint32_t b = o.nb[r];
+      double dn[5];
+      if (b & kInRing) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) dn[k] = ring[o.nslot[r] * 5 + k];
+      } else if ((b & kMark) && !rec5_ready(pre[r])) {
+        wait_rec(src + (int64_t)(b & kIdMask) * Q_STRIDE, dn, err, spin);
+      } else {  // read at the start of the item (see sweep_chunk)
+#pragma unroll
+        for (int k = 0; k < 5; k++) dn[k] = pre[r][k];
+      }
+      if constexpr (MX) {
+        // off-diagonal product in FP32, accumulated in FP64 below
+        float qf[Q_STRIDE], df[5], ff[5];
+#pragma unroll
+        for (int k = 0; k < Q_STRIDE; k++) qf[k] = st.qn[j][k];
+#pragma unroll
+        for (int k = 0; k < 5; k++) df[k] = (float)dn[k];
+        const SweepRecF rr = st.rec[j];
+        flux_lusgs_diff(qf, df, rr.nx, rr.ny, rr.nz, flux_params<float>(P), ff);
+#pragma unroll
+        for (int k = 0; k < 5; k++) sh[j * 5 + k] = (double)(rr.w * ff[k]);
+      } else {
+        double qn[Q_STRIDE], f[5];
+#pragma unroll
+        for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[j][k];
+        const SweepRec rr = st.rec[j];
+        flux_lusgs(qn, dn, rr.nx, rr.ny, rr.nz, P, f);
+#pragma unroll
+        for (int k = 0; k < 5; k++) sh[j * 5 + k] = rr.w * f[k];
+      }
     }
-#pragma unroll
-    for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[lane][k];
-    const SweepRec r = st.rec[lane];
-    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
-#pragma unroll
-    for (int k = 0; k < 5; k++) sh[lane * 5 + k] = r.w * f[k];
   }
   // LimitTimeStep's clamp (fused forward sweep only): every component lane
   // reads dt[c] before lane 0 may write it below
@@ -542,8 +680,8 @@ __device__ __forceinline__ void sweep_cell(
     }
   }
   __syncwarp(gmask);
-  // lane l: components l, l + W, ...; records summed in order
-  for (int k = lane; k < 5; k += W) {
+  // components k = lane, lane + L, ...; records summed in order
+  for (int k = lane; k < 5; k += L) {
     double acc = FWD ? st.in5[k] : 0.0;
     for (int32_t j = 0; j < o.ns; j++) {
       if (FWD)
@@ -579,71 +717,101 @@ __device__ __forceinline__ void sweep_cell(
   __syncwarp(gmask);  // sh is free for the group's next cell
 }
 
-// One persistent sweep: block b walks chunk b level by level.  Indices of a
-// group's first position of each level are loaded two levels ahead and its
-// read-only data staged into shared memory one level ahead (cp.async), so a
-// level's critical path holds the increments it depends on and one cell's
-// arithmetic.  A level wider than the block's groups takes further passes,
-// staged and waited for on the spot.
-template <int W, bool FWD>
+// One persistent sweep: block b walks chunk b level by level.  A level of
+// more cells than the block has groups takes several passes; the group's
+// work items (level, pass) form one sequence, pipelined as a whole: indices
+// loaded two items ahead, read-only data staged into shared memory one item
+// ahead (cp.async), so that an item's critical path holds the increments it
+// depends on and one cell's arithmetic.  Blocks synchronise only between
+// levels.
+template <int W, int L, bool FWD, bool MX>
 __device__ __forceinline__ void sweep_chunk(
     const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
-    const PosCell *__restrict__ pcs, const SweepRec *__restrict__ prec,
+    const PosCell *__restrict__ pcs, const typename SweepTypes<MX>::Rec *__restrict__ prec,
     const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
-    const double *__restrict__ q8, const double *src, double *dst, double *rearm,
+    const double *__restrict__ q8, const typename SweepTypes<MX>::Q *__restrict__ qnb,
+    const double *src, double *dst, double *rearm,
     const double *__restrict__ res, const double *__restrict__ dqf_own, int32_t C,
     double *__restrict__ diag, int32_t first_cell, const Params &P0, int clamp_check,
     double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
     const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
     const double *__restrict__ vol, int *err, long long spin, const Cases &cs) {
-  constexpr int kGroups = kPersistBlock / W;
-  __shared__ Stage<W> stg[3][kGroups];
+  constexpr int kGroups = kPersistBlock / L;
+  __shared__ Stage<W, MX> stg[2][kGroups];
   __shared__ double shm[kGroups][W * 5 + 5];
   __shared__ double ring[kRing * 5];
   __shared__ int32_t s_segs[kSegCache + 1];
   __shared__ double s_lim[FWD ? kCaseCache : 1];
   const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
-  const int32_t lane = threadIdx.x & (W - 1);
-  const int32_t grp = threadIdx.x / W;
+  const int32_t lane = threadIdx.x & (L - 1);
+  const int32_t grp = threadIdx.x / L;
   for (int32_t i = threadIdx.x; i <= sg1 - sg0 && i <= kSegCache; i += blockDim.x)
     s_segs[i] = segs[sg0 + i];
   if (FWD && clamp_check)
     for (int32_t k = threadIdx.x; k < cs.ncase && k < kCaseCache; k += blockDim.x)
       s_lim[k] = clamp_limit(cs.P ? cs.P[k] : P0, dt_ext + 2 * k);
   __syncthreads();
-  const unsigned gmask = ((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1));
+  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
   double *sh = shm[grp];
   const int32_t pbase = sg1 > sg0 ? s_segs[0] : 0;
-  LaneRegs cur, nxt, far;
-  fetch_lane<W>(s_segs, segs, sg0, sg0, sg1, pbase, grp, lane, pcs, pnb, pslot, cur);
-  fetch_lane<W>(s_segs, segs, sg0, sg0 + 1, sg1, pbase, grp, lane, pcs, pnb, pslot, nxt);
-  stage_copy<W, FWD>(cur, lane, stg[0][grp], q8, prec, res, diag, dqf_own, C);
-  cp_async_commit();
-  for (int32_t sg = sg0; sg < sg1; sg++) {
-    const int par = (sg - sg0) & 1;
-    fetch_lane<W>(s_segs, segs, sg0, sg + 2, sg1, pbase, grp, lane, pcs, pnb, pslot, far);
-    stage_copy<W, FWD>(nxt, lane, stg[par ^ 1][grp], q8, prec, res, diag, dqf_own, C);
-    cp_async_commit();
-    cp_async_wait<1>();  // this level's stage
-    __syncwarp(gmask);
-    sweep_cell<W, FWD>(cur, lane, stg[par][grp], sh, ring, src, dst, rearm, first_cell, P0,
-                       s_lim, clamp_check, dt, diag, dt_ext, cptr, slots, vol, err, spin, cs);
+  // work items (level sg, pass): the same sequence in every thread of the block
+  auto seg_at = [&](int32_t sg) {
     const int32_t i = sg - sg0;
-    const int32_t a = i < kSegCache ? s_segs[i] : segs[sg];
-    const int32_t b = i + 1 <= kSegCache ? s_segs[i + 1] : segs[sg + 1];
-    for (int32_t base = a + kGroups; base < b; base += kGroups) {  // uniform over the block
-      LaneRegs e;
-      fetch_lane<W>(s_segs, segs, sg0, sg, sg1, pbase, base - a + grp, lane, pcs, pnb, pslot, e);
-      stage_copy<W, FWD>(e, lane, stg[2][grp], q8, prec, res, diag, dqf_own, C);
-      cp_async_commit();
-      cp_async_wait<0>();
-      __syncwarp(gmask);
-      sweep_cell<W, FWD>(e, lane, stg[2][grp], sh, ring, src, dst, rearm, first_cell, P0, s_lim,
-                         clamp_check, dt, diag, dt_ext, cptr, slots, vol, err, spin, cs);
+    return i <= kSegCache ? s_segs[i] : segs[sg];
+  };
+  auto advance = [&](int32_t &sg, int32_t &pass) {
+    if (sg >= sg1) return;
+    const int32_t np = (seg_at(sg + 1) - seg_at(sg) + kGroups - 1) / kGroups;
+    if (++pass >= np) {
+      ++sg;
+      pass = 0;
     }
-    __syncthreads();
+  };
+  auto fetch = [&](int32_t sg, int32_t pass, LaneRegs<W / L> &o) {
+    fetch_lane<W, L>(s_segs, segs, sg0, sg, sg1, pbase, grp + pass * kGroups, lane, pcs, pnb,
+                     pslot, o);
+  };
+  int32_t sg = sg0, pass = 0;              // this item
+  int32_t sgn = sg, passn = pass;          // the next
+  advance(sgn, passn);
+  int32_t sgf = sgn, passf = passn;        // the one after
+  advance(sgf, passf);
+  LaneRegs<W / L> cur, nxt, far;
+  fetch(sg, pass, cur);
+  fetch(sgn, passn, nxt);
+  stage_copy<W, L, FWD, MX>(cur, lane, stg[0][grp], q8, qnb, prec, res, diag, dqf_own, C);
+  cp_async_commit();
+  int par = 0;
+  while (sg < sg1) {
+    // increments this item reads from L2 (older than the ring, or produced by
+    // another chunk): requested first, so that their round trip overlaps the
+    // staging of the next items; one that still holds the sentinel is waited
+    // for in sweep_cell
+    double pre[W / L][5];
+#pragma unroll
+    for (int r = 0; r < W / L; r++) {
+      const int j = lane + L * r;
+      if (cur.cell >= 0 && j < cur.ns && !(cur.nb[r] & kInRing))
+        load_rec5_l2(src + (int64_t)(cur.nb[r] & kIdMask) * Q_STRIDE, pre[r]);
+    }
+    fetch(sgf, passf, far);
+    stage_copy<W, L, FWD, MX>(nxt, lane, stg[par ^ 1][grp], q8, qnb, prec, res, diag, dqf_own,
+                              C);
+    cp_async_commit();
+    cp_async_wait<1>();  // this item's stage
+    __syncwarp(gmask);
+    sweep_cell<W, L, FWD, MX>(cur, lane, stg[par][grp], sh, ring, pre, src, dst, rearm, first_cell,
+                              P0, s_lim, clamp_check, dt, diag, dt_ext, cptr, slots, vol, err,
+                              spin, cs);
+    if (sgn != sg) __syncthreads();  // end of a level
+    sg = sgn;
+    pass = passn;
+    sgn = sgf;
+    passn = passf;
+    advance(sgf, passf);
     cur = nxt;
     nxt = far;
+    par ^= 1;
   }
   cp_async_wait<0>();
 }
@@ -651,38 +819,43 @@ __device__ __forceinline__ void sweep_chunk(
 // Forward sweep.  chunk_skip > 0 withholds the first chunk_skip chunks
 // (failure-detection self-test only: the cells that depend on them wait
 // until the bound runs out).
-template <int W>
+template <int W, int L, bool MX>
 __global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
 k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
-                  const PosCell *__restrict__ pcs, const SweepRec *__restrict__ prec,
+                  const PosCell *__restrict__ pcs,
+                  const typename SweepTypes<MX>::Rec *__restrict__ prec,
                   const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
-                  const double *__restrict__ q8, double *dqf, double *__restrict__ dqb,
-                  const double *__restrict__ res, int32_t C, double *__restrict__ diag,
-                  int32_t first_cell, Params P0, int clamp_check, double *__restrict__ dt,
-                  const unsigned long long *__restrict__ dt_ext,
+                  const double *__restrict__ q8,
+                  const typename SweepTypes<MX>::Q *__restrict__ qnb, double *dqf,
+                  double *__restrict__ dqb, const double *__restrict__ res, int32_t C,
+                  double *__restrict__ diag, int32_t first_cell, Params P0, int clamp_check,
+                  double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
                   const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
                   const double *__restrict__ vol, int *err, long long spin,
                   int32_t chunk_skip, Cases cs) {
   if ((int32_t)blockIdx.x < chunk_skip) return;
-  sweep_chunk<W, true>(seg_begin, segs, pcs, prec, pnb, pslot, q8, dqf, dqf, dqb, res, nullptr, C,
-                       diag, first_cell, P0, clamp_check, dt, dt_ext, cptr, slots, vol, err,
-                       spin, cs);
+  sweep_chunk<W, L, true, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqf, dqf, dqb, res,
+                              nullptr, C, diag, first_cell, P0, clamp_check, dt, dt_ext, cptr,
+                              slots, vol, err, spin, cs);
 }
 
 // Backward sweep.  The state update of a cell is not needed by any later
 // level, so it runs after the block has swept its whole chunk.
-template <int W>
+template <int W, int L, bool MX>
 __global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
 k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
-                  const PosCell *__restrict__ pcs, const SweepRec *__restrict__ prec,
+                  const PosCell *__restrict__ pcs,
+                  const typename SweepTypes<MX>::Rec *__restrict__ prec,
                   const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
-                  const double *__restrict__ q8, double *__restrict__ q8_new,
+                  const double *__restrict__ q8,
+                  const typename SweepTypes<MX>::Q *__restrict__ qnb,
+                  double *__restrict__ q8_new, float *__restrict__ q4_new,
                   double *__restrict__ dqf, double *dqb, const double *__restrict__ diag,
                   Params P0, int *err, long long spin, Cases cs) {
   const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
-  sweep_chunk<W, false>(seg_begin, segs, pcs, prec, pnb, pslot, q8, dqb, dqb, dqf, nullptr, dqf,
-                        0, const_cast<double *>(diag), 0, P0, 0, nullptr, nullptr, nullptr,
-                        nullptr, nullptr, err, spin, cs);
+  sweep_chunk<W, L, false, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqb, dqb, dqf,
+                               nullptr, dqf, 0, const_cast<double *>(diag), 0, P0, 0, nullptr,
+                               nullptr, nullptr, nullptr, nullptr, err, spin, cs);
   __syncthreads();  // the chunk's increments are final
   // UpdateFlowField3D_CFL3d for the chunk's cells
   if (sg1 > sg0) {
@@ -698,6 +871,7 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
       update_cell(qc, d, P);
       cell_props(qc, P);
       store_q(q8_new, c, qc);
+      if (MX) store_q4(q4_new, c, qc);
     }
   }
 }
@@ -814,6 +988,113 @@ k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
   }
 }
 
+// Mixed form of the gradient: node values and Green-Gauss face sums in FP32
+// over the same loops as the FP64 kernels above, carried as deviations from
+// the freestream state (formed in FP64 from the FP64 records): the reference
+// state drops out of a closed cell's face sum, so FP32 rounding scales with
+// the deviations instead of with the values.  Gradients stored in FP64.
+__global__ void __launch_bounds__(kBlock)
+k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
+                 const int32_t *__restrict__ nsrc, const double *__restrict__ nw,
+                 const int32_t *__restrict__ ninfo, const double *__restrict__ wnode,
+                 const double *__restrict__ nsym, const int32_t *__restrict__ bface_c1,
+                 const double *__restrict__ q8, float *__restrict__ qn4, Params P0, Cases cs) {
+  const int32_t nd = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nd >= N) return;
+  const int32_t info = ninfo[nd];
+  float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  const int32_t e0 = nptr[nd], e1 = nptr[nd + 1];
+  // the case of a node is that of any cell it touches
+  const Params P =
+      e1 > e0 ? params_of(P0, cs, (info & 1) ? bface_c1[nsrc[e0]] : nsrc[e0]) : P0;
+  if (info & 1) {
+    for (int32_t e = e0; e < e1; e++) {
+      const int32_t k = nsrc[e];
+      const float w = (float)nw[e];
+      double qa[Q_STRIDE], qb[Q_STRIDE];
+      load_q(q8, bface_c1[k], qa);
+      load_q(q8, (int64_t)C + k, qb);
+      for (int v = 0; v < 5; v++)
+        acc[v] += (float)(0.5 * ((qa[v] - P.ref[v]) + (qb[v] - P.ref[v]))) * w;
+    }
+  } else {
+    for (int32_t e = e0; e < e1; e++) {
+      double qa[Q_STRIDE];
+      load_q(q8, nsrc[e], qa);
+      const float w = (float)nw[e];
+      for (int v = 0; v < 5; v++) acc[v] += (float)(qa[v] - P.ref[v]) * w;
+    }
+  }
+  const float rden = __fdividef(1.0f, (float)(wnode[nd] + kTiny));
+  for (int v = 0; v < 5; v++) acc[v] *= rden;
+  if (info & 2) {  // symmetry plane: remove the normal velocity (of value = ref + deviation)
+    const float xs = (float)nsym[3 * nd], ys = (float)nsym[3 * nd + 1], zs = (float)nsym[3 * nd + 2];
+    const float vn = acc[1] * xs + acc[2] * ys + acc[3] * zs +
+                     (float)(P.ref[1] * nsym[3 * nd] + P.ref[2] * nsym[3 * nd + 1] +
+                             P.ref[3] * nsym[3 * nd + 2]);
+    acc[1] -= vn * xs;
+    acc[2] -= vn * ys;
+    acc[3] -= vn * zs;
+  }
+  float4 *o = reinterpret_cast<float4 *>(qn4 + (int64_t)nd * Q_STRIDE);
+  o[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+  o[1] = make_float4(acc[4], 0.f, 0.f, 0.f);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
+                const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+                const int32_t *__restrict__ fnodes, const float *__restrict__ qn4,
+                const double *__restrict__ q8, const double *__restrict__ vol,
+                double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz,
+                Params P0, Cases cs) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  const Params P = params_of(P0, cs, c);
+  float gx[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, gy[5] = {0.f, 0.f, 0.f, 0.f, 0.f},
+        gz[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  double qc[Q_STRIDE];
+  load_q(q8, c, qc);
+  const int32_t s1 = cptr[c + 1];
+  for (int32_t s = cptr[c]; s < s1; s++) {
+    const SlotRec sr = slots[s];
+    float qs[5];
+    if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
+      double qg[Q_STRIDE];
+      load_q(q8, sr.nb, qg);
+      for (int v = 0; v < 5; v++) qs[v] = (float)(0.5 * ((qc[v] - P.ref[v]) + (qg[v] - P.ref[v])));
+    } else {
+      for (int v = 0; v < 5; v++) qs[v] = 0.f;
+      const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+      for (int32_t j = j0; j < j1; j++) {
+        const float4 *p = reinterpret_cast<const float4 *>(qn4 + (int64_t)fnodes[j] * Q_STRIDE);
+        const float4 a = __ldg(p), b = __ldg(p + 1);
+        qs[0] += a.x;
+        qs[1] += a.y;
+        qs[2] += a.z;
+        qs[3] += a.w;
+        qs[4] += b.x;
+      }
+      const float rc = __fdividef(1.0f, (float)(j1 - j0));
+      for (int v = 0; v < 5; v++) qs[v] *= rc;
+    }
+    const float sg = (sr.flags & SLOT_IS_C2) ? -(float)sr.area : (float)sr.area;
+    const float nx = (float)sr.nx, ny = (float)sr.ny, nz = (float)sr.nz;
+    for (int v = 0; v < 5; v++) {
+      const float qsum = qs[v] * sg;
+      gx[v] += qsum * nx;
+      gy[v] += qsum * ny;
+      gz[v] += qsum * nz;
+    }
+  }
+  const float rv = __fdividef(1.0f, (float)vol[c]);
+  for (int v = 0; v < 5; v++) {
+    dqdx[v * n + c] = (double)(gx[v] * rv);
+    dqdy[v * n + c] = (double)(gy[v] * rv);
+    dqdz[v * n + c] = (double)(gz[v] * rv);
+  }
+}
+
 // Residual norm from res (main.cpp:294-317) as fixed-order block partials.
 __global__ void k_norm_partial(int32_t C, const double *__restrict__ res,
                                double *__restrict__ part) {
@@ -905,10 +1186,27 @@ __global__ void k_counter_inc(int32_t *__restrict__ counter) { *counter += 1; }
 // context
 // ---------------------------------------------------------------------------
 
+// The persistent sweep kernel for (W, lanes per cell, precision).
+static const void *sweep_kernel(bool fwd, int w, int lanes, bool mx) {
+#define MFG_SK(W_, L_)                                                                       \
+  if (w == W_ && lanes == L_)                                                                \
+    return fwd ? (mx ? (const void *)k_sweep_fwd_chunk<W_, L_, true>                           \
+                     : (const void *)k_sweep_fwd_chunk<W_, L_, false>)                         \
+               : (mx ? (const void *)k_sweep_bwd_chunk<W_, L_, true>                           \
+                     : (const void *)k_sweep_bwd_chunk<W_, L_, false>);
+  MFG_SK(4, 4)
+  MFG_SK(4, 2)
+  MFG_SK(8, 8)
+  MFG_SK(8, 4)
+#undef MFG_SK
+  return nullptr;
+}
+
 struct ChunkSweep {
   int32_t *seg_begin = nullptr, *segs = nullptr, *nbs = nullptr, *nslots = nullptr;
   PosCell *cells = nullptr;
   SweepRec *recs = nullptr;
+  SweepRecF *recs_f = nullptr;  // mixed form
   int32_t nseg = 0;
 };
 
@@ -926,6 +1224,10 @@ struct mfg_ctx {
   int sweep_mode = 0;
   // device arrays
   double *q8[2] = {nullptr, nullptr};
+  // mixed form: single-precision state records (kept with q8[cur]) and node
+  // values
+  float *q4[2] = {nullptr, nullptr};
+  float *qn4 = nullptr;
   double *dq8 = nullptr, *res = nullptr, *dt = nullptr, *diag = nullptr;
   double *dqdx = nullptr, *dqdy = nullptr, *dqdz = nullptr, *qn8 = nullptr;
   double *vol = nullptr, *staging = nullptr;
@@ -947,7 +1249,9 @@ struct mfg_ctx {
   int *sweep_err = nullptr;
   int persist_grid = 0;
   int sweep_w = 0;               // records per position of the persistent sweeps (4 or 8)
-  int persist_per_sm[2] = {0, 0};  // resident blocks per SM for W = 4, 8
+  int sweep_lanes = 0;           // lanes per cell of the persistent sweeps (W or W / 2)
+  int persist_occ[2][2] = {{0, 0}, {0, 0}};  // resident blocks per SM: [W = 4, 8][W, W / 2 lanes]
+  bool lanes_ok[2] = {false, false};         // lane counts [W, W / 2] usable with the chunk grid
   int n_sm = 0;
   unsigned long long *dt_ext = nullptr;
   double *norm_part = nullptr, *norm_out = nullptr, *norm_hist = nullptr, *cfl_tab = nullptr;
@@ -1007,6 +1311,11 @@ Params make_params(const mfg_params &p) {
   P.p_max = p.p_max;
   P.p_break = p.p_break;
   P.ratio_dtmax = p.ratio_dtmax;
+  P.ref[0] = p.rho_s;
+  P.ref[1] = p.u_s;
+  P.ref[2] = p.v_s;
+  P.ref[3] = p.w_s;
+  P.ref[4] = p.p_s;
   return P;
 }
 
@@ -1160,10 +1469,22 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     for (int32_t c = 0; c < C; c++) maxns = std::max(maxns, std::max(fw_cnt[c], bw_cnt[c]));
     ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
     if (n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
-    const int per_sm = ctx->sweep_w ? ctx->persist_per_sm[ctx->sweep_w == 4 ? 0 : 1] : 0;
+    const int wi = ctx->sweep_w == 8 ? 1 : 0;
+    const int occ_w = ctx->sweep_w ? ctx->persist_occ[wi][0] : 0;
+    const int occ_h = ctx->sweep_w ? ctx->persist_occ[wi][1] : 0;
+    auto chunks_for = [&](int per_sm) {
+      return std::max(1, std::min(per_sm * ctx->n_sm, (C + kMinChunk - 1) / kMinChunk));
+    };
+    // the grid of the W-lane kernels (measured faster than a smaller grid
+    // shared with the W/2-lane ones); W/2 lanes where they fit it too, for
+    // mfg_autotune_sweeps to try
+    const int per_sm = occ_w;
     ctx->persist_grid = per_sm * ctx->n_sm;
-    ctx->nchunks = std::max(1, std::min(ctx->persist_grid, (C + kMinChunk - 1) / kMinChunk));
+    ctx->nchunks = chunks_for(per_sm);
     ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
+    ctx->lanes_ok[0] = occ_w >= per_sm && per_sm > 0;
+    ctx->lanes_ok[1] = occ_h >= per_sm && per_sm > 0;
+    ctx->sweep_lanes = ctx->sweep_w;
   }
   const int W = std::max(ctx->sweep_w, 1);
   auto make = [&](const std::vector<int32_t> &lv, const std::vector<int32_t> &cnt, bool fwd,
@@ -1307,7 +1628,15 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     if ((rc = dupload(ctx, &cs.seg_begin, seg_begin))) return rc;
     if ((rc = dupload(ctx, &cs.segs, segs))) return rc;
     if ((rc = dupload(ctx, &cs.cells, packed))) return rc;
-    if ((rc = dupload(ctx, &cs.recs, crecs))) return rc;
+    if (ctx->precision == MFG_PREC_MIXED) {
+      std::vector<SweepRecF> rf(crecs.size());
+      for (size_t i = 0; i < crecs.size(); i++)
+        rf[i] = SweepRecF{(float)crecs[i].nx, (float)crecs[i].ny, (float)crecs[i].nz,
+                          (float)crecs[i].w};
+      if ((rc = dupload(ctx, &cs.recs_f, rf))) return rc;
+    } else {
+      if ((rc = dupload(ctx, &cs.recs, crecs))) return rc;
+    }
     if ((rc = dupload(ctx, &cs.nbs, cnbs))) return rc;
     if ((rc = dupload(ctx, &cs.nslots, cslot))) return rc;
     return MFG_OK;
@@ -1419,7 +1748,7 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   *out = nullptr;
   int rc = validate_mesh(m);
   if (rc) return rc;
-  if (precision != MFG_PREC_FP64) return MFG_ERR_UNSUPPORTED;
+  if (precision != MFG_PREC_FP64 && precision != MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) {
     g_cuda_error = "no CUDA device";
@@ -1505,22 +1834,33 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
     // most as many blocks as the occupancy of the heavier kernel allows
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
-    int b[4] = {0, 0, 0, 0};
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[0], k_sweep_fwd_chunk<4>,
-                                                      kPersistBlock, 0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[1], k_sweep_bwd_chunk<4>,
-                                                      kPersistBlock, 0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[2], k_sweep_fwd_chunk<8>,
-                                                      kPersistBlock, 0) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b[3], k_sweep_bwd_chunk<8>,
-                                                      kPersistBlock, 0) != cudaSuccess)
-      return fail(MFG_ERR_CUDA);
-    ctx->persist_per_sm[0] = coop ? std::min(b[0], b[1]) : 0;
-    ctx->persist_per_sm[1] = coop ? std::min(b[2], b[3]) : 0;
+    // resident blocks per SM of each kernel pair (both sweeps)
+    const bool mx = precision == MFG_PREC_MIXED;
+    for (int wi = 0; wi < 2; wi++)
+      for (int li = 0; li < 2; li++) {
+        const int w = wi ? 8 : 4, lanes = li ? w / 2 : w;
+        int per_sm = 1 << 30;
+        for (bool fwd : {true, false}) {
+          int b = 0;
+          if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sweep_kernel(fwd, w, lanes, mx),
+                                                            kPersistBlock, 0) != cudaSuccess)
+            return fail(MFG_ERR_CUDA);
+          per_sm = std::min(per_sm, b);
+        }
+        ctx->persist_occ[wi][li] = coop ? per_sm : 0;
+      }
     ctx->n_sm = prop.multiProcessorCount;
   }
   if ((rc = build_levels(ctx, m, cptr, c2f))) return fail(rc);
   if ((rc = build_node_lists(ctx, m))) return fail(rc);
+  if (precision == MFG_PREC_MIXED) {
+    // the mixed form runs the persistent sweeps only
+    if (ctx->sweep_mode != 1) return fail(MFG_ERR_UNSUPPORTED);
+    for (int k = 0; k < 2; k++)
+      if ((rc = dalloc(ctx, &ctx->q4[k], (size_t)n * Q_STRIDE))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->qn4, (size_t)ctx->N * Q_STRIDE))) return fail(rc);
+  }
+
 
   for (int k = 0; k < 2; k++)
     if ((rc = dalloc(ctx, &ctx->q8[k], (size_t)n * Q_STRIDE))) return fail(rc);
@@ -1727,6 +2067,7 @@ int mfg_set_params(mfg_ctx *ctx, const mfg_params *p) {
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode) {
   if (!ctx || (mode != 0 && mode != 1)) return MFG_ERR_INVALID;
   if (mode == 1 && ctx->persist_grid <= 0) return MFG_ERR_UNSUPPORTED;
+  if (mode == 0 && ctx->precision == MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
   ctx->sweep_mode = mode;
   for (int k = 0; k < 2; k++)
     if (ctx->graph[k]) {
@@ -1750,6 +2091,24 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
   info->sweep_mode = ctx->sweep_mode;
   info->graph_ready = ctx->graph[0] != nullptr;
   info->ncase = ctx->ncase;
+  info->sweep_chunks = ctx->sweep_mode == 1 ? ctx->nchunks : 0;
+  info->sweep_lanes = ctx->sweep_mode == 1 ? ctx->sweep_lanes : 0;
+  info->sweep_records = ctx->sweep_w;
+  return MFG_OK;
+}
+
+int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes) {
+  if (!ctx) return MFG_ERR_INVALID;
+  if (!ctx->sweep_w || ctx->sweep_mode != 1 ||
+      !((lanes == ctx->sweep_w && ctx->lanes_ok[0]) ||
+        (lanes == ctx->sweep_w / 2 && ctx->lanes_ok[1])))
+    return MFG_ERR_UNSUPPORTED;
+  ctx->sweep_lanes = lanes;
+  for (int k = 0; k < 2; k++)
+    if (ctx->graph[k]) {
+      cudaGraphExecDestroy(ctx->graph[k]);
+      ctx->graph[k] = nullptr;
+    }
   return MFG_OK;
 }
 
@@ -1786,16 +2145,28 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
   const double *tab = use_table ? ctx->cfl_tab : nullptr;
   double *np = (flux && ctx->ncase == 1) ? ctx->norm_part : nullptr;
   const Cases cs = cases_of(ctx);
-#define MFG_FACE(F, D, G)                                                                    \
-  k_face_gather<F, D, G><<<g, kBlock, 0, st>>>(ctx->C, ctx->cptr, ctx->slots, q, ctx->vol,   \
-                                                ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,    \
-                                                ctx->diag, tab, ctx->iter_counter, cfl,      \
-                                                ctx->P, ctx->dt_ext, np, cs)
-  if (flux && dtp && diag) MFG_FACE(true, true, true);
-  else if (flux && !dtp && !diag) MFG_FACE(true, false, false);
-  else if (!flux && dtp && !diag) MFG_FACE(false, true, false);
-  else if (!flux && !dtp && diag) MFG_FACE(false, false, true);
-  else return MFG_ERR_INVALID;
+#define MFG_FACE(F, D, G)                                                                     \
+  if (ctx->precision == MFG_PREC_MIXED)                                                       \
+    k_face_gather_mx<F, D, G><<<g, kBlock, 0, st>>>(                                          \
+        ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res,                                 \
+        ctx->res_zero ? 1 : 0, ctx->dt, ctx->diag, tab, ctx->iter_counter, cfl, ctx->P,        \
+        ctx->dt_ext, np, cs);                                                                 \
+  else                                                                                        \
+    k_face_gather<F, D, G><<<g, kBlock, 0, st>>>(ctx->C, ctx->cptr, ctx->slots, q, ctx->vol,  \
+                                                 ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,   \
+                                                 ctx->diag, tab, ctx->iter_counter, cfl,     \
+                                                 ctx->P, ctx->dt_ext, np, cs)
+  if (flux && dtp && diag) {
+    MFG_FACE(true, true, true);
+  } else if (flux && !dtp && !diag) {
+    MFG_FACE(true, false, false);
+  } else if (!flux && dtp && !diag) {
+    MFG_FACE(false, true, false);
+  } else if (!flux && !dtp && diag) {
+    MFG_FACE(false, false, true);
+  } else {
+    return MFG_ERR_INVALID;
+  }
 #undef MFG_FACE
   count_launch();
   if (flux) ctx->res_zero = false;
@@ -1855,30 +2226,38 @@ static int launch_coop(const void *fn, int blocks, cudaStream_t st, void **args)
 static int launch_fwd_persist(mfg_ctx *ctx, bool clamp_check, int32_t chunk_skip,
                               long long spin) {
   const double *q = ctx->q8[ctx->cur];
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const void *qnb = mx ? (const void *)ctx->q4[ctx->cur] : (const void *)q;
   int32_t C = ctx->C, first = ctx->first_cell, skip = chunk_skip;
   int clamp = clamp_check ? 1 : 0;
   Params P = ctx->P;
   Cases cs = cases_of(ctx);
   ChunkSweep &w = ctx->fwc;
-  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, &w.nslots, (void *)&q,
-                  &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P, &clamp, &ctx->dt,
-                  &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol, &ctx->sweep_err, &spin, &skip,
-                  &cs};
-  const void *fn = ctx->sweep_w == 8 ? (const void *)k_sweep_fwd_chunk<8>
-                                      : (const void *)k_sweep_fwd_chunk<4>;
+  void *recs = mx ? (void *)w.recs_f : (void *)w.recs;
+  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &recs, &w.nbs, &w.nslots, (void *)&q,
+                  (void *)&qnb, &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P,
+                  &clamp, &ctx->dt, &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol,
+                  &ctx->sweep_err, &spin, &skip, &cs};
+  const void *fn = sweep_kernel(true, ctx->sweep_w, ctx->sweep_lanes, mx);
+  if (!fn) return MFG_ERR_UNSUPPORTED;
   return launch_coop(fn, ctx->nchunks, ctx->stream, args);
 }
 
 static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
   const double *q = ctx->q8[ctx->cur];
   double *qn = ctx->q8[ctx->cur ^ 1];
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const void *qnb = mx ? (const void *)ctx->q4[ctx->cur] : (const void *)q;
+  float *q4n = mx ? ctx->q4[ctx->cur ^ 1] : nullptr;
   Params P = ctx->P;
   Cases cs = cases_of(ctx);
   ChunkSweep &w = ctx->bwc;
-  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &w.recs, &w.nbs, &w.nslots, (void *)&q, &qn,
-                  &ctx->dqf, &ctx->dq8, &ctx->diag, &P, &ctx->sweep_err, &spin, &cs};
-  const void *fn = ctx->sweep_w == 8 ? (const void *)k_sweep_bwd_chunk<8>
-                                      : (const void *)k_sweep_bwd_chunk<4>;
+  void *recs = mx ? (void *)w.recs_f : (void *)w.recs;
+  void *args[] = {&w.seg_begin, &w.segs, &w.cells, &recs, &w.nbs, &w.nslots, (void *)&q,
+                  (void *)&qnb, &qn, &q4n, &ctx->dqf, &ctx->dq8, &ctx->diag, &P,
+                  &ctx->sweep_err, &spin, &cs};
+  const void *fn = sweep_kernel(false, ctx->sweep_w, ctx->sweep_lanes, mx);
+  if (!fn) return MFG_ERR_UNSUPPORTED;
   return launch_coop(fn, ctx->nchunks, ctx->stream, args);
 }
 
@@ -1905,6 +2284,7 @@ static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
     if (rc) return rc;
     return launch_bwd_persist(ctx, kSpinCycles);
   }
+  if (ctx->precision == MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
   cudaStream_t st = ctx->stream;
   const double *q = ctx->q8[ctx->cur];
   double *qn = ctx->q8[ctx->cur ^ 1];
@@ -1967,16 +2347,33 @@ int mfg_selftest_sweep_timeout(mfg_ctx *ctx, int64_t spin_cycles) {
   return rc2;
 }
 
+static void launch_node_values(mfg_ctx *ctx, cudaStream_t st) {
+  if (ctx->precision == MFG_PREC_MIXED)
+    k_node_values_mx<<<grid_for(ctx->N), kBlock, 0, st>>>(
+        ctx->N, ctx->C, ctx->nptr, ctx->nsrc, ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
+        ctx->bface_c1, ctx->q8[ctx->cur], ctx->qn4, ctx->P, cases_of(ctx));
+  else
+    k_node_values<<<grid_for(ctx->N), kBlock, 0, st>>>(
+        ctx->N, ctx->C, ctx->nptr, ctx->nsrc, ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
+        ctx->bface_c1, ctx->q8[ctx->cur], ctx->qn8);
+  count_launch();
+}
+
+static void launch_grad_faces(mfg_ctx *ctx, cudaStream_t st) {
+  if (ctx->precision == MFG_PREC_MIXED)
+    k_grad_faces_mx<<<grid_for(ctx->C), kBlock, 0, st>>>(
+        ctx->C, ctx->n, ctx->cptr, ctx->slots, ctx->fnptr, ctx->fnodes, ctx->qn4,
+        ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->P, cases_of(ctx));
+  else
+    k_grad_faces<<<grid_for(ctx->C), kBlock, 0, st>>>(
+        ctx->C, ctx->n, ctx->cptr, ctx->slots, ctx->fnptr, ctx->fnodes, ctx->qn8,
+        ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
+  count_launch();
+}
+
 static int launch_gradient(mfg_ctx *ctx) {
-  cudaStream_t st = ctx->stream;
-  const double *q = ctx->q8[ctx->cur];
-  k_node_values<<<grid_for(ctx->N), kBlock, 0, st>>>(ctx->N, ctx->C, ctx->nptr, ctx->nsrc,
-                                                     ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
-                                                     ctx->bface_c1, q, ctx->qn8);
-  k_grad_faces<<<grid_for(ctx->C), kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,
-                                                    ctx->fnptr, ctx->fnodes, ctx->qn8, q,
-                                                    ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
-  count_launch(2);
+  launch_node_values(ctx, ctx->stream);
+  launch_grad_faces(ctx, ctx->stream);
   return check_kernel();
 }
 
@@ -2118,6 +2515,80 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
   return check_sweep_error(ctx);
 }
 
+int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double *ms_out) {
+  if (!ctx || n_trial <= 0) return MFG_ERR_INVALID;
+  if (ctx->sweep_mode != 1 || !ctx->sweep_w) return MFG_ERR_UNSUPPORTED;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const size_t qbytes = sizeof(double) * ctx->n * Q_STRIDE;
+  const size_t q4bytes = sizeof(float) * ctx->n * Q_STRIDE;
+  // the trial iterations must leave the state as it was: save the current
+  // records and the running dt extrema
+  void *save = nullptr;
+  if (cudaMalloc(&save, qbytes + (mx ? q4bytes : 0)) != cudaSuccess) {
+    g_cuda_error = "cudaMalloc: autotune scratch";
+    return MFG_ERR_NOMEM;
+  }
+  std::vector<unsigned long long> ext(2 * ctx->ncase);
+  int rc = MFG_OK;
+  auto save_state = [&]() {
+    cudaMemcpyAsync(save, ctx->q8[ctx->cur], qbytes, cudaMemcpyDeviceToDevice, st);
+    if (mx)
+      cudaMemcpyAsync((char *)save + qbytes, ctx->q4[ctx->cur], q4bytes, cudaMemcpyDeviceToDevice,
+                      st);
+    cudaMemcpyAsync(ext.data(), ctx->dt_ext, sizeof(unsigned long long) * ext.size(),
+                    cudaMemcpyDeviceToHost, st);
+    return cudaStreamSynchronize(st) == cudaSuccess ? MFG_OK : MFG_ERR_CUDA;
+  };
+  auto restore_state = [&]() {
+    cudaMemcpyAsync(ctx->q8[ctx->cur], save, qbytes, cudaMemcpyDeviceToDevice, st);
+    if (mx)
+      cudaMemcpyAsync(ctx->q4[ctx->cur], (char *)save + qbytes, q4bytes, cudaMemcpyDeviceToDevice,
+                      st);
+    cudaMemcpyAsync(ctx->dt_ext, ext.data(), sizeof(unsigned long long) * ext.size(),
+                    cudaMemcpyHostToDevice, st);
+    return cudaStreamSynchronize(st) == cudaSuccess ? MFG_OK : MFG_ERR_CUDA;
+  };
+  const bool res_zero0 = ctx->res_zero;
+  rc = save_state();
+  const int cand[2] = {ctx->sweep_w, ctx->sweep_w / 2};
+  double ms[2] = {0.0, 0.0};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (rc == MFG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    rc = MFG_ERR_CUDA;
+  double ms_best = 1e300;
+  int best = ctx->sweep_lanes;
+  for (int k = 0; k < 2 && rc == MFG_OK; k++) {
+    ms[k] = -1.0;  // not usable with this context's chunk grid
+    if (!ctx->lanes_ok[k]) continue;
+    if ((rc = mfg_set_sweep_lanes(ctx, cand[k]))) break;
+    if ((rc = mfg_iterate(ctx, 1, iter_done, nullptr))) break;  // builds the graphs
+    cudaEventRecord(e0, st);
+    if ((rc = mfg_iterate(ctx, n_trial, iter_done + 1, nullptr))) break;
+    cudaEventRecord(e1, st);
+    float t = 0.f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+      rc = MFG_ERR_CUDA;
+    ms[k] = (double)t / n_trial;
+    if (ms[k] < ms_best) {
+      ms_best = ms[k];
+      best = cand[k];
+    }
+    if (rc == MFG_OK) rc = restore_state();
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(save);
+  ctx->res_zero = res_zero0;
+  if (rc) return rc;
+  if (ms_out) {
+    ms_out[0] = ms[0];
+    ms_out[1] = ms[1];
+  }
+  return mfg_set_sweep_lanes(ctx, best);
+}
+
 int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *phase_ms) {
   if (!ctx || n_iter <= 0 || !phase_ms) return MFG_ERR_INVALID;
   MFG_CUDA(cudaSetDevice(ctx->device));
@@ -2162,18 +2633,12 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
     }
     cudaEventRecord(ev[3], st);
     ctx->cur ^= 1;
-    const double *q2 = ctx->q8[ctx->cur];
-    k_node_values<<<grid_for(ctx->N), kBlock, 0, st>>>(ctx->N, ctx->C, ctx->nptr, ctx->nsrc,
-                                                       ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
-                                                       ctx->bface_c1, q2, ctx->qn8);
+    launch_node_values(ctx, st);
     cudaEventRecord(ev[4], st);
-    k_grad_faces<<<grid_for(ctx->C), kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,
-                                                      ctx->fnptr, ctx->fnodes, ctx->qn8, q2,
-                                                      ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
+    launch_grad_faces(ctx, st);
     cudaEventRecord(ev[5], st);
     const int rn = launch_norm_tail(ctx, st);
     cudaEventRecord(ev[6], st);
-    count_launch(2);
     if (rc == MFG_OK) rc = rn;
     if (rc == MFG_OK) rc = check_kernel();
     if (cudaEventSynchronize(ev[6]) != cudaSuccess) rc = MFG_ERR_CUDA;
@@ -2317,7 +2782,8 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
   MFG_CUDA(cudaMemcpyAsync(ctx->staging, host, sizeof(double) * 5 * n, cudaMemcpyHostToDevice,
                            st));
   k_upload_q<<<grid_for(n), kBlock, 0, st>>>(ctx->staging, ctx->q8[ctx->cur],
-                                            ctx->q8[ctx->cur ^ 1], n, ctx->P, cases_of(ctx));
+                                            ctx->q8[ctx->cur ^ 1], ctx->q4[ctx->cur],
+                                            ctx->q4[ctx->cur ^ 1], n, ctx->P, cases_of(ctx));
   count_launch();
   MFG_CUDA(cudaGetLastError());
   return MFG_OK;

@@ -49,9 +49,15 @@ struct __align__(16) SweepRec {
   double nx, ny, nz, w;
 };
 
+// Mixed form: single-precision LU-SGS sweep record.
+struct __align__(16) SweepRecF {
+  float nx, ny, nz, w;
+};
+
 struct Params {
   double gam, gamm1, p_bar, alf_l, lhs_omga, peff;
   double rho_min, rho_max, p_min, p_max, p_break, ratio_dtmax;
+  double ref[5];  // freestream rho, u, v, w, gauge p (mixed gradient: values kept as deviations)
 };
 
 // Batched cases: several independent grids concatenated into one (cells,
@@ -73,6 +79,20 @@ __device__ __forceinline__ Params params_of(const Params &P0, const Cases &cs, i
 }
 
 __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+
+// Single-precision state record of the mixed form (32 bytes, same fields as
+// the FP64 record, rounded from it after every update).
+__device__ __forceinline__ void load_q4(const float *__restrict__ q4, int64_t c, float *q) {
+  const float4 *p = reinterpret_cast<const float4 *>(q4 + c * Q_STRIDE);
+  const float4 a = __ldg(p), b = __ldg(p + 1);
+  q[0] = a.x; q[1] = a.y; q[2] = a.z; q[3] = a.w;
+  q[4] = b.x; q[5] = b.y; q[6] = b.z; q[7] = b.w;
+}
+__device__ __forceinline__ void store_q4(float *q4, int64_t c, const double *q) {
+  float4 *p = reinterpret_cast<float4 *>(q4 + c * Q_STRIDE);
+  p[0] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+  p[1] = make_float4((float)q[4], (float)q[5], (float)q[6], (float)q[7]);
+}
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 
 __device__ __forceinline__ void load_q(const double *__restrict__ q8, int64_t c, double *q) {
@@ -120,73 +140,100 @@ __device__ __forceinline__ void cell_props(double *q, const Params &P) {
   q[Q_E] = p / P.gamm1 + rv2;
 }
 
+// Arithmetic of the flux routines in T = double (the FP64 form: exactly the
+// reference's operations) or T = float (the mixed form: single-precision
+// flux arithmetic with hardware reciprocal-based division).
+template <typename T>
+struct Num;
+template <>
+struct Num<double> {
+  __device__ static __forceinline__ double div(double a, double b) { return a / b; }
+  __device__ static __forceinline__ double sqrt_(double a) { return sqrt(a); }
+};
+template <>
+struct Num<float> {
+  __device__ static __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+  __device__ static __forceinline__ float sqrt_(float a) { return sqrtf(a); }
+};
+
+// The parameters the flux routines read, in T.
+template <typename T>
+struct FluxP {
+  T gamm1, alf_l, lhs_omga, peff, tiny;
+};
+template <typename T>
+__device__ __forceinline__ FluxP<T> flux_params(const Params &P) {
+  return FluxP<T>{(T)P.gamm1, (T)P.alf_l, (T)P.lhs_omga, (T)P.peff, (T)kTiny};
+}
+
 // RoeFlux_noprec serial body (cal_flux.cpp:676-834) for one face with
 // first-order face states ql = q[c1], qr = q[c2]; includes the 0.5*area
 // factor.  ht_l / ht_r come precomputed from the cell records.
-__device__ __forceinline__ void roe_flux(const double *ql, const double *qr, double areax,
-                                         double areay, double areaz, double area,
-                                         const Params &P, double *flux) {
-  const double ht_l = ql[Q_HT], ht_r = qr[Q_HT];
-  const double vn_l = areax * ql[1] + areay * ql[2] + areaz * ql[3];
-  const double vn_r = areax * qr[1] + areay * qr[2] + areaz * qr[3];
-  double tmp0 = vn_l * ql[0];
-  double tmp1 = vn_r * qr[0];
-  double f0 = tmp0 + tmp1;
-  double f1 = tmp0 * ql[1] + areax * ql[4] + tmp1 * qr[1] + areax * qr[4];
-  double f2 = tmp0 * ql[2] + areay * ql[4] + tmp1 * qr[2] + areay * qr[4];
-  double f3 = tmp0 * ql[3] + areaz * ql[4] + tmp1 * qr[3] + areaz * qr[4];
-  double f4 = ht_l * vn_l + ht_r * vn_r;
+template <typename T>
+__device__ __forceinline__ void roe_flux_t(const T *ql, const T *qr, T areax, T areay, T areaz,
+                                           T area, const FluxP<T> &P, T *flux) {
+  using N = Num<T>;
+  const T ht_l = ql[Q_HT], ht_r = qr[Q_HT];
+  const T vn_l = areax * ql[1] + areay * ql[2] + areaz * ql[3];
+  const T vn_r = areax * qr[1] + areay * qr[2] + areaz * qr[3];
+  T tmp0 = vn_l * ql[0];
+  T tmp1 = vn_r * qr[0];
+  T f0 = tmp0 + tmp1;
+  T f1 = tmp0 * ql[1] + areax * ql[4] + tmp1 * qr[1] + areax * qr[4];
+  T f2 = tmp0 * ql[2] + areay * ql[4] + tmp1 * qr[2] + areay * qr[4];
+  T f3 = tmp0 * ql[3] + areaz * ql[4] + tmp1 * qr[3] + areaz * qr[4];
+  T f4 = ht_l * vn_l + ht_r * vn_r;
 
-  tmp0 = sqrt(qr[0] / ql[0]);
-  tmp1 = 1.0 / (1.0 + tmp0);
-  const double rho_a = sqrt(qr[0] * ql[0]);
-  const double u_a = (ql[1] + qr[1] * tmp0) * tmp1;
-  const double v_a = (ql[2] + qr[2] * tmp0) * tmp1;
-  const double w_a = (ql[3] + qr[3] * tmp0) * tmp1;
-  const double vn_a = u_a * areax + v_a * areay + w_a * areaz;
-  const double h_a = (ht_l / ql[0] + ht_r / qr[0] * tmp0) * tmp1;
+  tmp0 = N::sqrt_(N::div(qr[0], ql[0]));
+  tmp1 = N::div(T(1.0), T(1.0) + tmp0);
+  const T rho_a = N::sqrt_(qr[0] * ql[0]);
+  const T u_a = (ql[1] + qr[1] * tmp0) * tmp1;
+  const T v_a = (ql[2] + qr[2] * tmp0) * tmp1;
+  const T w_a = (ql[3] + qr[3] * tmp0) * tmp1;
+  const T vn_a = u_a * areax + v_a * areay + w_a * areaz;
+  const T h_a = (N::div(ht_l, ql[0]) + N::div(ht_r, qr[0]) * tmp0) * tmp1;
 
-  const double q2 = 0.5 * (u_a * u_a + v_a * v_a + w_a * w_a);
-  double c2_a = P.gamm1 * (h_a - q2);
+  const T q2 = T(0.5) * (u_a * u_a + v_a * v_a + w_a * w_a);
+  T c2_a = P.gamm1 * (h_a - q2);
   c2_a = fabs(c2_a);
-  const double c_a = sqrt(c2_a);
+  const T c_a = N::sqrt_(c2_a);
 
-  double eigv1 = fabs(vn_a);
-  double eigv2 = fabs(vn_a + c_a);
-  double eigv3 = fabs(vn_a - c_a);
+  T eigv1 = fabs(vn_a);
+  T eigv2 = fabs(vn_a + c_a);
+  T eigv3 = fabs(vn_a - c_a);
 
-  const double spectral = fabs(u_a) + fabs(v_a) + fabs(w_a) + c_a;
-  const double epsaa = P.alf_l * spectral;
-  const double epsbb = 0.25 / smax(epsaa, kTiny);
-  const double epscc = 2.0 * epsaa;
+  const T spectral = fabs(u_a) + fabs(v_a) + fabs(w_a) + c_a;
+  const T epsaa = P.alf_l * spectral;
+  const T epsbb = N::div(T(0.25), (epsaa < P.tiny) ? P.tiny : epsaa);  // smax(epsaa, tiny)
+  const T epscc = T(2.0) * epsaa;
   if (eigv1 < epscc) eigv1 = eigv1 * eigv1 * epsbb + epsaa;
   if (eigv2 < epscc) eigv2 = eigv2 * eigv2 * epsbb + epsaa;
   if (eigv3 < epscc) eigv3 = eigv3 * eigv3 * epsbb + epsaa;
 
-  const double drho = qr[0] - ql[0];
-  const double du = qr[1] - ql[1];
-  const double dv = qr[2] - ql[2];
-  const double dw = qr[3] - ql[3];
-  const double dp = qr[4] - ql[4];
-  const double dvn = vn_r - vn_l;
-  const double dq2 = u_a * du + v_a * dv + w_a * dw;
+  const T drho = qr[0] - ql[0];
+  const T du = qr[1] - ql[1];
+  const T dv = qr[2] - ql[2];
+  const T dw = qr[3] - ql[3];
+  const T dp = qr[4] - ql[4];
+  const T dvn = vn_r - vn_l;
+  const T dq2 = u_a * du + v_a * dv + w_a * dw;
 
-  tmp0 = dp / c2_a;
-  tmp1 = rho_a * dvn / c_a;
-  const double alpha1 = (drho - tmp0) * eigv1;
-  const double alpha2 = 0.5 * (tmp0 + tmp1) * eigv2;
-  const double alpha3 = 0.5 * (tmp0 - tmp1) * eigv3;
+  tmp0 = N::div(dp, c2_a);
+  tmp1 = N::div(rho_a * dvn, c_a);
+  const T alpha1 = (drho - tmp0) * eigv1;
+  const T alpha2 = T(0.5) * (tmp0 + tmp1) * eigv2;
+  const T alpha3 = T(0.5) * (tmp0 - tmp1) * eigv3;
 
   tmp0 = alpha1 + alpha2 + alpha3;
   tmp1 = eigv1 * rho_a;
-  const double tmp2 = -tmp1 * dvn + (alpha2 - alpha3) * c_a;
+  const T tmp2 = -tmp1 * dvn + (alpha2 - alpha3) * c_a;
   f0 -= tmp0;
   f1 -= tmp0 * u_a + tmp1 * du + tmp2 * areax;
   f2 -= tmp0 * v_a + tmp1 * dv + tmp2 * areay;
   f3 -= tmp0 * w_a + tmp1 * dw + tmp2 * areaz;
   f4 -= alpha1 * q2 + (alpha2 + alpha3) * h_a + tmp1 * dq2 + tmp2 * vn_a;
 
-  const double half = 0.5 * area;
+  const T half = T(0.5) * area;
   flux[0] = f0 * half;
   flux[1] = f1 * half;
   flux[2] = f2 * half;
@@ -194,33 +241,41 @@ __device__ __forceinline__ void roe_flux(const double *ql, const double *qr, dou
   flux[4] = f4 * half;
 }
 
+__device__ __forceinline__ void roe_flux(const double *ql, const double *qr, double areax,
+                                         double areay, double areaz, double area,
+                                         const Params &P, double *flux) {
+  roe_flux_t<double>(ql, qr, areax, areay, areaz, area, flux_params<double>(P), flux);
+}
+
 // FluxLUSGS3D (forward_lusgs.cpp:1271-1324) with the neighbour's sound speed
 // and conserved energy taken from its record (same expressions).
-__device__ __forceinline__ void flux_lusgs(const double *q, const double *DQ, double nx, double ny,
-                                           double nz, const Params &P, double *flux) {
-  const double gam1 = P.gamm1;
-  double Q0 = q[0], Q1 = q[0] * q[1], Q2 = q[0] * q[2], Q3 = q[0] * q[3];
-  double Q4 = q[Q_E];
-  double p = q[4];
-  double v_n = q[1] * nx + q[2] * ny + q[3] * nz;
-  double eig = fabs(v_n) + q[Q_A];
+template <typename T>
+__device__ __forceinline__ void flux_lusgs_t(const T *q, const T *DQ, T nx, T ny, T nz,
+                                             const FluxP<T> &P, T *flux) {
+  using N = Num<T>;
+  const T gam1 = P.gamm1;
+  T Q0 = q[0], Q1 = q[0] * q[1], Q2 = q[0] * q[2], Q3 = q[0] * q[3];
+  T Q4 = q[Q_E];
+  T p = q[4];
+  T v_n = q[1] * nx + q[2] * ny + q[3] * nz;
+  T eig = fabs(v_n) + q[Q_A];
   eig *= P.lhs_omga;
-  const double peff = P.peff;
-  double f1 = -Q1 * v_n - p * nx;
-  double f2 = -Q2 * v_n - p * ny;
-  double f3 = -Q3 * v_n - p * nz;
-  double f4 = -(Q4 + p + peff) * v_n;
+  const T peff = P.peff;
+  T f1 = -Q1 * v_n - p * nx;
+  T f2 = -Q2 * v_n - p * ny;
+  T f3 = -Q3 * v_n - p * nz;
+  T f4 = -(Q4 + p + peff) * v_n;
   Q0 += DQ[0];
   Q1 += DQ[1];
   Q2 += DQ[2];
   Q3 += DQ[3];
   Q4 += DQ[4];
-  const double rv2 = 0.5 * (Q1 * Q1 + Q2 * Q2 + Q3 * Q3) / Q0;
+  const T rv2 = N::div(T(0.5) * (Q1 * Q1 + Q2 * Q2 + Q3 * Q3), Q0);
   p = gam1 * (Q4 - rv2);
-  double f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
+  T f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
   v_n *= q[0];
   v_n += f0;
-  v_n /= Q0;
+  v_n = N::div(v_n, Q0);
   f1 += Q1 * v_n + p * nx;
   f2 += Q2 * v_n + p * ny;
   f3 += Q3 * v_n + p * nz;
@@ -230,6 +285,112 @@ __device__ __forceinline__ void flux_lusgs(const double *q, const double *DQ, do
   flux[2] = f2 - eig * DQ[2];
   flux[3] = f3 - eig * DQ[3];
   flux[4] = f4 - eig * DQ[4];
+}
+
+__device__ __forceinline__ void flux_lusgs(const double *q, const double *DQ, double nx, double ny,
+                                           double nz, const Params &P, double *flux) {
+  flux_lusgs_t<double>(q, DQ, nx, ny, nz, flux_params<double>(P), flux);
+}
+
+// Mixed form of RoeFlux_noprec: the central part (the two one-sided fluxes)
+// in FP64 with the FP64 expressions above, so that a closed cell of uniform
+// state still sums to zero; the Roe average, eigenvalues and dissipation (the
+// square roots and divisions) in FP32 from state differences formed in FP64,
+// so that the FP32 rounding scales with the jump across the face.
+__device__ __forceinline__ void roe_flux_mx(const double *ql, const double *qr, double areax,
+                                           double areay, double areaz, double area,
+                                           const Params &P, const FluxP<float> &F,
+                                           double *flux) {
+  const double vn_l = areax * ql[1] + areay * ql[2] + areaz * ql[3];
+  const double vn_r = areax * qr[1] + areay * qr[2] + areaz * qr[3];
+  double tmp0 = vn_l * ql[0];
+  double tmp1 = vn_r * qr[0];
+  double f0 = tmp0 + tmp1;
+  double f1 = tmp0 * ql[1] + areax * ql[4] + tmp1 * qr[1] + areax * qr[4];
+  double f2 = tmp0 * ql[2] + areay * ql[4] + tmp1 * qr[2] + areay * qr[4];
+  double f3 = tmp0 * ql[3] + areaz * ql[4] + tmp1 * qr[3] + areaz * qr[4];
+  double f4 = ql[Q_HT] * vn_l + qr[Q_HT] * vn_r;
+
+  const float nx = (float)areax, ny = (float)areay, nz = (float)areaz;
+  const float rl = (float)ql[0], rr = (float)qr[0];
+  const float t0 = sqrtf(__fdividef(rr, rl));
+  const float t1 = __fdividef(1.0f, 1.0f + t0);
+  const float rho_a = sqrtf(rr * rl);
+  const float u_a = ((float)ql[1] + (float)qr[1] * t0) * t1;
+  const float v_a = ((float)ql[2] + (float)qr[2] * t0) * t1;
+  const float w_a = ((float)ql[3] + (float)qr[3] * t0) * t1;
+  const float vn_a = u_a * nx + v_a * ny + w_a * nz;
+  const float h_a =
+      (__fdividef((float)ql[Q_HT], rl) + __fdividef((float)qr[Q_HT], rr) * t0) * t1;
+  const float q2 = 0.5f * (u_a * u_a + v_a * v_a + w_a * w_a);
+  const float c2_a = fabsf(F.gamm1 * (h_a - q2));
+  const float c_a = sqrtf(c2_a);
+  float eigv1 = fabsf(vn_a);
+  float eigv2 = fabsf(vn_a + c_a);
+  float eigv3 = fabsf(vn_a - c_a);
+  const float spectral = fabsf(u_a) + fabsf(v_a) + fabsf(w_a) + c_a;
+  const float epsaa = F.alf_l * spectral;
+  const float epsbb = __fdividef(0.25f, fmaxf(epsaa, F.tiny));
+  const float epscc = 2.0f * epsaa;
+  if (eigv1 < epscc) eigv1 = eigv1 * eigv1 * epsbb + epsaa;
+  if (eigv2 < epscc) eigv2 = eigv2 * eigv2 * epsbb + epsaa;
+  if (eigv3 < epscc) eigv3 = eigv3 * eigv3 * epsbb + epsaa;
+  const float drho = (float)(qr[0] - ql[0]);
+  const float du = (float)(qr[1] - ql[1]);
+  const float dv = (float)(qr[2] - ql[2]);
+  const float dw = (float)(qr[3] - ql[3]);
+  const float dp = (float)(qr[4] - ql[4]);
+  const float dvn = (float)(vn_r - vn_l);
+  const float dq2 = u_a * du + v_a * dv + w_a * dw;
+  const float a0 = __fdividef(dp, c2_a);
+  const float a1 = __fdividef(rho_a * dvn, c_a);
+  const float alpha1 = (drho - a0) * eigv1;
+  const float alpha2 = 0.5f * (a0 + a1) * eigv2;
+  const float alpha3 = 0.5f * (a0 - a1) * eigv3;
+  const float s0 = alpha1 + alpha2 + alpha3;
+  const float s1 = eigv1 * rho_a;
+  const float s2 = -s1 * dvn + (alpha2 - alpha3) * c_a;
+  f0 -= (double)s0;
+  f1 -= (double)(s0 * u_a + s1 * du + s2 * nx);
+  f2 -= (double)(s0 * v_a + s1 * dv + s2 * ny);
+  f3 -= (double)(s0 * w_a + s1 * dw + s2 * nz);
+  f4 -= (double)(alpha1 * q2 + (alpha2 + alpha3) * h_a + s1 * dq2 + s2 * vn_a);
+  const double half = 0.5 * area;
+  flux[0] = f0 * half;
+  flux[1] = f1 * half;
+  flux[2] = f2 * half;
+  flux[3] = f3 * half;
+  flux[4] = f4 * half;
+}
+
+// Mixed form of FluxLUSGS3D: F(Q + DQ) - F(Q) - eig DQ (forward_lusgs.cpp
+// :1271-1324) in FP32, written in difference form so that every term is
+// formed from DQ directly: a zero increment gives exactly zero and the
+// rounding scales with the increment instead of with F.  With m = rho vn and
+// M = rho (u, v, w): vn' - vn = (DQ.n - vn DQ0) / Q0', rv2' - rv2 = (rho u.dM
+// + |dM|^2 / 2 - rho |u|^2 DQ0 / 2) / Q0', p' - p = gam1 (DQ4 - (rv2' - rv2)).
+__device__ __forceinline__ void flux_lusgs_diff(const float *q, const float *DQ, float nx,
+                                               float ny, float nz, const FluxP<float> &P,
+                                               float *flux) {
+  const float rho = q[0], u = q[1], v = q[2], w = q[3];
+  const float vn = u * nx + v * ny + w * nz;
+  const float eig = (fabsf(vn) + q[Q_A]) * P.lhs_omga;
+  const float rq0n = __fdividef(1.0f, rho + DQ[0]);
+  const float f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
+  const float dvn = (f0 - vn * DQ[0]) * rq0n;
+  const float vnn = vn + dvn;
+  const float udm = u * DQ[1] + v * DQ[2] + w * DQ[3];
+  const float dm2 = DQ[1] * DQ[1] + DQ[2] * DQ[2] + DQ[3] * DQ[3];
+  const float uu = u * u + v * v + w * w;
+  const float drv2 = (rho * udm + 0.5f * dm2 - 0.5f * rho * uu * DQ[0]) * rq0n;
+  const float dp = P.gamm1 * (DQ[4] - drv2);
+  const float H = q[Q_E] + q[4] + P.peff;
+  const float dH = DQ[4] + dp;
+  flux[0] = f0 - eig * DQ[0];
+  flux[1] = rho * u * dvn + DQ[1] * vnn + dp * nx - eig * DQ[1];
+  flux[2] = rho * v * dvn + DQ[2] * vnn + dp * ny - eig * DQ[2];
+  flux[3] = rho * w * dvn + DQ[3] * vnn + dp * nz - eig * DQ[3];
+  flux[4] = H * dvn + dH * vnn - eig * DQ[4];
 }
 
 // DQ_limit == 2 positivity limiter (forward_lusgs.cpp:939-973, :1184-1218).

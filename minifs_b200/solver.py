@@ -117,6 +117,20 @@ class Solver:
         """0 = one kernel per LU-SGS level, 1 = persistent dataflow sweeps."""
         self._call("mfg_set_sweep_mode", int(mode))
 
+    def set_sweep_lanes(self, lanes: int):
+        """Persistent sweeps: lanes per cell (W or W / 2)."""
+        self._call("mfg_set_sweep_lanes", int(lanes))
+
+    def autotune_sweeps(self, n_trial: int = 3) -> dict:
+        """Time both lane counts on this grid and keep the faster; the state
+        is left as it was.  Returns the choice and the ms per iteration."""
+        ms = np.zeros(2)
+        self._call("mfg_autotune_sweeps", int(n_trial), int(self.iter_done), _lib.ptr(ms))
+        info = self.info()
+        w = info["sweep_records"]
+        return {"lanes_per_cell": info["sweep_lanes"], "chunks": info["sweep_chunks"],
+                "ms_per_iter": {str(w): float(ms[0]), str(w // 2): float(ms[1])}}
+
     def selftest_sweep_timeout(self, spin_cycles: int = 2_000_000) -> int:
         """Run the bounded-wait self-test; returns the status code."""
         return int(self.lib.mfg_selftest_sweep_timeout(self._ctx, int(spin_cycles)))

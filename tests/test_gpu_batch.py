@@ -100,3 +100,41 @@ def test_batch_upload_round_trip_and_limits():
     with pytest.raises(_lib.MfgError):
         b._call("mfg_set_params", b.params_list[0])
     b.close()
+
+
+def test_sweep_lanes_identical_and_autotune_restores_state():
+    """A wide-level grid (24 cases of 24^3 x 6 cells: ~20k cells per LU-SGS
+    level; mixed form, whose W/2-lane sweeps fit the same chunk grid) sweeps
+    with W or W/2 lanes per cell to the same bits.  The autotuner times both
+    and leaves the state and dt extrema as they were."""
+    from minifs_b200 import grid as gr, meshgen
+    from minifs_b200.solver import BatchSolver
+    grids, params = [], []
+    for k in range(24):
+        m = meshgen.cube_mesh(24, jitter=0.1, seed=100 + k)
+        p = gr.make_params(mach=0.4 + 0.01 * k, alpha=1.0, cfl_start=10.0)
+        grids.append(gr.prepare(m, p, bump_amp=0.05, bump_sigma=0.1))
+        params.append(p)
+    a = BatchSolver(grids, params, precision="mixed")
+    info = a.info()
+    w = info["sweep_records"]
+    assert info["sweep_lanes"] == w, info
+    b = BatchSolver(grids, params, precision="mixed")
+    b.set_sweep_lanes(w // 2)
+    for s in (a, b):
+        s.calculate_gradient()
+        s.iterate(3)
+    for f in ("q", "dq", "diag", "res"):
+        assert_bitwise(a.download(f), b.download(f), f"lanes {w} vs {w // 2}: {f}")
+    q0, e0 = a.download("q"), a.dt_extrema
+    tuned = a.autotune_sweeps(2)
+    assert set(tuned["ms_per_iter"]) == {str(w), str(w // 2)}
+    assert all(v > 0 for v in tuned["ms_per_iter"].values())
+    assert tuned["lanes_per_cell"] in (w, w // 2)
+    assert_bitwise(a.download("q"), q0, "state after autotune")
+    assert a.dt_extrema == e0
+    a.iterate(2)
+    b.iterate(2)
+    assert_bitwise(a.download("q"), b.download("q"), "after autotune")
+    a.close()
+    b.close()

@@ -68,3 +68,21 @@ def test_bad_volume_is_reported():
     with pytest.raises(_lib.MfgError) as e:
         gr.prepare(m, p)
     assert e.value.code == -7
+
+
+def test_state_rel_err_scales():
+    """The FP64/mixed comparison measures velocity against the speed and the
+    gauge pressure against the absolute pressure."""
+    import numpy as np
+    from minifs_b200.compare import state_rel_err
+    n = 4
+    b = np.concatenate([np.full(n, 1.2), np.full(n, 1.0), np.zeros(n), np.full(n, 0.02),
+                        np.zeros(n)])
+    a = b.copy()
+    a[2 * n] = 1e-6           # v: 1e-6 against a speed of ~1
+    a[4 * n + 1] = 2e-6       # gauge p: 2e-6 against p + p_bar = 2
+    e = state_rel_err(a, b, n, 2.0)
+    # velocity 1e-6 / |(1, 0, 0.02)|, pressure 2e-6 / 2: the larger
+    assert abs(e["max_norm"] - max(1e-6 / np.hypot(1.0, 0.02), 1e-6)) < 1e-15
+    assert e["l2"] < 1e-6 and e["l2"] > 0
+    assert state_rel_err(b, b, n, 2.0) == {"l2": 0.0, "max_norm": 0.0}
