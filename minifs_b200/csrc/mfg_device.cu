@@ -665,8 +665,9 @@ __device__ __forceinline__ void sweep_cell(
       }
     }
   }
-  // LimitTimeStep's clamp (fused forward sweep only): every component lane
-  // reads dt[c] before lane 0 may write it below
+  // LimitTimeStep's clamp (fused forward sweep, and only when some case's
+  // dt ratio exceeds its limit): every component lane reads dt[c] before
+  // lane 0 may write it below
   double dg = st.diag, lim = -1.0;
   bool clamped = false;
   if (FWD && clamp_check && lane < 5) {
@@ -680,40 +681,54 @@ __device__ __forceinline__ void sweep_cell(
     }
   }
   __syncwarp(gmask);
-  // components k = lane, lane + L, ...; records summed in order
-  for (int k = lane; k < 5; k += L) {
-    double acc = FWD ? st.in5[k] : 0.0;
+  // components k = lane, lane + L, ... < 5 (at most two per lane, as two
+  // independent chains); records summed in order
+  {
+    constexpr int kC = (5 + L - 1) / L;
+    double acc[kC];
+#pragma unroll
+    for (int i = 0; i < kC; i++) {
+      const int k = lane + L * i;
+      acc[i] = (FWD && k < 5) ? st.in5[k] : 0.0;
+    }
     for (int32_t j = 0; j < o.ns; j++) {
-      if (FWD)
-        acc -= sh[j * 5 + k];
-      else
-        acc += sh[j * 5 + k];
+#pragma unroll
+      for (int i = 0; i < kC; i++) {
+        const int k = lane + L * i;
+        if (k < 5) {
+          if (FWD)
+            acc[i] -= sh[j * 5 + k];
+          else
+            acc[i] += sh[j * 5 + k];
+        }
+      }
     }
-    if (FWD) {
-      acc /= dg;
-    } else {
-      const double tmp = 2.0 * st.diag;
-      acc = st.in5[k] - acc / tmp;
+    const double tmp = 2.0 * st.diag;
+#pragma unroll
+    for (int i = 0; i < kC; i++) {
+      const int k = lane + L * i;
+      if (k < 5) sh[W * 5 + k] = FWD ? acc[i] / dg : st.in5[k] - acc[i] / tmp;
     }
-    sh[W * 5 + k] = acc;
   }
   __syncwarp(gmask);
+  // the limiter on every lane (same values), the stores spread over the lanes
+  double d[5], qc[Q_STRIDE];
+#pragma unroll
+  for (int k = 0; k < 5; k++) d[k] = sh[W * 5 + k];
+#pragma unroll
+  for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
+  if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit(qc, d, P);
   if (lane == 0) {
     if (FWD && clamped) {
       dt[c] = lim;
       diag[c] = dg;
     }
-    double d[5], qc[Q_STRIDE];
-#pragma unroll
-    for (int k = 0; k < 5; k++) d[k] = sh[W * 5 + k];
-#pragma unroll
-    for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
-    if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit(qc, d, P);
     store_dq(dst, c, d);
-    store_sentinel(rearm, c);  // armed for the other sweep
-#pragma unroll
-    for (int k = 0; k < 5; k++) ring[o.slot * 5 + k] = d[k];
   }
+  if (lane == (L > 1 ? 1 : 0)) store_sentinel(rearm, c);  // armed for the other sweep
+#pragma unroll
+  for (int k = 0; k < 5; k++)
+    if (k % L == lane) ring[o.slot * 5 + k] = d[k];
   __syncwarp(gmask);  // sh is free for the group's next cell
 }
 
@@ -747,10 +762,18 @@ __device__ __forceinline__ void sweep_chunk(
   const int32_t grp = threadIdx.x / L;
   for (int32_t i = threadIdx.x; i <= sg1 - sg0 && i <= kSegCache; i += blockDim.x)
     s_segs[i] = segs[sg0 + i];
-  if (FWD && clamp_check)
-    for (int32_t k = threadIdx.x; k < cs.ncase && k < kCaseCache; k += blockDim.x)
-      s_lim[k] = clamp_limit(cs.P ? cs.P[k] : P0, dt_ext + 2 * k);
+  __shared__ int s_clamp_any;
+  if (threadIdx.x == 0) s_clamp_any = 0;
   __syncthreads();
+  if (FWD && clamp_check)
+    for (int32_t k = threadIdx.x; k < cs.ncase && k < kCaseCache; k += blockDim.x) {
+      s_lim[k] = clamp_limit(cs.P ? cs.P[k] : P0, dt_ext + 2 * k);
+      if (s_lim[k] > 0.0) s_clamp_any = 1;
+    }
+  if (FWD && clamp_check && cs.ncase > kCaseCache && threadIdx.x == 0) s_clamp_any = 1;
+  __syncthreads();
+  // the per-cell clamp test only when some case needs it
+  clamp_check = (FWD && clamp_check && s_clamp_any) ? 1 : 0;
   const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
   double *sh = shm[grp];
   const int32_t pbase = sg1 > sg0 ? s_segs[0] : 0;
