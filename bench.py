@@ -13,11 +13,20 @@ larger than the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
   python bench.py --form batched [--ncase 64]
+  python bench.py --form mixed [--mixed-size 128] [--converge 3000]
 
 --form batched: 64 cube cases with n^3 x 6 tets, n uniform in [8, 48], Mach
 U(0.3, 0.8), alpha U(-5, 5) deg, jitter U(0, 0.2)h, all in one context (one
 launch per kernel covers every case), against the same cases run one after
 another in their own contexts.
+
+--form mixed: the 128^3 x 6 cube (jitter 0.1h, Mach 0.8, alpha 1.25 deg, CFL
+20) in the FP64 and the mixed-precision forms: throughput of each, the
+mixed state's error against FP64, and with --converge the iterations and
+time each form needs for a 1e-6 residual drop.
+
+Before the warm-up the sweep launch parameters are chosen by measurement
+on the workload's own grid (mfg_autotune_sweeps) and reported.
 
 With --gpus N > 1 (one process per GPU under torchrun) every rank runs its
 own replica of the workload (the path has no exchange step) and rank 0
@@ -67,6 +76,9 @@ def parse():
                     help="mixed form: also iterate both forms to a 1e-6 residual drop "
                          "(at most this many iterations) and time it")
     ap.add_argument("--ncase", type=int, default=64)
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed iterations with cudaProfilerStart/Stop (for ncu "
+                         "--profile-from-start off)")
     return ap.parse_args()
 
 
@@ -313,8 +325,11 @@ def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up (also builds the CUDA graphs)
+    # launch parameters of the sweeps chosen by measurement on this grid
+    # (the state is left as it was), then the warm-up (builds the CUDA graphs)
     s.calculate_gradient()
+    tuned = s.autotune_sweeps(2) if info["sweep_mode"] == 1 else None
+    info = s.info()
     s.iterate(max(args.warmup, 3), norms=False)
     barrier()
     launches0 = _lib.kernel_launches()
@@ -322,15 +337,22 @@ def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
         barrier()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
+        if args.profile_region:
+            torch.cuda.cudart().cudaProfilerStart()
         ev0.record(stream)
         s.iterate(args.steps, norms=False)
         ev1.record(stream)
         ev1.synchronize()
+        if args.profile_region:
+            torch.cuda.cudart().cudaProfilerStop()
         barrier()
     launches = _lib.kernel_launches() - launches0
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     out = {"ms": ms, "value": world * C * args.steps / (ms / 1e3), "launches": int(launches),
-           "clocks": clk.summary(), "info": info}
+           "clocks": clk.summary(), "info": info,
+           "autotuned": None if tuned is None else {
+               "sweep_lanes_per_cell": tuned["lanes_per_cell"], "sweep_chunks": tuned["chunks"],
+               "sweep_block_threads": 64, "trial_ms_per_iter": tuned["ms_per_iter"]}}
 
     # phase breakdown with CUDA events on the same stream (same fused kernels)
     phase_iters = max(3, min(args.steps, 10))
@@ -449,6 +471,7 @@ def run_single(args, rank, world, local, stream, dist):
                                         "backward": info["bw_levels"]},
                        "sweeps": "persistent chunked" if info["sweep_mode"] == 1 else
                                  "one launch per level"},
+            "autotuned": r["autotuned"],
             "roofline": r["roofline"],
             "flux_plus_gradient": r["flux_plus_gradient"],
             "phases": r["phases"],
@@ -553,10 +576,12 @@ def run_mixed(args, rank, world, local, stream, dist):
                        "lusgs_levels": {"forward": info["fw_levels"],
                                         "backward": info["bw_levels"]}},
             "fp64": {"value": d["value"], "ms_per_step": d["ms"] / args.steps,
+                     "autotuned": d["autotuned"],
                      "phases": d["phases"], "to_drop_1e-6": d.get("to_drop_1e-6")},
             "mixed_over_fp64": m["value"] / d["value"],
             "state_rel_err_vs_fp64": {"same_iterations": err_same_iters,
                                       "at_1e-6_drop": err_conv},
+            "autotuned": m["autotuned"],
             "roofline": m["roofline"],
             "flux_plus_gradient": m["flux_plus_gradient"],
             "phases": m["phases"],
@@ -625,6 +650,7 @@ def run_batched(args, rank, world, local, stream, dist):
                            "how": "each case in its own context, graph-captured fused "
                                   "iterations, cases one after another; device time summed"},
             "batched_over_sequential": r["value"] / seq_value,
+            "autotuned": r["autotuned"],
             "roofline": r["roofline"],
             "flux_plus_gradient": r["flux_plus_gradient"],
             "phases": r["phases"],
