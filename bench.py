@@ -293,10 +293,17 @@ def batched_workload(ncase=64, seed=2024):
     return dict(name=f"batched{ncase}_cube_n8-48_fp64", cases=cases)
 
 
-def build_batched(bw):
+def batched_cells(bw):
+    return [6 * c["n"] ** 3 for c in bw["cases"]]
+
+
+def build_batched(bw, which=None):
+    """Grids and parameters of the cases `which` (default: all)."""
     from minifs_b200 import grid as gr, meshgen
     grids, params = [], []
-    for c in bw["cases"]:
+    for k, c in enumerate(bw["cases"]):
+        if which is not None and k not in which:
+            continue
         m = meshgen.cube_mesh(c["n"], jitter=c["jitter"], seed=c["seed"])
         p = gr.make_params(mach=c["mach"], alpha=c["alpha"], cfl_start=c["cfl"])
         grids.append(gr.prepare(m, p, bump_amp=c["bump_amp"], bump_sigma=c["bump_sigma"]))
@@ -304,12 +311,15 @@ def build_batched(bw):
     return grids, params
 
 
-def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
+def measure(s, counts, args, stream, dist, world, local, total_cells=None):
     """Timed fused iterations of a context, its phase breakdown, roofline and
-    the end-to-end host-buffer run.  counts = (C, G, F, N, K, n)."""
+    the end-to-end host-buffer run.  counts = (C, G, F, N, K, n) of this
+    rank; total_cells: cells of the whole job (default: world replicas of
+    C).  Device times are the max over the ranks."""
     import torch
-    from minifs_b200 import _lib
+    from minifs_b200 import _lib, shard
     C, G, F, N, K, n = counts
+    total = world * C if total_cells is None else total_cells
     info = s.info()
 
     def barrier():
@@ -319,11 +329,7 @@ def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
         torch.cuda.synchronize()
 
     def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.reduce_max(ms, dist, "cuda")
 
     # launch parameters of the sweeps chosen by measurement on this grid
     # (the state is left as it was), then the warm-up (builds the CUDA graphs)
@@ -348,7 +354,7 @@ def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
         barrier()
     launches = _lib.kernel_launches() - launches0
     ms = max_over_ranks(ev0.elapsed_time(ev1))
-    out = {"ms": ms, "value": world * C * args.steps / (ms / 1e3), "launches": int(launches),
+    out = {"ms": ms, "value": total * args.steps / (ms / 1e3), "launches": int(launches),
            "clocks": clk.summary(), "info": info,
            "autotuned": None if tuned is None else {
                "sweep_lanes_per_cell": tuned["lanes_per_cell"], "sweep_chunks": tuned["chunks"],
@@ -401,7 +407,7 @@ def measure(s, counts, args, stream, dist, world, local, phase_kernels=True):
     e1.record(stream)
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    out["e2e"] = {"value": world * C * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+    out["e2e"] = {"value": total * args.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
                   "h2d_bytes_per_step": 8 * 5 * n, "d2h_bytes_per_step": 8 * 5 * n + 8 * 5 * C,
                   "steps": args.e2e_steps,
                   "api": "mfg_iterate_host (C ABI, pinned host buffers)"}
@@ -596,11 +602,19 @@ def run_mixed(args, rank, world, local, stream, dist):
 
 def run_batched(args, rank, world, local, stream, dist):
     """64 uneven cases in one context against the same cases run one after
-    another, each in its own context (sequential per-case launches)."""
+    another, each in its own context (sequential per-case launches).  Under
+    N ranks the cases are sharded by cell count (no collective during the
+    iterations); both figures are whole-job: all cells over the slowest
+    rank's device time."""
     import torch
+    from minifs_b200 import shard
     from minifs_b200.solver import BatchSolver, Solver
     bw = batched_workload(args.ncase)
-    grids, params = build_batched(bw)
+    cells = batched_cells(bw)
+    if world > len(cells):
+        raise SystemExit("more ranks than cases")
+    mine = shard.rank_cases(cells, world, rank)
+    grids, params = build_batched(bw, set(mine))
     counts = [0] * 6
     for pg in grids:
         for i, v in enumerate((pg.n_cell, pg.n_bface, pg.n_face, pg.n_node,
@@ -623,12 +637,14 @@ def run_batched(args, rank, world, local, stream, dist):
         seq_ms += e0.elapsed_time(e1)
         seq_cells += pg.n_cell
         s.close()
+    total_cells = int(shard.reduce_sum(counts[0], dist, "cuda"))
+    seq_ms = shard.reduce_max(seq_ms, dist, "cuda")
     b = BatchSolver(grids, params, device=local)
     b.set_stream(stream.cuda_stream)
-    r = measure(b, tuple(counts), args, stream, dist, world, local)
+    r = measure(b, tuple(counts), args, stream, dist, world, local, total_cells=total_cells)
     norms = b.residual_norm()
     info = r["info"]
-    seq_value = world * seq_cells * args.steps / (seq_ms / 1e3)
+    seq_value = total_cells * args.steps / (seq_ms / 1e3)
     if rank == 0:
         ns = [c["n"] for c in bw["cases"]]
         line = {
@@ -637,9 +653,11 @@ def run_batched(args, rank, world, local, stream, dist):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": bw["name"], "form": "batched", "ncase": len(ns),
-                       "n_min": min(ns), "n_max": max(ns), "cells": counts[0],
-                       "faces": counts[2], "precision": "fp64 (bit-faithful per case)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single",
+                       "n_min": min(ns), "n_max": max(ns), "cells": total_cells,
+                       "cells_rank0": counts[0], "cases_rank0": len(mine),
+                       "precision": "fp64 (bit-faithful per case)",
+                       "parallelism": (f"cases sharded over {world} ranks by cell count"
+                                       if world > 1 else "single"),
                        "l2": "no flush: working set "
                              f"{info['device_bytes'] / 2**20:.0f} MiB > 126 MB L2",
                        "lusgs_levels": {"forward": info["fw_levels"],
