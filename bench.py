@@ -107,16 +107,20 @@ def algorithmic_bytes(C, G, F, N, K):
 def kernel_of_phase(phase: str, sweep_mode: int) -> str:
     persistent = {"sweep_fwd": "k_sweep_fwd_chunk", "sweep_bwd_update": "k_sweep_bwd_chunk"}
     per_level = {"sweep_fwd": "k_sweep_fwd", "sweep_bwd_update": "k_sweep_bwd"}
-    other = {"face_gather": "k_face_gather", "node_values": "k_node_values",
+    other = {"face_gather": "k_face_flux+k_face_gather", "node_values": "k_node_values",
              "grad_faces": "k_grad_faces", "norm": "k_norm_final"}
     return (persistent if sweep_mode == 1 else per_level).get(phase, other.get(phase, phase))
 
 
 def read_traffic(kernel: str, workload_name: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    """DRAM bytes per launch of `kernel` (a "+"-joined phase of several
+    kernels: their sum) from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(path):
         return None
+    if "+" in kernel:
+        parts = [read_traffic(k, workload_name) for k in kernel.split("+")]
+        return None if any(p is None for p in parts) else sum(parts)
     for line in open(path):
         parts = line.split()
         if len(parts) >= 3 and not line.startswith("#") and parts[0] == kernel and \

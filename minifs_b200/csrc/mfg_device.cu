@@ -133,14 +133,23 @@ __device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double d
 // Per-cell face gather: Roe flux into the residual, local time step with
 // CellIsMG and LimitTimeStep, and the LU-SGS diagonal.  One thread per cell,
 // faces in ascending order (see the file header for why that is exact).
-template <bool FLUX, bool DT, bool DIAG>
-__global__ void __launch_bounds__(kBlock, 2)
+// Resident blocks of the face gathers and the face flux (register caps).
+#ifndef MFG_GATHER_MINB
+#define MFG_GATHER_MINB 3
+#endif
+#ifndef MFG_FLUX_MINB
+#define MFG_FLUX_MINB 3
+#endif
+
+template <bool FLUX, bool DT, bool DIAG, bool PRE>
+__global__ void __launch_bounds__(kBlock, MFG_GATHER_MINB)
 k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
               const double *__restrict__ q8, const double *__restrict__ vol,
               double *__restrict__ res, int res_zero, double *__restrict__ dt,
               double *__restrict__ diag, const double *__restrict__ cfl_tab,
               const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
-              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs) {
+              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs,
+              const double *__restrict__ fflux, int32_t F) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < C;
   const int32_t cse = live ? case_of(cs, c) : 0;
@@ -162,11 +171,16 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
         load_q(q8, sr.nb, qn);
         if (FLUX) {
           double f[5];
-          if (sr.flags & SLOT_IS_C2) {
+          if (PRE) {  // the face's flux, computed once by k_face_flux
+            for (int k = 0; k < 5; k++) f[k] = fflux[(int64_t)k * F + sr.face];
+          } else if (sr.flags & SLOT_IS_C2) {
             roe_flux(qn, qc, sr.nx, sr.ny, sr.nz, sr.area, P, f);
-            for (int k = 0; k < 5; k++) r[k] += f[k];
           } else {
             roe_flux(qc, qn, sr.nx, sr.ny, sr.nz, sr.area, P, f);
+          }
+          if (sr.flags & SLOT_IS_C2) {
+            for (int k = 0; k < 5; k++) r[k] += f[k];
+          } else {
             for (int k = 0; k < 5; k++) r[k] -= f[k];
           }
         }
@@ -210,20 +224,20 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
 // local time step and its CellIsMG switch (a discrete decision, kept in FP64
 // so that both forms take it alike), the Diag terms and all sums in FP64 in
 // the same face order.
-template <bool FLUX, bool DT, bool DIAG>
-__global__ void __launch_bounds__(kBlock, 2)
+template <bool FLUX, bool DT, bool DIAG, bool PRE>
+__global__ void __launch_bounds__(kBlock, MFG_GATHER_MINB)
 k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
                  const double *__restrict__ q8, const double *__restrict__ vol,
                  double *__restrict__ res, int res_zero, double *__restrict__ dt,
                  double *__restrict__ diag, const double *__restrict__ cfl_tab,
                  const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
                  unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part,
-                 Cases cs) {
+                 Cases cs, const double *__restrict__ fflux, int32_t F) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < C;
   const int32_t cse = live ? case_of(cs, c) : 0;
   const Params P = live ? params_of(P0, cs, c) : P0;
-  const FluxP<float> F = flux_params<float>(P);
+  const FluxP<float> FP = flux_params<float>(P);
   double qd[Q_STRIDE];
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   double dtc = 0.0;
@@ -241,11 +255,16 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
         load_q(q8, sr.nb, qn);
         if (FLUX) {
           double f[5];
+          if (PRE) {  // the face's flux, computed once by k_face_flux
+            for (int k = 0; k < 5; k++) f[k] = fflux[(int64_t)k * F + sr.face];
+          } else if (sr.flags & SLOT_IS_C2) {
+            roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
+          } else {
+            roe_flux_mx(qd, qn, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
+          }
           if (sr.flags & SLOT_IS_C2) {
-            roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, F, f);
             for (int k = 0; k < 5; k++) r[k] += f[k];
           } else {
-            roe_flux_mx(qd, qn, sr.nx, sr.ny, sr.nz, sr.area, P, F, f);
             for (int k = 0; k < 5; k++) r[k] -= f[k];
           }
         }
@@ -280,6 +299,30 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
       for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
   }
   gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
+}
+
+// RoeFlux_noprec once per face (the reference's own face loop,
+// cal_flux.cpp:84-192), from q[c1] and q[c2] with the stored normal, into
+// fflux[5][F]; the face gathers then add each face's flux to its cells in
+// ascending face order.  The arguments are those the per-cell form passes
+// from either side, so the sums are the same bits with half the flux work.
+template <bool MX>
+__global__ void __launch_bounds__(kBlock, MFG_FLUX_MINB)
+k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restrict__ q8,
+            Params P0, Cases cs, double *__restrict__ fflux) {
+  const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  const FaceRec fr = faces[f];
+  const Params P = params_of(P0, cs, fr.c1);
+  double ql[Q_STRIDE], qr[Q_STRIDE], fl[5];
+  load_q(q8, fr.c1, ql);
+  load_q(q8, fr.c2, qr);
+  if (MX)
+    roe_flux_mx(ql, qr, fr.nx, fr.ny, fr.nz, fr.area, P, flux_params<float>(P), fl);
+  else
+    roe_flux(ql, qr, fr.nx, fr.ny, fr.nz, fr.area, P, fl);
+#pragma unroll
+  for (int k = 0; k < 5; k++) fflux[(int64_t)k * F + f] = fl[k];
 }
 
 // LimitTimeStep's ratio clamp (compute_timestep.cpp:929-944), per case.
@@ -1256,6 +1299,8 @@ struct mfg_ctx {
   double *vol = nullptr, *staging = nullptr;
   int32_t *cptr = nullptr;
   SlotRec *slots = nullptr;
+  FaceRec *faces = nullptr;  // per-face flux: normal, area, cells
+  double *fflux = nullptr;   // per-face flux [5][F]
   int32_t *fnptr = nullptr, *fnodes = nullptr;
   int32_t *nptr = nullptr, *nsrc = nullptr, *ninfo = nullptr, *bface_c1 = nullptr;
   double *nw = nullptr, *wnode = nullptr, *nsym = nullptr;
@@ -1848,6 +1893,14 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   }
   if ((rc = dupload(ctx, &ctx->cptr, cptr))) return fail(rc);
   if ((rc = dupload(ctx, &ctx->slots, slots))) return fail(rc);
+  {
+    std::vector<FaceRec> fr(m->n_face);
+    for (int32_t f = 0; f < m->n_face; f++)
+      fr[f] = FaceRec{m->xfn[f], m->yfn[f], m->zfn[f], m->area[f], m->f2c[2 * f],
+                      m->f2c[2 * f + 1], 0, 0};
+    if ((rc = dupload(ctx, &ctx->faces, fr))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->fflux, (size_t)5 * m->n_face))) return fail(rc);
+  }
   slots.clear();
   slots.shrink_to_fit();
   std::vector<double> volv(m->vol, m->vol + n);
@@ -2168,17 +2221,27 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
   const double *tab = use_table ? ctx->cfl_tab : nullptr;
   double *np = (flux && ctx->ncase == 1) ? ctx->norm_part : nullptr;
   const Cases cs = cases_of(ctx);
-#define MFG_FACE(F, D, G)                                                                     \
-  if (ctx->precision == MFG_PREC_MIXED)                                                       \
-    k_face_gather_mx<F, D, G><<<g, kBlock, 0, st>>>(                                          \
-        ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res,                                 \
-        ctx->res_zero ? 1 : 0, ctx->dt, ctx->diag, tab, ctx->iter_counter, cfl, ctx->P,        \
-        ctx->dt_ext, np, cs);                                                                 \
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  if (flux) {  // each face's Roe flux once, then gathered per cell
+    if (mx)
+      k_face_flux<true><<<grid_for(ctx->F), kBlock, 0, st>>>(ctx->F, ctx->faces, q, ctx->P, cs,
+                                                              ctx->fflux);
+    else
+      k_face_flux<false><<<grid_for(ctx->F), kBlock, 0, st>>>(ctx->F, ctx->faces, q, ctx->P, cs,
+                                                               ctx->fflux);
+    count_launch();
+  }
+#define MFG_FACE(F_, D_, G_)                                                                  \
+  if (mx)                                                                                     \
+    k_face_gather_mx<F_, D_, G_, F_><<<g, kBlock, 0, st>>>(                                   \
+        ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
+        ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
+        ctx->F);                                                                              \
   else                                                                                        \
-    k_face_gather<F, D, G><<<g, kBlock, 0, st>>>(ctx->C, ctx->cptr, ctx->slots, q, ctx->vol,  \
-                                                 ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,   \
-                                                 ctx->diag, tab, ctx->iter_counter, cfl,     \
-                                                 ctx->P, ctx->dt_ext, np, cs)
+    k_face_gather<F_, D_, G_, F_><<<g, kBlock, 0, st>>>(                                      \
+        ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
+        ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
+        ctx->F)
   if (flux && dtp && diag) {
     MFG_FACE(true, true, true);
   } else if (flux && !dtp && !diag) {

@@ -49,6 +49,12 @@ struct __align__(16) SweepRec {
   double nx, ny, nz, w;
 };
 
+// One face for the per-face flux: the stored normal and area, and its cells.
+struct __align__(16) FaceRec {
+  double nx, ny, nz, area;
+  int32_t c1, c2, pad0, pad1;
+};
+
 // Mixed form: single-precision LU-SGS sweep record.
 struct __align__(16) SweepRecF {
   float nx, ny, nz, w;
