@@ -529,6 +529,14 @@ struct SweepTypes<true> {
   using Q = float;
   using Rec = SweepRecF;
 };
+// Padding of a stage so that consecutive groups' stages start 16 bytes
+// apart modulo 128: the groups of a warp then read their records from
+// different shared-memory banks (without it every group's record k sits in
+// the same bank and a warp's stage reads are 4- to 8-way conflicts).
+constexpr int stage_pad_bytes(int raw) {
+  const int a16 = (raw + 15) / 16 * 16;
+  return a16 - raw + ((16 - a16 % 128) % 128 + 128) % 128;
+}
 template <int W, bool MX>
 struct __align__(16) Stage {
   typename SweepTypes<MX>::Q qn[W][Q_STRIDE];
@@ -536,8 +544,12 @@ struct __align__(16) Stage {
   double qc[Q_STRIDE];
   double in5[5];
   double diag;
-  double pad[2];
+  char pad[stage_pad_bytes(int(sizeof(typename SweepTypes<MX>::Q)) * W * Q_STRIDE +
+                           int(sizeof(typename SweepTypes<MX>::Rec)) * W + 8 * (Q_STRIDE + 6))];
 };
+static_assert(sizeof(Stage<4, false>) % 128 == 16 && sizeof(Stage<4, true>) % 128 == 16 &&
+                  sizeof(Stage<8, false>) % 128 == 16 && sizeof(Stage<8, true>) % 128 == 16,
+              "stage stride");
 
 __device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
