@@ -370,7 +370,7 @@ def measure(s, counts, args, stream, dist, world, local, total_cells=None):
     alg = algorithmic_bytes(C, G, F, N, K)
     peak, peak_kind = measured_peak()
     per_level = info["sweep_mode"] == 0
-    nl = {"face_gather": 1, "sweep_fwd": info["fw_levels"] if per_level else 1,
+    nl = {"face_gather": 2, "sweep_fwd": info["fw_levels"] if per_level else 1,
           "sweep_bwd_update": info["bw_levels"] if per_level else 1,
           "node_values": 1, "grad_faces": 1, "norm": 1}
     phase_out = {}
