@@ -247,11 +247,35 @@ def cpu_baseline(mesh, pg, params, wl, iters=2):
 # ---------------------------------------------------------------------------
 
 def build_case(wl):
+    """(mesh, params, prepared grid, seconds of the host preprocessing)."""
     from minifs_b200 import grid as gr, meshgen
     mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
     params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+    t = time.perf_counter()
     pg = gr.prepare(mesh, params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
-    return mesh, params, pg
+    return mesh, params, pg, time.perf_counter() - t
+
+
+def prep_on_gpu(mesh, params, wl, pg, host_s, device):
+    """The same preprocessing with metrics and node weights on the GPU: wall
+    seconds from the raw host mesh to host arrays (copies included; the
+    second of two runs), device time of its kernels, and whether every array
+    matches the host result bit for bit."""
+    from minifs_b200 import grid as gr
+    kw = dict(bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"], device=device)
+    gr.prepare(mesh, params, **kw)
+    st = {}
+    t = time.perf_counter()
+    pgd = gr.prepare(mesh, params, stats=st, **kw)
+    gpu_s = time.perf_counter() - t
+    same = all(np.asarray(pgd.arrays[k]).tobytes() == np.asarray(pg.arrays[k]).tobytes()
+               for k in pg.arrays) and pgd.q0.tobytes() == pg.q0.tobytes()
+    return {"host_s": host_s, "gpu_s": gpu_s, "gpu_kernels_ms": st["gpu_kernels_s"] * 1e3,
+            "gpu_upload_and_kernels_s": st["gpu_run_s"], "gpu_download_s": st["gpu_download_s"],
+            "init_flow_on_host_s": st["init_flow_s"], "speedup": host_s / gpu_s,
+            "bitwise_equal": bool(same),
+            "steps": "SpecifyBC, ComputeMetrics, AllocAndInitFlowfield + SetGhostVariables, "
+                     "CalC2N, ComputeWeight3D_Node, FindNodeSYMM"}
 
 
 def run_reference_arm(args, rank, world):
@@ -451,7 +475,8 @@ def main():
 def run_single(args, rank, world, local, stream, dist):
     from minifs_b200.solver import Solver
     wl = workload(args.size)
-    mesh, params, pg = build_case(wl)
+    mesh, params, pg, host_prep_s = build_case(wl)
+    prep = prep_on_gpu(mesh, params, wl, pg, host_prep_s, local)
     s = Solver(pg, params, device=local)
     s.set_stream(stream.cuda_stream)
     C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
@@ -490,6 +515,7 @@ def run_single(args, rank, world, local, stream, dist):
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
             "residual_norm": [float(x) for x in norms],
+            "prep": prep,
         }
         print(json.dumps(line), flush=True)
     s.close()

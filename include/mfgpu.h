@@ -290,6 +290,33 @@ int mfg_prep_node_weights(const mfg_raw_grid *g, const int32_t *bctype, const do
                           int32_t *nodesymm, double *xfn_n_symm, double *yfn_n_symm,
                           double *zfn_n_symm);
 
+/* ---- the same preprocessing on a GPU ------------------------------------ */
+/* ComputeMetrics, CalnNPC/CalC2N, ComputeWeight3D_Node and FindNodeSYMM run
+ * on `device`: every output is bit-identical to mfg_prep_metrics,
+ * mfg_prep_c2n_size and mfg_prep_node_weights on the same raw grid.
+ * mfg_prep_gpu_run copies the raw grid (host arrays, f2c as rewritten by
+ * mfg_prep_specify_bc) and bctype to the device, checks every node and cell
+ * index there (MFG_ERR_BADMESH, nothing computed, if one is out of range),
+ * and computes all outputs; it returns MFG_ERR_BADMESH for a cell volume
+ * below 1e-40, as mfg_prep_metrics does.  The getters copy the results into
+ * host arrays sized and laid out as the host entries' outputs.  The
+ * initial flow field (mfg_prep_init_flow) stays on the host: its exp and pow
+ * are the C library's. */
+typedef struct mfg_prep_gpu mfg_prep_gpu;
+int mfg_prep_gpu_run(const mfg_raw_grid *g, const int32_t *bctype, int32_t device,
+                     mfg_prep_gpu **out);
+int mfg_prep_gpu_c2n_size(const mfg_prep_gpu *p, int64_t *n_c2n);
+int mfg_prep_gpu_metrics(mfg_prep_gpu *p, double *xfn, double *yfn, double *zfn, double *area,
+                         double *xfc, double *yfc, double *zfc, double *xcc, double *ycc,
+                         double *zcc, double *vol);
+int mfg_prep_gpu_node_weights(mfg_prep_gpu *p, double *wnode, int32_t *nmark, double *wbface,
+                              int32_t *nnpc, int32_t *c2n, double *wc2n, int32_t *nodesymm,
+                              double *xfn_n_symm, double *yfn_n_symm, double *zfn_n_symm);
+/* Device time of the preprocessing kernels of the last mfg_prep_gpu_run, ms
+ * (CUDA events around them; the copies of the raw grid are outside). */
+int mfg_prep_gpu_kernel_ms(const mfg_prep_gpu *p, double *ms);
+int mfg_prep_gpu_destroy(mfg_prep_gpu *p);
+
 #ifdef __cplusplus
 }
 #endif

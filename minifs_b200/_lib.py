@@ -142,6 +142,14 @@ def load(build_if_missing: bool = True):
         "mfg_prep_c2n_size": (ct.c_int, [ct.POINTER(RawGrid), ct.POINTER(ct.c_int64)]),
         "mfg_prep_node_weights": (ct.c_int, [ct.POINTER(RawGrid), i32p] + [f64p] * 9 +
                                   [f64p, i32p, f64p, i32p, i32p, f64p, i32p, f64p, f64p, f64p]),
+        "mfg_prep_gpu_run": (ct.c_int, [ct.POINTER(RawGrid), i32p, ct.c_int32,
+                                        ct.POINTER(ct.c_void_p)]),
+        "mfg_prep_gpu_c2n_size": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int64)]),
+        "mfg_prep_gpu_kernel_ms": (ct.c_int, [ct.c_void_p, f64p]),
+        "mfg_prep_gpu_metrics": (ct.c_int, [ct.c_void_p] + [f64p] * 11),
+        "mfg_prep_gpu_node_weights": (ct.c_int, [ct.c_void_p, f64p, i32p, f64p, i32p, i32p, f64p,
+                                                 i32p, f64p, f64p, f64p]),
+        "mfg_prep_gpu_destroy": (ct.c_int, [ct.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1458,6 +1458,15 @@ int validate_mesh(const mfg_mesh *m) {
 
 }  // namespace
 
+// Shared with the other translation units of the library (mesh
+// preprocessing): the thread's last CUDA error text and the launch count.
+namespace mfg {
+void note_cuda_error(const char *what, int code) {
+  g_cuda_error = std::string(what) + ": " + cudaGetErrorString((cudaError_t)code);
+}
+void note_launches(int64_t k) { count_launch(k); }
+}  // namespace mfg
+
 extern "C" {
 
 const char *mfg_error_string(int32_t code) {

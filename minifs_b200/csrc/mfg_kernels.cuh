@@ -20,6 +20,12 @@ namespace mfg {
 constexpr double kTiny = 1.e-40;  // number_type.h:29
 constexpr double kBig = 1.e40;    // number_type.h:28
 
+// Host-side state shared by the library's translation units (defined with
+// the iteration path): record a CUDA error for mfg_last_cuda_error, and
+// count kernel launches for mfg_kernel_launches.
+void note_cuda_error(const char *what, int code);
+void note_launches(int64_t k);
+
 // Per-cell state record, 64 bytes: the five primitive variables of the
 // reference's SoA arrays plus three derived per-cell quantities.
 enum : int {

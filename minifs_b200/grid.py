@@ -7,11 +7,15 @@ consumes, calling the C++ restatements in ``libmfgpu.so``:
   SpecifyBC -> ComputeMetrics -> AllocAndInitFlowfield (+ seeded density
   bump) -> SetGhostVariables -> ComputeWeight3D_Node -> FindNodeSYMM
 
+or, with ``device=``, the same chain with ComputeMetrics, CalC2N,
+ComputeWeight3D_Node and FindNodeSYMM on a GPU (bit-identical arrays).
+
 The LU-SGS order is the serial build's identity order
 (``ReorderCellforLUSGS_0``, grid_polyhedra.cpp:1127-1142).
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -67,8 +71,17 @@ def _raw(mesh: RawMesh, f2c: np.ndarray) -> _lib.RawGrid:
 
 
 def prepare(mesh: RawMesh, params: _lib.Params, bump_amp: float = 0.05, bump_sigma: float = 0.1,
-            bump_center=(0.5, 0.5, 0.5)) -> PreparedGrid:
-    """Run the preprocessing chain on ``mesh`` (not modified)."""
+            bump_center=(0.5, 0.5, 0.5), device: int | None = None,
+            stats: dict | None = None) -> PreparedGrid:
+    """Run the preprocessing chain on ``mesh`` (not modified).
+
+    With ``device`` (a CUDA device index) the metrics and node weights are
+    computed on that GPU (``mfg_prep_gpu_*``, the same bits as the host
+    entries); the initial flow field is set on the host either way.
+    ``stats``, if given, receives the seconds of each step ("gpu_kernels_s":
+    device time of the GPU kernels alone)."""
+    if device is not None:
+        return _prepare_gpu(mesh, params, bump_amp, bump_sigma, bump_center, int(device), stats)
     lib = _lib.load()
     mesh_x = np.ascontiguousarray(mesh.x, np.float64)
     mesh = RawMesh(x=mesh_x, y=np.ascontiguousarray(mesh.y, np.float64),
@@ -112,6 +125,75 @@ def prepare(mesh: RawMesh, params: _lib.Params, bump_amp: float = 0.05, bump_sig
         _lib.ptr(W["nnpc"], _lib.i32p), _lib.ptr(W["c2n"], _lib.i32p), _lib.ptr(W["wc2n"]),
         _lib.ptr(W["nodesymm"], _lib.i32p), _lib.ptr(W["xfn_n_symm"]),
         _lib.ptr(W["yfn_n_symm"]), _lib.ptr(W["zfn_n_symm"])))
+    arrays = dict(f2c=f2c, nnpf=mesh.nnpf, f2n=mesh.f2n, bctype=bctype[:G] if G else bctype)
+    arrays.update(A)
+    arrays.update(W)
+    return PreparedGrid(n_node=N, n_face=F, n_cell=C, n_bface=G, arrays=arrays, q0=q0)
+
+
+def _contiguous(mesh: RawMesh) -> RawMesh:
+    return RawMesh(x=np.ascontiguousarray(mesh.x, np.float64),
+                   y=np.ascontiguousarray(mesh.y, np.float64),
+                   z=np.ascontiguousarray(mesh.z, np.float64),
+                   nnpf=np.ascontiguousarray(mesh.nnpf, np.int32),
+                   f2n=np.ascontiguousarray(mesh.f2n, np.int32), f2c=mesh.f2c,
+                   n_cell=mesh.n_cell, n_bface=mesh.n_bface, patches=mesh.patches)
+
+
+def _prepare_gpu(mesh, params, bump_amp, bump_sigma, bump_center, device, stats):
+    import time
+    lib = _lib.load()
+    st = stats if stats is not None else {}
+    mesh = _contiguous(mesh)
+    f2c = np.array(mesh.f2c, dtype=np.int32, copy=True)
+    g = _raw(mesh, f2c)
+    C, G, F, N = mesh.n_cell, mesh.n_bface, mesh.n_face, mesh.n_node
+    n = C + G
+    t0 = time.perf_counter()
+    types = np.array([t for _, t in mesh.patches], dtype=np.int32)
+    bctype = np.zeros(max(G, 1), dtype=np.int32)
+    _lib.check("mfg_prep_specify_bc",
+               lib.mfg_prep_specify_bc(ct_byref(g), len(types), _lib.ptr(types, _lib.i32p),
+                                       _lib.ptr(bctype, _lib.i32p)))
+    t1 = time.perf_counter()
+    h = ctypes.c_void_p()
+    _lib.check("mfg_prep_gpu_run",
+               lib.mfg_prep_gpu_run(ct_byref(g), _lib.ptr(bctype, _lib.i32p), device,
+                                    ctypes.byref(h)))
+    try:
+        t2 = time.perf_counter()
+        kms = ctypes.c_double(0.0)
+        lib.mfg_prep_gpu_kernel_ms(h, ctypes.byref(kms))
+        nc2n = ctypes.c_int64(0)
+        _lib.check("mfg_prep_gpu_c2n_size", lib.mfg_prep_gpu_c2n_size(h, ctypes.byref(nc2n)))
+        A = {name: np.empty(F) for name in ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc")}
+        A.update({name: np.empty(n) for name in ("xcc", "ycc", "zcc", "vol")})
+        _lib.check("mfg_prep_gpu_metrics", lib.mfg_prep_gpu_metrics(
+            h, *[_lib.ptr(A[k]) for k in ("xfn", "yfn", "zfn", "area", "xfc", "yfc", "zfc",
+                                          "xcc", "ycc", "zcc", "vol")]))
+        nb_nodes = int(mesh.nnpf[:G].sum())
+        W = dict(wnode=np.empty(N), nmark=np.empty(N, np.int32),
+                 wbface=np.zeros(max(nb_nodes, 1)), nnpc=np.empty(C, np.int32),
+                 c2n=np.empty(nc2n.value, np.int32), wc2n=np.empty(nc2n.value),
+                 nodesymm=np.empty(N, np.int32), xfn_n_symm=np.empty(N),
+                 yfn_n_symm=np.empty(N), zfn_n_symm=np.empty(N))
+        _lib.check("mfg_prep_gpu_node_weights", lib.mfg_prep_gpu_node_weights(
+            h, _lib.ptr(W["wnode"]), _lib.ptr(W["nmark"], _lib.i32p), _lib.ptr(W["wbface"]),
+            _lib.ptr(W["nnpc"], _lib.i32p), _lib.ptr(W["c2n"], _lib.i32p), _lib.ptr(W["wc2n"]),
+            _lib.ptr(W["nodesymm"], _lib.i32p), _lib.ptr(W["xfn_n_symm"]),
+            _lib.ptr(W["yfn_n_symm"]), _lib.ptr(W["zfn_n_symm"])))
+        t3 = time.perf_counter()
+    finally:
+        lib.mfg_prep_gpu_destroy(h)
+    q0 = np.zeros(5 * n)
+    bx, by, bz = bump_center
+    _lib.check("mfg_prep_init_flow", lib.mfg_prep_init_flow(
+        ct_byref(g), ct_byref(params), _lib.ptr(bctype, _lib.i32p),
+        *[_lib.ptr(A[k]) for k in ("xfn", "yfn", "zfn", "xcc", "ycc", "zcc")],
+        float(bump_amp), float(bump_sigma), float(bx), float(by), float(bz), _lib.ptr(q0)))
+    t4 = time.perf_counter()
+    st.update(specify_bc_s=t1 - t0, gpu_run_s=t2 - t1, gpu_kernels_s=kms.value / 1e3,
+              gpu_download_s=t3 - t2, init_flow_s=t4 - t3, total_s=t4 - t0)
     arrays = dict(f2c=f2c, nnpf=mesh.nnpf, f2n=mesh.f2n, bctype=bctype[:G] if G else bctype)
     arrays.update(A)
     arrays.update(W)
