@@ -477,7 +477,9 @@ def run_single(args, rank, world, local, stream, dist):
     wl = workload(args.size)
     mesh, params, pg, host_prep_s = build_case(wl)
     prep = prep_on_gpu(mesh, params, wl, pg, host_prep_s, local)
+    t = time.perf_counter()
     s = Solver(pg, params, device=local)
+    prep["solver_create_s"] = time.perf_counter() - t
     s.set_stream(stream.cuda_stream)
     C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
     K = int(pg.arrays["nnpc"].sum())
