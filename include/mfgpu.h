@@ -36,6 +36,7 @@ extern "C" {
 #define MFG_ERR_UNSUPPORTED (-6) /* LU-SGS order inconsistent with layers, etc. */
 #define MFG_ERR_BADMESH (-7)     /* degenerate volume, bad connectivity */
 #define MFG_ERR_NODEVICE (-8)    /* no CUDA device / wrong architecture */
+#define MFG_ERR_IO (-9)          /* file missing, unreadable, truncated or malformed */
 
 /* Boundary-condition codes (src/Base/constant.h:47-51). */
 #define MFG_BC_WALL 3
@@ -289,6 +290,48 @@ int mfg_prep_node_weights(const mfg_raw_grid *g, const int32_t *bctype, const do
                           double *wbface, int32_t *nnpc, int32_t *c2n, double *wc2n,
                           int32_t *nodesymm, double *xfn_n_symm, double *yfn_n_symm,
                           double *zfn_n_symm);
+
+/* ---- FlowStar files ----------------------------------------------------- */
+/* A binary grid file as ReadMFlowGrid_binary (load_grid.cpp:129-273) reads
+ * it: int32 n_node, n_face, n_cell; double x[n_node], y[], z[]; int32
+ * nnpf[n_face], f2n[sum nnpf], f2c[2 n_face]; then, in a partitioned file,
+ * the interface block int32 n_iface, nbz[n_iface] (zone of the face's other
+ * side), nbf[n_iface] (its face there), int32 n_inode, nbsn[n_inode] (own
+ * node), nbzn[] (zone), nbrn[] (node there).  A serial file ends with
+ * n_iface = n_inode = 0 (the reference reads the block unless the stream
+ * has already hit its end, which an exact read never does); a file that
+ * ends right after f2c reads as having no interfaces.  On reading, a face
+ * whose first cell is a boundary (f2c[2i] < 0) has its node order reversed
+ * after the first node and its two cells swapped, and n_bface counts the
+ * faces with a negative neighbour, as the reference does (:209-229); the
+ * boundary faces must come first for SpecifyBC, as in the format.  The
+ * fields n_node ... f2c are mfg_raw_grid's, in the same order. */
+typedef struct mfg_mfl {
+  int32_t n_node, n_face, n_cell, n_bface;
+  double *x, *y, *z;
+  int32_t *nnpf, *f2n, *f2c;
+  int32_t n_iface;
+  int32_t *nbz, *nbf;
+  int32_t n_inode;
+  int32_t *nbsn, *nbzn, *nbrn;
+} mfg_mfl;
+/* Allocates *out (free with mfg_mfl_free).  MFG_ERR_IO for a missing,
+ * truncated or inconsistent file (negative counts, nnpf < 1, extra bytes
+ * after the interface block). */
+int mfg_mfl_read(const char *path, mfg_mfl **out);
+/* Writes the arrays as given, with the interface block (zeros when
+ * n_iface = n_inode = 0).  n_bface is not stored: the reader recounts it. */
+int mfg_mfl_write(const char *path, const mfg_mfl *g);
+int mfg_mfl_free(mfg_mfl *g);
+/* bc.para (ReadMFlowBoundaryCondition, load_grid.cpp:282-314): the patch
+ * count, then one "patch_id type" pair per patch, in file order (SpecifyBC
+ * indexes this table by position: patch p is record p - 1).  Reads at most
+ * `cap` records; *n_patch is the file's count (MFG_ERR_INVALID if above
+ * cap, MFG_ERR_IO if the file is short or malformed). */
+int mfg_bc_read(const char *path, int32_t cap, int32_t *n_patch, int32_t *patch_id,
+                int32_t *type);
+int mfg_bc_write(const char *path, int32_t n_patch, const int32_t *patch_id,
+                 const int32_t *type);
 
 /* ---- the same preprocessing on a GPU ------------------------------------ */
 /* ComputeMetrics, CalnNPC/CalC2N, ComputeWeight3D_Node and FindNodeSYMM run

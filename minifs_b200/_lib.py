@@ -19,7 +19,8 @@ f64p = ct.POINTER(ct.c_double)
 MFG_OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -4: "device wait timed out", -5: "non-finite value", -6: "unsupported configuration",
-          -7: "bad mesh", -8: "no usable CUDA device"}
+          -7: "bad mesh", -8: "no usable CUDA device",
+          -9: "file missing, truncated or malformed"}
 
 FIELD = {"q": 0, "res": 1, "dt": 2, "dq": 3, "dqdx": 4, "dqdy": 5, "dqdz": 6, "diag": 7}
 PREC = {"fp64": 0, "mixed": 1}
@@ -71,6 +72,14 @@ class RawGrid(ct.Structure):
     _fields_ = [("n_node", ct.c_int32), ("n_face", ct.c_int32), ("n_cell", ct.c_int32),
                 ("n_bface", ct.c_int32), ("x", f64p), ("y", f64p), ("z", f64p),
                 ("nnpf", i32p), ("f2n", i32p), ("f2c", i32p)]
+
+
+class Mfl(ct.Structure):
+    _fields_ = [("n_node", ct.c_int32), ("n_face", ct.c_int32), ("n_cell", ct.c_int32),
+                ("n_bface", ct.c_int32), ("x", f64p), ("y", f64p), ("z", f64p),
+                ("nnpf", i32p), ("f2n", i32p), ("f2c", i32p),
+                ("n_iface", ct.c_int32), ("nbz", i32p), ("nbf", i32p),
+                ("n_inode", ct.c_int32), ("nbsn", i32p), ("nbzn", i32p), ("nbrn", i32p)]
 
 
 class MfgError(RuntimeError):
@@ -150,6 +159,11 @@ def load(build_if_missing: bool = True):
         "mfg_prep_gpu_node_weights": (ct.c_int, [ct.c_void_p, f64p, i32p, f64p, i32p, i32p, f64p,
                                                  i32p, f64p, f64p, f64p]),
         "mfg_prep_gpu_destroy": (ct.c_int, [ct.c_void_p]),
+        "mfg_mfl_read": (ct.c_int, [ct.c_char_p, ct.POINTER(ct.POINTER(Mfl))]),
+        "mfg_mfl_write": (ct.c_int, [ct.c_char_p, ct.POINTER(Mfl)]),
+        "mfg_mfl_free": (ct.c_int, [ct.POINTER(Mfl)]),
+        "mfg_bc_read": (ct.c_int, [ct.c_char_p, ct.c_int32, i32p, i32p, i32p]),
+        "mfg_bc_write": (ct.c_int, [ct.c_char_p, ct.c_int32, i32p, i32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

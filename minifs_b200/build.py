@@ -19,7 +19,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libmfgpu.so")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["mfg_device.cu", "mfg_prep.cu", "mfg_host.cpp"]
+SOURCES = ["mfg_device.cu", "mfg_prep.cu", "mfg_host.cpp", "mfg_io.cpp"]
 DEPS = SOURCES + ["mfg_kernels.cuh"]
 
 

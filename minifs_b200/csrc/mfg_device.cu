@@ -1480,6 +1480,7 @@ const char *mfg_error_string(int32_t code) {
     case MFG_ERR_UNSUPPORTED: return "unsupported configuration";
     case MFG_ERR_BADMESH: return "bad mesh";
     case MFG_ERR_NODEVICE: return "no usable CUDA device";
+    case MFG_ERR_IO: return "file missing, truncated or malformed";
     default: return "unknown error";
   }
 }
