@@ -194,6 +194,20 @@ int mfg_forward_lusgs(mfg_ctx *ctx);
 /* [CalculateGradient, cal_gradient.cpp:87-167: CompNodeVar3D_dist +
  * CompGradientQ_Gauss_Node for rho,u,v,w,p] */
 int mfg_calculate_gradient(mfg_ctx *ctx);
+/* [SetGhostVariables, load_grid.cpp:953-1212, inviscid steady case]: the
+ * ghost state of every boundary face from its inner cell's current state
+ * (WALL and SYMM mirror the velocity, FAR_FIELD from Riemann invariants,
+ * INTERFACE untouched, other types keep their ghost; then the rho and p
+ * clamps).  The reference calls it once, in PreprocessGrid (its main loop
+ * has the call commented out, main.cpp:286); mfg_prep_init_flow does that
+ * one.  The subsonic far-field branches use CUDA's pow where the reference
+ * uses the C library's, so those ghosts may differ in the last bit. */
+int mfg_set_ghost_variables(mfg_ctx *ctx);
+/* on = 1: mfg_iterate (and mfg_iterate_host, mfg_profile_phases) call
+ * mfg_set_ghost_variables after the LU-SGS update and before the gradient
+ * of every iteration, where main.cpp:286 would; on = 0 (the default, the
+ * reference's frozen ghosts): they do not. */
+int mfg_set_live_bc(mfg_ctx *ctx, int32_t on);
 /* The whole main-loop body (main.cpp:201-291) n times, fused kernels in a
  * CUDA graph.  norms (optional, host) receives 5 residual L2 norms per
  * iteration (main.cpp:294-317 evaluated every iteration); for a batch

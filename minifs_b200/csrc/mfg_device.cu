@@ -78,6 +78,116 @@ __global__ void k_download_rec(const double *__restrict__ rec, double *__restric
   for (int k = 0; k < 5; k++) soa[k * n + i] = rec[i * Q_STRIDE + k];
 }
 
+// SetGhostVariables (load_grid.cpp:953-1212), inviscid steady case: the
+// ghost state of every boundary face from its inner cell's current state,
+// one thread per boundary face, written into both state buffers (which keep
+// identical ghost rows) and, in the mixed form, both single-precision
+// copies.  The same expressions as the reference; its only libm calls whose
+// arguments change with the flow are the two pow of the subsonic far-field
+// branches, which here are CUDA's pow.
+__global__ void k_ghost_bc(int32_t G, int32_t C, const FaceRec *__restrict__ faces,
+                           const int32_t *__restrict__ bctype, double *__restrict__ qa,
+                           double *__restrict__ qb, float *__restrict__ q4a,
+                           float *__restrict__ q4b, Params P0, Cases cs) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= G) return;
+  const int type = bctype[i];
+  if (type == MFG_BC_INTERFACE) return;  // :1030-1031
+  const FaceRec fr = faces[i];
+  const int32_t c1 = fr.c1;
+  const int64_t c2 = (int64_t)C + i;
+  const Params P = params_of(P0, cs, c1);
+  const double xfn = fr.nx, yfn = fr.ny, zfn = fr.nz;
+  double q1[Q_STRIDE], g[Q_STRIDE];
+  load_q(qa, c1, q1);
+  load_q(qa, c2, g);  // kept by types the reference does not handle
+  const double gam = P.gam, p_bar = P.p_bar;
+  switch (type) {
+    case MFG_BC_WALL:
+    case MFG_BC_SYMM: {  // :1036-1044, :1084-1095 (same assignments)
+      g[4] = q1[4];
+      g[0] = q1[0];
+      const double vn = 2. * (xfn * q1[1] + yfn * q1[2] + zfn * q1[3]);
+      g[1] = q1[1] - vn * xfn;
+      g[2] = q1[2] - vn * yfn;
+      g[3] = q1[3] - vn * zfn;
+      break;
+    }
+    case MFG_BC_FAR_FIELD: {  // :1097-1194
+      const double um = P.ref[1], vm = P.ref[2], wm = P.ref[3];
+      const double up = q1[1], vp = q1[2], wp = q1[3];
+      const double rhom = P.ref[0], pm = P.ref[4] + p_bar;
+      const double rhop = q1[0], pp = q1[4] + p_bar;
+      const double vnm = xfn * um + yfn * vm + zfn * wm;
+      const double vnp = xfn * up + yfn * vp + zfn * wp;
+      const double cm = sqrt(gam * pm / rhom);
+      const double cp = sqrt(gam * pp / rhop);
+      const double riemm = vnm - 2. * cm / (gam - 1.);
+      const double riemp = vnp + 2. * cp / (gam - 1.);
+      const double vnb = 0.5 * (riemp + riemm);
+      const double cb = 0.25 * (riemp - riemm) * (gam - 1.);
+      if (fabs(vnb / cb) > 1.) {
+        if (vnb <= 0.0) {
+          g[0] = rhom;
+          g[1] = um;
+          g[2] = vm;
+          g[3] = wm;
+          g[4] = pm;
+        } else {
+          g[0] = rhop;
+          g[1] = up;
+          g[2] = vp;
+          g[3] = wp;
+          g[4] = pp;
+        }
+      } else {
+        const double rela_vnb = vnb / P.uvw_norm;
+        const double eps_of_farfield_vn = 0.0;
+        if (rela_vnb <= -eps_of_farfield_vn) {
+          const double vtx = um - vnm * xfn, vty = vm - vnm * yfn, vtz = wm - vnm * zfn;
+          g[0] = pow((cb * cb / (P.entr_m * gam)), double(1. / (gam - 1.)));
+          g[1] = vtx + vnb * xfn;
+          g[2] = vty + vnb * yfn;
+          g[3] = vtz + vnb * zfn;
+          g[4] = cb * cb * g[0] / gam;
+        } else if (rela_vnb > eps_of_farfield_vn) {
+          const double vtx = up - vnp * xfn, vty = vp - vnp * yfn, vtz = wp - vnp * zfn;
+          const double entr = pp / pow(rhop, gam);
+          g[0] = pow((cb * cb / (entr * gam)), double(1. / (gam - 1.)));
+          g[1] = vtx + vnb * xfn;
+          g[2] = vty + vnb * yfn;
+          g[3] = vtz + vnb * zfn;
+          g[4] = cb * cb * g[0] / gam;
+        } else {
+          g[0] = 0.5 * (rhop + rhom);
+          g[1] = 0.5 * (up + um);
+          g[2] = 0.5 * (vp + vm);
+          g[3] = 0.5 * (wp + wm);
+          g[4] = 0.5 * (pp + pm);
+        }
+      }
+      g[0] = 2 * g[0] - rhop;
+      g[1] = 2 * g[1] - up;
+      g[2] = 2 * g[2] - vp;
+      g[3] = 2 * g[3] - wp;
+      g[4] = 2 * g[4] - pp;
+      g[4] -= p_bar;
+      break;
+    }
+    default:
+      break;  // the reference reports "Error in SetGhostVariables 001" and goes on
+  }
+  g[0] = smax(g[0], P.rho_min);  // :1204-1208
+  g[0] = smin(g[0], P.rho_max);
+  g[4] = smax(g[4], P.p_min);
+  g[4] = smin(g[4], P.p_max);
+  cell_props(g, P);
+  store_q(qa, c2, g);
+  store_q(qb, c2, g);
+  if (q4a) store_q4(q4a, c2, g);
+  if (q4b) store_q4(q4b, c2, g);
+}
+
 // Interior rows of an increment array set to the "not yet written" sentinel.
 __global__ void k_arm_sentinel(int32_t C, double *__restrict__ dq8) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1313,6 +1423,8 @@ struct mfg_ctx {
   SlotRec *slots = nullptr;
   FaceRec *faces = nullptr;  // per-face flux: normal, area, cells
   double *fflux = nullptr;   // per-face flux [5][F]
+  int32_t *bctype_d = nullptr;  // BC type of each boundary face [G]
+  int32_t live_bc = 0;          // ghost states recomputed every iteration
   int32_t *fnptr = nullptr, *fnodes = nullptr;
   int32_t *nptr = nullptr, *nsrc = nullptr, *ninfo = nullptr, *bface_c1 = nullptr;
   double *nw = nullptr, *wnode = nullptr, *nsym = nullptr;
@@ -1396,6 +1508,11 @@ Params make_params(const mfg_params &p) {
   P.ref[2] = p.v_s;
   P.ref[3] = p.w_s;
   P.ref[4] = p.p_s;
+  P.uvw_norm = sqrt(p.u_s * p.u_s + p.v_s * p.v_s + p.w_s * p.w_s);
+  {
+    const double pm = p.p_s + p.p_bar, rhom = p.rho_s;
+    P.entr_m = pm / pow(rhom, p.gam);
+  }
   return P;
 }
 
@@ -1922,6 +2039,8 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
                       m->f2c[2 * f + 1], 0, 0};
     if ((rc = dupload(ctx, &ctx->faces, fr))) return fail(rc);
     if ((rc = dalloc(ctx, &ctx->fflux, (size_t)5 * m->n_face))) return fail(rc);
+    std::vector<int32_t> bt(m->bctype, m->bctype + m->n_bface);
+    if ((rc = dupload(ctx, &ctx->bctype_d, bt))) return fail(rc);
   }
   slots.clear();
   slots.shrink_to_fit();
@@ -2192,6 +2311,40 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
   info->sweep_chunks = ctx->sweep_mode == 1 ? ctx->nchunks : 0;
   info->sweep_lanes = ctx->sweep_mode == 1 ? ctx->sweep_lanes : 0;
   info->sweep_records = ctx->sweep_w;
+  return MFG_OK;
+}
+
+static void drop_graphs(mfg_ctx *ctx) {
+  for (int k = 0; k < 2; k++)
+    if (ctx->graph[k]) {
+      cudaGraphExecDestroy(ctx->graph[k]);
+      ctx->graph[k] = nullptr;
+    }
+}
+
+static int launch_ghost_bc(mfg_ctx *ctx, cudaStream_t st) {
+  if (ctx->G == 0) return MFG_OK;
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  k_ghost_bc<<<grid_for(ctx->G), kBlock, 0, st>>>(
+      ctx->G, ctx->C, ctx->faces, ctx->bctype_d, ctx->q8[ctx->cur], ctx->q8[ctx->cur ^ 1],
+      mx ? ctx->q4[ctx->cur] : nullptr, mx ? ctx->q4[ctx->cur ^ 1] : nullptr, ctx->P,
+      cases_of(ctx));
+  count_launch();
+  return check_kernel();
+}
+
+int mfg_set_ghost_variables(mfg_ctx *ctx) {
+  if (!ctx) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  return launch_ghost_bc(ctx, ctx->stream);
+}
+
+int mfg_set_live_bc(mfg_ctx *ctx, int32_t on) {
+  if (!ctx || (on != 0 && on != 1)) return MFG_ERR_INVALID;
+  if (ctx->live_bc != on) {
+    ctx->live_bc = on;
+    drop_graphs(ctx);  // the captured iteration gains or loses the ghost update
+  }
   return MFG_OK;
 }
 
@@ -2556,6 +2709,11 @@ static int launch_iteration(mfg_ctx *ctx) {
   rc = launch_sweeps(ctx, true);
   if (rc) return rc;
   ctx->cur ^= 1;
+  if (ctx->live_bc) {
+    // main.cpp:286 with its SetGhostVariables call enabled
+    rc = launch_ghost_bc(ctx, ctx->stream);
+    if (rc) return rc;
+  }
   rc = launch_gradient(ctx);
   if (rc) return rc;
   return launch_norm_tail(ctx, ctx->stream);
@@ -2739,8 +2897,9 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
       }
       count_launch(Lf + Lb);
     }
-    cudaEventRecord(ev[3], st);
     ctx->cur ^= 1;
+    if (ctx->live_bc && rc == MFG_OK) rc = launch_ghost_bc(ctx, st);  // with the update
+    cudaEventRecord(ev[3], st);
     launch_node_values(ctx, st);
     cudaEventRecord(ev[4], st);
     launch_grad_faces(ctx, st);

@@ -70,6 +70,10 @@ struct Params {
   double gam, gamm1, p_bar, alf_l, lhs_omga, peff;
   double rho_min, rho_max, p_min, p_max, p_break, ratio_dtmax;
   double ref[5];  // freestream rho, u, v, w, gauge p (mixed gradient: values kept as deviations)
+  // SetGhostVariables' far-field constants (load_grid.cpp:1000-1003, :1105):
+  // |freestream velocity| and the freestream entropy pm / pow(rhom, gam),
+  // evaluated on the host with the C library's sqrt and pow
+  double uvw_norm, entr_m;
 };
 
 // Batched cases: several independent grids concatenated into one (cells,

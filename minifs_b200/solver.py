@@ -78,12 +78,25 @@ class Solver:
     def calculate_gradient(self):
         self._call("mfg_calculate_gradient")
 
+    def set_ghost_variables(self):
+        """``SetGhostVariables``: ghost states from the current inner cells."""
+        self._call("mfg_set_ghost_variables")
+
+    def set_live_bc(self, on: bool):
+        """Recompute the ghost states every iteration (after the LU-SGS
+        update, where ``main.cpp:286`` has the call commented out) instead
+        of keeping the initial ones."""
+        self._call("mfg_set_live_bc", 1 if on else 0)
+        self.live_bc = bool(on)
+
     def step(self):
         """One ``main.cpp:201-291`` iteration through the per-routine calls."""
         self.zero_residuals()
         self.inviscid_flux()
         self.compute_timestep()
         self.forward_lusgs()
+        if getattr(self, "live_bc", False):
+            self.set_ghost_variables()
         self.calculate_gradient()
         self.iter_done += 1
 

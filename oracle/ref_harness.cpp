@@ -11,8 +11,10 @@
 //   * the seeded initial state: a Gaussian density bump at the cell
 //     centroids, applied between AllocAndInitFlowfield and SetGhostVariables
 //     in the PreprocessGrid sequence (load_grid.cpp:443-531).
-// The iteration loop is main.cpp:201-291 verbatim in call order.  Arrays are
-// dumped to a simple tagged binary file for the Python tests.
+// The iteration loop is main.cpp:201-291 verbatim in call order (with
+// --live-bc, also the SetGhostVariables call that main.cpp:286 comments
+// out).  Arrays are dumped to a simple tagged binary file for the Python
+// tests.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -200,6 +202,7 @@ int main(int argc, char **argv) {
   std::set<int> dump_iters;
   bool dump_all_iters = false;
   bool light = false;  // timings and norms only
+  bool live_bc = false;  // SetGhostVariables in the loop, where main.cpp:286 has it commented out
   for (int a = 1; a < argc; a++) {
     std::string k = argv[a];
     auto need = [&](void) -> const char * {
@@ -212,6 +215,7 @@ int main(int argc, char **argv) {
     else if (k == "--out") out = need();
     else if (k == "--write-mesh") write_mesh = need();
     else if (k == "--light") light = true;
+    else if (k == "--live-bc") live_bc = true;
     else if (k == "--dump-iters") {
       std::string v = need();
       if (v == "all") dump_all_iters = true;
@@ -228,7 +232,8 @@ int main(int argc, char **argv) {
   }
   if (!mesh || !bcf || !params) {
     fprintf(stderr, "usage: %s --mesh f.mfl --bc bc.para --params p.txt [--out dump.bin] "
-                    "[--dump-iters 0,1,5|all] [--write-mesh renumbered.mfl]\n", argv[0]);
+                    "[--dump-iters 0,1,5|all] [--write-mesh renumbered.mfl] [--light] "
+                    "[--live-bc]\n", argv[0]);
     return 2;
   }
   std::map<std::string, double> kv = read_params(params);
@@ -340,6 +345,7 @@ int main(int argc, char **argv) {
     t_a = now_s();
     ForwardLUSGS(grid, 0);
     PassInterfaceData(grid);
+    if (live_bc) SetGhostVariables(grid);
     t_b = now_s();
     CalculateGradient(grid);
     iter_done++;

@@ -61,7 +61,7 @@ def write_params(path: str, params: dict) -> None:
 
 def run(mesh, params: dict, *, tdtree: bool = False, dump_iters="0", threads: int | None = None,
         write_mesh: bool = False, workdir: str | None = None, dump: bool = True,
-        timeout: float | None = None, light: bool = False) -> dict:
+        timeout: float | None = None, light: bool = False, live_bc: bool = False) -> dict:
     """Run the reference on ``mesh`` (a ``meshgen.RawMesh``) and return the dump.
 
     The returned dict also carries ``"summary"`` (the JSON line the harness
@@ -86,6 +86,8 @@ def run(mesh, params: dict, *, tdtree: bool = False, dump_iters="0", threads: in
         cmd += ["--out", out, "--dump-iters", str(dump_iters) if dump else "-1"]
     if light:
         cmd += ["--light"]
+    if live_bc:
+        cmd += ["--live-bc"]
     ren = os.path.join(tmp, "renumbered.mfl")
     if write_mesh:
         cmd += ["--write-mesh", ren]
