@@ -215,7 +215,10 @@ int mfg_set_live_bc(mfg_ctx *ctx, int32_t on);
 int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms);
 /* End-to-end form with host buffers: copies q_in [5n] (host) in, runs
  * n_iter iterations, copies the state to q_out [5n] and the residual to
- * res_out [5C] (either may be NULL).  Pinned host memory is fastest. */
+ * res_out [5C] (either may be NULL).  Pinned host memory is fastest.  The
+ * copies out overlap the last iteration: the residual leaves during its
+ * LU-SGS sweeps, the state during its gradient (on a second stream of the
+ * context); the call returns when both are in host memory. */
 int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const double *q_in,
                      double *q_out, double *res_out, double *norms);
 /* Phases of one fused iteration, for mfg_profile_phases. */

@@ -1402,6 +1402,10 @@ struct mfg_ctx {
   int device = 0;
   int precision = MFG_PREC_FP64;
   cudaStream_t own_stream = nullptr, stream = nullptr;
+  // mfg_iterate_host: results copied out on a second stream while the last
+  // iteration's later kernels run
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_res = nullptr, ev_state = nullptr;
   int32_t C = 0, G = 0, F = 0, N = 0;
   int64_t n = 0, S = 0;
   mfg_params hp{};
@@ -1613,6 +1617,9 @@ static void free_ctx(mfg_ctx *ctx) {
     if (ctx->graph[k]) cudaGraphExecDestroy(ctx->graph[k]);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->ev_res) cudaEventDestroy(ctx->ev_res);
+  if (ctx->ev_state) cudaEventDestroy(ctx->ev_state);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -2703,9 +2710,15 @@ static int fill_cfl_table(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done) {
 
 // One fused iteration: flux + dt + Diag in one gather, level sweeps with the
 // update, gradient, residual norm.  Reads the CFL from cfl_tab[counter].
-static int launch_iteration(mfg_ctx *ctx) {
+// Optional hooks for a caller that copies results out while the iteration
+// runs on: `after_face` is recorded once the residual is final (nothing
+// later in the iteration writes it), `after_update` once the new state has
+// been unpacked into the SoA staging buffer.
+static int launch_iteration(mfg_ctx *ctx, cudaEvent_t after_face = nullptr,
+                            cudaEvent_t after_update = nullptr) {
   int rc = launch_face(ctx, true, true, true, 0.0, true);
   if (rc) return rc;
+  if (after_face) MFG_CUDA(cudaEventRecord(after_face, ctx->stream));
   rc = launch_sweeps(ctx, true);
   if (rc) return rc;
   ctx->cur ^= 1;
@@ -2713,6 +2726,13 @@ static int launch_iteration(mfg_ctx *ctx) {
     // main.cpp:286 with its SetGhostVariables call enabled
     rc = launch_ghost_bc(ctx, ctx->stream);
     if (rc) return rc;
+  }
+  if (after_update) {
+    k_download_rec<<<grid_for(ctx->n), kBlock, 0, ctx->stream>>>(ctx->q8[ctx->cur],
+                                                                  ctx->staging, ctx->n);
+    count_launch();
+    MFG_CUDA(cudaGetLastError());
+    MFG_CUDA(cudaEventRecord(after_update, ctx->stream));
   }
   rc = launch_gradient(ctx);
   if (rc) return rc;
@@ -2921,15 +2941,61 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
   return check_sweep_error(ctx);
 }
 
+// The state and the residual of the last iteration leave on a second stream
+// as soon as each is final: the residual (written only by the face gather)
+// during the sweeps, the state during the gradient.  The first n_iter - 1
+// iterations run as graphs, the last one as plain launches with two event
+// hooks (the same kernels in the same order as the graph).
 int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const double *q_in,
                      double *q_out, double *res_out, double *norms) {
-  if (!ctx) return MFG_ERR_INVALID;
+  if (!ctx || n_iter < 0) return MFG_ERR_INVALID;
   int rc;
   if (q_in && (rc = mfg_upload(ctx, MFG_FIELD_Q, q_in))) return rc;
-  if ((rc = mfg_iterate(ctx, n_iter, iter_done, norms))) return rc;
-  if (q_out && (rc = mfg_download(ctx, MFG_FIELD_Q, q_out))) return rc;
-  if (res_out && (rc = mfg_download(ctx, MFG_FIELD_RES, res_out))) return rc;
-  return MFG_OK;
+  if (n_iter == 0 || (!q_out && !res_out)) {
+    if ((rc = mfg_iterate(ctx, n_iter, iter_done, norms))) return rc;
+    if (q_out && (rc = mfg_download(ctx, MFG_FIELD_Q, q_out))) return rc;
+    if (res_out && (rc = mfg_download(ctx, MFG_FIELD_RES, res_out))) return rc;
+    return MFG_OK;
+  }
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (!ctx->copy_stream) {
+    MFG_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    MFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_res, cudaEventDisableTiming));
+    MFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_state, cudaEventDisableTiming));
+  }
+  if ((rc = fill_cfl_table(ctx, n_iter, iter_done))) return rc;
+  ctx->res_zero = true;
+  if (n_iter > 1 && (rc = ensure_graphs(ctx))) return rc;
+  for (int32_t i = 0; i + 1 < n_iter; i++) {
+    MFG_CUDA(cudaGraphLaunch(ctx->graph[ctx->cur], st));
+    count_launch(ctx->graph_nodes);
+    ctx->cur ^= 1;
+  }
+  ctx->res_zero = true;  // the plain iteration starts with ZeroResiduals too
+  rc = launch_iteration(ctx, res_out ? ctx->ev_res : nullptr, q_out ? ctx->ev_state : nullptr);
+  ctx->res_zero = false;
+  if (rc) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
+  cudaStream_t cp = ctx->copy_stream;
+  if (res_out) {
+    MFG_CUDA(cudaStreamWaitEvent(cp, ctx->ev_res, 0));
+    MFG_CUDA(cudaMemcpyAsync(res_out, ctx->res, sizeof(double) * 5 * ctx->C,
+                             cudaMemcpyDeviceToHost, cp));
+  }
+  if (q_out) {
+    MFG_CUDA(cudaStreamWaitEvent(cp, ctx->ev_state, 0));
+    MFG_CUDA(cudaMemcpyAsync(q_out, ctx->staging, sizeof(double) * 5 * ctx->n,
+                             cudaMemcpyDeviceToHost, cp));
+  }
+  if (norms)
+    MFG_CUDA(cudaMemcpyAsync(norms, ctx->norm_hist, sizeof(double) * 5 * n_iter * ctx->ncase,
+                             cudaMemcpyDeviceToHost, st));
+  MFG_CUDA(cudaStreamSynchronize(st));
+  MFG_CUDA(cudaStreamSynchronize(cp));
+  return check_sweep_error(ctx);
 }
 
 int mfg_residual_norm(mfg_ctx *ctx, double out[5]) {

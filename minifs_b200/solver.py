@@ -109,11 +109,12 @@ class Solver:
         self.iter_done += n
         return out.reshape(n, 5) if norms else None
 
-    def iterate_host(self, n: int, q_in: np.ndarray, q_out: np.ndarray | None,
+    def iterate_host(self, n: int, q_in: np.ndarray | None, q_out: np.ndarray | None,
                      res_out: np.ndarray | None):
-        """End-to-end form: host state in, ``n`` iterations, host state and
-        residual out."""
-        self._call("mfg_iterate_host", int(n), int(self.iter_done), _lib.ptr(q_in),
+        """End-to-end form: host state in (None: keep the context's), ``n``
+        iterations, host state and residual out (either may be None)."""
+        self._call("mfg_iterate_host", int(n), int(self.iter_done),
+                   _lib.ptr(q_in) if q_in is not None else None,
                    _lib.ptr(q_out) if q_out is not None else None,
                    _lib.ptr(res_out) if res_out is not None else None, None)
         self.iter_done += n
