@@ -278,6 +278,26 @@ def prep_on_gpu(mesh, params, wl, pg, host_s, device):
                      "CalC2N, ComputeWeight3D_Node, FindNodeSYMM"}
 
 
+def setup_on_device(mesh, params, wl, device):
+    """Raw host mesh to a ready context with the grid kept on the device:
+    the GPU preprocessing, the initial state on the host from the device's
+    centroids and normals, and the context built on the device
+    (mfg_create_from_prep).  Seconds of each part."""
+    from minifs_b200 import grid as gr
+    from minifs_b200.solver import Solver
+    t0 = time.perf_counter()
+    prep = gr.DevicePrep(mesh, device=device)
+    t1 = time.perf_counter()
+    q0 = prep.init_flow(params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
+    t2 = time.perf_counter()
+    s = Solver.from_device_prep(prep, params, q0)
+    t3 = time.perf_counter()
+    s.close()
+    prep.close()
+    return {"total_s": t3 - t0, "prep_s": t1 - t0, "init_flow_s": t2 - t1,
+            "create_s": t3 - t2}
+
+
 def run_reference_arm(args, rank, world):
     wl = workload(args.size)
     if rank != 0:
@@ -480,6 +500,8 @@ def run_single(args, rank, world, local, stream, dist):
     t = time.perf_counter()
     s = Solver(pg, params, device=local)
     prep["solver_create_s"] = time.perf_counter() - t
+    prep["device_path"] = setup_on_device(mesh, params, wl, local)
+    prep["host_path_setup_s"] = host_prep_s + prep["solver_create_s"]
     s.set_stream(stream.cuda_stream)
     C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
     K = int(pg.arrays["nnpc"].sum())

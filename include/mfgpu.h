@@ -376,6 +376,21 @@ int mfg_prep_gpu_node_weights(mfg_prep_gpu *p, double *wnode, int32_t *nmark, do
  * (CUDA events around them; the copies of the raw grid are outside). */
 int mfg_prep_gpu_kernel_ms(const mfg_prep_gpu *p, double *ms);
 int mfg_prep_gpu_destroy(mfg_prep_gpu *p);
+/* mfg_prep_init_flow for a device-resident preprocessing: the boundary
+ * normals, cell centroids, boundary f2c and BC types it reads are copied to
+ * the host and the host routine fills q [5n] (host memory). */
+int mfg_prep_gpu_init_flow(mfg_prep_gpu *p, const mfg_params *params, double bump_amp,
+                           double bump_sigma, double bump_x0, double bump_y0, double bump_z0,
+                           double *q);
+/* A context built on the device from a device-resident preprocessing, for
+ * the identity LU-SGS order: the context mfg_create makes from the arrays
+ * of that preprocessing (the same tables, the same results), without their
+ * round trip through the host.  Slots, face records, level sets, sweep
+ * records and node lists are built by device kernels; the chunk assignment
+ * of the persistent sweeps runs on the host (both sweeps at once).  q0 [5n]
+ * is host memory; the device is the preprocessing's, which stays valid. */
+int mfg_create_from_prep(const mfg_prep_gpu *prep, const mfg_params *params, const double *q0,
+                         int32_t precision, mfg_ctx **out);
 
 #ifdef __cplusplus
 }

@@ -161,6 +161,10 @@ def load(build_if_missing: bool = True):
         "mfg_prep_gpu_node_weights": (ct.c_int, [ct.c_void_p, f64p, i32p, f64p, i32p, i32p, f64p,
                                                  i32p, f64p, f64p, f64p]),
         "mfg_prep_gpu_destroy": (ct.c_int, [ct.c_void_p]),
+        "mfg_prep_gpu_init_flow": (ct.c_int, [ct.c_void_p, ct.POINTER(Params)] +
+                                   [ct.c_double] * 5 + [f64p]),
+        "mfg_create_from_prep": (ct.c_int, [ct.c_void_p, ct.POINTER(Params), f64p, ct.c_int32,
+                                            ct.POINTER(ctxp)]),
         "mfg_mfl_read": (ct.c_int, [ct.c_char_p, ct.POINTER(ct.POINTER(Mfl))]),
         "mfg_mfl_write": (ct.c_int, [ct.c_char_p, ct.POINTER(Mfl)]),
         "mfg_mfl_free": (ct.c_int, [ct.POINTER(Mfl)]),

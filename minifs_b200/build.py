@@ -20,7 +20,7 @@ LIB = os.path.join(LIBDIR, "libmfgpu.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 SOURCES = ["mfg_device.cu", "mfg_prep.cu", "mfg_host.cpp", "mfg_io.cpp"]
-DEPS = SOURCES + ["mfg_kernels.cuh"]
+DEPS = SOURCES + ["mfg_kernels.cuh", "mfg_internal.h"]
 
 
 def nvcc() -> str:

@@ -24,6 +24,12 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <thread>
+
+#include "mfg_internal.h"
 #include "mfg_kernels.cuh"
 #include "mfgpu.h"
 
@@ -44,6 +50,16 @@ constexpr int kSegBlocks = 32;     // blocks per case of the batched norm reduct
     if (e_ != cudaSuccess) {                                                      \
       g_cuda_error = std::string(#call) + ": " + cudaGetErrorString(e_);          \
       return MFG_ERR_CUDA;                                                        \
+    }                                                                             \
+  } while (0)
+
+// The same inside a context build: the partly built context is released.
+#define MFG_CUDA_OR(call)                                                         \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      g_cuda_error = std::string(#call) + ": " + cudaGetErrorString(e_);          \
+      return fail(MFG_ERR_CUDA);                                                  \
     }                                                                             \
   } while (0)
 
@@ -1588,6 +1604,329 @@ void note_cuda_error(const char *what, int code) {
 void note_launches(int64_t k) { count_launch(k); }
 }  // namespace mfg
 
+// ---------------------------------------------------------------------------
+// Context tables built on the device from a device-resident preprocessing
+// (mfg_create_from_prep): the arrays create_impl builds on the host, for the
+// identity LU-SGS order, from the preprocessing's own lists.
+// ---------------------------------------------------------------------------
+namespace {
+
+// create_impl's slot loop, one thread per cell
+__global__ void k_dev_slots(int32_t C, int32_t B, const int32_t *__restrict__ cptr,
+                            const int32_t *__restrict__ cf, const int32_t *__restrict__ f2c,
+                            const int32_t *__restrict__ bctype, const double *__restrict__ xfn,
+                            const double *__restrict__ yfn, const double *__restrict__ zfn,
+                            const double *__restrict__ area, const double *__restrict__ xfc,
+                            const double *__restrict__ yfc, const double *__restrict__ zfc,
+                            const double *__restrict__ xcc, const double *__restrict__ ycc,
+                            const double *__restrict__ zcc, SlotRec *__restrict__ slots,
+                            int32_t *__restrict__ bad) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  const double cx = xcc[c], cy = ycc[c], cz = zcc[c];
+  for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+    const int32_t f = cf[j];
+    SlotRec sr;
+    const bool is_c1 = f2c[2 * f] == c;
+    sr.nx = xfn[f];
+    sr.ny = yfn[f];
+    sr.nz = zfn[f];
+    sr.area = area[f];
+    // compute_timestep.cpp:762, the same expression for either side
+    sr.dn = fabs((xfc[f] - cx) * sr.nx + (yfc[f] - cy) * sr.ny + (zfc[f] - cz) * sr.nz);
+    sr.nb = is_c1 ? f2c[2 * f + 1] : f2c[2 * f];
+    if (sr.nb == c) atomicAdd(bad, 1);  // the cell on both sides of a face
+    sr.face = f;
+    sr.flags = is_c1 ? 0 : SLOT_IS_C2;
+    if (f < B) {
+      sr.flags |= SLOT_BOUNDARY;
+      const int t = bctype[f];
+      if (t == MFG_BC_INTERFACE || t == MFG_BC_SYMM) sr.flags |= SLOT_NODE_AVG;
+    }
+    sr.pad = 0;
+    slots[j] = sr;
+  }
+}
+
+__global__ void k_dev_faces(int32_t F, const int32_t *__restrict__ f2c,
+                            const double *__restrict__ xfn, const double *__restrict__ yfn,
+                            const double *__restrict__ zfn, const double *__restrict__ area,
+                            FaceRec *__restrict__ faces) {
+  const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= F) return;
+  faces[f] = FaceRec{xfn[f], yfn[f], zfn[f], area[f], f2c[2 * f], f2c[2 * f + 1], 0, 0};
+}
+
+// Records per cell of each sweep (forward: the neighbours before the cell in
+// the identity order; backward: those after it, ghosts included) and the
+// in-degrees of the level computation (interior dependencies only).
+__global__ void k_dev_counts(int32_t C, const int32_t *__restrict__ cptr,
+                             const SlotRec *__restrict__ slots, int32_t *__restrict__ fw_cnt,
+                             int32_t *__restrict__ bw_cnt, int32_t *__restrict__ fw_deg,
+                             int32_t *__restrict__ bw_deg, int32_t *__restrict__ maxns) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  int32_t fw = 0, bw = 0, bwi = 0;
+  for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+    const int32_t nb = slots[j].nb;
+    if (nb < c) {
+      fw++;
+    } else {
+      bw++;
+      if (nb < C) bwi++;
+    }
+  }
+  fw_cnt[c] = fw;
+  bw_cnt[c] = bw;
+  fw_deg[c] = fw;
+  bw_deg[c] = bwi;
+  atomicMax(maxns, max(fw, bw));
+}
+
+// Level sets as a breadth-first release: a cell joins level l + 1 when the
+// last of its dependencies (all on levels <= l) has been processed, which is
+// 1 + the longest dependency chain below it, the level create_impl computes.
+__global__ void k_dev_level_seed(int32_t C, const int32_t *__restrict__ deg,
+                                 int32_t *__restrict__ lvl, int32_t *__restrict__ front,
+                                 int32_t *__restrict__ count) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  if (deg[c] == 0) {
+    lvl[c] = 0;
+    front[atomicAdd(count, 1)] = c;
+  }
+}
+
+__global__ void k_dev_level_step(int32_t nf, const int32_t *__restrict__ front, int32_t level,
+                                 int fwd, int32_t C, const int32_t *__restrict__ cptr,
+                                 const SlotRec *__restrict__ slots, int32_t *__restrict__ deg,
+                                 int32_t *__restrict__ lvl, int32_t *__restrict__ next,
+                                 int32_t *__restrict__ next_count) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const int32_t c = front[i];
+  for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+    const int32_t nb = slots[j].nb;
+    if (nb >= C || (fwd ? nb <= c : nb >= c)) continue;  // not a dependant of c
+    if (atomicSub(&deg[nb], 1) == 1) {
+      lvl[nb] = level + 1;
+      next[atomicAdd(next_count, 1)] = nb;
+    }
+  }
+}
+
+__global__ void k_dev_iota(int32_t C, int32_t *__restrict__ v) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < C) v[i] = i;
+}
+
+// g[i] = cnt[cells[i]] (and g[C] = 0), for the record offsets of the
+// level-sorted cells
+__global__ void k_dev_gather_cnt(int32_t C, const int32_t *__restrict__ cells,
+                                 const int32_t *__restrict__ cnt, int32_t *__restrict__ g) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < C) g[i] = cnt[cells[i]];
+  if (i == C) g[C] = 0;
+}
+
+// build_levels' per-level sweep records, one thread per level-sorted cell
+__global__ void k_dev_level_records(int32_t C, const int32_t *__restrict__ cells,
+                                    const int32_t *__restrict__ sptr,
+                                    const int32_t *__restrict__ cptr,
+                                    const SlotRec *__restrict__ slots, int fwd,
+                                    SweepRec *__restrict__ recs, int32_t *__restrict__ nbs) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const int32_t c = cells[i];
+  if (fwd && c == 0) return;  // the first cell of the order only divides by Diag
+  int32_t o = sptr[i];
+  for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
+    const SlotRec sr = slots[j];
+    const int32_t nb = sr.nb;
+    if (fwd ? nb > c : nb < c) continue;
+    const bool is_c1 = (sr.flags & SLOT_IS_C2) == 0;
+    SweepRec r;
+    r.nx = is_c1 ? sr.nx : -sr.nx;
+    r.ny = is_c1 ? sr.ny : -sr.ny;
+    r.nz = is_c1 ? sr.nz : -sr.nz;
+    r.w = fwd ? 0.5 * sr.area : sr.area;
+    recs[o] = r;
+    nbs[o] = nb;
+    o++;
+  }
+}
+
+// chunk of each level-sorted position (sort key) and its index (value)
+__global__ void k_dev_chunk_keys(int32_t C, const int32_t *__restrict__ cells,
+                                 const int32_t *__restrict__ assign, int32_t *__restrict__ keys,
+                                 int32_t *__restrict__ idx, int32_t *__restrict__ chunk_cnt) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C) return;
+  const int32_t p = assign[cells[i]];
+  keys[i] = p;
+  idx[i] = i;
+  atomicAdd(&chunk_cnt[p], 1);
+}
+
+// chunk-major positions: cell, position of each cell, segment heads
+// (chunk start or level change)
+__global__ void k_dev_positions(int32_t C, const int32_t *__restrict__ order,
+                                const int32_t *__restrict__ cells,
+                                const int32_t *__restrict__ pchunk, const int32_t *__restrict__ lvl,
+                                int32_t *__restrict__ ccells, int32_t *__restrict__ posof,
+                                int32_t *__restrict__ head) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > C) return;
+  if (k == C) {
+    head[C] = 0;
+    return;
+  }
+  const int32_t c = cells[order[k]];
+  ccells[k] = c;
+  posof[c] = k;
+  head[k] = (k == 0 || pchunk[k] != pchunk[k - 1] || lvl[c] != lvl[cells[order[k - 1]]]) ? 1 : 0;
+}
+
+__global__ void k_dev_segs(int32_t C, const int32_t *__restrict__ head,
+                           const int32_t *__restrict__ hscan, int32_t *__restrict__ segs) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > C) return;
+  if (k == C)
+    segs[hscan[C]] = C;
+  else if (head[k])
+    segs[hscan[k]] = k;
+}
+
+__global__ void k_dev_seg_begin(int32_t P, const int32_t *__restrict__ chunk_ptr,
+                                const int32_t *__restrict__ hscan,
+                                int32_t *__restrict__ seg_begin) {
+  const int32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p <= P) seg_begin[p] = hscan[chunk_ptr[p]];
+}
+
+// build_levels' position-major tables, one thread per chunk-major position
+template <bool MX>
+__global__ void k_dev_pack(int32_t C, int32_t W, int with_recs, const int32_t *__restrict__ order,
+                           const int32_t *__restrict__ ccells, const int32_t *__restrict__ pchunk,
+                           const int32_t *__restrict__ head, const int32_t *__restrict__ hscan,
+                           const int32_t *__restrict__ segs, const int32_t *__restrict__ chunk_ptr,
+                           const int32_t *__restrict__ posof, const int32_t *__restrict__ assign,
+                           const int32_t *__restrict__ sptr, const int32_t *__restrict__ nbs,
+                           const SweepRec *__restrict__ recs, PosCell *__restrict__ packed,
+                           int32_t *__restrict__ cnbs, SweepRec *__restrict__ crecs,
+                           SweepRecF *__restrict__ crecs_f, int32_t *__restrict__ cslot,
+                           int32_t *__restrict__ chunk0_exported) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= C) return;
+  const int32_t gi = order[k];
+  const int32_t c = ccells[k];
+  const int32_t s0 = sptr[gi], ns = sptr[gi + 1] - s0;
+  packed[k] = PosCell{c, ns};
+  if (!with_recs) return;
+  const int32_t p = pchunk[k];
+  const int32_t seg_end = segs[hscan[k] + head[k]];  // next segment head
+  for (int32_t j = 0; j < ns; j++) {
+    const int32_t nb = nbs[s0 + j];
+    const int64_t o = (int64_t)k * W + j;
+    const bool cross = nb < C && assign[nb] != p;
+    if (cross && assign[nb] == 0) *chunk0_exported = 1;
+    uint32_t e = (uint32_t)nb;
+    if (cross) {
+      e |= kMark;
+    } else if (nb < C && posof[nb] >= seg_end - kRing) {
+      e |= kInRing;
+      cslot[o] = (posof[nb] - chunk_ptr[p]) & (kRing - 1);
+    }
+    cnbs[o] = (int32_t)e;
+    const SweepRec r = recs[s0 + j];
+    if (MX)
+      crecs_f[o] = SweepRecF{(float)r.nx, (float)r.ny, (float)r.nz, (float)r.w};
+    else
+      crecs[o] = r;
+  }
+}
+
+// build_node_lists' passes (CompNodeVar3D_dist, cal_gradient.cpp:2041-2125,
+// :2261-2279): a boundary entry of pass 0 (walls), 1 (far field) or 2
+// (other types), and whether the node's mark lets it through
+__device__ __forceinline__ bool node_pass_takes(int pass, int t, int mark) {
+  if (pass == 0) return t == MFG_BC_WALL;
+  if (pass == 1) return t == MFG_BC_FAR_FIELD && mark != MFG_BC_WALL;
+  return !(t == MFG_BC_WALL || t == MFG_BC_SYMM || t == MFG_BC_FAR_FIELD ||
+           t == MFG_BC_INTERFACE) &&
+         mark != MFG_BC_WALL && mark != MFG_BC_FAR_FIELD;
+}
+
+template <bool FILL>
+__global__ void k_dev_node_lists(int32_t N, const int32_t *__restrict__ nbptr,
+                                 const int32_t *__restrict__ nblist,
+                                 const int32_t *__restrict__ bent_face,
+                                 const int32_t *__restrict__ bctype,
+                                 const int32_t *__restrict__ ncptr,
+                                 const int32_t *__restrict__ nclist,
+                                 const int32_t *__restrict__ c2n_cell,
+                                 const int32_t *__restrict__ nmark,
+                                 const double *__restrict__ wbface,
+                                 const double *__restrict__ wc2n, int32_t *__restrict__ cnt,
+                                 int32_t *__restrict__ bad, const int32_t *__restrict__ nptr,
+                                 int32_t *__restrict__ nsrc, double *__restrict__ nw) {
+  const int32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int mark = nmark[p];
+  const int32_t o0 = FILL ? nptr[p] : 0;
+  int32_t o = o0;
+  for (int pass = 0; pass < 3; pass++)
+    for (int32_t s = nbptr[p]; s < nbptr[p + 1]; s++) {
+      const int32_t k = nblist[s];
+      const int32_t i = bent_face[k];
+      if (!node_pass_takes(pass, bctype[i], mark)) continue;
+      if (FILL) {
+        nsrc[o] = i;
+        nw[o] = wbface[k];
+      }
+      o++;
+    }
+  const int32_t nbnd = o - o0;
+  if (mark == 0) {
+    for (int32_t s = ncptr[p]; s < ncptr[p + 1]; s++) {
+      const int32_t m = nclist[s];
+      if (FILL) {
+        nsrc[o] = c2n_cell[m];
+        nw[o] = wc2n[m];
+      }
+      o++;
+    }
+  }
+  if (!FILL) {
+    cnt[p] = o;
+    if (nbnd > 0 && o > nbnd) atomicAdd(bad, 1);  // both kinds of entry
+  }
+}
+
+__global__ void k_dev_node_info(int32_t N, const int32_t *__restrict__ nmark,
+                                const int32_t *__restrict__ nodesymm,
+                                const double *__restrict__ xs, const double *__restrict__ ys,
+                                const double *__restrict__ zs, int32_t *__restrict__ info,
+                                double *__restrict__ nsym) {
+  const int32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  int32_t v = nmark[p] != 0 ? 1 : 0;
+  const bool sym = nodesymm[p] == 1;
+  if (sym) v |= 2;
+  info[p] = v;
+  nsym[3 * (int64_t)p] = sym ? xs[p] : 0.0;
+  nsym[3 * (int64_t)p + 1] = sym ? ys[p] : 0.0;
+  nsym[3 * (int64_t)p + 2] = sym ? zs[p] : 0.0;
+}
+
+__global__ void k_dev_bface_c1(int32_t G, const int32_t *__restrict__ f2c,
+                               int32_t *__restrict__ bc1) {
+  const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < G) bc1[k] = f2c[2 * k];
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *mfg_error_string(int32_t code) {
@@ -1628,6 +1967,52 @@ int mfg_destroy(mfg_ctx *ctx) {
   if (!ctx) return MFG_ERR_INVALID;
   free_ctx(ctx);
   return MFG_OK;
+}
+
+// Chunks for the persistent sweeps, one per resident block.  Level by level
+// (lptr over the level-sorted cells, sptr/nbs their dependencies), a cell
+// joins the chunk that most of its dependencies are in, unless that chunk
+// already holds its share of the level; the remaining cells fill the chunks
+// in order.  Every level is thereby spread evenly over the chunks while
+// dependency chains mostly stay in one chunk.
+static void assign_chunks(int32_t C, int32_t P, const std::vector<int32_t> &lptr,
+                          const int32_t *cells, const int32_t *sptr, const int32_t *nbs,
+                          std::vector<int32_t> &assign) {
+  const int32_t L = (int32_t)lptr.size() - 1;
+  assign.assign(C, -1);
+  std::vector<int32_t> load(P), pending;
+  for (int32_t l = 0; l < L; l++) {
+    const int32_t a0 = lptr[l], a1 = lptr[l + 1];
+    const int32_t quota = (a1 - a0 + P - 1) / P;
+    std::fill(load.begin(), load.end(), 0);
+    pending.clear();
+    for (int32_t i = a0; i < a1; i++) {
+      int32_t best = -1, bestn = 0;
+      for (int32_t s0 = sptr[i]; s0 < sptr[i + 1]; s0++) {
+        if (nbs[s0] >= C) continue;
+        const int32_t ch = assign[nbs[s0]];
+        int32_t votes = 0;
+        for (int32_t t = sptr[i]; t < sptr[i + 1]; t++)
+          if (nbs[t] < C && assign[nbs[t]] == ch) votes++;
+        if (votes > bestn) {
+          best = ch;
+          bestn = votes;
+        }
+      }
+      if (best >= 0 && load[best] < quota) {
+        assign[cells[i]] = best;
+        load[best]++;
+      } else {
+        pending.push_back(cells[i]);
+      }
+    }
+    int32_t pp = 0;
+    for (int32_t c : pending) {
+      while (load[pp] >= quota) pp++;
+      assign[c] = pp;
+      load[pp]++;
+    }
+  }
 }
 
 static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32_t> &cptr,
@@ -1737,45 +2122,9 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
         s++;
       }
     }
-    // Chunks for the persistent sweeps, one per resident block.  Level by
-    // level, a cell joins the chunk that most of its dependencies are in,
-    // unless that chunk already holds its share of the level; the remaining
-    // cells fill the chunks in order.  Every level is thereby spread evenly
-    // over the chunks while dependency chains mostly stay in one chunk.
     const int32_t P = ctx->nchunks;
-    std::vector<int32_t> assign(C, -1), load(P), pending, chunk_cnt(P, 0);
-    for (int32_t l = 0; l < L; l++) {
-      const int32_t a0 = lptr[l], a1 = lptr[l + 1];
-      const int32_t quota = (a1 - a0 + P - 1) / P;
-      std::fill(load.begin(), load.end(), 0);
-      pending.clear();
-      for (int32_t i = a0; i < a1; i++) {
-        int32_t best = -1, bestn = 0;
-        for (int32_t s0 = sptr[i]; s0 < sptr[i + 1]; s0++) {
-          if (nbs[s0] >= C) continue;
-          const int32_t ch = assign[nbs[s0]];
-          int32_t votes = 0;
-          for (int32_t t = sptr[i]; t < sptr[i + 1]; t++)
-            if (nbs[t] < C && assign[nbs[t]] == ch) votes++;
-          if (votes > bestn) {
-            best = ch;
-            bestn = votes;
-          }
-        }
-        if (best >= 0 && load[best] < quota) {
-          assign[cells[i]] = best;
-          load[best]++;
-        } else {
-          pending.push_back(cells[i]);
-        }
-      }
-      int32_t pp = 0;
-      for (int32_t c : pending) {
-        while (load[pp] >= quota) pp++;
-        assign[c] = pp;
-        load[pp]++;
-      }
-    }
+    std::vector<int32_t> assign, chunk_cnt(P, 0);
+    assign_chunks(C, P, lptr, cells.data(), sptr.data(), nbs.data(), assign);
     // chunk-major, level-sorted cell lists (the level order is already sorted)
     for (int32_t c = 0; c < C; c++) chunk_cnt[assign[c]]++;
     std::vector<int32_t> chunk_ptr(P + 1, 0);
@@ -1956,12 +2305,12 @@ struct CaseLayout {
   std::vector<int32_t> cell0, bface0, of, first;
 };
 
-static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLayout &cl,
-                       const double *q0, int32_t device, int32_t precision, mfg_ctx **out) {
-  if (!out || !params || !q0) return MFG_ERR_INVALID;
+// Device, stream, sizes, parameters, case tables and sweep occupancy of a
+// new context (whatever builds its grid tables next).
+static int ctx_begin(int32_t n_node, int32_t n_face, int32_t n_cell, int32_t n_bface,
+                     const mfg_params *params, const CaseLayout &cl, int32_t device,
+                     int32_t precision, mfg_ctx **out) {
   *out = nullptr;
-  int rc = validate_mesh(m);
-  if (rc) return rc;
   if (precision != MFG_PREC_FP64 && precision != MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) {
@@ -1969,6 +2318,7 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
     return MFG_ERR_NODEVICE;
   }
   mfg_ctx *ctx = new mfg_ctx();
+  int rc;
   ctx->device = device;
   ctx->precision = precision;
   auto fail = [&](int code) {
@@ -1982,17 +2332,16 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(MFG_ERR_CUDA);
   ctx->stream = ctx->own_stream;
-  ctx->C = m->n_cell;
-  ctx->G = m->n_bface;
-  ctx->F = m->n_face;
-  ctx->N = m->n_node;
-  ctx->n = (int64_t)m->n_cell + m->n_bface;
+  ctx->C = n_cell;
+  ctx->G = n_bface;
+  ctx->F = n_face;
+  ctx->N = n_node;
+  ctx->n = (int64_t)n_cell + n_bface;
   ctx->hp = *params;
   ctx->P = make_params(*params);
   ctx->ncase = cl.ncase;
   ctx->hps.assign(params, params + cl.ncase);
   const int32_t C = ctx->C;
-  const int64_t n = ctx->n;
   if (cl.ncase > 1) {
     ctx->case_cell0 = cl.cell0;
     ctx->case_bface0 = cl.bface0;
@@ -2008,6 +2357,106 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
     ctx->case_bface0 = {0, ctx->G};
   }
 
+  {
+    // persistent sweeps need every block resident: one chunk per block, at
+    // most as many blocks as the occupancy of the heavier kernel allows
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    // resident blocks per SM of each kernel pair (both sweeps)
+    const bool mx = precision == MFG_PREC_MIXED;
+    for (int wi = 0; wi < 2; wi++)
+      for (int li = 0; li < 2; li++) {
+        const int w = wi ? 8 : 4, lanes = li ? w / 2 : w;
+        int per_sm = 1 << 30;
+        for (bool fwd : {true, false}) {
+          int b = 0;
+          if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sweep_kernel(fwd, w, lanes, mx),
+                                                            kPersistBlock, 0) != cudaSuccess)
+            return fail(MFG_ERR_CUDA);
+          per_sm = std::min(per_sm, b);
+        }
+        ctx->persist_occ[wi][li] = coop ? per_sm : 0;
+      }
+    ctx->n_sm = prop.multiProcessorCount;
+  }
+  *out = ctx;
+  return MFG_OK;
+}
+
+// Buffers of the iteration, their initial contents and the initial state:
+// the end of every context creation.
+static int ctx_finish(mfg_ctx *ctx, const double *q0, const CaseLayout &cl) {
+  const int32_t C = ctx->C;
+  const int64_t n = ctx->n;
+  const int32_t precision = ctx->precision;
+  int rc;
+  if (precision == MFG_PREC_MIXED) {
+    // the mixed form runs the persistent sweeps only
+    if (ctx->sweep_mode != 1) return MFG_ERR_UNSUPPORTED;
+    for (int k = 0; k < 2; k++)
+      if ((rc = dalloc(ctx, &ctx->q4[k], (size_t)n * Q_STRIDE))) return rc;
+    if ((rc = dalloc(ctx, &ctx->qn4, (size_t)ctx->N * Q_STRIDE))) return rc;
+  }
+  for (int k = 0; k < 2; k++)
+    if ((rc = dalloc(ctx, &ctx->q8[k], (size_t)n * Q_STRIDE))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dq8, (size_t)n * Q_STRIDE))) return rc;
+  if ((rc = dalloc(ctx, &ctx->res, (size_t)5 * C))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dt, (size_t)C))) return rc;
+  if ((rc = dalloc(ctx, &ctx->diag, (size_t)C))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dqdx, (size_t)5 * n))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dqdy, (size_t)5 * n))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dqdz, (size_t)5 * n))) return rc;
+  if ((rc = dalloc(ctx, &ctx->qn8, (size_t)ctx->N * Q_STRIDE))) return rc;
+  if ((rc = dalloc(ctx, &ctx->staging, (size_t)5 * n))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dt_ext, (size_t)2 * cl.ncase))) return rc;
+  const int nparts = std::max(grid_for(C), kNormBlocks);
+  if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return rc;
+  if ((rc = dalloc(ctx, &ctx->norm_out, (size_t)5 * cl.ncase))) return rc;
+  if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return rc;
+  if ((rc = dalloc(ctx, &ctx->dqf, (size_t)n * Q_STRIDE))) return rc;
+  if ((rc = dalloc(ctx, &ctx->sweep_err, 1))) return rc;
+  if (cudaMallocHost((void **)&ctx->h_pinned, (64 + 5 * (size_t)cl.ncase) * sizeof(double)) !=
+      cudaSuccess)
+    return MFG_ERR_NOMEM;
+
+  cudaStream_t st = ctx->stream;
+  if (cudaMemsetAsync(ctx->dq8, 0, sizeof(double) * n * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->res, 0, sizeof(double) * 5 * C, st) ||
+      cudaMemsetAsync(ctx->dt, 0, sizeof(double) * C, st) ||
+      cudaMemsetAsync(ctx->diag, 0, sizeof(double) * C, st) ||
+      cudaMemsetAsync(ctx->dqdx, 0, sizeof(double) * 5 * n, st) ||
+      cudaMemsetAsync(ctx->dqdy, 0, sizeof(double) * 5 * n, st) ||
+      cudaMemsetAsync(ctx->dqdz, 0, sizeof(double) * 5 * n, st) ||
+      cudaMemsetAsync(ctx->qn8, 0, sizeof(double) * ctx->N * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->dqf, 0, sizeof(double) * n * Q_STRIDE, st) ||
+      cudaMemsetAsync(ctx->sweep_err, 0, sizeof(int), st) ||
+      cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st))
+    return MFG_ERR_CUDA;
+  k_arm_sentinel<<<grid_for(C), kBlock, 0, st>>>(C, ctx->dqf);  // ready for a forward sweep
+  count_launch();
+  if (cudaGetLastError() != cudaSuccess) return MFG_ERR_CUDA;
+  if ((rc = mfg_set_dt_extrema(ctx, 0.0, kBig))) return rc;  // para_field_global.cpp:220-221
+  if ((rc = mfg_upload(ctx, MFG_FIELD_Q, q0))) return rc;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MFG_ERR_CUDA;
+  return MFG_OK;
+}
+
+static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLayout &cl,
+                       const double *q0, int32_t device, int32_t precision, mfg_ctx **out) {
+  if (!out || !params || !q0) return MFG_ERR_INVALID;
+  *out = nullptr;
+  int rc = validate_mesh(m);
+  if (rc) return rc;
+  mfg_ctx *ctx = nullptr;
+  if ((rc = ctx_begin(m->n_node, m->n_face, m->n_cell, m->n_bface, params, cl, device, precision,
+                      &ctx)))
+    return rc;
+  auto fail = [&](int code) {
+    free_ctx(ctx);
+    return code;
+  };
+  const int32_t C = ctx->C;
+  const int64_t n = ctx->n;
   std::vector<int32_t> cptr, c2f;
   build_c2f(m, cptr, c2f);
   ctx->S = cptr[C];
@@ -2053,80 +2502,9 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   slots.shrink_to_fit();
   std::vector<double> volv(m->vol, m->vol + n);
   if ((rc = dupload(ctx, &ctx->vol, volv))) return fail(rc);
-  {
-    // persistent sweeps need every block resident: one chunk per block, at
-    // most as many blocks as the occupancy of the heavier kernel allows
-    int coop = 0;
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
-    // resident blocks per SM of each kernel pair (both sweeps)
-    const bool mx = precision == MFG_PREC_MIXED;
-    for (int wi = 0; wi < 2; wi++)
-      for (int li = 0; li < 2; li++) {
-        const int w = wi ? 8 : 4, lanes = li ? w / 2 : w;
-        int per_sm = 1 << 30;
-        for (bool fwd : {true, false}) {
-          int b = 0;
-          if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sweep_kernel(fwd, w, lanes, mx),
-                                                            kPersistBlock, 0) != cudaSuccess)
-            return fail(MFG_ERR_CUDA);
-          per_sm = std::min(per_sm, b);
-        }
-        ctx->persist_occ[wi][li] = coop ? per_sm : 0;
-      }
-    ctx->n_sm = prop.multiProcessorCount;
-  }
   if ((rc = build_levels(ctx, m, cptr, c2f))) return fail(rc);
   if ((rc = build_node_lists(ctx, m))) return fail(rc);
-  if (precision == MFG_PREC_MIXED) {
-    // the mixed form runs the persistent sweeps only
-    if (ctx->sweep_mode != 1) return fail(MFG_ERR_UNSUPPORTED);
-    for (int k = 0; k < 2; k++)
-      if ((rc = dalloc(ctx, &ctx->q4[k], (size_t)n * Q_STRIDE))) return fail(rc);
-    if ((rc = dalloc(ctx, &ctx->qn4, (size_t)ctx->N * Q_STRIDE))) return fail(rc);
-  }
-
-
-  for (int k = 0; k < 2; k++)
-    if ((rc = dalloc(ctx, &ctx->q8[k], (size_t)n * Q_STRIDE))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dq8, (size_t)n * Q_STRIDE))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->res, (size_t)5 * C))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dt, (size_t)C))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->diag, (size_t)C))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dqdx, (size_t)5 * n))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dqdy, (size_t)5 * n))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dqdz, (size_t)5 * n))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->qn8, (size_t)ctx->N * Q_STRIDE))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->staging, (size_t)5 * n))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dt_ext, (size_t)2 * cl.ncase))) return fail(rc);
-  const int nparts = std::max(grid_for(C), kNormBlocks);
-  if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->norm_out, (size_t)5 * cl.ncase))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->dqf, (size_t)n * Q_STRIDE))) return fail(rc);
-  if ((rc = dalloc(ctx, &ctx->sweep_err, 1))) return fail(rc);
-  if (cudaMallocHost((void **)&ctx->h_pinned, (64 + 5 * (size_t)cl.ncase) * sizeof(double)) !=
-      cudaSuccess)
-    return fail(MFG_ERR_NOMEM);
-
-  cudaStream_t st = ctx->stream;
-  if (cudaMemsetAsync(ctx->dq8, 0, sizeof(double) * n * Q_STRIDE, st) ||
-      cudaMemsetAsync(ctx->res, 0, sizeof(double) * 5 * C, st) ||
-      cudaMemsetAsync(ctx->dt, 0, sizeof(double) * C, st) ||
-      cudaMemsetAsync(ctx->diag, 0, sizeof(double) * C, st) ||
-      cudaMemsetAsync(ctx->dqdx, 0, sizeof(double) * 5 * n, st) ||
-      cudaMemsetAsync(ctx->dqdy, 0, sizeof(double) * 5 * n, st) ||
-      cudaMemsetAsync(ctx->dqdz, 0, sizeof(double) * 5 * n, st) ||
-      cudaMemsetAsync(ctx->qn8, 0, sizeof(double) * ctx->N * Q_STRIDE, st) ||
-      cudaMemsetAsync(ctx->dqf, 0, sizeof(double) * n * Q_STRIDE, st) ||
-      cudaMemsetAsync(ctx->sweep_err, 0, sizeof(int), st) ||
-      cudaMemsetAsync(ctx->iter_counter, 0, sizeof(int32_t), st))
-    return fail(MFG_ERR_CUDA);
-  k_arm_sentinel<<<grid_for(C), kBlock, 0, st>>>(C, ctx->dqf);  // ready for a forward sweep
-  count_launch();
-  if (cudaGetLastError() != cudaSuccess) return fail(MFG_ERR_CUDA);
-  if ((rc = mfg_set_dt_extrema(ctx, 0.0, kBig))) return fail(rc);  // para_field_global.cpp:220-221
-  if ((rc = mfg_upload(ctx, MFG_FIELD_Q, q0))) return fail(rc);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return fail(MFG_ERR_CUDA);
+  if ((rc = ctx_finish(ctx, q0, cl))) return fail(rc);
   *out = ctx;
   return MFG_OK;
 }
@@ -2266,6 +2644,356 @@ int mfg_create_batch(int32_t ncase, const mfg_mesh *ms, const mfg_params *params
   u.yfn_n_symm = na[2].data();
   u.zfn_n_symm = na[3].data();
   return create_impl(&u, params, cl, q0.data(), device, precision, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Scratch device memory of a context build, freed on every exit.
+struct DevScratch {
+  std::vector<void *> ptrs;
+  ~DevScratch() {
+    for (void *q : ptrs) cudaFree(q);
+  }
+  template <typename T>
+  int get(T **p, int64_t count) {
+    const size_t bytes = std::max<size_t>(1, (size_t)std::max<int64_t>(count, 0)) * sizeof(T);
+    const cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+      g_cuda_error = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+      return MFG_ERR_NOMEM;
+    }
+    ptrs.push_back((void *)*p);
+    return MFG_OK;
+  }
+};
+
+int dev_read_i32(const int32_t *d, int32_t *h, cudaStream_t st) {
+  MFG_CUDA(cudaMemcpyAsync(h, d, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  MFG_CUDA(cudaStreamSynchronize(st));
+  return MFG_OK;
+}
+
+int dev_scan(DevScratch &sc, const int32_t *in, int32_t *out, int32_t m, cudaStream_t st) {
+  size_t bytes = 0;
+  MFG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, m, st));
+  char *tmp = nullptr;
+  const int rc = sc.get(&tmp, (int64_t)bytes);
+  if (rc) return rc;
+  MFG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, m, st));
+  return MFG_OK;
+}
+
+// stable: equal keys keep the order of their values' input positions
+int dev_sort_pairs(DevScratch &sc, const int32_t *kin, int32_t *kout, const int32_t *vin,
+                   int32_t *vout, int32_t m, int32_t max_key, cudaStream_t st) {
+  int bits = 1;
+  while (bits < 31 && (1 << bits) <= max_key) bits++;
+  size_t bytes = 0;
+  MFG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, m, 0, bits, st));
+  char *tmp = nullptr;
+  const int rc = sc.get(&tmp, (int64_t)bytes);
+  if (rc) return rc;
+  MFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, m, 0, bits, st));
+  return MFG_OK;
+}
+
+template <typename T>
+int d2h(std::vector<T> &h, const T *d, int64_t count, cudaStream_t st) {
+  h.resize((size_t)std::max<int64_t>(count, 0));
+  if (count > 0)
+    MFG_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(T) * count, cudaMemcpyDeviceToHost, st));
+  return MFG_OK;
+}
+
+// One sweep direction of build_levels on the device: levels, level-sorted
+// cells and their per-level records, then (after the chunk assignment) the
+// chunk-major persistent tables.
+struct DevSweep {
+  bool fwd = true;
+  int32_t *cnt = nullptr, *deg = nullptr, *lvl = nullptr;  // device scratch
+  std::vector<int32_t> lptr;                              // level starts
+  int32_t L = 0;
+  std::vector<int32_t> h_cells, h_sptr, h_nbs, h_assign;  // for the chunk assignment
+};
+
+int dev_levels(mfg_ctx *ctx, DevScratch &sc, DevSweep &d, int32_t *front, int32_t *next,
+               int32_t *counter) {
+  const int32_t C = ctx->C;
+  cudaStream_t st = ctx->stream;
+  MFG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+  k_dev_level_seed<<<grid_for(C), kBlock, 0, st>>>(C, d.deg, d.lvl, front, counter);
+  count_launch();
+  MFG_CUDA(cudaGetLastError());
+  int32_t nf = 0;
+  int rc;
+  if ((rc = dev_read_i32(counter, &nf, st))) return rc;
+  d.lptr.assign(1, 0);
+  int64_t done = 0;
+  int32_t level = 0;
+  while (nf > 0) {
+    d.lptr.push_back(d.lptr.back() + nf);
+    ctx->max_level_cells = std::max(ctx->max_level_cells, nf);
+    done += nf;
+    MFG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
+    k_dev_level_step<<<grid_for(nf), kBlock, 0, st>>>(nf, front, level, d.fwd ? 1 : 0, C,
+                                                     ctx->cptr, ctx->slots, d.deg, d.lvl, next,
+                                                     counter);
+    count_launch();
+    MFG_CUDA(cudaGetLastError());
+    if ((rc = dev_read_i32(counter, &nf, st))) return rc;
+    std::swap(front, next);
+    if (++level > C) return MFG_ERR_BADMESH;
+  }
+  if (done != C) return MFG_ERR_BADMESH;  // a dependency cycle
+  d.L = level;
+  // level-sorted cells (ascending index within a level) and their records
+  int32_t *idx = nullptr, *keys = nullptr, *g = nullptr;
+  int32_t **cells = d.fwd ? &ctx->fw_cells : &ctx->bw_cells;
+  int32_t **sptr = d.fwd ? &ctx->fw_sptr : &ctx->bw_sptr;
+  int32_t **nbs = d.fwd ? &ctx->fw_nb : &ctx->bw_nb;
+  SweepRec **recs = d.fwd ? &ctx->fw_recs : &ctx->bw_recs;
+  if ((rc = sc.get(&idx, C)) || (rc = sc.get(&keys, C)) || (rc = sc.get(&g, (int64_t)C + 1)) ||
+      (rc = dalloc(ctx, cells, C)) || (rc = dalloc(ctx, sptr, (size_t)C + 1)))
+    return rc;
+  k_dev_iota<<<grid_for(C), kBlock, 0, st>>>(C, idx);
+  count_launch();
+  if ((rc = dev_sort_pairs(sc, d.lvl, keys, idx, *cells, C, d.L, st))) return rc;
+  k_dev_gather_cnt<<<grid_for((int64_t)C + 1), kBlock, 0, st>>>(C, *cells, d.cnt, g);
+  count_launch();
+  if ((rc = dev_scan(sc, g, *sptr, C + 1, st))) return rc;
+  int32_t S = 0;
+  if ((rc = dev_read_i32(*sptr + C, &S, st))) return rc;
+  if ((rc = dalloc(ctx, recs, S)) || (rc = dalloc(ctx, nbs, S))) return rc;
+  k_dev_level_records<<<grid_for(C), kBlock, 0, st>>>(C, *cells, *sptr, ctx->cptr, ctx->slots,
+                                                       d.fwd ? 1 : 0, *recs, *nbs);
+  count_launch();
+  MFG_CUDA(cudaGetLastError());
+  // what the chunk assignment on the host reads
+  if ((rc = d2h(d.h_cells, (const int32_t *)*cells, C, st)) ||
+      (rc = d2h(d.h_sptr, (const int32_t *)*sptr, (int64_t)C + 1, st)) ||
+      (rc = d2h(d.h_nbs, (const int32_t *)*nbs, S, st)))
+    return rc;
+  MFG_CUDA(cudaStreamSynchronize(st));
+  return MFG_OK;
+}
+
+int dev_pack(mfg_ctx *ctx, DevScratch &sc, DevSweep &d) {
+  const int32_t C = ctx->C, P = ctx->nchunks, W = std::max(ctx->sweep_w, 1);
+  cudaStream_t st = ctx->stream;
+  int rc;
+  int32_t *assign = nullptr, *keys = nullptr, *idx = nullptr, *pchunk = nullptr, *order = nullptr;
+  int32_t *chunk_cnt = nullptr, *chunk_ptr = nullptr, *ccells = nullptr, *posof = nullptr;
+  int32_t *head = nullptr, *hscan = nullptr, *exported = nullptr;
+  if ((rc = sc.get(&assign, C)) || (rc = sc.get(&keys, C)) || (rc = sc.get(&idx, C)) ||
+      (rc = sc.get(&pchunk, C)) || (rc = sc.get(&order, C)) ||
+      (rc = sc.get(&chunk_cnt, (int64_t)P + 1)) || (rc = sc.get(&chunk_ptr, (int64_t)P + 1)) ||
+      (rc = sc.get(&ccells, C)) || (rc = sc.get(&posof, C)) ||
+      (rc = sc.get(&head, (int64_t)C + 1)) || (rc = sc.get(&hscan, (int64_t)C + 1)) ||
+      (rc = sc.get(&exported, 1)))
+    return rc;
+  MFG_CUDA(cudaMemcpyAsync(assign, d.h_assign.data(), sizeof(int32_t) * C,
+                           cudaMemcpyHostToDevice, st));
+  MFG_CUDA(cudaMemsetAsync(chunk_cnt, 0, sizeof(int32_t) * ((size_t)P + 1), st));
+  MFG_CUDA(cudaMemsetAsync(exported, 0, sizeof(int32_t), st));
+  const int32_t *cells = d.fwd ? ctx->fw_cells : ctx->bw_cells;
+  const int32_t *sptr = d.fwd ? ctx->fw_sptr : ctx->bw_sptr;
+  const int32_t *nbs = d.fwd ? ctx->fw_nb : ctx->bw_nb;
+  const SweepRec *recs = d.fwd ? ctx->fw_recs : ctx->bw_recs;
+  k_dev_chunk_keys<<<grid_for(C), kBlock, 0, st>>>(C, cells, assign, keys, idx, chunk_cnt);
+  count_launch();
+  if ((rc = dev_sort_pairs(sc, keys, pchunk, idx, order, C, P, st))) return rc;
+  if ((rc = dev_scan(sc, chunk_cnt, chunk_ptr, P + 1, st))) return rc;
+  k_dev_positions<<<grid_for((int64_t)C + 1), kBlock, 0, st>>>(C, order, cells, pchunk, d.lvl,
+                                                               ccells, posof, head);
+  count_launch();
+  if ((rc = dev_scan(sc, head, hscan, C + 1, st))) return rc;
+  int32_t nseg = 0;
+  if ((rc = dev_read_i32(hscan + C, &nseg, st))) return rc;
+  ChunkSweep &cs = d.fwd ? ctx->fwc : ctx->bwc;
+  cs.nseg = nseg;
+  if ((rc = dalloc(ctx, &cs.seg_begin, (size_t)P + 1)) ||
+      (rc = dalloc(ctx, &cs.segs, (size_t)nseg + 1)) || (rc = dalloc(ctx, &cs.cells, C)))
+    return rc;
+  k_dev_segs<<<grid_for((int64_t)C + 1), kBlock, 0, st>>>(C, head, hscan, cs.segs);
+  k_dev_seg_begin<<<grid_for((int64_t)P + 1), kBlock, 0, st>>>(P, chunk_ptr, hscan, cs.seg_begin);
+  count_launch(2);
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const bool with_recs = ctx->sweep_w != 0;
+  const size_t nrec = with_recs ? (size_t)C * W : 0;
+  const size_t nrec1 = std::max<size_t>(nrec, 1);
+  if ((rc = dalloc(ctx, &cs.nbs, nrec)) || (rc = dalloc(ctx, &cs.nslots, nrec))) return rc;
+  if (mx) {
+    if ((rc = dalloc(ctx, &cs.recs_f, nrec))) return rc;
+    MFG_CUDA(cudaMemsetAsync(cs.recs_f, 0, sizeof(SweepRecF) * nrec1, st));
+  } else {
+    if ((rc = dalloc(ctx, &cs.recs, nrec))) return rc;
+    MFG_CUDA(cudaMemsetAsync(cs.recs, 0, sizeof(SweepRec) * nrec1, st));
+  }
+  MFG_CUDA(cudaMemsetAsync(cs.nbs, 0, sizeof(int32_t) * nrec1, st));
+  MFG_CUDA(cudaMemsetAsync(cs.nslots, 0, sizeof(int32_t) * nrec1, st));
+  if (mx)
+    k_dev_pack<true><<<grid_for(C), kBlock, 0, st>>>(
+        C, W, with_recs, order, ccells, pchunk, head, hscan, cs.segs, chunk_ptr, posof, assign,
+        sptr, nbs, recs, cs.cells, cs.nbs, nullptr, cs.recs_f, cs.nslots, exported);
+  else
+    k_dev_pack<false><<<grid_for(C), kBlock, 0, st>>>(
+        C, W, with_recs, order, ccells, pchunk, head, hscan, cs.segs, chunk_ptr, posof, assign,
+        sptr, nbs, recs, cs.cells, cs.nbs, cs.recs, nullptr, cs.nslots, exported);
+  count_launch();
+  MFG_CUDA(cudaGetLastError());
+  int32_t ex = 0;
+  if ((rc = dev_read_i32(exported, &ex, st))) return rc;
+  if (d.fwd) ctx->chunk0_exported = ex != 0;
+  (d.fwd ? ctx->fw_lptr : ctx->bw_lptr) = d.lptr;
+  return MFG_OK;
+}
+
+int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, const double *q0,
+                          int32_t precision, mfg_ctx **out) {
+  if (!out || !pp || !params || !q0) return MFG_ERR_INVALID;
+  *out = nullptr;
+  CaseLayout cl;
+  mfg_ctx *ctx = nullptr;
+  int rc = ctx_begin(pp->N, pp->F, pp->C, pp->B, params, cl, pp->device, precision, &ctx);
+  if (rc) return rc;
+  auto fail = [&](int code) {
+    cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+    return code;
+  };
+  const int32_t C = ctx->C, F = ctx->F, G = ctx->G, N = ctx->N;
+  const int64_t n = ctx->n;
+  cudaStream_t st = ctx->stream;
+  DevScratch sc;
+  int32_t *flags = nullptr;  // [0] bad slot, [1] most records of a cell, [2] bad node list
+  if ((rc = sc.get(&flags, 3))) return fail(rc);
+  MFG_CUDA_OR(cudaMemsetAsync(flags, 0, 3 * sizeof(int32_t), st));
+  // slots, faces, volumes, BC types
+  ctx->S = pp->S;
+  if ((rc = dalloc(ctx, &ctx->cptr, (size_t)C + 1)) || (rc = dalloc(ctx, &ctx->slots, pp->S)) ||
+      (rc = dalloc(ctx, &ctx->faces, F)) || (rc = dalloc(ctx, &ctx->fflux, (size_t)5 * F)) ||
+      (rc = dalloc(ctx, &ctx->bctype_d, G)) || (rc = dalloc(ctx, &ctx->vol, n)))
+    return fail(rc);
+  MFG_CUDA_OR(cudaMemcpyAsync(ctx->cptr, pp->cptr, sizeof(int32_t) * ((size_t)C + 1),
+                              cudaMemcpyDeviceToDevice, st));
+  if (G > 0)
+    MFG_CUDA_OR(cudaMemcpyAsync(ctx->bctype_d, pp->bctype, sizeof(int32_t) * G,
+                                cudaMemcpyDeviceToDevice, st));
+  MFG_CUDA_OR(
+      cudaMemcpyAsync(ctx->vol, pp->vol, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  k_dev_slots<<<grid_for(C), kBlock, 0, st>>>(C, G, pp->cptr, pp->cf, pp->f2c, pp->bctype,
+                                              pp->xfn, pp->yfn, pp->zfn, pp->area, pp->xfc,
+                                              pp->yfc, pp->zfc, pp->xcc, pp->ycc, pp->zcc,
+                                              ctx->slots, flags);
+  k_dev_faces<<<grid_for(F), kBlock, 0, st>>>(F, pp->f2c, pp->xfn, pp->yfn, pp->zfn, pp->area,
+                                              ctx->faces);
+  count_launch(2);
+  // record counts, the record width W and the chunk grid
+  DevSweep fw, bw;
+  fw.fwd = true;
+  bw.fwd = false;
+  if ((rc = sc.get(&fw.cnt, C)) || (rc = sc.get(&bw.cnt, C)) || (rc = sc.get(&fw.deg, C)) ||
+      (rc = sc.get(&bw.deg, C)) || (rc = sc.get(&fw.lvl, C)) || (rc = sc.get(&bw.lvl, C)))
+    return fail(rc);
+  k_dev_counts<<<grid_for(C), kBlock, 0, st>>>(C, ctx->cptr, ctx->slots, fw.cnt, bw.cnt, fw.deg,
+                                               bw.deg, flags + 1);
+  count_launch();
+  MFG_CUDA_OR(cudaGetLastError());
+  int32_t h_flags[3] = {0, 0, 0};
+  MFG_CUDA_OR(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, st));
+  MFG_CUDA_OR(cudaStreamSynchronize(st));
+  if (h_flags[0]) return fail(MFG_ERR_BADMESH);
+  {
+    // the choices of build_levels
+    const int32_t maxns = h_flags[1];
+    ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
+    if (n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
+    const int wi = ctx->sweep_w == 8 ? 1 : 0;
+    const int occ_w = ctx->sweep_w ? ctx->persist_occ[wi][0] : 0;
+    const int occ_h = ctx->sweep_w ? ctx->persist_occ[wi][1] : 0;
+    const int per_sm = occ_w;
+    ctx->persist_grid = per_sm * ctx->n_sm;
+    ctx->nchunks = std::max(1, std::min(per_sm * ctx->n_sm, (C + kMinChunk - 1) / kMinChunk));
+    ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
+    ctx->lanes_ok[0] = occ_w >= per_sm && per_sm > 0;
+    ctx->lanes_ok[1] = occ_h >= per_sm && per_sm > 0;
+    ctx->sweep_lanes = ctx->sweep_w;
+    ctx->first_cell = 0;
+  }
+  {
+    int32_t *front = nullptr, *next = nullptr, *counter = nullptr;
+    if ((rc = sc.get(&front, C)) || (rc = sc.get(&next, C)) || (rc = sc.get(&counter, 1)))
+      return fail(rc);
+    if ((rc = dev_levels(ctx, sc, fw, front, next, counter))) return fail(rc);
+    if ((rc = dev_levels(ctx, sc, bw, front, next, counter))) return fail(rc);
+  }
+  // the chunk assignment runs on the host, both sweeps at once
+  {
+    const int32_t P = ctx->nchunks;
+    std::thread tb([&] {
+      assign_chunks(C, P, bw.lptr, bw.h_cells.data(), bw.h_sptr.data(), bw.h_nbs.data(),
+                    bw.h_assign);
+    });
+    assign_chunks(C, P, fw.lptr, fw.h_cells.data(), fw.h_sptr.data(), fw.h_nbs.data(),
+                  fw.h_assign);
+    tb.join();
+  }
+  if ((rc = dev_pack(ctx, sc, fw))) return fail(rc);
+  if ((rc = dev_pack(ctx, sc, bw))) return fail(rc);
+  // node lists
+  {
+    int32_t *cnt = nullptr;
+    if ((rc = sc.get(&cnt, (int64_t)N + 1))) return fail(rc);
+    MFG_CUDA_OR(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * ((size_t)N + 1), st));
+    k_dev_node_lists<false><<<grid_for(N), kBlock, 0, st>>>(
+        N, pp->nbptr, pp->nblist, pp->bent_face, pp->bctype, pp->ncptr, pp->nclist,
+        pp->c2n_cell, pp->nmark, pp->wbface, pp->wc2n, cnt, flags + 2, nullptr, nullptr, nullptr);
+    count_launch();
+    if ((rc = dalloc(ctx, &ctx->nptr, (size_t)N + 1))) return fail(rc);
+    if ((rc = dev_scan(sc, cnt, ctx->nptr, N + 1, st))) return fail(rc);
+    int32_t tot = 0, badn = 0;
+    if ((rc = dev_read_i32(ctx->nptr + N, &tot, st))) return fail(rc);
+    if ((rc = dev_read_i32(flags + 2, &badn, st))) return fail(rc);
+    if (badn) return fail(MFG_ERR_UNSUPPORTED);  // as build_node_lists
+    if ((rc = dalloc(ctx, &ctx->nsrc, tot)) || (rc = dalloc(ctx, &ctx->nw, tot)) ||
+        (rc = dalloc(ctx, &ctx->ninfo, N)) || (rc = dalloc(ctx, &ctx->nsym, 3 * (size_t)N)) ||
+        (rc = dalloc(ctx, &ctx->wnode, N)) ||
+        (rc = dalloc(ctx, &ctx->bface_c1, (size_t)std::max(G, 1))) ||
+        (rc = dalloc(ctx, &ctx->fnptr, (size_t)F + 1)) || (rc = dalloc(ctx, &ctx->fnodes, pp->L)))
+      return fail(rc);
+    k_dev_node_lists<true><<<grid_for(N), kBlock, 0, st>>>(
+        N, pp->nbptr, pp->nblist, pp->bent_face, pp->bctype, pp->ncptr, pp->nclist,
+        pp->c2n_cell, pp->nmark, pp->wbface, pp->wc2n, nullptr, nullptr, ctx->nptr, ctx->nsrc,
+        ctx->nw);
+    k_dev_node_info<<<grid_for(N), kBlock, 0, st>>>(N, pp->nmark, pp->nodesymm, pp->xsym,
+                                                    pp->ysym, pp->zsym, ctx->ninfo, ctx->nsym);
+    MFG_CUDA_OR(cudaMemsetAsync(ctx->bface_c1, 0, sizeof(int32_t), st));
+    k_dev_bface_c1<<<grid_for(std::max(G, 1)), kBlock, 0, st>>>(G, pp->f2c, ctx->bface_c1);
+    count_launch(3);
+    MFG_CUDA_OR(cudaMemcpyAsync(ctx->wnode, pp->wnode, sizeof(double) * N,
+                                cudaMemcpyDeviceToDevice, st));
+    MFG_CUDA_OR(cudaMemcpyAsync(ctx->fnptr, pp->fptr, sizeof(int32_t) * ((size_t)F + 1),
+                                cudaMemcpyDeviceToDevice, st));
+    if (pp->L > 0)
+      MFG_CUDA_OR(cudaMemcpyAsync(ctx->fnodes, pp->f2n, sizeof(int32_t) * pp->L,
+                                  cudaMemcpyDeviceToDevice, st));
+    MFG_CUDA_OR(cudaGetLastError());
+  }
+  MFG_CUDA_OR(cudaStreamSynchronize(st));
+  if ((rc = ctx_finish(ctx, q0, cl))) return fail(rc);
+  *out = ctx;
+  return MFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfg_create_from_prep(const mfg_prep_gpu *prep, const mfg_params *params, const double *q0,
+                         int32_t precision, mfg_ctx **out) {
+  return create_from_prep_impl(prep, params, q0, precision, out);
 }
 
 int mfg_set_stream(mfg_ctx *ctx, void *s) {

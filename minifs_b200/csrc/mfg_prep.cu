@@ -30,6 +30,7 @@
 #include <cstring>
 #include <vector>
 
+#include "mfg_internal.h"
 #include "mfg_kernels.cuh"
 #include "mfgpu.h"
 
@@ -580,29 +581,7 @@ __global__ void k_node_weights(int32_t N, const int32_t *__restrict__ nbptr,
 
 }  // namespace
 
-struct mfg_prep_gpu {
-  int32_t device = 0;
-  int32_t N = 0, F = 0, C = 0, B = 0;
-  int64_t n = 0;   // C + B
-  int32_t L = 0;   // face-node positions
-  int32_t LB = 0;  // of the boundary faces
-  int32_t S = 0;   // cell-face slots
-  int32_t K = 0;   // c2n entries
-  double kernel_ms = 0.0;
-  std::vector<void *> allocs;
-  double *x = nullptr, *y = nullptr, *z = nullptr;
-  int32_t *nnpf = nullptr, *f2n = nullptr, *f2c = nullptr, *bctype = nullptr;
-  int32_t *fptr = nullptr, *cptr = nullptr, *cf = nullptr;
-  double *xfn = nullptr, *yfn = nullptr, *zfn = nullptr, *area = nullptr;
-  double *xfc = nullptr, *yfc = nullptr, *zfc = nullptr;
-  double *xcc = nullptr, *ycc = nullptr, *zcc = nullptr, *vol = nullptr;
-  int32_t *c2n_ptr = nullptr, *c2n = nullptr, *c2n_cell = nullptr, *nnpc = nullptr;
-  int32_t *nbptr = nullptr, *nblist = nullptr, *bent_face = nullptr;
-  int32_t *ncptr = nullptr, *nclist = nullptr;
-  double *wnode = nullptr, *wbface = nullptr, *wc2n = nullptr;
-  int32_t *nmark = nullptr, *nodesymm = nullptr;
-  double *xsym = nullptr, *ysym = nullptr, *zsym = nullptr;
-};
+
 
 namespace {
 
@@ -935,6 +914,33 @@ int mfg_prep_gpu_node_weights(mfg_prep_gpu *p, double *wnode, int32_t *nmark, do
       (rc = pdownload(yfn_n_symm, p->ysym, N)) || (rc = pdownload(zfn_n_symm, p->zsym, N)))
     return rc;
   return MFG_OK;
+}
+
+int mfg_prep_gpu_init_flow(mfg_prep_gpu *p, const mfg_params *params, double bump_amp,
+                           double bump_sigma, double bump_x0, double bump_y0, double bump_z0,
+                           double *q) {
+  if (!p || !params || !q) return MFG_ERR_INVALID;
+  DeviceScope scope(p->device);
+  const int64_t n = p->n, B = p->B, B1 = std::max<int64_t>(B, 1);
+  std::vector<int32_t> f2c(2 * (size_t)B1, 0), bt((size_t)B1, 0);
+  std::vector<double> nx(B1), ny(B1), nz(B1), cx(n), cy(n), cz(n);
+  int rc;
+  if ((rc = pdownload(f2c.data(), p->f2c, 2 * B)) || (rc = pdownload(bt.data(), p->bctype, B)) ||
+      (rc = pdownload(nx.data(), p->xfn, B)) || (rc = pdownload(ny.data(), p->yfn, B)) ||
+      (rc = pdownload(nz.data(), p->zfn, B)) || (rc = pdownload(cx.data(), p->xcc, n)) ||
+      (rc = pdownload(cy.data(), p->ycc, n)) || (rc = pdownload(cz.data(), p->zcc, n)))
+    return rc;
+  // the host routine reads the sizes and, of boundary faces only, f2c, the
+  // normals and the BC types
+  mfg_raw_grid g{};
+  g.n_node = p->N;
+  g.n_face = p->F;
+  g.n_cell = p->C;
+  g.n_bface = p->B;
+  g.f2c = f2c.data();
+  return mfg_prep_init_flow(&g, params, bt.data(), nx.data(), ny.data(), nz.data(), cx.data(),
+                            cy.data(), cz.data(), bump_amp, bump_sigma, bump_x0, bump_y0, bump_z0,
+                            q);
 }
 
 int mfg_prep_gpu_destroy(mfg_prep_gpu *p) {

@@ -200,6 +200,56 @@ def _prepare_gpu(mesh, params, bump_amp, bump_sigma, bump_center, device, stats)
     return PreparedGrid(n_node=N, n_face=F, n_cell=C, n_bface=G, arrays=arrays, q0=q0)
 
 
+class DevicePrep:
+    """The preprocessing kept in device memory (``mfg_prep_gpu_run``): the
+    input of ``Solver.from_device_prep``, which builds the context on the
+    device without copying the grid through the host."""
+
+    def __init__(self, mesh: RawMesh, device: int = 0):
+        lib = _lib.load()
+        self.mesh = _contiguous(mesh)
+        self.f2c = np.array(mesh.f2c, dtype=np.int32, copy=True)
+        g = _raw(self.mesh, self.f2c)
+        self.n_node, self.n_face = self.mesh.n_node, self.mesh.n_face
+        self.n_cell, self.n_bface = self.mesh.n_cell, self.mesh.n_bface
+        types = np.array([t for _, t in mesh.patches], dtype=np.int32)
+        self.bctype = np.zeros(max(self.n_bface, 1), dtype=np.int32)
+        _lib.check("mfg_prep_specify_bc",
+                   lib.mfg_prep_specify_bc(ct_byref(g), len(types), _lib.ptr(types, _lib.i32p),
+                                           _lib.ptr(self.bctype, _lib.i32p)))
+        self.handle = ctypes.c_void_p()
+        _lib.check("mfg_prep_gpu_run",
+                   lib.mfg_prep_gpu_run(ct_byref(g), _lib.ptr(self.bctype, _lib.i32p),
+                                        int(device), ctypes.byref(self.handle)))
+        self.device = int(device)
+
+    @property
+    def n(self) -> int:
+        return self.n_cell + self.n_bface
+
+    def init_flow(self, params: _lib.Params, bump_amp: float = 0.05, bump_sigma: float = 0.1,
+                  bump_center=(0.5, 0.5, 0.5)) -> np.ndarray:
+        """The initial state (AllocAndInitFlowfield + bump + SetGhostVariables),
+        computed on the host from the device's centroids and normals."""
+        q0 = np.zeros(5 * self.n)
+        bx, by, bz = bump_center
+        _lib.check("mfg_prep_gpu_init_flow", _lib.load().mfg_prep_gpu_init_flow(
+            self.handle, ct_byref(params), float(bump_amp), float(bump_sigma), float(bx),
+            float(by), float(bz), _lib.ptr(q0)))
+        return q0
+
+    def close(self):
+        if self.handle:
+            _lib.load().mfg_prep_gpu_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def from_arrays(dims, arrays: dict, q0: np.ndarray) -> PreparedGrid:
     """Wrap arrays already produced elsewhere (e.g. by the reference's own
     preprocessing, as a drop-in caller would pass them)."""

@@ -37,6 +37,25 @@ class Solver:
                                                      ct.byref(self._ctx)))
         del keep
 
+    @classmethod
+    def from_device_prep(cls, prep, params: _lib.Params, q0: np.ndarray,
+                         precision: str = "fp64") -> "Solver":
+        """A solver whose context is built on the device from a
+        ``grid.DevicePrep`` (``mfg_create_from_prep``; identity LU-SGS
+        order), on the preprocessing's device."""
+        self = cls.__new__(cls)
+        self.lib = _lib.load()
+        self.grid = PreparedGrid(n_node=prep.n_node, n_face=prep.n_face, n_cell=prep.n_cell,
+                                 n_bface=prep.n_bface, arrays={},
+                                 q0=np.ascontiguousarray(q0, np.float64))
+        self.params = params
+        self.iter_done = 0
+        self._ctx = ct.c_void_p()
+        _lib.check("mfg_create_from_prep", self.lib.mfg_create_from_prep(
+            prep.handle, ct.byref(params), _lib.ptr(self.grid.q0), _lib.PREC[precision],
+            ct.byref(self._ctx)))
+        return self
+
     # -- lifetime ----------------------------------------------------------
     def close(self):
         if self._ctx:
