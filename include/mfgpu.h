@@ -209,7 +209,9 @@ int mfg_set_ghost_variables(mfg_ctx *ctx);
  * reference's frozen ghosts): they do not. */
 int mfg_set_live_bc(mfg_ctx *ctx, int32_t on);
 /* The whole main-loop body (main.cpp:201-291) n times, fused kernels in a
- * CUDA graph.  norms (optional, host) receives 5 residual L2 norms per
+ * CUDA graph.  Each iteration's gradient is computed once, as in the loop;
+ * all but the last run beside the next iteration's face kernels (same
+ * values; on return the gradient is that of the final state).  norms (optional, host) receives 5 residual L2 norms per
  * iteration (main.cpp:294-317 evaluated every iteration); for a batch
  * norms[(i * ncase + k) * 5 + v]. */
 int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms);

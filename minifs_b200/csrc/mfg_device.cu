@@ -1422,6 +1422,10 @@ struct mfg_ctx {
   // iteration's later kernels run
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_res = nullptr, ev_state = nullptr;
+  // fused iterations: the gradient of the state an iteration starts from
+  // runs on a second stream beside that iteration's face kernels
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int32_t C = 0, G = 0, F = 0, N = 0;
   int64_t n = 0, S = 0;
   mfg_params hp{};
@@ -1959,6 +1963,9 @@ static void free_ctx(mfg_ctx *ctx) {
   if (ctx->ev_res) cudaEventDestroy(ctx->ev_res);
   if (ctx->ev_state) cudaEventDestroy(ctx->ev_state);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -3442,11 +3449,42 @@ static int fill_cfl_table(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done) {
 // runs on: `after_face` is recorded once the residual is final (nothing
 // later in the iteration writes it), `after_update` once the new state has
 // been unpacked into the SoA staging buffer.
+//
+// Where the iteration's gradient goes (`grad`): GRAD_AT_END after the update,
+// as the reference orders it; GRAD_DEFER not in this iteration; GRAD_LEAD
+// the gradient of the state the iteration starts from -- the one the
+// previous, deferred, iteration owes -- on the side stream beside this
+// iteration's face kernels (both only read that state; neither reads what
+// the other writes).  A run of n iterations defers the first, leads the
+// others and ends with one gradient of the final state (run_iterations):
+// every iteration's gradient is computed once, with the same kernels and
+// values, the n - 1 inner ones overlapping the next iteration's face phase.
+static int ensure_side_stream(mfg_ctx *ctx) {
+  if (ctx->side_stream) return MFG_OK;
+  MFG_CUDA(cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking));
+  MFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  MFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  return MFG_OK;
+}
+
+enum : int { GRAD_AT_END = 0, GRAD_DEFER = 1, GRAD_LEAD = 2 };
+
 static int launch_iteration(mfg_ctx *ctx, cudaEvent_t after_face = nullptr,
-                            cudaEvent_t after_update = nullptr) {
+                            cudaEvent_t after_update = nullptr, int grad = GRAD_AT_END) {
+  const bool lead_gradient = grad == GRAD_LEAD;
+  if (lead_gradient) {
+    MFG_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+    MFG_CUDA(cudaStreamWaitEvent(ctx->side_stream, ctx->ev_fork, 0));
+    launch_node_values(ctx, ctx->side_stream);
+    launch_grad_faces(ctx, ctx->side_stream);
+    MFG_CUDA(cudaGetLastError());
+    MFG_CUDA(cudaEventRecord(ctx->ev_join, ctx->side_stream));
+  }
   int rc = launch_face(ctx, true, true, true, 0.0, true);
   if (rc) return rc;
   if (after_face) MFG_CUDA(cudaEventRecord(after_face, ctx->stream));
+  // the persistent sweeps need every SM: the gradient ends before them
+  if (lead_gradient) MFG_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0));
   rc = launch_sweeps(ctx, true);
   if (rc) return rc;
   ctx->cur ^= 1;
@@ -3462,13 +3500,17 @@ static int launch_iteration(mfg_ctx *ctx, cudaEvent_t after_face = nullptr,
     MFG_CUDA(cudaGetLastError());
     MFG_CUDA(cudaEventRecord(after_update, ctx->stream));
   }
-  rc = launch_gradient(ctx);
-  if (rc) return rc;
+  if (grad == GRAD_AT_END) {
+    rc = launch_gradient(ctx);
+    if (rc) return rc;
+  }
   return launch_norm_tail(ctx, ctx->stream);
 }
 
 static int ensure_graphs(mfg_ctx *ctx) {
   if (ctx->graph[0] && ctx->graph[1]) return MFG_OK;
+  int rc0 = ensure_side_stream(ctx);
+  if (rc0) return rc0;
   const int start = ctx->cur;
   for (int k = 0; k < 2; k++) {
     const int par = start ^ k;
@@ -3477,7 +3519,7 @@ static int ensure_graphs(mfg_ctx *ctx) {
     cudaGraph_t g = nullptr;
     MFG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const long long before = g_launches.load();
-    int rc = launch_iteration(ctx);
+    int rc = launch_iteration(ctx, nullptr, nullptr, GRAD_LEAD);
     const long long nodes = g_launches.load() - before;
     g_launches.fetch_sub(nodes);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
@@ -3504,6 +3546,40 @@ static int ensure_graphs(mfg_ctx *ctx) {
   return MFG_OK;
 }
 
+// n_iter >= 1 fused iterations after fill_cfl_table: the first launched
+// plainly with its gradient deferred, the inner ones as captured graphs that
+// lead with the previous iteration's gradient, the last one plainly when it
+// carries the copy hooks, then the gradient of the final state.
+static int run_iterations(mfg_ctx *ctx, int32_t n_iter, cudaEvent_t after_face = nullptr,
+                          cudaEvent_t after_update = nullptr) {
+  cudaStream_t st = ctx->stream;
+  const bool hooks = after_face || after_update;
+  const int32_t n_graph = n_iter - 1 - ((hooks && n_iter > 1) ? 1 : 0);
+  int rc;
+  if ((rc = ensure_side_stream(ctx))) return rc;
+  if (n_graph > 0 && (rc = ensure_graphs(ctx))) return rc;
+  ctx->res_zero = true;  // ZeroResiduals at the top of each iteration
+  rc = launch_iteration(ctx, n_iter == 1 ? after_face : nullptr,
+                        n_iter == 1 ? after_update : nullptr, GRAD_DEFER);
+  for (int32_t i = 0; rc == MFG_OK && i < n_graph; i++) {
+    const cudaError_t e = cudaGraphLaunch(ctx->graph[ctx->cur], st);
+    if (e != cudaSuccess) {
+      g_cuda_error = std::string("cudaGraphLaunch: ") + cudaGetErrorString(e);
+      rc = MFG_ERR_CUDA;
+      break;
+    }
+    count_launch(ctx->graph_nodes);
+    ctx->cur ^= 1;
+  }
+  if (rc == MFG_OK && hooks && n_iter > 1) {
+    ctx->res_zero = true;
+    rc = launch_iteration(ctx, after_face, after_update, GRAD_LEAD);
+  }
+  if (rc == MFG_OK) rc = launch_gradient(ctx);  // of the final state
+  ctx->res_zero = false;
+  return rc;
+}
+
 int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) {
   if (!ctx || n_iter < 0) return MFG_ERR_INVALID;
   if (n_iter == 0) return MFG_OK;
@@ -3511,15 +3587,10 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
   cudaStream_t st = ctx->stream;
   int rc = fill_cfl_table(ctx, n_iter, iter_done);
   if (rc) return rc;
-  ctx->res_zero = true;  // ZeroResiduals at the top of each iteration
-  rc = ensure_graphs(ctx);
-  if (rc) return rc;
-  for (int32_t i = 0; i < n_iter; i++) {
-    MFG_CUDA(cudaGraphLaunch(ctx->graph[ctx->cur], st));
-    count_launch(ctx->graph_nodes);
-    ctx->cur ^= 1;
+  if ((rc = run_iterations(ctx, n_iter))) {
+    cudaStreamSynchronize(st);
+    return rc;
   }
-  ctx->res_zero = false;
   if (norms) {
     MFG_CUDA(cudaMemcpyAsync(norms, ctx->norm_hist, sizeof(double) * 5 * n_iter * ctx->ncase,
                              cudaMemcpyDeviceToHost, st));
@@ -3577,9 +3648,9 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
     ms[k] = -1.0;  // not usable with this context's chunk grid
     if (!ctx->lanes_ok[k]) continue;
     if ((rc = mfg_set_sweep_lanes(ctx, cand[k]))) break;
-    if ((rc = mfg_iterate(ctx, 1, iter_done, nullptr))) break;  // builds the graphs
+    if ((rc = mfg_iterate(ctx, 2, iter_done, nullptr))) break;  // builds the graphs
     cudaEventRecord(e0, st);
-    if ((rc = mfg_iterate(ctx, n_trial, iter_done + 1, nullptr))) break;
+    if ((rc = mfg_iterate(ctx, n_trial, iter_done + 2, nullptr))) break;
     cudaEventRecord(e1, st);
     float t = 0.f;
     if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
@@ -3693,16 +3764,8 @@ int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const doub
     MFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_state, cudaEventDisableTiming));
   }
   if ((rc = fill_cfl_table(ctx, n_iter, iter_done))) return rc;
-  ctx->res_zero = true;
-  if (n_iter > 1 && (rc = ensure_graphs(ctx))) return rc;
-  for (int32_t i = 0; i + 1 < n_iter; i++) {
-    MFG_CUDA(cudaGraphLaunch(ctx->graph[ctx->cur], st));
-    count_launch(ctx->graph_nodes);
-    ctx->cur ^= 1;
-  }
-  ctx->res_zero = true;  // the plain iteration starts with ZeroResiduals too
-  rc = launch_iteration(ctx, res_out ? ctx->ev_res : nullptr, q_out ? ctx->ev_state : nullptr);
-  ctx->res_zero = false;
+  rc = run_iterations(ctx, n_iter, res_out ? ctx->ev_res : nullptr,
+                      q_out ? ctx->ev_state : nullptr);
   if (rc) {
     cudaStreamSynchronize(st);
     return rc;
