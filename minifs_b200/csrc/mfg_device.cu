@@ -1156,17 +1156,26 @@ k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
       for (int v = 0; v < 5; v++) qs[v] = 0.5 * (qc[v] + qg[v]);
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.0;
-      const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
-      for (int32_t j = j0; j < j1; j++) {
-        const double2 *p = reinterpret_cast<const double2 *>(qn8 + (int64_t)fnodes[j] * Q_STRIDE);
+      auto add = [&](int32_t node) {
+        const double2 *p = reinterpret_cast<const double2 *>(qn8 + (int64_t)node * Q_STRIDE);
         const double2 a = __ldg(p), b = __ldg(p + 1), e = __ldg(p + 2);
         qs[0] += a.x;
         qs[1] += a.y;
         qs[2] += b.x;
         qs[3] += b.y;
         qs[4] += e.x;
+      };
+      int32_t nn = 3;
+      if (sr.flags & SLOT_TRI) {
+        add(sr.tri[0]);
+        add(sr.tri[1]);
+        add(sr.tri[2]);
+      } else {
+        const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+        for (int32_t j = j0; j < j1; j++) add(fnodes[j]);
+        nn = j1 - j0;
       }
-      const double cnt = (double)(j1 - j0);
+      const double cnt = (double)nn;
       for (int v = 0; v < 5; v++) qs[v] /= cnt;
     }
     const bool minus = (sr.flags & SLOT_IS_C2) != 0;
@@ -1269,17 +1278,26 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
       for (int v = 0; v < 5; v++) qs[v] = (float)(0.5 * ((qc[v] - P.ref[v]) + (qg[v] - P.ref[v])));
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.f;
-      const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
-      for (int32_t j = j0; j < j1; j++) {
-        const float4 *p = reinterpret_cast<const float4 *>(qn4 + (int64_t)fnodes[j] * Q_STRIDE);
+      auto add = [&](int32_t node) {
+        const float4 *p = reinterpret_cast<const float4 *>(qn4 + (int64_t)node * Q_STRIDE);
         const float4 a = __ldg(p), b = __ldg(p + 1);
         qs[0] += a.x;
         qs[1] += a.y;
         qs[2] += a.z;
         qs[3] += a.w;
         qs[4] += b.x;
+      };
+      int32_t nn = 3;
+      if (sr.flags & SLOT_TRI) {
+        add(sr.tri[0]);
+        add(sr.tri[1]);
+        add(sr.tri[2]);
+      } else {
+        const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+        for (int32_t j = j0; j < j1; j++) add(fnodes[j]);
+        nn = j1 - j0;
       }
-      const float rc = __fdividef(1.0f, (float)(j1 - j0));
+      const float rc = __fdividef(1.0f, (float)nn);
       for (int v = 0; v < 5; v++) qs[v] *= rc;
     }
     const float sg = (sr.flags & SLOT_IS_C2) ? -(float)sr.area : (float)sr.area;
@@ -1617,7 +1635,8 @@ namespace {
 
 // create_impl's slot loop, one thread per cell
 __global__ void k_dev_slots(int32_t C, int32_t B, const int32_t *__restrict__ cptr,
-                            const int32_t *__restrict__ cf, const int32_t *__restrict__ f2c,
+                            const int32_t *__restrict__ cf, const int32_t *__restrict__ fptr,
+                            const int32_t *__restrict__ f2n, const int32_t *__restrict__ f2c,
                             const int32_t *__restrict__ bctype, const double *__restrict__ xfn,
                             const double *__restrict__ yfn, const double *__restrict__ zfn,
                             const double *__restrict__ area, const double *__restrict__ xfc,
@@ -1647,7 +1666,10 @@ __global__ void k_dev_slots(int32_t C, int32_t B, const int32_t *__restrict__ cp
       const int t = bctype[f];
       if (t == MFG_BC_INTERFACE || t == MFG_BC_SYMM) sr.flags |= SLOT_NODE_AVG;
     }
-    sr.pad = 0;
+    const int32_t k0 = fptr[f];
+    const bool tri = fptr[f + 1] - k0 == 3;
+    if (tri) sr.flags |= SLOT_TRI;
+    for (int t = 0; t < 3; t++) sr.tri[t] = tri ? f2n[k0 + t] : 0;
     slots[j] = sr;
   }
 }
@@ -2467,6 +2489,8 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   std::vector<int32_t> cptr, c2f;
   build_c2f(m, cptr, c2f);
   ctx->S = cptr[C];
+  std::vector<int64_t> fnp((size_t)m->n_face + 1, 0);
+  for (int32_t f = 0; f < m->n_face; f++) fnp[f + 1] = fnp[f] + m->nnpf[f];
   std::vector<SlotRec> slots(ctx->S);
   for (int32_t c = 0; c < C; c++) {
     for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
@@ -2489,7 +2513,9 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
         const int t = m->bctype[f];
         if (t == MFG_BC_INTERFACE || t == MFG_BC_SYMM) s.flags |= SLOT_NODE_AVG;
       }
-      s.pad = 0;
+      const bool tri = m->nnpf[f] == 3;
+      if (tri) s.flags |= SLOT_TRI;
+      for (int t = 0; t < 3; t++) s.tri[t] = tri ? m->f2n[fnp[f] + t] : 0;
       slots[j] = s;
     }
   }
@@ -2890,7 +2916,8 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
                                 cudaMemcpyDeviceToDevice, st));
   MFG_CUDA_OR(
       cudaMemcpyAsync(ctx->vol, pp->vol, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  k_dev_slots<<<grid_for(C), kBlock, 0, st>>>(C, G, pp->cptr, pp->cf, pp->f2c, pp->bctype,
+  k_dev_slots<<<grid_for(C), kBlock, 0, st>>>(C, G, pp->cptr, pp->cf, pp->fptr, pp->f2n,
+                                              pp->f2c, pp->bctype,
                                               pp->xfn, pp->yfn, pp->zfn, pp->area, pp->xfc,
                                               pp->yfc, pp->zfc, pp->xcc, pp->ycc, pp->zcc,
                                               ctx->slots, flags);

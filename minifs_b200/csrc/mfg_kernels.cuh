@@ -42,12 +42,15 @@ enum : int {
 // (compute_timestep.cpp:762), the other cell, and flags.
 struct __align__(16) SlotRec {
   double nx, ny, nz, area, dn;
-  int32_t nb;     // neighbour cell (ghost C+k for boundary face k)
-  int32_t face;   // face index
-  int32_t flags;  // SLOT_*
-  int32_t pad;
+  int32_t nb;      // neighbour cell (ghost C+k for boundary face k)
+  int32_t face;    // face index
+  int32_t flags;   // SLOT_*
+  int32_t tri[3];  // a triangular face's nodes in file order (SLOT_TRI), else 0
 };
-enum : int32_t { SLOT_IS_C2 = 1, SLOT_BOUNDARY = 2, SLOT_NODE_AVG = 4 };
+static_assert(sizeof(SlotRec) == 64, "slot record: one 64-byte line");
+// SLOT_TRI: the gradient reads the face's nodes from the slot instead of
+// through the face -> node offsets
+enum : int32_t { SLOT_IS_C2 = 1, SLOT_BOUNDARY = 2, SLOT_NODE_AVG = 4, SLOT_TRI = 8 };
 
 // LU-SGS sweep record: normal oriented out of the swept cell and the
 // multiplier of the flux (0.5*area forward, area backward).
