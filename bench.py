@@ -238,10 +238,21 @@ def cpu_baseline(mesh, pg, params, wl, iters=2):
     if r is None:
         r = cpu_port_run(pg, params, iters)
     t = sum(r["iter_times"])
-    return {"value": pg.n_cell * len(r["iter_times"]) / t, "unit": UNIT, "cores": r["threads"],
-            "kind": r["kind"],
-            "sample": f"{wl['name']}, {len(r['iter_times'])} full iterations after setup, "
-                      f"{r['desc']}, {t:.2f} s"}
+    out = {"value": pg.n_cell * len(r["iter_times"]) / t, "unit": UNIT, "cores": r["threads"],
+           "kind": r["kind"],
+           "sample": f"{wl['name']}, {len(r['iter_times'])} full iterations after setup, "
+                     f"{r['desc']}, {t:.2f} s"}
+    # the serial build on one core beside the threaded one, same sample
+    from oracle import refrun
+    if r["kind"] == "reference" and r["threads"] > 1 and refrun.available():
+        flow = dict(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"], cfl_end=wl["cfl"],
+                    n_steps=iters, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
+                    bump_x0=0.5, bump_y0=0.5, bump_z0=0.5)
+        rs = refrun.run(mesh, flow, light=True, dump=False)
+        ts = sum(rs["iter_times"])
+        out["serial_1core"] = {"value": pg.n_cell * len(rs["iter_times"]) / ts, "unit": UNIT,
+                               "cores": 1, "sample": f"reference serial build, {ts:.2f} s"}
+    return out
 
 
 # ---------------------------------------------------------------------------
