@@ -94,19 +94,11 @@ def _node_id(i, j, k, nx, ny):
     return i + (nx + 1) * (j + (ny + 1) * k)
 
 
-def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0,
-             lz: float = 1.0, jitter: float = 0.15, seed: int = 1,
-             bc_types=(FAR_FIELD,) * 6, bump=None) -> RawMesh:
-    """Kuhn-split hex block on ``[0,lx]x[0,ly]x[0,lz]``.
-
-    ``jitter`` is the half-width, in units of the local spacing, of the
-    uniform displacement applied to every coordinate that does not lie on a
-    boundary plane (boundary nodes stay on their planes).  ``bc_types`` gives
-    the BC type of the patches x-, x+, y-, y+, z-, z+ (patch ids 1..6).
-    ``bump=(height, width, x0)`` lifts the bottom wall to
-    ``zb(x) = height*exp(-((x-x0)/width)^2)`` and stretches each column as
-    ``z = zb + (lz - zb) * zeta``.
-    """
+def _box_nodes(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float, jitter: float,
+               seed: int, bump):
+    """Node coordinates of an ``nx*ny*nz`` hex block: node
+    ``i + (nx+1)*(j + (ny+1)*k)``, interior coordinates jittered by up to
+    ``jitter`` local spacings, the optional bottom bump (see ``box_mesh``)."""
     nx, ny, nz = int(nx), int(ny), int(nz)
     nn = (nx + 1) * (ny + 1) * (nz + 1)
     ii, jj, kk = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1),
@@ -134,6 +126,24 @@ def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0,
         zeta = z / lz
         z = zb + (lz - zb) * zeta
 
+    return x, y, z
+
+
+def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0,
+             lz: float = 1.0, jitter: float = 0.15, seed: int = 1,
+             bc_types=(FAR_FIELD,) * 6, bump=None) -> RawMesh:
+    """Kuhn-split hex block on ``[0,lx]x[0,ly]x[0,lz]``.
+
+    ``jitter`` is the half-width, in units of the local spacing, of the
+    uniform displacement applied to every coordinate that does not lie on a
+    boundary plane (boundary nodes stay on their planes).  ``bc_types`` gives
+    the BC type of the patches x-, x+, y-, y+, z-, z+ (patch ids 1..6).
+    ``bump=(height, width, x0)`` lifts the bottom wall to
+    ``zb(x) = height*exp(-((x-x0)/width)^2)`` and stretches each column as
+    ``z = zb + (lz - zb) * zeta``.
+    """
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    x, y, z = _box_nodes(nx, ny, nz, lx, ly, lz, jitter, seed, bump)
     nhex = nx * ny * nz
     hidx = np.arange(nhex, dtype=np.int64)
     hi = hidx % nx
@@ -239,6 +249,117 @@ def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0,
                    nnpf=np.full(c1.shape[0], 3, dtype=np.int32),
                    f2n=np.ascontiguousarray(fn.reshape(-1).astype(np.int32)),
                    f2c=f2c, n_cell=ncell, n_bface=nb, patches=patches)
+
+
+def poly_mesh(x, y, z, cells, n_patch_types) -> RawMesh:
+    """A FlowStar mesh from polyhedral cells.
+
+    ``cells[c]`` lists the faces of cell ``c`` as ``(nodes, patch)``: the
+    face's node ids in cyclic order and, for a face on the domain boundary,
+    its patch id (1-based; None inside).  A face shared by two cells appears
+    once in each.  Faces come out in the layout ``box_mesh`` documents:
+    boundary faces first by (cell, local slot), interior faces by (lower
+    cell, higher cell) with ``c1`` the lower cell, each face's nodes ordered
+    so that its normal (Newell's, about the node mean) points out of ``c1``
+    (the cyclic order reversed behind the first node otherwise).
+    ``n_patch_types`` gives the BC type of patches 1, 2, ...
+    """
+    x = np.asarray(x, np.float64)
+    y = np.asarray(y, np.float64)
+    z = np.asarray(z, np.float64)
+    open_faces = {}
+    interior = []   # (c1, c2, nodes of the c1 side)
+    boundary = []   # (c, slot, nodes, patch)
+    for c, flist in enumerate(cells):
+        for slot, (nodes, patch) in enumerate(flist):
+            key = tuple(sorted(nodes))
+            other = open_faces.pop(key, None)
+            if other is None:
+                open_faces[key] = (c, slot, tuple(nodes), patch)
+            else:
+                oc, _, onodes, _ = other
+                c1, c2 = (oc, c) if oc < c else (c, oc)
+                interior.append((c1, c2, onodes if oc < c else tuple(nodes)))
+    for key, (c, slot, nodes, patch) in open_faces.items():
+        if patch is None:
+            raise ValueError(f"face {nodes} of cell {c} has no neighbour and no patch")
+        boundary.append((c, slot, nodes, patch))
+    boundary.sort(key=lambda t: (t[0], t[1]))
+    interior.sort(key=lambda t: (t[0], t[1]))
+    ncell = len(cells)
+    cnodes = [sorted({n for nodes, _ in flist for n in nodes}) for flist in cells]
+    cc = np.array([[x[v].mean(), y[v].mean(), z[v].mean()] for v in cnodes])
+
+    def oriented(nodes, c1):
+        v = np.array(nodes)
+        px, py, pz = x[v], y[v], z[v]
+        qx, qy, qz = np.roll(px, -1), np.roll(py, -1), np.roll(pz, -1)
+        nrm = np.array([np.sum((py - qy) * (pz + qz)), np.sum((pz - qz) * (px + qx)),
+                        np.sum((px - qx) * (py + qy))])
+        fc = np.array([px.mean(), py.mean(), pz.mean()])
+        if float(np.dot(nrm, fc - cc[c1])) < 0.0:
+            nodes = (nodes[0],) + tuple(reversed(nodes[1:]))
+        return nodes
+
+    f2n, nnpf, f2c = [], [], []
+    for c, _, nodes, patch in boundary:
+        nodes = oriented(nodes, c)
+        f2n.extend(nodes)
+        nnpf.append(len(nodes))
+        f2c.extend((c, -patch))
+    for c1, c2, nodes in interior:
+        nodes = oriented(nodes, c1)
+        f2n.extend(nodes)
+        nnpf.append(len(nodes))
+        f2c.extend((c1, c2))
+    patches = [(pid, int(t)) for pid, t in enumerate(n_patch_types, start=1)]
+    return RawMesh(x=np.ascontiguousarray(x), y=np.ascontiguousarray(y),
+                   z=np.ascontiguousarray(z), nnpf=np.array(nnpf, np.int32),
+                   f2n=np.array(f2n, np.int32), f2c=np.array(f2c, np.int32), n_cell=ncell,
+                   n_bface=len(boundary), patches=patches)
+
+
+def hexprism_mesh(nx: int, ny: int, nz: int, jitter: float = 0.1, seed: int = 1,
+                  bc_types=(FAR_FIELD,) * 6, prism_columns=lambda i, j: (i + j) % 2 == 0,
+                  bump=None) -> RawMesh:
+    """A mixed hexahedron / triangular-prism block on the unit cube: the hex
+    columns (i, j) for which ``prism_columns`` holds are split by their
+    vertical diagonal plane into two prisms per layer (the split is
+    conforming: prisms meet prisms on triangles, hexes on whole quads).
+    Nodes, jitter, bump and patches (x-, x+, y-, y+, z-, z+ = 1..6) as in
+    ``box_mesh``; cells in hex order ``i + nx*(j + ny*k)``, a split hex
+    giving two consecutive cells."""
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    x, y, z = _box_nodes(nx, ny, nz, 1.0, 1.0, 1.0, jitter, seed, bump)
+
+    def nid(i, j, k):
+        return i + (nx + 1) * (j + (ny + 1) * k)
+
+    cells = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                v = {(a, b, c): nid(i + a, j + b, k + c)
+                     for a in (0, 1) for b in (0, 1) for c in (0, 1)}
+                q = lambda *corners: tuple(v[t] for t in corners)  # noqa: E731
+                xm = (q((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0)), 1 if i == 0 else None)
+                xp = (q((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1)), 2 if i == nx - 1 else None)
+                ym = (q((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)), 3 if j == 0 else None)
+                yp = (q((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0)), 4 if j == ny - 1 else None)
+                bot, top = (5 if k == 0 else None), (6 if k == nz - 1 else None)
+                if not prism_columns(i, j):
+                    cells.append([xm, xp, ym, yp,
+                                  (q((0, 0, 0), (0, 1, 0), (1, 1, 0), (1, 0, 0)), bot),
+                                  (q((0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)), top)])
+                    continue
+                diag = (q((0, 0, 0), (1, 1, 0), (1, 1, 1), (0, 0, 1)), None)
+                cells.append([ym, xp, diag,
+                              (q((0, 0, 0), (1, 1, 0), (1, 0, 0)), bot),
+                              (q((0, 0, 1), (1, 0, 1), (1, 1, 1)), top)])
+                cells.append([xm, yp, diag,
+                              (q((0, 0, 0), (0, 1, 0), (1, 1, 0)), bot),
+                              (q((0, 0, 1), (1, 1, 1), (0, 1, 1)), top)])
+    return poly_mesh(x, y, z, cells, bc_types)
 
 
 def cube_mesh(n: int, jitter: float = 0.15, seed: int = 1) -> RawMesh:
