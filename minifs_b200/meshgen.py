@@ -362,6 +362,49 @@ def hexprism_mesh(nx: int, ny: int, nz: int, jitter: float = 0.1, seed: int = 1,
     return poly_mesh(x, y, z, cells, bc_types)
 
 
+def merged_hex_mesh(nx: int, ny: int, nz: int, jitter: float = 0.1, seed: int = 1,
+                    bc_types=(FAR_FIELD,) * 6, merge=lambda i, j, k: (j + k) % 2 == 0,
+                    at_boundary: bool = False, bump=None) -> RawMesh:
+    """A hex block (``nx`` even) in which the hex pairs (i, i+1) with even i
+    and ``merge(i, j, k)`` form one cell of 10 faces and 12 nodes (the pair's
+    shared face removed): an interior merged cell has 5 neighbours before it
+    and 5 after it in the cell order.  Pairs on the boundary merge only with
+    ``at_boundary`` (they then have up to 10 faces after them, ghosts
+    included).  Nodes and patches as in ``box_mesh``."""
+    nx, ny, nz = int(nx), int(ny), int(nz)
+    if nx % 2:
+        raise ValueError("nx must be even")
+    x, y, z = _box_nodes(nx, ny, nz, 1.0, 1.0, 1.0, jitter, seed, bump)
+
+    def nid(i, j, k):
+        return i + (nx + 1) * (j + (ny + 1) * k)
+
+    def hex_faces(i, j, k):
+        v = {(a, b, c): nid(i + a, j + b, k + c) for a in (0, 1) for b in (0, 1) for c in (0, 1)}
+        q = lambda *corners: tuple(v[t] for t in corners)  # noqa: E731
+        return {"xm": (q((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0)), 1 if i == 0 else None),
+                "xp": (q((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1)), 2 if i == nx - 1 else None),
+                "ym": (q((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)), 3 if j == 0 else None),
+                "yp": (q((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0)), 4 if j == ny - 1 else None),
+                "zm": (q((0, 0, 0), (0, 1, 0), (1, 1, 0), (1, 0, 0)), 5 if k == 0 else None),
+                "zp": (q((0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)), 6 if k == nz - 1 else None)}
+
+    order = ("xm", "xp", "ym", "yp", "zm", "zp")
+    cells = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(0, nx, 2):
+                a, b = hex_faces(i, j, k), hex_faces(i + 1, j, k)
+                inner = 0 < i and i + 2 < nx and 0 < j < ny - 1 and 0 < k < nz - 1
+                if merge(i, j, k) and (inner or at_boundary):
+                    cells.append([a["xm"], b["xp"], a["ym"], b["ym"], a["yp"], b["yp"],
+                                  a["zm"], b["zm"], a["zp"], b["zp"]])
+                else:
+                    cells.append([a[f] for f in order])
+                    cells.append([b[f] for f in order])
+    return poly_mesh(x, y, z, cells, bc_types)
+
+
 def cube_mesh(n: int, jitter: float = 0.15, seed: int = 1) -> RawMesh:
     """Unit cube, ``n^3`` hexes x 6 tets, far-field on every side."""
     return box_mesh(n, n, n, jitter=jitter, seed=seed)

@@ -1,13 +1,15 @@
 """The CUDA path on mixed hexahedron / triangular-prism meshes (quadrilateral
-faces take the gradient's face -> node route, triangles the slot record's):
-bit for bit against the reference run on the same grid, per routine and
-fused; the GPU preprocessing and the device-built context against the host
-path."""
+faces take the gradient's face -> node route, triangles the slot record's)
+and on hex blocks with merged hex pairs (cells with 5-6 sweep records: the
+8-record persistent sweeps; with boundary merges up to 10: one launch per
+level): bit for bit against the reference run on the same grid, per routine
+and fused; the GPU preprocessing and the device-built context against the
+host path."""
 import numpy as np
 import pytest
 
 from helpers import assert_bitwise
-from minifs_b200 import grid as gr, meshgen
+from minifs_b200 import _lib, grid as gr, meshgen
 from minifs_b200.compare import state_rel_err
 from minifs_b200.solver import Solver
 from oracle import refrun
@@ -70,3 +72,53 @@ def test_mixed_precision_close():
     a.iterate(ITERS)
     b.iterate(ITERS)
     assert state_rel_err(b.download("q"), a.download("q"), pg.n, p.p_bar)["max_norm"] < 1e-6
+
+
+def merged_case(at_boundary):
+    m = meshgen.merged_hex_mesh(12, 9, 8, jitter=0.15, seed=5, bc_types=(6, 6, 4, 6, 3, 6),
+                                at_boundary=at_boundary)
+    _, flow, p, _ = case(n=(2, 2, 2))
+    pg = gr.prepare(m, p, bump_amp=0.05, bump_sigma=0.15)
+    return m, flow, p, pg
+
+
+@pytest.mark.parametrize("at_boundary", [False, True])
+def test_merged_cells_bitexact_with_reference(at_boundary):
+    m, flow, p, pg = merged_case(at_boundary)
+    ref = refrun.run(m, flow, dump_iters="-1")
+    for fused in (False, True):
+        s = Solver(pg, p)
+        info = s.info()
+        if at_boundary:
+            assert info["sweep_mode"] == 0 and info["sweep_records"] == 0
+        else:
+            assert info["sweep_mode"] == 1 and info["sweep_records"] == 8
+        if fused:
+            s.iterate(ITERS)
+        else:
+            for _ in range(ITERS):
+                s.step()
+        what = "fused" if fused else "per routine"
+        assert_bitwise(s.download("q"), ref["final.q"], f"{what} state")
+        assert_bitwise(s.download("dqdx"), ref["final.dqdx"], f"{what} dqdx")
+        s.close()
+
+
+def test_merged_cells_lanes_mixed_and_device_context():
+    m, flow, p, pg = merged_case(False)
+    a = Solver(pg, p)
+    tuned = a.autotune_sweeps(2)
+    assert tuned["lanes_per_cell"] in (4, 8)
+    a.iterate(ITERS)
+    prep = gr.DevicePrep(m, device=0)
+    b = Solver.from_device_prep(prep, p, prep.init_flow(p, bump_amp=0.05, bump_sigma=0.15))
+    b.iterate(ITERS)
+    assert_bitwise(b.download("q"), a.download("q"), "device-built context")
+    c = Solver(pg, p, precision="mixed")
+    c.iterate(ITERS)
+    assert state_rel_err(c.download("q"), a.download("q"), pg.n, p.p_bar)["max_norm"] < 1e-6
+    # the mixed form needs the persistent sweeps, which 10-record cells rule out
+    m2, _, _, pg2 = merged_case(True)
+    with pytest.raises(_lib.MfgError) as e:
+        Solver(pg2, p, precision="mixed")
+    assert e.value.code == -6

@@ -1,7 +1,8 @@
 """Mixed hexahedron / triangular-prism meshes (quadrilateral and triangular
-faces, cells of 5 and 6 faces, 6 and 8 nodes): the host preprocessing and
-the C oracle against the reference compiled from its own sources, run on
-the same grid file.  Host only."""
+faces, cells of 5 and 6 faces, 6 and 8 nodes) and hex blocks with merged
+hex pairs (cells of 10 faces and 12 nodes): the host preprocessing and the
+C oracle against the reference compiled from its own sources, run on the
+same grid file.  Host only."""
 import numpy as np
 import pytest
 
@@ -67,3 +68,21 @@ def test_grid_file_round_trip(tmp_path):
     for k in ("nnpf", "f2n", "f2c"):
         assert np.array_equal(getattr(got, k), getattr(m, k)), k
     assert got.n_bface == m.n_bface
+
+
+@pytest.mark.parametrize("at_boundary", [False, True])
+def test_merged_cells_match_reference(at_boundary, tmp_path):
+    m = meshgen.merged_hex_mesh(8, 5, 5, jitter=0.15, seed=3, bc_types=(6, 6, 4, 6, 3, 6),
+                                at_boundary=at_boundary)
+    _, flow, p = case()
+    ref = refrun.run(m, flow, dump_iters="-1", workdir=str(tmp_path))
+    pg = gr.prepare(m, p, bump_amp=0.05, bump_sigma=0.15)
+    for k in PREP:
+        assert_bitwise(pg.arrays[k], ref[k], k)
+    assert_bitwise(pg.q0, ref["init.q"], "initial state")
+    assert pg.arrays["nnpc"].max() == 12
+    o = oracle_from(pg.arrays, p.as_dict() | {"cfl_nstep": p.cfl_nstep}, pg.q0,
+                    (pg.n_node, pg.n_face, pg.n_cell, pg.n_bface))
+    for _ in range(flow["n_steps"]):
+        o.step()
+    assert_bitwise(o.q, ref["final.q"], "oracle state")
