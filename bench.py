@@ -14,6 +14,8 @@ larger than the 126 MB L2, so no flush is needed between steps.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
   python bench.py --form batched [--ncase 64]
   python bench.py --form mixed [--mixed-size 128] [--converge 3000]
+  python bench.py --form channel [--converge 20000]
+  python bench.py --form batched --precision mixed
 
 --form batched: 64 cube cases with n^3 x 6 tets, n uniform in [8, 48], Mach
 U(0.3, 0.8), alpha U(-5, 5) deg, jitter U(0, 0.2)h, all in one context (one
@@ -24,6 +26,14 @@ another in their own contexts.
 20) in the FP64 and the mixed-precision forms: throughput of each, the
 mixed state's error against FP64, and with --converge the iterations and
 time each form needs for a 1e-6 residual drop.
+
+--form channel: the 4x1x1 channel (192x48x48 hexes x 6 tets, slip wall with
+a bump at the bottom, Mach 0.7, CFL 30) in both forms, as --form mixed, to a
+1e-8 residual drop with --converge, and the mixed form's wall pressure
+against FP64.
+
+--precision mixed (batched form): the batch and its sequential per-case
+reference both in the mixed form.
 
 Before the warm-up the sweep launch parameters are chosen by measurement
 on the workload's own grid (mfg_autotune_sweeps) and reported.
@@ -67,11 +77,14 @@ def parse():
     ap.add_argument("--size", type=int, default=64, help="hexes per cube edge (64 = 1.57M tets)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="fp64", choices=["fp64", "batched", "mixed"],
+    ap.add_argument("--form", default="fp64", choices=["fp64", "batched", "mixed", "channel"],
                     help="fp64: the single-grid workload; batched: 64 uneven cases in one "
                          "context against the same cases run one after another; mixed: the "
                          "mixed-precision form against FP64 on the 128^3 x 6 cube")
     ap.add_argument("--mixed-size", type=int, default=128)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="batched form: the precision of the batch and of its sequential "
+                         "per-case reference")
     ap.add_argument("--converge", type=int, default=0,
                     help="mixed form: also iterate both forms to a 1e-6 residual drop "
                          "(at most this many iterations) and time it")
@@ -494,7 +507,7 @@ def main():
     torch.cuda.set_stream(stream)
     if args.form == "batched":
         run_batched(args, rank, world, local, stream, dist)
-    elif args.form == "mixed":
+    elif args.form in ("mixed", "channel"):
         run_mixed(args, rank, world, local, stream, dist)
     else:
         run_single(args, rank, world, local, stream, dist)
@@ -563,12 +576,27 @@ def mixed_workload(n: int) -> dict:
                 alpha=1.25, cfl=20.0, bump_amp=0.05, bump_sigma=0.1)
 
 
-def to_drop(s, stream, target, max_iter, chunk=100):
+def channel_workload() -> dict:
+    """Box 4x1x1 of 192x48x48 hexes x 6 tets (2,654,208 cells), jitter 0.1h,
+    a slip wall at the bottom carrying a Gaussian bump (height 0.05, width
+    0.2, at x = 1.5), far field on the other faces; Mach 0.7, alpha 0, CFL
+    30, 5% density bump; converged to a 1e-8 residual drop."""
+    return dict(name="channel192x48x48x6_M0.7_a0_cfl30", jitter=0.1, seed=5, mach=0.7,
+                alpha=0.0, cfl=30.0, bump_amp=0.05, bump_sigma=0.1, drop=1e-8,
+                bump_center=(2.0, 0.5, 0.5))
+
+
+def to_drop(s, stream, target, max_iter, chunk=100, fp64_flux_below=None):
     """Iterate until the rho residual norm falls below target x its first
-    value; returns (iterations, device ms, drop reached)."""
+    value; returns (iterations, device ms, drop reached, iterations at the
+    switch to the FP64 flux or None).  With ``fp64_flux_below`` (mixed form)
+    the flux switches to FP64 once the drop is below that value."""
     import torch
-    first, it, ms, drop = None, 0, 0.0, 1.0
+    first, it, ms, drop, switched = None, 0, 0.0, 1.0, None
     while it < max_iter:
+        if fp64_flux_below is not None and switched is None and drop <= fp64_flux_below:
+            s.set_flux_fp64(True)
+            switched = it
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -585,7 +613,7 @@ def to_drop(s, stream, target, max_iter, chunk=100):
             break
         it += chunk
         drop = float(nrm[-1, 0] / first)
-    return it, ms, drop
+    return it, ms, drop, switched
 
 
 def run_mixed(args, rank, world, local, stream, dist):
@@ -594,10 +622,17 @@ def run_mixed(args, rank, world, local, stream, dist):
     the iterations and time each needs for a 1e-6 residual drop."""
     from minifs_b200 import grid as gr, meshgen
     from minifs_b200.solver import Solver
-    wl = mixed_workload(args.mixed_size)
-    mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
+    if args.form == "channel":
+        wl = channel_workload()
+        mesh = meshgen.channel_mesh(jitter=wl["jitter"], seed=wl["seed"])
+    else:
+        wl = mixed_workload(args.mixed_size)
+        wl["drop"] = 1e-6
+        mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
     params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
-    pg = gr.prepare(mesh, params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
+    pg = gr.prepare(mesh, params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
+                    bump_center=wl.get("bump_center", (0.5, 0.5, 0.5)))
+    drop_key = f"to_drop_{wl['drop']:.0e}".replace("e-0", "e-")
     C, G, F, N = pg.n_cell, pg.n_bface, pg.n_face, pg.n_node
     K = int(pg.arrays["nnpc"].sum())
     res = {}
@@ -612,9 +647,15 @@ def run_mixed(args, rank, world, local, stream, dist):
             s2 = Solver(pg, params, device=local, precision=prec)
             s2.set_stream(stream.cuda_stream)
             s2.calculate_gradient()
-            it, ms, drop = to_drop(s2, stream, 1e-6, args.converge)
-            r["to_drop_1e-6"] = {"iterations": it, "ms": ms, "drop": drop,
-                                 "cell_updates_per_s": C * it / (ms / 1e3)}
+            # below a 1e-6 drop the mixed form's FP32 dissipation would hold the
+            # residual at its rounding floor: the flux goes FP64 from there
+            tail = 1e-6 if (prec == "mixed" and wl["drop"] < 1e-6) else None
+            it, ms, drop, switched = to_drop(s2, stream, wl["drop"], args.converge,
+                                             fp64_flux_below=tail)
+            r[drop_key] = {"iterations": it, "ms": ms, "drop": drop,
+                           "cell_updates_per_s": C * it / (ms / 1e3)}
+            if prec == "mixed" and tail is not None:
+                r[drop_key]["fp64_flux_from_iteration"] = switched
             states[prec + "_conv"] = s2.download("q")
             s2.close()
         res[prec] = r
@@ -629,6 +670,22 @@ def run_mixed(args, rank, world, local, stream, dist):
     # and the phase-profile iterations of measure()
     err_same_iters = rel_err(states["mixed"], states["fp64"])
     err_conv = rel_err(states["mixed_conv"], states["fp64_conv"]) if args.converge else None
+    wall = None
+    bct = np.asarray(pg.arrays["bctype"])[:G]
+    wf = np.nonzero(bct == 3)[0]
+    if wf.size:
+        # pressure on the wall faces (the inner cell's, which the mirror ghost
+        # copies): the mixed form against FP64, relative to p + p_bar
+        c1 = np.asarray(pg.arrays["f2c"])[2 * wf]
+
+        def wall_err(a, b):
+            pa, pb = a[4 * n + c1], b[4 * n + c1]
+            d = np.abs(pa - pb) / (np.abs(pb) + params.p_bar)
+            return {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d))),
+                    "faces": int(wf.size)}
+        wall = {"same_iterations": wall_err(states["mixed"], states["fp64"]),
+                "at_drop": wall_err(states["mixed_conv"], states["fp64_conv"])
+                if args.converge else None}
     if rank == 0:
         m, d = res["mixed"], res["fp64"]
         info = m["info"]
@@ -637,7 +694,7 @@ def run_mixed(args, rank, world, local, stream, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": wl["name"], "form": "mixed", "cells": C, "faces": F,
+            "config": {"workload": wl["name"], "form": args.form, "cells": C, "faces": F,
                        "precision": "mixed: FP32 Roe averages/dissipation, LU-SGS off-diagonal "
                                     "products and gradient; FP64 central flux, residual, "
                                     "Diag, norm, update",
@@ -648,15 +705,16 @@ def run_mixed(args, rank, world, local, stream, dist):
                                         "backward": info["bw_levels"]}},
             "fp64": {"value": d["value"], "ms_per_step": d["ms"] / args.steps,
                      "autotuned": d["autotuned"],
-                     "phases": d["phases"], "to_drop_1e-6": d.get("to_drop_1e-6")},
+                     "phases": d["phases"], drop_key: d.get(drop_key)},
             "mixed_over_fp64": m["value"] / d["value"],
             "state_rel_err_vs_fp64": {"same_iterations": err_same_iters,
-                                      "at_1e-6_drop": err_conv},
+                                      "at_" + drop_key[len("to_drop_"):] + "_drop": err_conv},
+            "wall_pressure_rel_err_vs_fp64": wall,
             "autotuned": m["autotuned"],
             "roofline": m["roofline"],
             "flux_plus_gradient": m["flux_plus_gradient"],
             "phases": m["phases"],
-            "to_drop_1e-6": m.get("to_drop_1e-6"),
+            drop_key: m.get(drop_key),
             "cpu_baseline": None,
             "e2e": m["e2e"],
             "gpu_launches": m["launches"],
@@ -688,7 +746,7 @@ def run_batched(args, rank, world, local, stream, dist):
     # sequential per-case launches: each case alone, timed on the device
     seq_ms, seq_cells = 0.0, 0
     for pg, p in zip(grids, params):
-        s = Solver(pg, p, device=local)
+        s = Solver(pg, p, device=local, precision=args.precision)
         s.set_stream(stream.cuda_stream)
         s.calculate_gradient()
         s.iterate(max(args.warmup, 3), norms=False)
@@ -704,7 +762,7 @@ def run_batched(args, rank, world, local, stream, dist):
         s.close()
     total_cells = int(shard.reduce_sum(counts[0], dist, "cuda"))
     seq_ms = shard.reduce_max(seq_ms, dist, "cuda")
-    b = BatchSolver(grids, params, device=local)
+    b = BatchSolver(grids, params, device=local, precision=args.precision)
     b.set_stream(stream.cuda_stream)
     r = measure(b, tuple(counts), args, stream, dist, world, local, total_cells=total_cells)
     norms = b.residual_norm()
@@ -715,12 +773,15 @@ def run_batched(args, rank, world, local, stream, dist):
         line = {
             "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": bw["name"], "form": "batched", "ncase": len(ns),
+            "config": {"workload": bw["name"] + ("" if args.precision == "fp64" else "_mixed"),
+                       "form": "batched", "ncase": len(ns),
                        "n_min": min(ns), "n_max": max(ns), "cells": total_cells,
                        "cells_rank0": counts[0], "cases_rank0": len(mine),
-                       "precision": "fp64 (bit-faithful per case)",
+                       "precision": ("fp64 (bit-faithful per case)" if args.precision == "fp64"
+                                     else "mixed (each case as its own mixed run)"),
                        "parallelism": (f"cases sharded over {world} ranks by cell count"
                                        if world > 1 else "single"),
                        "l2": "no flush: working set "

@@ -208,6 +208,14 @@ int mfg_set_ghost_variables(mfg_ctx *ctx);
  * of every iteration, where main.cpp:286 would; on = 0 (the default, the
  * reference's frozen ghosts): they do not. */
 int mfg_set_live_bc(mfg_ctx *ctx, int32_t on);
+/* Mixed form only (no counterpart in the reference): on = 1 computes the Roe
+ * flux wholly in FP64 (the face kernel of the FP64 form; the rest of the
+ * iteration stays mixed), on = 0 (the default) its dissipation in FP32.  The
+ * FP32 dissipation's rounding leaves a residual floor (near 4e-8 of the
+ * initial residual on the wall channel); with the FP64 flux the residual is
+ * evaluated in FP64 and converges like the FP64 form's.  The FP64 form
+ * accepts on = 1 (its flux is FP64) and rejects on = 0. */
+int mfg_set_flux_fp64(mfg_ctx *ctx, int32_t on);
 /* The whole main-loop body (main.cpp:201-291) n times, fused kernels in a
  * CUDA graph.  Each iteration's gradient is computed once, as in the loop;
  * all but the last run beside the next iteration's face kernels (same

@@ -132,6 +132,7 @@ def load(build_if_missing: bool = True):
         "mfg_calculate_gradient": (ct.c_int, [ctxp]),
         "mfg_set_ghost_variables": (ct.c_int, [ctxp]),
         "mfg_set_live_bc": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_set_flux_fp64": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_iterate": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
         "mfg_iterate_host": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p, f64p, f64p, f64p]),
         "mfg_residual_norm": (ct.c_int, [ctxp, f64p]),

@@ -1467,6 +1467,7 @@ struct mfg_ctx {
   double *fflux = nullptr;   // per-face flux [5][F]
   int32_t *bctype_d = nullptr;  // BC type of each boundary face [G]
   int32_t live_bc = 0;          // ghost states recomputed every iteration
+  int32_t flux_fp64 = 0;        // mixed form: the Roe flux wholly in FP64
   int32_t *fnptr = nullptr, *fnodes = nullptr;
   int32_t *nptr = nullptr, *nsrc = nullptr, *ninfo = nullptr, *bface_c1 = nullptr;
   double *nw = nullptr, *wnode = nullptr, *nsym = nullptr;
@@ -3108,6 +3109,16 @@ int mfg_set_ghost_variables(mfg_ctx *ctx) {
   return launch_ghost_bc(ctx, ctx->stream);
 }
 
+int mfg_set_flux_fp64(mfg_ctx *ctx, int32_t on) {
+  if (!ctx || (on != 0 && on != 1)) return MFG_ERR_INVALID;
+  if (ctx->precision != MFG_PREC_MIXED) return on ? MFG_OK : MFG_ERR_UNSUPPORTED;
+  if (ctx->flux_fp64 != on) {
+    ctx->flux_fp64 = on;
+    drop_graphs(ctx);
+  }
+  return MFG_OK;
+}
+
 int mfg_set_live_bc(mfg_ctx *ctx, int32_t on) {
   if (!ctx || (on != 0 && on != 1)) return MFG_ERR_INVALID;
   if (ctx->live_bc != on) {
@@ -3167,7 +3178,7 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
   const Cases cs = cases_of(ctx);
   const bool mx = ctx->precision == MFG_PREC_MIXED;
   if (flux) {  // each face's Roe flux once, then gathered per cell
-    if (mx)
+    if (mx && !ctx->flux_fp64)
       k_face_flux<true><<<grid_for(ctx->F), kBlock, 0, st>>>(ctx->F, ctx->faces, q, ctx->P, cs,
                                                               ctx->fflux);
     else

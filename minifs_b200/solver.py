@@ -108,6 +108,11 @@ class Solver:
         self._call("mfg_set_live_bc", 1 if on else 0)
         self.live_bc = bool(on)
 
+    def set_flux_fp64(self, on: bool):
+        """Mixed form: the Roe flux wholly in FP64 (True) or with its
+        dissipation in FP32 (False, the default)."""
+        self._call("mfg_set_flux_fp64", 1 if on else 0)
+
     def step(self):
         """One ``main.cpp:201-291`` iteration through the per-routine calls."""
         self.zero_residuals()

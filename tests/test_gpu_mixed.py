@@ -124,3 +124,33 @@ def test_mixed_requires_persistent_sweeps():
     with pytest.raises(_lib.MfgError):
         s.set_sweep_mode(0)
     s.close()
+
+
+def test_mixed_form_with_fp64_flux():
+    """mfg_set_flux_fp64: the mixed form's face flux from the FP64 kernel
+    gives the FP64 form's residual bit for bit on the same state; switching
+    back restores the FP32 dissipation; the FP64 form refuses to go FP32."""
+    from minifs_b200 import _lib, grid as gr, meshgen
+    from minifs_b200.solver import Solver
+    m = meshgen.box_mesh(10, 8, 6, jitter=0.15, seed=2, bc_types=(6, 6, 4, 6, 3, 6))
+    m.patches = [(i + 1, t) for i, t in enumerate((6, 6, 4, 6, 3, 6))]
+    p = gr.make_params(mach=0.7, alpha=1.0, cfl_start=30.0)
+    pg = gr.prepare(m, p)
+    a = Solver(pg, p)
+    b = Solver(pg, p, precision="mixed")
+    b.set_flux_fp64(True)
+    for s in (a, b):
+        s.zero_residuals()
+        s.inviscid_flux()
+    assert np.array_equal(a.download("res"), b.download("res"))
+    b.set_flux_fp64(False)
+    b.zero_residuals()
+    b.inviscid_flux()
+    assert not np.array_equal(a.download("res"), b.download("res"))
+    a.set_flux_fp64(True)
+    with pytest.raises(_lib.MfgError) as e:
+        a.set_flux_fp64(False)
+    assert e.value.code == -6
+    b.set_flux_fp64(True)
+    b.iterate(5)
+    assert np.all(np.isfinite(b.download("q")))
