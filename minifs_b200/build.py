@@ -63,5 +63,33 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+SHIM = os.path.join(HERE, "shim")
+DROPIN = os.path.join(SHIM, "_build", "minifs_dropin")
+
+
+def build_dropin(ref: str = "/root/reference", verbose: bool = False) -> str | None:
+    """The reference's driver sequence on libmfgpu through the shim
+    (``shim/mfgpu_shim.cpp`` in place of the reference's four kernel files,
+    ``shim/dropin_main.cpp`` for main.cpp's hard-coded set-up), linked with
+    the reference's unmodified ``src/Base`` and ``load_grid.cpp`` read in
+    place.  Built only where the reference sources exist; the binary finds
+    libmfgpu.so next to the package through its run path."""
+    src = os.path.join(ref, "src")
+    if not os.path.isdir(src):
+        return None
+    os.makedirs(os.path.dirname(DROPIN), exist_ok=True)
+    base = sorted(os.path.join(src, "Base", f) for f in os.listdir(os.path.join(src, "Base"))
+                  if f.endswith(".cpp"))
+    cmd = [host_cxx(), "-std=c++11", "-O3", "-ffp-contract=off", "-w", "-o", DROPIN,
+           os.path.join(SHIM, "dropin_main.cpp"), os.path.join(SHIM, "mfgpu_shim.cpp")] + \
+        base + [os.path.join(src, "Kernels", "load_grid.cpp"),
+                "-I" + os.path.join(src, "Base"), "-I" + os.path.join(src, "Kernels"),
+                "-I" + INCLUDE, "-L" + LIBDIR, "-lmfgpu", "-Wl,-rpath,$ORIGIN/../../_lib"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return DROPIN
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
