@@ -54,6 +54,7 @@ extern "C" {
 #define MFG_FIELD_DQDY 5 /* [5n] gradient y (download) */
 #define MFG_FIELD_DQDZ 6 /* [5n] gradient z (download) */
 #define MFG_FIELD_DIAG 7 /* [C] LU-SGS diagonal of the last sweep (download) */
+#define MFG_FIELD_LIMITER 8 /* [5C] reconstruction limiter of the last flux (order 3, 4) */
 
 /* Precision modes. */
 #define MFG_PREC_FP64 0  /* the drop-in: every operation in FP64, bit-faithful */
@@ -216,6 +217,20 @@ int mfg_set_live_bc(mfg_ctx *ctx, int32_t on);
  * evaluated in FP64 and converges like the FP64 form's.  The FP64 form
  * accepts on = 1 (its flux is FP64) and rejects on = 0. */
 int mfg_set_flux_fp64(mfg_ctx *ctx, int32_t on);
+/* The reference's `order` switch (para_field_global.cpp:100: 1 first
+ * order; 2 second order without limiter; 3 with Barth's limiter; 4 with
+ * Venkatakrishnan's), which the reference declares but does not implement
+ * (its reconstruction call is commented out, cal_flux.cpp:175): order >= 2
+ * reconstructs each face's inner-cell states linearly from the cell's
+ * Green-Gauss gradient to the face centroid, limited per cell and variable
+ * for 3 (Barth-Jespersen) and 4 (Venkatakrishnan, eps^2 = (venkat_k h)^3,
+ * h = vol^(1/3)); ghost states stay first order; a face whose
+ * reconstructed density or absolute pressure is not positive keeps its
+ * first-order states.  The flux reads the gradient the previous
+ * CalculateGradient left (main.cpp's order of calls); this call and
+ * mfg_upload compute it for the current state.  LU-SGS stays first order.
+ * No reference output exists for order >= 2.  Default 1. */
+int mfg_set_order(mfg_ctx *ctx, int32_t order, double venkat_k);
 /* The whole main-loop body (main.cpp:201-291) n times, fused kernels in a
  * CUDA graph.  Each iteration's gradient is computed once, as in the loop;
  * all but the last run beside the next iteration's face kernels (same

@@ -22,7 +22,8 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory",
           -7: "bad mesh", -8: "no usable CUDA device",
           -9: "file missing, truncated or malformed"}
 
-FIELD = {"q": 0, "res": 1, "dt": 2, "dq": 3, "dqdx": 4, "dqdy": 5, "dqdz": 6, "diag": 7}
+FIELD = {"q": 0, "res": 1, "dt": 2, "dq": 3, "dqdx": 4, "dqdy": 5, "dqdz": 6, "diag": 7,
+         "limiter": 8}
 PREC = {"fp64": 0, "mixed": 1}
 PHASES = ("face_gather", "sweep_fwd", "sweep_bwd_update", "node_values", "grad_faces", "norm")
 
@@ -133,6 +134,7 @@ def load(build_if_missing: bool = True):
         "mfg_set_ghost_variables": (ct.c_int, [ctxp]),
         "mfg_set_live_bc": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_flux_fp64": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_set_order": (ct.c_int, [ctxp, ct.c_int32, ct.c_double]),
         "mfg_iterate": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
         "mfg_iterate_host": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p, f64p, f64p, f64p]),
         "mfg_residual_norm": (ct.c_int, [ctxp, f64p]),

@@ -432,15 +432,44 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
   gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
 }
 
+// Second-order face state (RECON): q + phi * grad(q) . (x_f - x_c) for an
+// inner cell, the ghost's own state otherwise (the reference's switch
+// `order`, para_field_global.cpp:100, has no implementation behind it, so
+// this is this library's own reconstruction: linear from the Green-Gauss
+// gradient of the state the face kernel reads, limited per cell).
+__device__ __forceinline__ void reconstruct(double *q, int32_t c, int32_t C, int64_t n,
+                                            const Cen &fc, const Cen *__restrict__ ccen,
+                                            const double *__restrict__ dqdx,
+                                            const double *__restrict__ dqdy,
+                                            const double *__restrict__ dqdz,
+                                            const double *__restrict__ phi) {
+  if (c >= C) return;
+  const Cen cc = ccen[c];
+  const double rx = fc.x - cc.x, ry = fc.y - cc.y, rz = fc.z - cc.z;
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    const int64_t k = (int64_t)v * n + c;
+    const double d = dqdx[k] * rx + dqdy[k] * ry + dqdz[k] * rz;
+    q[v] += (phi ? phi[(int64_t)v * C + c] : 1.0) * d;
+  }
+}
+
 // RoeFlux_noprec once per face (the reference's own face loop,
 // cal_flux.cpp:84-192), from q[c1] and q[c2] with the stored normal, into
 // fflux[5][F]; the face gathers then add each face's flux to its cells in
 // ascending face order.  The arguments are those the per-cell form passes
 // from either side, so the sums are the same bits with half the flux work.
-template <bool MX>
+// RECON:
+// the face states reconstructed to second order first (a face whose
+// reconstructed density or absolute pressure is not positive keeps its
+// first-order states).
+template <bool MX, bool RECON>
 __global__ void __launch_bounds__(kBlock, MFG_FLUX_MINB)
 k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restrict__ q8,
-            Params P0, Cases cs, double *__restrict__ fflux) {
+            Params P0, Cases cs, double *__restrict__ fflux, int32_t C, int64_t n,
+            const Cen *__restrict__ fcen, const Cen *__restrict__ ccen,
+            const double *__restrict__ dqdx, const double *__restrict__ dqdy,
+            const double *__restrict__ dqdz, const double *__restrict__ phi) {
   const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= F) return;
   const FaceRec fr = faces[f];
@@ -448,12 +477,99 @@ k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restri
   double ql[Q_STRIDE], qr[Q_STRIDE], fl[5];
   load_q(q8, fr.c1, ql);
   load_q(q8, fr.c2, qr);
+  if (RECON) {
+    double al[Q_STRIDE], ar[Q_STRIDE];
+#pragma unroll
+    for (int v = 0; v < Q_STRIDE; v++) {
+      al[v] = ql[v];
+      ar[v] = qr[v];
+    }
+    const Cen fc = fcen[f];
+    reconstruct(al, fr.c1, C, n, fc, ccen, dqdx, dqdy, dqdz, phi);
+    reconstruct(ar, fr.c2, C, n, fc, ccen, dqdx, dqdy, dqdz, phi);
+    if (al[0] > 0.0 && ar[0] > 0.0 && al[4] + P.p_bar > 0.0 && ar[4] + P.p_bar > 0.0) {
+      cell_props(al, P);
+      cell_props(ar, P);
+#pragma unroll
+      for (int v = 0; v < Q_STRIDE; v++) {
+        ql[v] = al[v];
+        qr[v] = ar[v];
+      }
+    }
+  }
   if (MX)
     roe_flux_mx(ql, qr, fr.nx, fr.ny, fr.nz, fr.area, P, flux_params<float>(P), fl);
   else
     roe_flux(ql, qr, fr.nx, fr.ny, fr.nz, fr.area, P, fl);
 #pragma unroll
   for (int k = 0; k < 5; k++) fflux[(int64_t)k * F + f] = fl[k];
+}
+
+// Per-cell limiter of the reconstruction, per variable: the minimum over the
+// cell's faces of the bound on the face's extrapolated change that keeps it
+// within the range of the cell and its face neighbours (ghosts included) --
+// Barth and Jespersen (AIAA 89-0366) -- or Venkatakrishnan's smooth form of
+// the same bound (AIAA 93-0880; eps^2 = (K h)^3, h = vol^(1/3)).
+template <bool VENKAT>
+__global__ void __launch_bounds__(kBlock)
+k_limiter(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
+          const SlotRec *__restrict__ slots, const double *__restrict__ q8,
+          const double *__restrict__ dqdx, const double *__restrict__ dqdy,
+          const double *__restrict__ dqdz, const Cen *__restrict__ fcen,
+          const Cen *__restrict__ ccen, double venkat_k, double *__restrict__ phi) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  double qc[Q_STRIDE], qmin[5], qmax[5], lim[5], gx[5], gy[5], gz[5];
+  load_q(q8, c, qc);
+  for (int v = 0; v < 5; v++) {
+    qmin[v] = qc[v];
+    qmax[v] = qc[v];
+    lim[v] = 1.0;
+    const int64_t k = (int64_t)v * n + c;
+    gx[v] = dqdx[k];
+    gy[v] = dqdy[k];
+    gz[v] = dqdz[k];
+  }
+  const int32_t s0 = cptr[c], s1 = cptr[c + 1];
+  for (int32_t s = s0; s < s1; s++) {
+    double qn[Q_STRIDE];
+    load_q(q8, slots[s].nb, qn);
+    for (int v = 0; v < 5; v++) {
+      qmin[v] = fmin(qmin[v], qn[v]);
+      qmax[v] = fmax(qmax[v], qn[v]);
+    }
+  }
+  const Cen cc = ccen[c];
+  const double eps2 = VENKAT ? (venkat_k * cc.h) * (venkat_k * cc.h) * (venkat_k * cc.h) : 0.0;
+  for (int32_t s = s0; s < s1; s++) {
+    const Cen fc = fcen[slots[s].face];
+    const double rx = fc.x - cc.x, ry = fc.y - cc.y, rz = fc.z - cc.z;
+    for (int v = 0; v < 5; v++) {
+      const double d2 = gx[v] * rx + gy[v] * ry + gz[v] * rz;
+      if (d2 == 0.0) continue;
+      const double d1 = (d2 > 0.0 ? qmax[v] : qmin[v]) - qc[v];
+      double psi;
+      if (VENKAT) {
+        const double a = d1 * d1 + eps2;
+        psi = (a + 2.0 * d2 * d1) / (a + 2.0 * d2 * d2 + d1 * d2);
+      } else {
+        psi = fmin(1.0, d1 / d2);
+      }
+      lim[v] = fmin(lim[v], psi);
+    }
+  }
+  for (int v = 0; v < 5; v++) phi[(int64_t)v * C + c] = fmax(0.0, fmin(1.0, lim[v]));
+}
+
+// Centroids for the reconstruction: faces and cells (with h = vol^(1/3)).
+__global__ void k_centroids(int32_t F, int64_t n, const double *__restrict__ xfc,
+                            const double *__restrict__ yfc, const double *__restrict__ zfc,
+                            const double *__restrict__ xcc, const double *__restrict__ ycc,
+                            const double *__restrict__ zcc, const double *__restrict__ vol,
+                            Cen *__restrict__ fcen, Cen *__restrict__ ccen) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < F) fcen[i] = Cen{xfc[i], yfc[i], zfc[i], 0.0};
+  if (i < n) ccen[i] = Cen{xcc[i], ycc[i], zcc[i], cbrt(fabs(vol[i]))};
 }
 
 // LimitTimeStep's ratio clamp (compute_timestep.cpp:929-944), per case.
@@ -1473,6 +1589,12 @@ struct mfg_ctx {
   int32_t *bctype_d = nullptr;  // BC type of each boundary face [G]
   int32_t live_bc = 0;          // ghost states recomputed every iteration
   int32_t flux_fp64 = 0;        // mixed form: the Roe flux wholly in FP64
+  // second-order reconstruction (the reference's `order`: 1 first order, 2
+  // unlimited, 3 Barth-Jespersen, 4 Venkatakrishnan)
+  int32_t order = 1;
+  double venkat_k = 5.0;
+  Cen *fcen = nullptr, *ccen = nullptr;  // face centroids [F], cell centroids + h [n]
+  double *phi = nullptr;                 // limiter [5][C]
   int32_t *fnptr = nullptr, *fnodes = nullptr;
   int32_t *nptr = nullptr, *nsrc = nullptr, *ninfo = nullptr, *bface_c1 = nullptr;
   double *nw = nullptr, *wnode = nullptr, *nsym = nullptr;
@@ -2541,6 +2663,14 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   slots.shrink_to_fit();
   std::vector<double> volv(m->vol, m->vol + n);
   if ((rc = dupload(ctx, &ctx->vol, volv))) return fail(rc);
+  {
+    std::vector<Cen> fc(m->n_face), cc(n);
+    for (int32_t f = 0; f < m->n_face; f++) fc[f] = Cen{m->xfc[f], m->yfc[f], m->zfc[f], 0.0};
+    for (int64_t i = 0; i < n; i++)
+      cc[i] = Cen{m->xcc[i], m->ycc[i], m->zcc[i], std::cbrt(std::fabs(m->vol[i]))};
+    if ((rc = dupload(ctx, &ctx->fcen, fc)) || (rc = dupload(ctx, &ctx->ccen, cc)))
+      return fail(rc);
+  }
   if ((rc = build_levels(ctx, m, cptr, c2f))) return fail(rc);
   if ((rc = build_node_lists(ctx, m))) return fail(rc);
   if ((rc = ctx_finish(ctx, q0, cl))) return fail(rc);
@@ -2929,7 +3059,10 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
                                               ctx->slots, flags);
   k_dev_faces<<<grid_for(F), kBlock, 0, st>>>(F, pp->f2c, pp->xfn, pp->yfn, pp->zfn, pp->area,
                                               ctx->faces);
-  count_launch(2);
+  if ((rc = dalloc(ctx, &ctx->fcen, F)) || (rc = dalloc(ctx, &ctx->ccen, n))) return fail(rc);
+  k_centroids<<<grid_for(std::max<int64_t>(F, n)), kBlock, 0, st>>>(
+      F, n, pp->xfc, pp->yfc, pp->zfc, pp->xcc, pp->ycc, pp->zcc, pp->vol, ctx->fcen, ctx->ccen);
+  count_launch(3);
   // record counts, the record width W and the chunk grid
   DevSweep fw, bw;
   fw.fwd = true;
@@ -3124,6 +3257,22 @@ int mfg_set_flux_fp64(mfg_ctx *ctx, int32_t on) {
   return MFG_OK;
 }
 
+static int launch_gradient(mfg_ctx *ctx);
+
+int mfg_set_order(mfg_ctx *ctx, int32_t order, double venkat_k) {
+  if (!ctx || order < 1 || order > 4 || !(venkat_k > 0.0)) return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  int rc;
+  if (order >= 3 && !ctx->phi && (rc = dalloc(ctx, &ctx->phi, (size_t)5 * ctx->C))) return rc;
+  if (order != ctx->order) drop_graphs(ctx);
+  ctx->order = order;
+  ctx->venkat_k = venkat_k;
+  if (order >= 3)
+    MFG_CUDA(cudaMemsetAsync(ctx->phi, 0, sizeof(double) * 5 * ctx->C, ctx->stream));
+  // the next flux reads the gradient of the current state
+  return order >= 2 ? launch_gradient(ctx) : MFG_OK;
+}
+
 int mfg_set_live_bc(mfg_ctx *ctx, int32_t on) {
   if (!ctx || (on != 0 && on != 1)) return MFG_ERR_INVALID;
   if (ctx->live_bc != on) {
@@ -3183,12 +3332,33 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
   const Cases cs = cases_of(ctx);
   const bool mx = ctx->precision == MFG_PREC_MIXED;
   if (flux) {  // each face's Roe flux once, then gathered per cell
-    if (mx && !ctx->flux_fp64)
-      k_face_flux<true><<<grid_for(ctx->F), kBlock, 0, st>>>(ctx->F, ctx->faces, q, ctx->P, cs,
-                                                              ctx->fflux);
+    const bool recon = ctx->order >= 2;
+    const double *phi = ctx->order >= 3 ? ctx->phi : nullptr;
+    if (ctx->order >= 3) {
+      if (ctx->order == 4)
+        k_limiter<true><<<g, kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots, q,
+                                              ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->fcen,
+                                              ctx->ccen, ctx->venkat_k, ctx->phi);
+      else
+        k_limiter<false><<<g, kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots, q,
+                                               ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->fcen,
+                                               ctx->ccen, ctx->venkat_k, ctx->phi);
+      count_launch();
+    }
+#define MFG_FLUX(MX_, R_)                                                                     \
+  k_face_flux<MX_, R_><<<grid_for(ctx->F), kBlock, 0, st>>>(                                   \
+      ctx->F, ctx->faces, q, ctx->P, cs, ctx->fflux, ctx->C, ctx->n, ctx->fcen, ctx->ccen,     \
+      ctx->dqdx, ctx->dqdy, ctx->dqdz, phi)
+    const bool fmx = mx && !ctx->flux_fp64;
+    if (fmx && recon)
+      MFG_FLUX(true, true);
+    else if (fmx)
+      MFG_FLUX(true, false);
+    else if (recon)
+      MFG_FLUX(false, true);
     else
-      k_face_flux<false><<<grid_for(ctx->F), kBlock, 0, st>>>(ctx->F, ctx->faces, q, ctx->P, cs,
-                                                               ctx->fflux);
+      MFG_FLUX(false, false);
+#undef MFG_FLUX
     count_launch();
   }
 #define MFG_FACE(F_, D_, G_)                                                                  \
@@ -3562,7 +3732,9 @@ static int ensure_graphs(mfg_ctx *ctx) {
     cudaGraph_t g = nullptr;
     MFG_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const long long before = g_launches.load();
-    int rc = launch_iteration(ctx, nullptr, nullptr, GRAD_LEAD);
+    // second order: the flux reads the gradient of the state it starts
+    // from, so each iteration keeps its gradient at its end
+    int rc = launch_iteration(ctx, nullptr, nullptr, ctx->order >= 2 ? GRAD_AT_END : GRAD_LEAD);
     const long long nodes = g_launches.load() - before;
     g_launches.fetch_sub(nodes);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
@@ -3602,8 +3774,9 @@ static int run_iterations(mfg_ctx *ctx, int32_t n_iter, cudaEvent_t after_face =
   if ((rc = ensure_side_stream(ctx))) return rc;
   if (n_graph > 0 && (rc = ensure_graphs(ctx))) return rc;
   ctx->res_zero = true;  // ZeroResiduals at the top of each iteration
+  const bool second = ctx->order >= 2;
   rc = launch_iteration(ctx, n_iter == 1 ? after_face : nullptr,
-                        n_iter == 1 ? after_update : nullptr, GRAD_DEFER);
+                        n_iter == 1 ? after_update : nullptr, second ? GRAD_AT_END : GRAD_DEFER);
   for (int32_t i = 0; rc == MFG_OK && i < n_graph; i++) {
     const cudaError_t e = cudaGraphLaunch(ctx->graph[ctx->cur], st);
     if (e != cudaSuccess) {
@@ -3616,9 +3789,9 @@ static int run_iterations(mfg_ctx *ctx, int32_t n_iter, cudaEvent_t after_face =
   }
   if (rc == MFG_OK && hooks && n_iter > 1) {
     ctx->res_zero = true;
-    rc = launch_iteration(ctx, after_face, after_update, GRAD_LEAD);
+    rc = launch_iteration(ctx, after_face, after_update, second ? GRAD_AT_END : GRAD_LEAD);
   }
-  if (rc == MFG_OK) rc = launch_gradient(ctx);  // of the final state
+  if (rc == MFG_OK && !second) rc = launch_gradient(ctx);  // of the final state
   ctx->res_zero = false;
   return rc;
 }
@@ -3930,6 +4103,11 @@ int mfg_download(mfg_ctx *ctx, int32_t field, double *host) {
       break;
     case MFG_FIELD_DT: src = ctx->dt; count = C; break;
     case MFG_FIELD_DIAG: src = ctx->diag; count = C; break;
+    case MFG_FIELD_LIMITER:
+      if (!ctx->phi) return MFG_ERR_INVALID;
+      src = ctx->phi;
+      count = 5 * C;
+      break;
     case MFG_FIELD_DQDX: src = ctx->dqdx; count = 5 * n; break;
     case MFG_FIELD_DQDY: src = ctx->dqdy; count = 5 * n; break;
     case MFG_FIELD_DQDZ: src = ctx->dqdz; count = 5 * n; break;
@@ -3953,7 +4131,8 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
                                             ctx->q4[ctx->cur ^ 1], n, ctx->P, cases_of(ctx));
   count_launch();
   MFG_CUDA(cudaGetLastError());
-  return MFG_OK;
+  // second order: the next flux reads the gradient of the uploaded state
+  return ctx->order >= 2 ? launch_gradient(ctx) : MFG_OK;
 }
 
 }  // extern "C"

@@ -52,6 +52,12 @@ static_assert(sizeof(SlotRec) == 64, "slot record: one 64-byte line");
 // through the face -> node offsets
 enum : int32_t { SLOT_IS_C2 = 1, SLOT_BOUNDARY = 2, SLOT_NODE_AVG = 4, SLOT_TRI = 8 };
 
+// A centroid (face or cell) and, for a cell, its length scale vol^(1/3)
+// (second-order reconstruction and its limiters).
+struct __align__(16) Cen {
+  double x, y, z, h;
+};
+
 // LU-SGS sweep record: normal oriented out of the swept cell and the
 // multiplier of the flux (0.5*area forward, area backward).
 struct __align__(16) SweepRec {

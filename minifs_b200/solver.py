@@ -108,6 +108,11 @@ class Solver:
         self._call("mfg_set_live_bc", 1 if on else 0)
         self.live_bc = bool(on)
 
+    def set_order(self, order: int, venkat_k: float = 5.0):
+        """The reference's ``order`` switch: 1 first order (default), 2
+        second order unlimited, 3 Barth-Jespersen, 4 Venkatakrishnan."""
+        self._call("mfg_set_order", int(order), float(venkat_k))
+
     def set_flux_fp64(self, on: bool):
         """Mixed form: the Roe flux wholly in FP64 (True) or with its
         dissipation in FP32 (False, the default)."""
@@ -192,7 +197,7 @@ class Solver:
     def download(self, field: str) -> np.ndarray:
         C, n = self.grid.n_cell, self.grid.n
         size = {"q": 5 * n, "res": 5 * C, "dt": C, "dq": 5 * n, "dqdx": 5 * n, "dqdy": 5 * n,
-                "dqdz": 5 * n, "diag": C}[field]
+                "dqdz": 5 * n, "diag": C, "limiter": 5 * C}[field]
         out = np.empty(size)
         self._call("mfg_download", _lib.FIELD[field], _lib.ptr(out))
         return out
@@ -267,7 +272,7 @@ class BatchSolver(Solver):
         """The union array (cells of all cases, then ghosts of all cases)."""
         C, n = self.n_cell, self.n
         size = {"q": 5 * n, "res": 5 * C, "dt": C, "dq": 5 * n, "dqdx": 5 * n, "dqdy": 5 * n,
-                "dqdz": 5 * n, "diag": C}[field]
+                "dqdz": 5 * n, "diag": C, "limiter": 5 * C}[field]
         out = np.empty(size)
         self._call("mfg_download", _lib.FIELD[field], _lib.ptr(out))
         return out
