@@ -284,6 +284,81 @@ int mfg_residual_norm_static(const double *res, int32_t n_cell, double *norms, v
 int mfg_get_dt_extrema(mfg_ctx *ctx, double *dt_max, double *dt_min);
 int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min);
 
+/* ---- one mesh over several contexts (the reference's MPI mode) ---------- */
+/* A context created from one part of a partitioned mesh, whose faces on a
+ * partition cut are boundary faces of type MFG_BC_INTERFACE (their ghost
+ * holds the neighbouring part's cell), iterates as the reference's MPI
+ * build does when the caller moves the exchange buffers between the parts
+ * (NCCL, peer copies, CUDA-aware MPI) between the phases of
+ * mfg_halo_phase.  One iteration, every part in step:
+ *   MFG_HALO_FACE      ZeroResiduals, InviscidFlux, the part's dt and Diag;
+ *                      dt extrema -> ext, squared residual sums -> norm_sq
+ *     caller: ext[0] = max over parts, ext[1] = min over parts
+ *             (compute_timestep.cpp:921-925)
+ *   MFG_HALO_FORWARD   dt limited with ext; forward sweep; DQ* of the sent
+ *                      cells -> send_rows
+ *     caller: each neighbour's send_rows -> recv_rows
+ *             (forward_lusgs.cpp:1030-1053)
+ *   MFG_HALO_BACKWARD  recv_rows -> ghost DQ; backward sweep and update; the
+ *                      new states of the sent cells -> send_rows
+ *     caller: send_rows -> recv_rows (PassInterfaceData, main.cpp:280)
+ *   MFG_HALO_NODES     recv_rows -> ghost states; node values, the shared
+ *                      nodes' left as partial sums -> node_send
+ *     caller: each neighbour's node_send -> node_recv
+ *             (CommInternodeDataMPI, cal_gradient.cpp:2293-2301)
+ *   MFG_HALO_GRADIENT  shared nodes: own + received partial sums, divided by
+ *                      the node weight; Green-Gauss face sums
+ *     caller: norm_sq summed over parts (main.cpp:311-312), sqrt
+ * Before the first iteration: MFG_HALO_PACK_Q (current states of the sent
+ * cells -> send_rows), exchange, then MFG_HALO_NODES and MFG_HALO_GRADIENT
+ * for the gradient of the initial state.  MFG_HALO_CHECK synchronises and
+ * reports a sweep timeout (MFG_ERR_TIMEOUT).  The LU-SGS sweeps of a part
+ * see a neighbour's increment only through the ghost DQ of the backward
+ * sweep, as in the reference, so several parts converge along another
+ * path than one mesh does; one part with no neighbours gives mfg_iterate's
+ * bits.  The node weights, marks and symmetry normals of the part's mesh
+ * must be those of the whole mesh (the reference sums them over parts,
+ * grid_polyhedra_auxiliary_functions.cpp:951-1047).  FP64, first order,
+ * single-case contexts only (MFG_ERR_UNSUPPORTED otherwise); a context with
+ * a halo refuses mfg_iterate, mfg_iterate_host, mfg_forward_lusgs,
+ * mfg_calculate_gradient, mfg_profile_phases and mfg_autotune_sweeps. */
+typedef struct mfg_halo {
+  int32_t n_send;             /* rows sent, all neighbours' segments concatenated */
+  const int32_t *send_cells;  /* host [n_send]: local cell of each sent row */
+  int32_t n_recv;             /* rows received */
+  const int32_t *recv_bfaces; /* host [n_recv]: boundary face (type MFG_BC_INTERFACE)
+                                 whose ghost each received row fills */
+  int32_t n_node;             /* node entries: a shared node once per neighbour
+                                 holding it; sent and received alike */
+  const int32_t *nodes;       /* host [n_node]: local node of each entry; a node's
+                                 received partial sums are added in entry order */
+  double *send_rows;          /* device [n_send][8] (state record: rho,u,v,w,p and
+                                 three derived words; DQ rows use the first 5) */
+  double *recv_rows;          /* device [n_recv][8] */
+  double *node_send;          /* device [n_node][8] (first 5 words used) */
+  double *node_recv;          /* device [n_node][8] */
+  int64_t *ext;               /* device [2]: dt_max, dt_min as the bits of positive
+                                 doubles (their order is that of the int64 values) */
+  double *norm_sq;            /* device [5]: the part's sums of squared residuals */
+} mfg_halo;
+#define MFG_HALO_PACK_Q 0
+#define MFG_HALO_FACE 1
+#define MFG_HALO_FORWARD 2
+#define MFG_HALO_BACKWARD 3
+#define MFG_HALO_NODES 4
+#define MFG_HALO_GRADIENT 5
+#define MFG_HALO_CHECK 6
+/* Registers the exchange lists (copied) and the caller's device buffers
+ * (kept; on the context's device, alive while the context is), once per
+ * context.  MFG_ERR_INVALID for an index out of range or a received row
+ * whose boundary face is not of type MFG_BC_INTERFACE. */
+int mfg_halo_set(mfg_ctx *ctx, const mfg_halo *halo);
+/* Launches one phase on the context's stream (mfg_set_stream shares it
+ * with the communication library); iter_done sets the CFL of
+ * MFG_HALO_FACE as in mfg_compute_timestep.  Asynchronous except
+ * MFG_HALO_CHECK. */
+int mfg_halo_phase(mfg_ctx *ctx, int32_t phase, int32_t iter_done);
+
 /* ---- data movement ----------------------------------------------------- */
 int mfg_download(mfg_ctx *ctx, int32_t field, double *host);
 int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host);

@@ -83,6 +83,19 @@ class Mfl(ct.Structure):
                 ("n_inode", ct.c_int32), ("nbsn", i32p), ("nbzn", i32p), ("nbrn", i32p)]
 
 
+class Halo(ct.Structure):
+    _fields_ = [("n_send", ct.c_int32), ("send_cells", i32p), ("n_recv", ct.c_int32),
+                ("recv_bfaces", i32p), ("n_node", ct.c_int32), ("nodes", i32p),
+                ("send_rows", ct.c_void_p), ("recv_rows", ct.c_void_p),
+                ("node_send", ct.c_void_p), ("node_recv", ct.c_void_p),
+                ("ext", ct.c_void_p), ("norm_sq", ct.c_void_p)]
+
+
+# mfg_halo_phase phases
+HALO = {"pack_q": 0, "face": 1, "forward": 2, "backward": 3, "nodes": 4, "gradient": 5,
+        "check": 6}
+
+
 class MfgError(RuntimeError):
     def __init__(self, func: str, code: int, detail: str = ""):
         msg = f"{func} failed: {ERRORS.get(code, code)}"
@@ -143,6 +156,8 @@ def load(build_if_missing: bool = True):
                                                 ct.c_void_p]),
         "mfg_get_dt_extrema": (ct.c_int, [ctxp, f64p, f64p]),
         "mfg_set_dt_extrema": (ct.c_int, [ctxp, ct.c_double, ct.c_double]),
+        "mfg_halo_set": (ct.c_int, [ctxp, ct.POINTER(Halo)]),
+        "mfg_halo_phase": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32]),
         "mfg_download": (ct.c_int, [ctxp, ct.c_int32, f64p]),
         "mfg_upload": (ct.c_int, [ctxp, ct.c_int32, f64p]),
         "mfg_sync": (ct.c_int, [ctxp]),

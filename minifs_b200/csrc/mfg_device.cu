@@ -1201,6 +1201,23 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
   }
 }
 
+// A node's weighted sums divided by its weight (cal_gradient.cpp:2314-2324),
+// then the symmetry-plane projection of the velocity (:2330-2350).
+__device__ __forceinline__ void node_finish(int32_t nd, int32_t info,
+                                            const double *__restrict__ wnode,
+                                            const double *__restrict__ nsym, double acc[5]) {
+  const double den = wnode[nd] + kTiny;
+  for (int v = 0; v < 5; v++) acc[v] /= den;
+  if (info & 2) {
+    const double xs = nsym[3 * nd], ys = nsym[3 * nd + 1], zs = nsym[3 * nd + 2];
+    const double un = acc[1], vn_ = acc[2], wn = acc[3];
+    const double vn = un * xs + vn_ * ys + wn * zs;
+    acc[1] = un - vn * xs;
+    acc[2] = vn_ - vn * ys;
+    acc[3] = wn - vn * zs;
+  }
+}
+
 // Node values of all five variables (CompNodeVar3D_dist, cal_gradient.cpp
 // :1922-2372): boundary-marked nodes average their boundary-face states,
 // the others their cells, each in the reference's accumulation order; then
@@ -1237,16 +1254,9 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
       for (int v = 0; v < 5; v++) acc[v] += qa[v] * w;
     }
   }
-  const double den = wnode[nd] + kTiny;
-  for (int v = 0; v < 5; v++) acc[v] /= den;
-  if (info & 2) {
-    const double xs = nsym[3 * nd], ys = nsym[3 * nd + 1], zs = nsym[3 * nd + 2];
-    const double un = acc[1], vn_ = acc[2], wn = acc[3];
-    const double vn = un * xs + vn_ * ys + wn * zs;
-    acc[1] = un - vn * xs;
-    acc[2] = vn_ - vn * ys;
-    acc[3] = wn - vn * zs;
-  }
+  // a node shared with other parts of a partitioned mesh keeps its partial
+  // sum until theirs are added (k_halo_nodes)
+  if (!(info & 4)) node_finish(nd, info, wnode, nsym, acc);
   double *o = qn8 + (int64_t)nd * Q_STRIDE;
   reinterpret_cast<double2 *>(o)[0] = make_double2(acc[0], acc[1]);
   reinterpret_cast<double2 *>(o)[1] = make_double2(acc[2], acc[3]);
@@ -1523,6 +1533,74 @@ __global__ void k_norm_seg_final(int32_t nparts, const double *__restrict__ part
 
 __global__ void k_counter_inc(int32_t *__restrict__ counter) { *counter += 1; }
 
+// ---- one part of a partitioned mesh (the reference's MPI mode) ------------
+
+// The partials of k_norm_final, summed in its order, left squared: a part's
+// share of main.cpp:311-312's MPI_Reduce.
+__global__ void k_norm_sums(int32_t nparts, const double *__restrict__ part,
+                            double *__restrict__ out) {
+  __shared__ double sh[5][32];
+  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+  if (k < 5) {
+    double acc = 0.0;
+    for (int32_t b = lane; b < nparts; b += 32) acc += part[(int64_t)b * 5 + k];
+    sh[k][lane] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double acc = 0.0;
+    for (int l = 0; l < 32; l++) acc += sh[threadIdx.x][l];
+    out[threadIdx.x] = acc;
+  }
+}
+
+// Rows (Q_STRIDE doubles) of the listed records into a packed buffer [n][8];
+// words from `width` on are written as 0.  One thread per word.
+__global__ void k_halo_gather(int32_t n, int32_t width, const int32_t *__restrict__ idx,
+                              const double *__restrict__ src, double *__restrict__ dst) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * Q_STRIDE) return;
+  const int32_t i = (int32_t)(t / Q_STRIDE), k = (int32_t)(t % Q_STRIDE);
+  dst[t] = k < width ? src[(int64_t)idx[i] * Q_STRIDE + k] : 0.0;
+}
+
+// A packed buffer [n][8] into the listed rows of one or two arrays (words
+// below `width`).
+__global__ void k_halo_scatter(int32_t n, int32_t width, const int32_t *__restrict__ rows,
+                               const double *__restrict__ src, double *__restrict__ a,
+                               double *__restrict__ b) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * Q_STRIDE) return;
+  const int32_t i = (int32_t)(t / Q_STRIDE), k = (int32_t)(t % Q_STRIDE);
+  if (k >= width) return;
+  const int64_t o = (int64_t)rows[i] * Q_STRIDE + k;
+  const double v = src[t];
+  a[o] = v;
+  if (b) b[o] = v;
+}
+
+// Shared nodes: the local partial sums plus each neighbour's (in entry
+// order, RecvSendVarNeighbor_Node, parallel_mpi.cpp:1997-2004), then the
+// division and projection of every node (cal_gradient.cpp:2314-2350).
+__global__ void k_halo_nodes(int32_t nu, const int32_t *__restrict__ unodes,
+                             const int32_t *__restrict__ eptr, const int32_t *__restrict__ eidx,
+                             const double *__restrict__ recv, const int32_t *__restrict__ ninfo,
+                             const double *__restrict__ wnode, const double *__restrict__ nsym,
+                             double *__restrict__ qn8) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nu) return;
+  const int32_t nd = unodes[i];
+  double *o = qn8 + (int64_t)nd * Q_STRIDE;
+  double acc[5];
+  for (int v = 0; v < 5; v++) acc[v] = o[v];
+  for (int32_t e = eptr[i]; e < eptr[i + 1]; e++) {
+    const double *r = recv + (int64_t)eidx[e] * Q_STRIDE;
+    for (int v = 0; v < 5; v++) acc[v] += r[v];
+  }
+  node_finish(nd, ninfo[nd], wnode, nsym, acc);
+  for (int v = 0; v < 5; v++) o[v] = acc[v];
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1633,6 +1711,15 @@ struct mfg_ctx {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int64_t graph_nodes = 0;
   int max_level_cells = 0;
+  // one part of a partitioned mesh (mfg_halo_set): the caller's exchange
+  // buffers and the device copies of the exchange lists
+  bool halo = false;
+  mfg_halo hb{};
+  int32_t *h_send = nullptr;            // local cell of each sent row
+  int32_t *h_recv = nullptr;            // ghost record (C + boundary face) of each received row
+  int32_t *h_nodes = nullptr;           // local node of each node entry
+  int32_t *h_unodes = nullptr, *h_eptr = nullptr, *h_eidx = nullptr;  // entries per shared node
+  int32_t h_nu = 0;
 };
 
 namespace {
@@ -3261,6 +3348,7 @@ static int launch_gradient(mfg_ctx *ctx);
 
 int mfg_set_order(mfg_ctx *ctx, int32_t order, double venkat_k) {
   if (!ctx || order < 1 || order > 4 || !(venkat_k > 0.0)) return MFG_ERR_INVALID;
+  if (ctx->halo && order != 1) return MFG_ERR_UNSUPPORTED;  // first order across parts
   MFG_CUDA(cudaSetDevice(ctx->device));
   int rc;
   if (order >= 3 && !ctx->phi && (rc = dalloc(ctx, &ctx->phi, (size_t)5 * ctx->C))) return rc;
@@ -3494,36 +3582,48 @@ static int check_sweep_error(mfg_ctx *ctx) {
   return MFG_ERR_TIMEOUT;
 }
 
-static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
-  if (ctx->sweep_mode == 1) {
-    int rc = launch_fwd_persist(ctx, clamp_check, 0, kSpinCycles);
-    if (rc) return rc;
-    return launch_bwd_persist(ctx, kSpinCycles);
-  }
+// One LU-SGS sweep: forward (DQ* into dqf) or backward (DQ into dq8 and the
+// updated state into the other state buffer).
+static int launch_sweep(mfg_ctx *ctx, bool fwd, bool clamp_check) {
+  if (ctx->sweep_mode == 1)
+    return fwd ? launch_fwd_persist(ctx, clamp_check, 0, kSpinCycles)
+               : launch_bwd_persist(ctx, kSpinCycles);
   if (ctx->precision == MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
   cudaStream_t st = ctx->stream;
   const double *q = ctx->q8[ctx->cur];
   double *qn = ctx->q8[ctx->cur ^ 1];
-  const int Lf = (int)ctx->fw_lptr.size() - 1, Lb = (int)ctx->bw_lptr.size() - 1;
-  for (int l = 0; l < Lf; l++) {
-    const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
-    k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
-        a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
-        ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt,
-        ctx->dt_ext, ctx->cptr, ctx->slots, ctx->vol, cases_of(ctx));
+  if (fwd) {
+    const int Lf = (int)ctx->fw_lptr.size() - 1;
+    for (int l = 0; l < Lf; l++) {
+      const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
+      k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
+          a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
+          ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt,
+          ctx->dt_ext, ctx->cptr, ctx->slots, ctx->vol, cases_of(ctx));
+    }
+    count_launch(Lf);
+  } else {
+    const int Lb = (int)ctx->bw_lptr.size() - 1;
+    for (int l = 0; l < Lb; l++) {
+      const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
+      k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
+                                                      ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dqf,
+                                                      ctx->dq8, ctx->diag, ctx->P, cases_of(ctx));
+    }
+    count_launch(Lb);
   }
-  for (int l = 0; l < Lb; l++) {
-    const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
-    k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
-                                                    ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dqf,
-                                                    ctx->dq8, ctx->diag, ctx->P, cases_of(ctx));
-  }
-  count_launch(Lf + Lb);
   return check_kernel();
+}
+
+static int launch_sweeps(mfg_ctx *ctx, bool clamp_check) {
+  const int rc = launch_sweep(ctx, true, clamp_check);
+  if (rc) return rc;
+  return launch_sweep(ctx, false, clamp_check);
 }
 
 int mfg_forward_lusgs(mfg_ctx *ctx) {
   if (!ctx) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
   MFG_CUDA(cudaSetDevice(ctx->device));
   int rc = launch_face(ctx, false, false, true, 0.0, false);
   if (rc) return rc;
@@ -3595,6 +3695,7 @@ static int launch_gradient(mfg_ctx *ctx) {
 
 int mfg_calculate_gradient(mfg_ctx *ctx) {
   if (!ctx) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
   MFG_CUDA(cudaSetDevice(ctx->device));
   return launch_gradient(ctx);
 }
@@ -3798,6 +3899,7 @@ static int run_iterations(mfg_ctx *ctx, int32_t n_iter, cudaEvent_t after_face =
 
 int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) {
   if (!ctx || n_iter < 0) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
   if (n_iter == 0) return MFG_OK;
   MFG_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
@@ -3818,6 +3920,7 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
 
 int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double *ms_out) {
   if (!ctx || n_trial <= 0) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
   if (ctx->sweep_mode != 1 || !ctx->sweep_w) return MFG_ERR_UNSUPPORTED;
   MFG_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
@@ -3892,6 +3995,7 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
 
 int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *phase_ms) {
   if (!ctx || n_iter <= 0 || !phase_ms) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
   MFG_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   {
@@ -3964,6 +4068,7 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
 int mfg_iterate_host(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, const double *q_in,
                      double *q_out, double *res_out, double *norms) {
   if (!ctx || n_iter < 0) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
   int rc;
   if (q_in && (rc = mfg_upload(ctx, MFG_FIELD_Q, q_in))) return rc;
   if (n_iter == 0 || (!q_out && !res_out)) {
@@ -4133,6 +4238,150 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
   MFG_CUDA(cudaGetLastError());
   // second order: the next flux reads the gradient of the uploaded state
   return ctx->order >= 2 ? launch_gradient(ctx) : MFG_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// one part of a partitioned mesh: the reference's MPI mode in phases, the
+// exchanges between them left to the caller
+// ---------------------------------------------------------------------------
+
+int mfg_halo_set(mfg_ctx *ctx, const mfg_halo *h) {
+  if (!ctx || !h) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_INVALID;  // once per context
+  if (ctx->ncase != 1 || ctx->precision != MFG_PREC_FP64 || ctx->order != 1)
+    return MFG_ERR_UNSUPPORTED;
+  if (h->n_send < 0 || h->n_recv < 0 || h->n_node < 0 || !h->ext || !h->norm_sq)
+    return MFG_ERR_INVALID;
+  if ((h->n_send && (!h->send_cells || !h->send_rows)) ||
+      (h->n_recv && (!h->recv_bfaces || !h->recv_rows)) ||
+      (h->n_node && (!h->nodes || !h->node_send || !h->node_recv)))
+    return MFG_ERR_INVALID;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  for (int32_t i = 0; i < h->n_send; i++)
+    if (h->send_cells[i] < 0 || h->send_cells[i] >= ctx->C) return MFG_ERR_INVALID;
+  for (int32_t i = 0; i < h->n_node; i++)
+    if (h->nodes[i] < 0 || h->nodes[i] >= ctx->N) return MFG_ERR_INVALID;
+  std::vector<int32_t> bct(std::max(ctx->G, 1));
+  if (ctx->G)
+    MFG_CUDA(cudaMemcpy(bct.data(), ctx->bctype_d, sizeof(int32_t) * ctx->G,
+                        cudaMemcpyDeviceToHost));
+  std::vector<int32_t> recv(h->n_recv);
+  for (int32_t i = 0; i < h->n_recv; i++) {
+    const int32_t k = h->recv_bfaces[i];
+    if (k < 0 || k >= ctx->G || bct[k] != MFG_BC_INTERFACE) return MFG_ERR_INVALID;
+    recv[i] = ctx->C + k;
+  }
+  // the entries of each shared node, in entry order
+  std::vector<int32_t> order(h->n_node);
+  for (int32_t i = 0; i < h->n_node; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t a, int32_t b) { return h->nodes[a] < h->nodes[b]; });
+  std::vector<int32_t> unodes, eptr(1, 0), eidx;
+  for (int32_t j = 0; j < h->n_node; j++) {
+    const int32_t e = order[j];
+    if (unodes.empty() || unodes.back() != h->nodes[e]) {
+      if (!unodes.empty()) eptr.push_back((int32_t)eidx.size());
+      unodes.push_back(h->nodes[e]);
+    }
+    eidx.push_back(e);
+  }
+  if (!unodes.empty()) eptr.push_back((int32_t)eidx.size());
+  int rc;
+  std::vector<int32_t> send(h->send_cells, h->send_cells + h->n_send),
+      nodes(h->nodes, h->nodes + h->n_node);
+  if ((rc = dupload(ctx, &ctx->h_send, send))) return rc;
+  if ((rc = dupload(ctx, &ctx->h_recv, recv))) return rc;
+  if ((rc = dupload(ctx, &ctx->h_nodes, nodes))) return rc;
+  if ((rc = dupload(ctx, &ctx->h_unodes, unodes))) return rc;
+  if ((rc = dupload(ctx, &ctx->h_eptr, eptr))) return rc;
+  if ((rc = dupload(ctx, &ctx->h_eidx, eidx))) return rc;
+  // shared nodes keep their partial sums in k_node_values (info bit 4)
+  std::vector<int32_t> info(ctx->N);
+  MFG_CUDA(cudaMemcpy(info.data(), ctx->ninfo, sizeof(int32_t) * ctx->N, cudaMemcpyDeviceToHost));
+  for (int32_t nd : unodes) info[nd] |= 4;
+  MFG_CUDA(cudaMemcpy(ctx->ninfo, info.data(), sizeof(int32_t) * ctx->N, cudaMemcpyHostToDevice));
+  ctx->h_nu = (int32_t)unodes.size();
+  ctx->hb = *h;
+  ctx->hb.send_cells = ctx->hb.recv_bfaces = ctx->hb.nodes = nullptr;  // not kept
+  ctx->halo = true;
+  drop_graphs(ctx);
+  return MFG_OK;
+}
+
+static void halo_gather(mfg_ctx *ctx, int32_t n, int32_t width, const int32_t *idx,
+                        const double *src, double *dst) {
+  if (n == 0) return;
+  k_halo_gather<<<grid_for((int64_t)n * Q_STRIDE), kBlock, 0, ctx->stream>>>(n, width, idx, src,
+                                                                             dst);
+  count_launch();
+}
+
+static void halo_scatter(mfg_ctx *ctx, int32_t n, int32_t width, const double *src, double *a,
+                         double *b) {
+  if (n == 0) return;
+  k_halo_scatter<<<grid_for((int64_t)n * Q_STRIDE), kBlock, 0, ctx->stream>>>(
+      n, width, ctx->h_recv, src, a, b);
+  count_launch();
+}
+
+int mfg_halo_phase(mfg_ctx *ctx, int32_t phase, int32_t iter_done) {
+  if (!ctx) return MFG_ERR_INVALID;
+  if (!ctx->halo) return MFG_ERR_UNSUPPORTED;
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const mfg_halo &h = ctx->hb;
+  int rc = MFG_OK;
+  switch (phase) {
+    case MFG_HALO_PACK_Q:
+      halo_gather(ctx, h.n_send, Q_STRIDE, ctx->h_send, ctx->q8[ctx->cur], h.send_rows);
+      break;
+    case MFG_HALO_FACE: {
+      ctx->res_zero = true;
+      rc = launch_face(ctx, true, true, true, cfl_for(ctx->hp, iter_done), false);
+      if (rc) return rc;
+      k_norm_sums<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, h.norm_sq);
+      count_launch();
+      MFG_CUDA(cudaMemcpyAsync(h.ext, ctx->dt_ext, 2 * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                               st));
+      break;
+    }
+    case MFG_HALO_FORWARD:
+      MFG_CUDA(cudaMemcpyAsync(ctx->dt_ext, h.ext, 2 * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                               st));
+      rc = launch_sweep(ctx, true, true);
+      if (rc) return rc;
+      halo_gather(ctx, h.n_send, 5, ctx->h_send, ctx->dqf, h.send_rows);
+      break;
+    case MFG_HALO_BACKWARD:
+      halo_scatter(ctx, h.n_recv, 5, h.recv_rows, ctx->dq8, nullptr);
+      rc = launch_sweep(ctx, false, false);
+      if (rc) return rc;
+      ctx->cur ^= 1;
+      if (ctx->live_bc && (rc = launch_ghost_bc(ctx, st))) return rc;
+      halo_gather(ctx, h.n_send, Q_STRIDE, ctx->h_send, ctx->q8[ctx->cur], h.send_rows);
+      break;
+    case MFG_HALO_NODES:
+      halo_scatter(ctx, h.n_recv, Q_STRIDE, h.recv_rows, ctx->q8[0], ctx->q8[1]);
+      launch_node_values(ctx, st);
+      halo_gather(ctx, h.n_node, 5, ctx->h_nodes, ctx->qn8, h.node_send);
+      break;
+    case MFG_HALO_GRADIENT:
+      if (ctx->h_nu) {
+        k_halo_nodes<<<grid_for(ctx->h_nu), kBlock, 0, st>>>(
+            ctx->h_nu, ctx->h_unodes, ctx->h_eptr, ctx->h_eidx, h.node_recv, ctx->ninfo,
+            ctx->wnode, ctx->nsym, ctx->qn8);
+        count_launch();
+      }
+      launch_grad_faces(ctx, st);
+      break;
+    case MFG_HALO_CHECK:
+      MFG_CUDA(cudaStreamSynchronize(st));
+      return check_sweep_error(ctx);
+    default:
+      return MFG_ERR_INVALID;
+  }
+  return check_kernel();
 }
 
 }  // extern "C"

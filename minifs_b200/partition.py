@@ -1,0 +1,492 @@
+"""One mesh split into parts, each iterated by its own context (one per GPU):
+the counterpart of the reference's MPI mode (src/Base/parallel_mpi.cpp,
+PassInterfaceData in src/Kernels/load_grid.cpp:912-942) for the iteration
+path.
+
+Each part is an ordinary FlowStar mesh of its cells.  A face between two
+parts becomes, in each of them, a boundary face of type INTERFACE (10) whose
+ghost holds the other part's cell -- the reference's own representation of a
+partition cut (its ghost update skips the type, load_grid.cpp:1030-1031; the
+gradient takes node means there, cal_gradient.cpp:1749) -- and the part
+carries the FlowStar interface block that names, for every such face and
+every node shared with another part, the zone and the index on the other
+side (the block ``flowstar.write_grid`` stores).
+
+``split`` makes the parts, ``halo_lists`` turns one part's interface block
+into the exchange lists of ``mfg_halo_set``, ``prepare_parts`` runs the
+preprocessing per part with the node data of the whole mesh, and
+``Decomposed`` iterates the parts in step through ``mfg_halo_phase`` with
+the exchanges in between, either all parts in this process (``LocalExchange``,
+device copies) or one part per rank (``DistExchange``, torch.distributed:
+NCCL on GPUs).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .flowstar import Interfaces
+from .meshgen import INTERFACE, RawMesh
+
+
+@dataclass
+class Part:
+    mesh: RawMesh            # the part as a FlowStar mesh (its patches plus the interface patch)
+    interfaces: Interfaces   # FlowStar interface block, zones numbered from 0
+    rank: int                # zone of this part
+    cells: np.ndarray        # whole-mesh cell of each local cell (ascending)
+    nodes: np.ndarray        # whole-mesh node of each local node (ascending)
+    bfaces: np.ndarray       # whole-mesh boundary face of each of the part's own boundary faces
+    iface_cells: np.ndarray  # whole-mesh cell on the other side of each interface face
+    n_own_bface: int = 0     # boundary faces before the interface faces
+
+    @property
+    def iface_bfaces(self) -> np.ndarray:
+        """Local boundary-face index of each interface face."""
+        return np.arange(self.n_own_bface, self.mesh.n_bface, dtype=np.int32)
+
+
+def slab_parts(n_cell: int, world: int) -> np.ndarray:
+    """Part of every cell: `world` contiguous, balanced ranges of the cell
+    numbering (slabs of hex layers on the generated block meshes)."""
+    if world < 1:
+        raise ValueError("at least one part")
+    return (np.arange(n_cell, dtype=np.int64) * world // max(n_cell, 1)).astype(np.int32)
+
+
+def split(mesh: RawMesh, part_of, world: int) -> list[Part]:
+    """The parts of `mesh` for the cell -> part map `part_of` (values in
+    [0, world)).
+
+    Local cells and nodes keep the whole mesh's order.  Faces of a part: its
+    own boundary faces, then its interface faces, then its interior faces,
+    each group in the whole mesh's order.  An interface face whose inner cell
+    is the face's second cell is turned round as the reference's reader turns
+    a face with a boundary on its left (load_grid.cpp:214-221): first node
+    kept, the others reversed, so that its normal points out of the part.
+    """
+    part_of = np.asarray(part_of, np.int32)
+    if part_of.shape != (mesh.n_cell,):
+        raise ValueError("part_of needs one entry per cell")
+    if world < 1 or part_of.min(initial=0) < 0 or part_of.max(initial=0) >= world:
+        raise ValueError("part numbers must lie in [0, world)")
+    f2c = np.asarray(mesh.f2c, np.int64).reshape(-1, 2)
+    nnpf = np.asarray(mesh.nnpf, np.int64)
+    fptr = np.concatenate([[0], np.cumsum(nnpf)])
+    f2n = np.asarray(mesh.f2n, np.int64)
+    F, G = mesh.n_face, mesh.n_bface
+    iface_patch = max([pid for pid, _ in mesh.patches] + [0]) + 1
+    c1, c2 = f2c[:, 0], f2c[:, 1]
+    p1 = part_of[c1]
+    p2 = np.where(c2 >= 0, part_of[np.maximum(c2, 0)], -1)
+    fidx = np.arange(F)
+    interior = fidx >= G
+    cut = interior & (p1 != p2)
+    # each part's own boundary faces, cut faces and interior faces
+    sides = []
+    for p in range(world):
+        own_b = fidx[(~interior) & (p1 == p)]
+        cut_p = fidx[cut & ((p1 == p) | (p2 == p))]
+        inner = fidx[interior & (p1 == p) & (p2 == p)]
+        sides.append((own_b, cut_p, inner))
+    # local boundary-face index of each cut face in each of its two parts
+    cut_local = {}
+    for p, (own_b, cut_p, _) in enumerate(sides):
+        for k, f in enumerate(cut_p.tolist()):
+            cut_local[(p, f)] = own_b.size + k
+    parts = []
+    for p, (own_b, cut_p, inner) in enumerate(sides):
+        cells = np.nonzero(part_of == p)[0]
+        local = np.full(mesh.n_cell, -1, np.int64)
+        local[cells] = np.arange(cells.size)
+        faces = np.concatenate([own_b, cut_p, inner])
+        lf2c = np.empty((faces.size, 2), np.int64)
+        nodes_of = []
+        nbz, nbf, ocell = [], [], []
+        for i, f in enumerate(faces.tolist()):
+            nd = f2n[fptr[f]:fptr[f + 1]]
+            a, b = int(c1[f]), int(c2[f])
+            if f < G:
+                lf2c[i] = (local[a], b)
+            elif p1[f] == p and p2[f] == p:
+                lf2c[i] = (local[a], local[b])
+            else:
+                other = int(p2[f]) if p1[f] == p else int(p1[f])
+                if p1[f] != p:  # inner cell on the right: turned round
+                    nd = np.concatenate([nd[:1], nd[1:][::-1]])
+                    a, b = b, a
+                lf2c[i] = (local[a], -iface_patch)
+                nbz.append(other)
+                nbf.append(cut_local[(other, f)])
+                ocell.append(b)
+            nodes_of.append(nd)
+        allnodes = np.concatenate(nodes_of) if nodes_of else np.zeros(0, np.int64)
+        used = np.unique(allnodes)
+        nmap = np.full(mesh.n_node, -1, np.int64)
+        nmap[used] = np.arange(used.size)
+        raw = RawMesh(x=np.ascontiguousarray(mesh.x[used], np.float64),
+                      y=np.ascontiguousarray(mesh.y[used], np.float64),
+                      z=np.ascontiguousarray(mesh.z[used], np.float64),
+                      nnpf=np.array([v.size for v in nodes_of], np.int32),
+                      f2n=nmap[allnodes].astype(np.int32),
+                      f2c=lf2c.reshape(-1).astype(np.int32),
+                      n_cell=int(cells.size), n_bface=int(own_b.size + cut_p.size),
+                      patches=list(mesh.patches) + [(iface_patch, INTERFACE)])
+        parts.append(Part(mesh=raw, interfaces=Interfaces(nbz=np.array(nbz, np.int32),
+                                                          nbf=np.array(nbf, np.int32)),
+                          rank=p, cells=cells.astype(np.int32), nodes=used.astype(np.int32),
+                          bfaces=own_b.astype(np.int32), iface_cells=np.array(ocell, np.int32),
+                          n_own_bface=int(own_b.size)))
+    # the node half of the interface block: every node shared with another
+    # part, once per such part, with its index there
+    holders = {}
+    for pt in parts:
+        for i, g in enumerate(pt.nodes.tolist()):
+            holders.setdefault(g, []).append((pt.rank, i))
+    sn = [[] for _ in range(world)]
+    for g, hs in holders.items():
+        if len(hs) < 2:
+            continue
+        for p, i in hs:
+            for r, j in hs:
+                if r != p:
+                    sn[p].append((r, i, j))
+    for pt in parts:
+        e = sorted(sn[pt.rank])
+        pt.interfaces.nbsn = np.array([i for _, i, _ in e], np.int32)
+        pt.interfaces.nbzn = np.array([r for r, _, _ in e], np.int32)
+        pt.interfaces.nbrn = np.array([j for _, _, j in e], np.int32)
+    return parts
+
+
+@dataclass
+class HaloLists:
+    """Exchange lists of one part (the arguments of mfg_halo_set), one
+    segment per neighbour, neighbours ascending.  Within the segments shared
+    by zones p < r, faces and nodes are ordered by their index in p, so that
+    the rows p sends are the rows r expects and the reverse."""
+    rank: int
+    neighbors: list = field(default_factory=list)
+    send_cells: np.ndarray = None   # local cell of each sent row
+    recv_bfaces: np.ndarray = None  # local interface face whose ghost each received row fills
+    nodes: np.ndarray = None        # local node of each node entry
+    row_ptr: np.ndarray = None      # segment bounds of the rows (sent and received alike)
+    node_ptr: np.ndarray = None     # segment bounds of the node entries
+
+
+def halo_lists(mesh: RawMesh, interfaces: Interfaces, rank: int) -> HaloLists:
+    """The exchange lists of zone `rank` from its own mesh and interface
+    block alone (what one process reading its own grid file has)."""
+    itf = interfaces
+    G = mesh.n_bface
+    f2c = np.asarray(mesh.f2c, np.int64).reshape(-1, 2)
+    nif = len(itf.nbz)
+    ib = np.arange(G - nif, G, dtype=np.int64)  # interface faces close the boundary block
+    if nif and np.any(f2c[ib, 1] >= 0):
+        raise ValueError("interface faces must be the last boundary faces")
+    nbz, nbf = np.asarray(itf.nbz, np.int64), np.asarray(itf.nbf, np.int64)
+    nbzn = np.asarray(itf.nbzn, np.int64)
+    nbsn, nbrn = np.asarray(itf.nbsn, np.int64), np.asarray(itf.nbrn, np.int64)
+    neighbors = sorted(set(nbz.tolist()) | set(nbzn.tolist()))
+    send, recv, nodes, row_ptr, node_ptr = [], [], [], [0], [0]
+    for r in neighbors:
+        sel = np.nonzero(nbz == r)[0]
+        key = ib[sel] if rank < r else nbf[sel]
+        sel = sel[np.argsort(key, kind="stable")]
+        recv.append(ib[sel])
+        send.append(f2c[ib[sel], 0])
+        row_ptr.append(row_ptr[-1] + sel.size)
+        seln = np.nonzero(nbzn == r)[0]
+        keyn = nbsn[seln] if rank < r else nbrn[seln]
+        seln = seln[np.argsort(keyn, kind="stable")]
+        nodes.append(nbsn[seln])
+        node_ptr.append(node_ptr[-1] + seln.size)
+
+    def cat(v):
+        return np.concatenate(v).astype(np.int32) if v else np.zeros(0, np.int32)
+
+    return HaloLists(rank=rank, neighbors=neighbors, send_cells=cat(send), recv_bfaces=cat(recv),
+                     nodes=cat(nodes), row_ptr=np.array(row_ptr, np.int64),
+                     node_ptr=np.array(node_ptr, np.int64))
+
+
+def prepare_parts(mesh: RawMesh, params, parts: list[Part], bump_amp: float = 0.05,
+                  bump_sigma: float = 0.1, bump_center=(0.5, 0.5, 0.5)):
+    """Preprocessing of every part (``grid.prepare``) with the node data of
+    the whole mesh: node weights, marks and symmetry normals are sums and
+    minima over the parts in the reference (CommInternodeDataMPI /
+    CommInternodeDataMPI2, grid_polyhedra_auxiliary_functions.cpp:951-1047,
+    :2114-2119), here taken from the whole mesh's preprocessing; the
+    initial state is the whole mesh's, each interface ghost holding the
+    neighbouring cell (PassInterfaceData after AllocAndInitFlowfield,
+    load_grid.cpp:505-507).  Returns (whole-mesh grid, part grids)."""
+    from . import grid as gr
+    kw = dict(bump_amp=bump_amp, bump_sigma=bump_sigma, bump_center=bump_center)
+    whole = gr.prepare(mesh, params, **kw)
+    C = whole.n_cell
+    q = whole.q0.reshape(5, whole.n)
+    out = []
+    for pt in parts:
+        pg = gr.prepare(pt.mesh, params, **kw)
+        for k in ("wnode", "nmark", "nodesymm", "xfn_n_symm", "yfn_n_symm", "zfn_n_symm"):
+            pg.arrays[k] = np.ascontiguousarray(whole.arrays[k][pt.nodes])
+        rows = np.concatenate([pt.cells, C + pt.bfaces.astype(np.int64), pt.iface_cells])
+        pg.q0 = np.ascontiguousarray(q[:, rows].reshape(-1))
+        out.append(pg)
+    return whole, out
+
+
+def assemble(parts: list[Part], values: list[np.ndarray], n_cell: int, width: int = 5):
+    """Whole-mesh cell array [width][n_cell] from per-part arrays laid out
+    [width][n_local] (n_local = the part's cells, or cells + ghosts)."""
+    out = np.zeros((width, n_cell))
+    for pt, v in zip(parts, values):
+        v = np.asarray(v).reshape(width, -1)
+        out[:, pt.cells] = v[:, :pt.cells.size]
+    return out
+
+
+# ---- iteration -------------------------------------------------------------
+
+class HaloBuffers:
+    """The exchange buffers of one part (torch tensors on `device`): rows of
+    8 doubles for cells and node entries, the dt extrema and the residual
+    sums, laid out as ``mfg_halo`` describes."""
+
+    def __init__(self, lists: HaloLists, device):
+        import torch
+        self.lists = lists
+        self.device = torch.device(device)
+        ns, nr, nn = lists.send_cells.size, lists.recv_bfaces.size, lists.nodes.size
+
+        def buf(n):
+            return torch.zeros((max(n, 1), 8), dtype=torch.float64, device=self.device)
+
+        self.send_rows, self.recv_rows = buf(ns), buf(nr)
+        self.node_send, self.node_recv = buf(nn), buf(nn)
+        self.ext = torch.zeros(2, dtype=torch.int64, device=self.device)
+        self.norm_sq = torch.zeros(5, dtype=torch.float64, device=self.device)
+
+    def seg(self, which: str, k: int):
+        """Rows of segment k (the k-th neighbour) of a buffer."""
+        ptr = self.lists.node_ptr if which.startswith("node") else self.lists.row_ptr
+        return getattr(self, which)[int(ptr[k]):int(ptr[k + 1])]
+
+
+class HaloPart(HaloBuffers):
+    """One part's context with its exchange lists and buffers.  The context
+    runs on `stream` (a torch.cuda.Stream of its device, shared by the parts
+    on that device); the exchanges run on it too (``Decomposed`` makes it
+    the current stream)."""
+
+    def __init__(self, pg, params, lists: HaloLists, stream, precision: str = "fp64"):
+        import ctypes as ct
+
+        import torch
+
+        from . import _lib
+        from .solver import Solver
+        self.stream = stream
+        with torch.cuda.stream(stream):
+            super().__init__(lists, stream.device)
+        self.solver = Solver(pg, params, device=stream.device.index, precision=precision)
+        h = _lib.Halo()
+        keep = [np.ascontiguousarray(a, np.int32) for a in
+                (lists.send_cells, lists.recv_bfaces, lists.nodes)]
+        h.n_send, h.n_recv, h.n_node = (int(a.size) for a in keep)
+        h.send_cells, h.recv_bfaces, h.nodes = (_lib.ptr(a, _lib.i32p) for a in keep)
+        for name in ("send_rows", "recv_rows", "node_send", "node_recv", "ext", "norm_sq"):
+            setattr(h, name, ct.c_void_p(getattr(self, name).data_ptr()))
+        lib = self.solver.lib
+        _lib.check("mfg_set_stream", lib.mfg_set_stream(self.solver.ctx,
+                                                        ct.c_void_p(stream.cuda_stream)))
+        _lib.check("mfg_halo_set", lib.mfg_halo_set(self.solver.ctx, ct.byref(h)))
+        del keep
+
+    def phase(self, ph: int, iter_done: int = 0):
+        from . import _lib
+        _lib.check("mfg_halo_phase", self.solver.lib.mfg_halo_phase(self.solver.ctx, int(ph),
+                                                                      int(iter_done)))
+
+    def close(self):
+        self.solver.close()
+
+
+def build_parts(mesh: RawMesh, params, world: int, part_of=None, zones=None, device_of=None,
+                **bump) -> tuple:
+    """Split `mesh` (slabs unless `part_of` is given), prepare every part and
+    create the contexts of `zones` (default: all), zone z on CUDA device
+    ``device_of(z)`` (default 0).  Returns (parts, whole-mesh grid,
+    {zone: HaloPart})."""
+    import torch
+    if part_of is None:
+        part_of = slab_parts(mesh.n_cell, world)
+    parts = split(mesh, part_of, world)
+    whole, pgs = prepare_parts(mesh, params, parts, **bump)
+    zones = list(range(world)) if zones is None else list(zones)
+    streams = {}
+    held = {}
+    for z in zones:
+        dev = 0 if device_of is None else int(device_of(z))
+        if dev not in streams:
+            streams[dev] = torch.cuda.Stream(device=dev)
+        pt = parts[z]
+        held[z] = HaloPart(pgs[z], params, halo_lists(pt.mesh, pt.interfaces, z), streams[dev])
+    return parts, whole, held
+
+
+class LocalExchange:
+    """Every part in this process: exchanges as device copies (peer copies
+    between GPUs), reductions on the device."""
+
+    def rows(self, parts: dict):
+        self._pairs(parts, "send_rows", "recv_rows")
+
+    def nodes(self, parts: dict):
+        self._pairs(parts, "node_send", "node_recv")
+
+    @staticmethod
+    def _pairs(parts, src, dst):
+        for p, hp in parts.items():
+            for k, r in enumerate(hp.lists.neighbors):
+                other = parts[r]
+                j = other.lists.neighbors.index(p)
+                hp.seg(dst, k).copy_(other.seg(src, j), non_blocking=True)
+
+    def extrema(self, parts: dict):
+        import torch
+        ranks = sorted(parts)
+        ext = torch.stack([parts[r].ext.to(parts[ranks[0]].device) for r in ranks])
+        g = torch.stack([ext[:, 0].max(), ext[:, 1].min()])
+        for r in ranks:
+            parts[r].ext.copy_(g, non_blocking=True)
+
+    def sum(self, t):
+        return t
+
+
+class DistExchange:
+    """One part (or several) per process, parts of other processes reached
+    through torch.distributed point-to-point operations (NCCL over NVLink on
+    GPUs); the reductions are all-reduces.  Each process must call every
+    step in the same order."""
+
+    def __init__(self, group=None):
+        self.group = group
+
+    def _p2p(self, parts, src, dst):
+        import torch.distributed as dist
+        ops = []
+        local = set(parts)
+        for p, hp in parts.items():
+            for k, r in enumerate(hp.lists.neighbors):
+                if r in local:
+                    j = parts[r].lists.neighbors.index(p)
+                    hp.seg(dst, k).copy_(parts[r].seg(src, j))
+                    continue
+                ops.append(dist.P2POp(dist.isend, hp.seg(src, k).contiguous(), r, self.group))
+                ops.append(dist.P2POp(dist.irecv, hp.seg(dst, k), r, self.group))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+
+    def rows(self, parts: dict):
+        self._p2p(parts, "send_rows", "recv_rows")
+
+    def nodes(self, parts: dict):
+        self._p2p(parts, "node_send", "node_recv")
+
+    def extrema(self, parts: dict):
+        import torch
+        import torch.distributed as dist
+        LocalExchange().extrema(parts)
+        hp = parts[min(parts)]
+        mx, mn = hp.ext[0:1].clone(), hp.ext[1:2].clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX, group=self.group)
+        dist.all_reduce(mn, op=dist.ReduceOp.MIN, group=self.group)
+        g = torch.cat([mx, mn])
+        for p in parts.values():
+            p.ext.copy_(g)
+
+    def sum(self, t):
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+        return t
+
+
+class Decomposed:
+    """Parts iterated in step: the main-loop body (main.cpp:201-291) with the
+    reference's MPI exchanges (phases of ``mfg_halo_phase``).  ``parts``
+    maps zone -> HaloPart for the zones this process holds."""
+
+    def __init__(self, parts: dict, exchange=None):
+        self.parts = dict(sorted(parts.items()))
+        self.ex = exchange if exchange is not None else LocalExchange()
+        self.iter_done = 0
+        self.streams = []
+        for hp in self.parts.values():
+            if all(hp.stream is not s for s in self.streams):
+                self.streams.append(hp.stream)
+        for s in self.streams:
+            s.synchronize()  # the buffers' allocation and zero fill
+        with self._on_streams():
+            self._initial_gradient()
+
+    def _on_streams(self):
+        import contextlib
+
+        import torch
+        stack = contextlib.ExitStack()
+        for s in self.streams:
+            stack.enter_context(torch.cuda.stream(s))
+        return stack
+
+    def _each(self, ph):
+        for hp in self.parts.values():
+            hp.phase(ph, self.iter_done)
+
+    def _initial_gradient(self):
+        """PassInterfaceData and the gradient of the initial state
+        (load_grid.cpp:507, AllocAndCalQuantityGradient)."""
+        from . import _lib
+        self._each(_lib.HALO["pack_q"])
+        self.ex.rows(self.parts)
+        self._each(_lib.HALO["nodes"])
+        self.ex.nodes(self.parts)
+        self._each(_lib.HALO["gradient"])
+
+    def iterate(self, n: int) -> np.ndarray:
+        """n iterations; returns the residual norms of every iteration over
+        all parts, [n][5]."""
+        import torch
+
+        from . import _lib
+        H = _lib.HALO
+        first = next(iter(self.parts.values()))
+        with self._on_streams():
+            hist = torch.zeros((max(n, 1), 5), dtype=torch.float64, device=first.device)
+            for i in range(n):
+                self._each(H["face"])
+                self.ex.extrema(self.parts)
+                self._each(H["forward"])
+                self.ex.rows(self.parts)
+                self._each(H["backward"])
+                self.ex.rows(self.parts)
+                self._each(H["nodes"])
+                self.ex.nodes(self.parts)
+                self._each(H["gradient"])
+                for hp in self.parts.values():
+                    hist[i] += hp.norm_sq.to(first.device)
+                self.iter_done += 1
+            self._each(H["check"])
+            hist = self.ex.sum(hist)
+            out = torch.sqrt(hist[:n]).cpu().numpy()
+        return out
+
+    def download(self, field: str) -> dict:
+        return {r: hp.solver.download(field) for r, hp in self.parts.items()}
+
+    def close(self):
+        for hp in self.parts.values():
+            hp.close()
