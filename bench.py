@@ -16,6 +16,7 @@ larger than the 126 MB L2, so no flush is needed between steps.
   python bench.py --form mixed [--mixed-size 128] [--converge 3000]
   python bench.py --form channel [--converge 20000]
   python bench.py --form batched --precision mixed
+  python bench.py --form partition [--parts K]
 
 --form batched: 64 cube cases with n^3 x 6 tets, n uniform in [8, 48], Mach
 U(0.3, 0.8), alpha U(-5, 5) deg, jitter U(0, 0.2)h, all in one context (one
@@ -34,6 +35,13 @@ against FP64.
 
 --precision mixed (batched form): the batch and its sequential per-case
 reference both in the mixed form.
+
+--form partition: the fp64 workload's cube split into K parts (recursive
+coordinate bisection; K = --parts, default the number of GPUs), each part
+its own context iterating through the halo phases with the reference's
+MPI-mode exchanges between them: device copies between the parts of one
+process, NCCL point-to-point and all-reduce between processes (part z on
+rank z mod N).  Strong scaling: the whole mesh's cells per step.
 
 Before the warm-up the sweep launch parameters are chosen by measurement
 on the workload's own grid (mfg_autotune_sweeps) and reported.
@@ -77,7 +85,8 @@ def parse():
     ap.add_argument("--size", type=int, default=64, help="hexes per cube edge (64 = 1.57M tets)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", default="fp64", choices=["fp64", "batched", "mixed", "channel"],
+    ap.add_argument("--form", default="fp64",
+                    choices=["fp64", "batched", "mixed", "channel", "partition"],
                     help="fp64: the single-grid workload; batched: 64 uneven cases in one "
                          "context against the same cases run one after another; mixed: the "
                          "mixed-precision form against FP64 on the 128^3 x 6 cube")
@@ -89,6 +98,8 @@ def parse():
                     help="mixed form: also iterate both forms to a 1e-6 residual drop "
                          "(at most this many iterations) and time it")
     ap.add_argument("--ncase", type=int, default=64)
+    ap.add_argument("--parts", type=int, default=0,
+                    help="partition form: parts of the mesh (default: one per GPU)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed iterations with cudaProfilerStart/Stop (for ncu "
                          "--profile-from-start off)")
@@ -509,6 +520,8 @@ def main():
         run_batched(args, rank, world, local, stream, dist)
     elif args.form in ("mixed", "channel"):
         run_mixed(args, rank, world, local, stream, dist)
+    elif args.form == "partition":
+        run_partition(args, rank, world, local, dist)
     else:
         run_single(args, rank, world, local, stream, dist)
     if dist is not None:
@@ -567,6 +580,70 @@ def run_single(args, rank, world, local, stream, dist):
         }
         print(json.dumps(line), flush=True)
     s.close()
+
+
+def run_partition(args, rank, world, local, dist):
+    """The fp64 workload's mesh as K parts iterated in step (the reference's
+    MPI mode), part z on rank z mod world."""
+    import torch
+    from minifs_b200 import _lib, grid as gr, meshgen, shard
+    from minifs_b200 import partition as pa
+    wl = workload(args.size)
+    mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
+    params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+    K = args.parts or world
+    t = time.perf_counter()
+    part_of = pa.rcb_parts(mesh, K)
+    zones = [z for z in range(K) if z % world == rank]
+    parts, whole, held = pa.build_parts(mesh, params, K, part_of=part_of, zones=zones,
+                                        device_of=lambda z: local, bump_amp=wl["bump_amp"],
+                                        bump_sigma=wl["bump_sigma"])
+    ex = pa.DistExchange() if world > 1 else pa.LocalExchange()
+    d = pa.Decomposed(held, ex)
+    setup_s = time.perf_counter() - t
+    stream = next(iter(held.values())).stream
+    d.iterate(max(args.warmup, 3))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    launches0 = _lib.kernel_launches()
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        norms = d.iterate(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+    launches = _lib.kernel_launches() - launches0
+    ms = shard.reduce_max(ev0.elapsed_time(ev1), dist, "cuda")
+    C = whole.n_cell
+    cut = sum(len(p.interfaces.nbz) for p in parts) // 2
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": C * args.steps / (ms / 1e3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl["name"], "form": "partition", "cells": C, "parts": K,
+                       "part_cells": [int(p.cells.size) for p in parts], "cut_faces": cut,
+                       "partitioner": "recursive coordinate bisection",
+                       "parallelism": f"{K} parts on {world} GPU(s)",
+                       "exchange": "NCCL p2p + all-reduce" if world > 1 else "device copies",
+                       "l2": "no flush: working set far above the 126 MB L2"},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "residual_norm": [float(x) for x in norms[-1]],
+            "setup_s": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+    d.close()
 
 
 def mixed_workload(n: int) -> dict:

@@ -65,6 +65,23 @@ def test_split_covers_the_mesh(kind, world, how):
             assert np.array_equal(np.asarray(getattr(p.mesh, k)), np.asarray(getattr(m, k)))
 
 
+@pytest.mark.parametrize("world", [1, 2, 3, 4, 7])
+def test_rcb_parts_balanced_and_compact(world):
+    m = meshgen.box_mesh(8, 6, 5, jitter=0.1, seed=1)
+    part_of = pa.rcb_parts(m, world)
+    counts = np.bincount(part_of, minlength=world)
+    assert counts.sum() == m.n_cell and counts.min() >= m.n_cell // world - world
+    assert counts.max() - counts.min() <= world
+    # far fewer cut faces than a random assignment
+    f2c = np.asarray(m.f2c).reshape(-1, 2)[m.n_bface:]
+    cut = np.sum(part_of[f2c[:, 0]] != part_of[f2c[:, 1]])
+    rnd = _scatter(m.n_cell, world)
+    cut_rnd = np.sum(rnd[f2c[:, 0]] != rnd[f2c[:, 1]])
+    assert world == 1 and cut == 0 or cut < 0.25 * cut_rnd
+    pts = pa.cell_points(m)
+    assert pts.shape == (m.n_cell, 3) and np.all((pts > 0) & (pts < 1))
+
+
 def test_split_rejects_bad_maps():
     m = _mesh()
     with pytest.raises(ValueError):
