@@ -935,6 +935,15 @@ __device__ __forceinline__ void sweep_cell(
     const int j = lane + L * r;
     if (j < o.ns) {
       const uint32_t b = o.nb[r];
+      // FP64: the part of the product the neighbour's state and the face
+      // give, before the increment is waited for
+      LusgsPre<double> a{};
+      if constexpr (!MX) {
+        double qn[Q_STRIDE];
+#pragma unroll
+        for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[j][k];
+        a = flux_lusgs_pre(qn, st.rec[j].nx, st.rec[j].ny, st.rec[j].nz, flux_params<double>(P));
+      }
       double dn[5];
       if (b & kInRing) {
 #pragma unroll
@@ -957,11 +966,9 @@ __device__ __forceinline__ void sweep_cell(
 #pragma unroll
         for (int k = 0; k < 5; k++) sh[j * 5 + k] = (double)(rr.w * ff[k]);
       } else {
-        double qn[Q_STRIDE], f[5];
-#pragma unroll
-        for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[j][k];
+        double f[5];
         const SweepRec rr = st.rec[j];
-        flux_lusgs(qn, dn, rr.nx, rr.ny, rr.nz, P, f);
+        flux_lusgs_fin(a, dn, rr.nx, rr.ny, rr.nz, flux_params<double>(P), f);
 #pragma unroll
         for (int k = 0; k < 5; k++) sh[j * 5 + k] = rr.w * f[k];
       }

@@ -273,43 +273,69 @@ __device__ __forceinline__ void roe_flux(const double *ql, const double *qr, dou
 }
 
 // FluxLUSGS3D (forward_lusgs.cpp:1271-1324) with the neighbour's sound speed
-// and conserved energy taken from its record (same expressions).
+// and conserved energy taken from its record (same expressions), in two
+// parts: what the neighbour's state and the face give, which an LU-SGS sweep
+// evaluates while it still waits for the neighbour's increment, and the rest.
+template <typename T>
+struct LusgsPre {
+  T Q0, Q1, Q2, Q3, Q4, vq, eig, f1, f2, f3, f4;
+};
+
+template <typename T>
+__device__ __forceinline__ LusgsPre<T> flux_lusgs_pre(const T *q, T nx, T ny, T nz,
+                                                      const FluxP<T> &P) {
+  LusgsPre<T> a;
+  a.Q0 = q[0];
+  a.Q1 = q[0] * q[1];
+  a.Q2 = q[0] * q[2];
+  a.Q3 = q[0] * q[3];
+  a.Q4 = q[Q_E];
+  const T p = q[4];
+  const T v_n = q[1] * nx + q[2] * ny + q[3] * nz;
+  T eig = fabs(v_n) + q[Q_A];
+  eig *= P.lhs_omga;
+  a.eig = eig;
+  const T peff = P.peff;
+  a.f1 = -a.Q1 * v_n - p * nx;
+  a.f2 = -a.Q2 * v_n - p * ny;
+  a.f3 = -a.Q3 * v_n - p * nz;
+  a.f4 = -(a.Q4 + p + peff) * v_n;
+  a.vq = v_n * q[0];
+  return a;
+}
+
+template <typename T>
+__device__ __forceinline__ void flux_lusgs_fin(const LusgsPre<T> &a, const T *DQ, T nx, T ny,
+                                               T nz, const FluxP<T> &P, T *flux) {
+  using N = Num<T>;
+  const T gam1 = P.gamm1;
+  const T peff = P.peff;
+  const T Q0 = a.Q0 + DQ[0];
+  const T Q1 = a.Q1 + DQ[1];
+  const T Q2 = a.Q2 + DQ[2];
+  const T Q3 = a.Q3 + DQ[3];
+  const T Q4 = a.Q4 + DQ[4];
+  const T rv2 = N::div(T(0.5) * (Q1 * Q1 + Q2 * Q2 + Q3 * Q3), Q0);
+  const T p = gam1 * (Q4 - rv2);
+  const T f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
+  T v_n = a.vq;
+  v_n += f0;
+  v_n = N::div(v_n, Q0);
+  const T f1 = a.f1 + (Q1 * v_n + p * nx);
+  const T f2 = a.f2 + (Q2 * v_n + p * ny);
+  const T f3 = a.f3 + (Q3 * v_n + p * nz);
+  const T f4 = a.f4 + ((Q4 + p + peff) * v_n);
+  flux[0] = f0 - a.eig * DQ[0];
+  flux[1] = f1 - a.eig * DQ[1];
+  flux[2] = f2 - a.eig * DQ[2];
+  flux[3] = f3 - a.eig * DQ[3];
+  flux[4] = f4 - a.eig * DQ[4];
+}
+
 template <typename T>
 __device__ __forceinline__ void flux_lusgs_t(const T *q, const T *DQ, T nx, T ny, T nz,
                                              const FluxP<T> &P, T *flux) {
-  using N = Num<T>;
-  const T gam1 = P.gamm1;
-  T Q0 = q[0], Q1 = q[0] * q[1], Q2 = q[0] * q[2], Q3 = q[0] * q[3];
-  T Q4 = q[Q_E];
-  T p = q[4];
-  T v_n = q[1] * nx + q[2] * ny + q[3] * nz;
-  T eig = fabs(v_n) + q[Q_A];
-  eig *= P.lhs_omga;
-  const T peff = P.peff;
-  T f1 = -Q1 * v_n - p * nx;
-  T f2 = -Q2 * v_n - p * ny;
-  T f3 = -Q3 * v_n - p * nz;
-  T f4 = -(Q4 + p + peff) * v_n;
-  Q0 += DQ[0];
-  Q1 += DQ[1];
-  Q2 += DQ[2];
-  Q3 += DQ[3];
-  Q4 += DQ[4];
-  const T rv2 = N::div(T(0.5) * (Q1 * Q1 + Q2 * Q2 + Q3 * Q3), Q0);
-  p = gam1 * (Q4 - rv2);
-  T f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
-  v_n *= q[0];
-  v_n += f0;
-  v_n = N::div(v_n, Q0);
-  f1 += Q1 * v_n + p * nx;
-  f2 += Q2 * v_n + p * ny;
-  f3 += Q3 * v_n + p * nz;
-  f4 += (Q4 + p + peff) * v_n;
-  flux[0] = f0 - eig * DQ[0];
-  flux[1] = f1 - eig * DQ[1];
-  flux[2] = f2 - eig * DQ[2];
-  flux[3] = f3 - eig * DQ[3];
-  flux[4] = f4 - eig * DQ[4];
+  flux_lusgs_fin(flux_lusgs_pre(q, nx, ny, nz, P), DQ, nx, ny, nz, P, flux);
 }
 
 __device__ __forceinline__ void flux_lusgs(const double *q, const double *DQ, double nx, double ny,
@@ -544,6 +570,9 @@ __device__ __forceinline__ bool wait_rec(const double *rec, double *d, int *err,
   load_rec5_l2(rec, d);
   if (rec5_ready(d)) return true;
   const long long t0 = clock64();
+  // the error word is read on every poll: polling faster (reading it every
+  // 16th poll, two polls in flight, one word per poll) or backing off with
+  // __nanosleep each measured slower on the 64^3 x 6 cube
   int polls = 0;
   for (;;) {
     if (polls > 64) __nanosleep(64);

@@ -139,13 +139,18 @@ class Solver:
         return out.reshape(n, 5) if norms else None
 
     def iterate_host(self, n: int, q_in: np.ndarray | None, q_out: np.ndarray | None,
-                     res_out: np.ndarray | None):
+                     res_out: np.ndarray | None, norms: np.ndarray | None = None):
         """End-to-end form: host state in (None: keep the context's), ``n``
-        iterations, host state and residual out (either may be None)."""
+        iterations, host state and residual out (either may be None);
+        ``norms`` (optional, [n][ncase][5]) receives the residual norms of
+        every iteration."""
+        if norms is not None and norms.size < 5 * n * getattr(self, "ncase", 1):
+            raise ValueError("norms needs 5 entries per iteration and case")
         self._call("mfg_iterate_host", int(n), int(self.iter_done),
                    _lib.ptr(q_in) if q_in is not None else None,
                    _lib.ptr(q_out) if q_out is not None else None,
-                   _lib.ptr(res_out) if res_out is not None else None, None)
+                   _lib.ptr(res_out) if res_out is not None else None,
+                   _lib.ptr(norms) if norms is not None else None)
         self.iter_done += n
 
     def profile_phases(self, n: int) -> dict:
