@@ -273,15 +273,13 @@ __device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double d
 #endif
 
 template <bool FLUX, bool DT, bool DIAG, bool PRE>
-__global__ void __launch_bounds__(kBlock, MFG_GATHER_MINB)
-k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
-              const double *__restrict__ q8, const double *__restrict__ vol,
-              double *__restrict__ res, int res_zero, double *__restrict__ dt,
-              double *__restrict__ diag, const double *__restrict__ cfl_tab,
-              const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
-              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs,
-              const double *__restrict__ fflux, int32_t F) {
-  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void face_gather_cell(
+    int32_t c, int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+    const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ res,
+    int res_zero, double *__restrict__ dt, double *__restrict__ diag,
+    const double *__restrict__ cfl_tab, const int32_t *__restrict__ iter_counter, double cfl_arg,
+    const Params &P0, unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part,
+    const Cases &cs, const double *__restrict__ fflux, int32_t F) {
   const bool live = c < C;
   const int32_t cse = live ? case_of(cs, c) : 0;
   const Params P = live ? params_of(P0, cs, c) : P0;
@@ -349,6 +347,20 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
       for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
   }
   gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
+}
+
+template <bool FLUX, bool DT, bool DIAG, bool PRE>
+__global__ void __launch_bounds__(kBlock, MFG_GATHER_MINB)
+k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+              const double *__restrict__ q8, const double *__restrict__ vol,
+              double *__restrict__ res, int res_zero, double *__restrict__ dt,
+              double *__restrict__ diag, const double *__restrict__ cfl_tab,
+              const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
+              unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs,
+              const double *__restrict__ fflux, int32_t F) {
+  face_gather_cell<FLUX, DT, DIAG, PRE>(blockIdx.x * blockDim.x + threadIdx.x, C, cptr, slots,
+                                        q8, vol, res, res_zero, dt, diag, cfl_tab, iter_counter,
+                                        cfl_arg, P0, dt_ext, norm_part, cs, fflux, F);
 }
 
 // Mixed form of the face gather: the Roe flux in the mixed form above; the
@@ -1272,13 +1284,12 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
 
 // Green-Gauss face sums per cell (CompGradientQ_Gauss_Node face loops,
 // cal_gradient.cpp:1740-1897), divided by the volume.
-__global__ void __launch_bounds__(kGradBlock)
-k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-             const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
-             const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
-             const double *__restrict__ q8, const double *__restrict__ vol,
-             double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz) {
-  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void grad_faces_cell(
+    int32_t c, int32_t C, int64_t n, const int32_t *__restrict__ cptr,
+    const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+    const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
+    const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ dqdx,
+    double *__restrict__ dqdy, double *__restrict__ dqdz) {
   if (c >= C) return;
   double gx[5] = {0., 0., 0., 0., 0.}, gy[5] = {0., 0., 0., 0., 0.},
          gz[5] = {0., 0., 0., 0., 0.};
@@ -1337,6 +1348,16 @@ k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
     dqdy[v * n + c] = gy[v] / vc;
     dqdz[v * n + c] = gz[v] / vc;
   }
+}
+
+__global__ void __launch_bounds__(kGradBlock)
+k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
+             const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+             const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
+             const double *__restrict__ q8, const double *__restrict__ vol,
+             double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz) {
+  grad_faces_cell(blockIdx.x * blockDim.x + threadIdx.x, C, n, cptr, slots, fnptr, fnodes, qn8,
+                  q8, vol, dqdx, dqdy, dqdz);
 }
 
 // Mixed form of the gradient: node values and Green-Gauss face sums in FP32
