@@ -281,6 +281,122 @@ def prepare_parts(mesh: RawMesh, params, parts: list[Part], bump_amp: float = 0.
     return whole, out
 
 
+# kinds of the node-weight passes of ComputeWeight3D_Node
+# (grid_polyhedra_auxiliary_functions.cpp:929-1001): wall faces, far-field
+# faces (both far-field types), then the other types bar symmetry and
+# interfaces; the mark each gives a node
+_KIND_MARK = {1: 3, 2: 6, 3: 101}
+
+
+def _face_kinds(bctype) -> np.ndarray:
+    t = np.asarray(bctype, np.int64)
+    kind = np.zeros(t.size, np.int64)
+    kind[t == 3] = 1
+    kind[(t == 6) | (t == 61)] = 2
+    kind[~np.isin(t, (3, 4, 6, 61, 10))] = 3
+    return kind
+
+
+def _add_received(local: np.ndarray, lists: HaloLists, recv: np.ndarray, combine) -> np.ndarray:
+    """A node's own value combined with every neighbour's entry for it, the
+    entries in order (RecvSendVarNeighbor_Node, parallel_mpi.cpp:1997-2004)."""
+    out = local.copy()
+    for e, nd in enumerate(lists.nodes.tolist()):
+        out[nd] = combine(out[nd], recv[e])
+    return out
+
+
+def zone_node_data(pgs: dict, lists: dict, exchange, device="cpu") -> None:
+    """The node data of zones that know only their own grids: node marks,
+    weights and symmetry normals combined over the zones as the reference's
+    MPI build does at set-up (CommInternodeDataMPI2 / CommInternodeDataMPI,
+    grid_polyhedra_auxiliary_functions.cpp:951-1047 and :2114-2119).
+    `pgs` maps zone -> its PreparedGrid (from ``grid.prepare`` of its own
+    mesh; its wnode, nmark, nodesymm and symmetry normals are replaced),
+    `lists` zone -> HaloLists; `exchange` moves the node entries between
+    the zones (``LocalExchange`` or ``DistExchange``; every process calls
+    this with its own zones)."""
+    import torch
+    bufs = {z: HaloBuffers(lists[z], device) for z in pgs}
+
+    def swap(values):
+        for z, b in bufs.items():
+            v = np.zeros((max(lists[z].nodes.size, 1), 8))
+            v[:lists[z].nodes.size, :values[z].shape[1]] = values[z]
+            b.node_send.copy_(torch.from_numpy(v))
+        exchange.nodes(bufs)
+        return {z: b.node_recv.cpu().numpy()[:lists[z].nodes.size] for z, b in bufs.items()}
+
+    geo = {}
+    for z, pg in pgs.items():
+        A = pg.arrays
+        N, G = pg.n_node, pg.n_bface
+        nnpf = np.asarray(A["nnpf"], np.int64)
+        fptr = np.concatenate([[0], np.cumsum(nnpf)])
+        f2n = np.asarray(A["f2n"], np.int64)
+        kind = _face_kinds(A["bctype"][:G])
+        has = np.zeros((N, 3))
+        sym = np.zeros((N, 5))  # flag, sums of the normals, face count
+        for i in range(G):
+            nodes = f2n[fptr[i]:fptr[i + 1]]
+            if kind[i]:
+                has[nodes, kind[i] - 1] = 1.0
+            if A["bctype"][i] == 4:
+                for nd in nodes.tolist():  # FindNodeSYMM's loop order
+                    sym[nd, 0] = 1.0
+                    sym[nd, 1] += A["xfn"][i]
+                    sym[nd, 2] += A["yfn"][i]
+                    sym[nd, 3] += A["zfn"][i]
+                    sym[nd, 4] += 1.0
+        geo[z] = (fptr, f2n, kind, has, sym)
+    recv = swap({z: np.concatenate([g[3], g[4]], 1)[lists[z].nodes] for z, g in geo.items()})
+    marks = {}
+    for z, pg in pgs.items():
+        fptr, f2n, kind, has, sym = geo[z]
+        both = np.concatenate([has, sym], 1)
+
+        def comb(a, b):
+            r = a + b
+            r[:4] = np.maximum(a[:4], b[:4])  # flags: set on any zone
+            return r
+
+        both = _add_received(both, lists[z], recv[z], comb)
+        hw, hf, ho = both[:, 0] > 0, both[:, 1] > 0, both[:, 2] > 0
+        mark = np.where(hw, 3, np.where(hf, 6, np.where(ho, 101, 0))).astype(np.int32)
+        marks[z] = mark
+        sflag = both[:, 3] > 0
+        A = pg.arrays
+        A["nmark"] = mark
+        A["nodesymm"] = sflag.astype(np.int32)
+        for k, name in enumerate(("xfn_n_symm", "yfn_n_symm", "zfn_n_symm")):
+            v = np.zeros(pg.n_node)
+            v[sflag] = both[sflag, 4 + k] / both[sflag, 7]
+            A[name] = v
+    # each zone's share of the node weights under the combined marks, in the
+    # passes' order (faces, then cells), then the sums over zones
+    part = {}
+    for z, pg in pgs.items():
+        fptr, f2n, kind, has, sym = geo[z]
+        A = pg.arrays
+        mark = marks[z]
+        w = np.zeros(pg.n_node)
+        wb = np.asarray(A["wbface"])
+        for kd in (1, 2, 3):
+            for i in np.nonzero(kind == kd)[0].tolist():
+                for j in range(fptr[i], fptr[i + 1]):
+                    nd = f2n[j]
+                    if mark[nd] == _KIND_MARK[kd]:
+                        w[nd] += wb[j]
+        c2n = np.asarray(A["c2n"], np.int64)
+        wc = np.asarray(A["wc2n"])
+        for k in np.nonzero(mark[c2n] == 0)[0].tolist():
+            w[c2n[k]] += wc[k]
+        part[z] = w
+    recv = swap({z: part[z][lists[z].nodes][:, None] for z in pgs})
+    for z, pg in pgs.items():
+        pg.arrays["wnode"] = _add_received(part[z], lists[z], recv[z][:, 0], lambda a, b: a + b)
+
+
 def assemble(parts: list[Part], values: list[np.ndarray], n_cell: int, width: int = 5):
     """Whole-mesh cell array [width][n_cell] from per-part arrays laid out
     [width][n_local] (n_local = the part's cells, or cells + ghosts)."""
@@ -289,6 +405,37 @@ def assemble(parts: list[Part], values: list[np.ndarray], n_cell: int, width: in
         v = np.asarray(v).reshape(width, -1)
         out[:, pt.cells] = v[:, :pt.cells.size]
     return out
+
+
+def build_zones(zones: dict, params, exchange=None, device_of=None, **bump) -> dict:
+    """Contexts of zones known only from their own grids, as one process of
+    the reference's MPI build reads its zone file: `zones` maps zone ->
+    (mesh, interfaces), e.g. from ``flowstar.read_grid`` (the mesh's
+    patches set from the zone's bc.para).  Each zone is preprocessed on its
+    own, its node data combined with the other zones' through `exchange`
+    (``zone_node_data``; every process passes its zones and the same
+    exchange kind), and its context created on ``device_of(z)``; the
+    interface ghosts get the neighbours' states in ``Decomposed``'s first
+    exchange.  Returns {zone: HaloPart}."""
+    import torch
+
+    from . import grid as gr
+    exchange = exchange if exchange is not None else LocalExchange()
+    pgs, lists = {}, {}
+    for z, (mesh, itf) in sorted(zones.items()):
+        pgs[z] = gr.prepare(mesh, params, **bump)
+        lists[z] = halo_lists(mesh, itf, z)
+    dev0 = 0 if device_of is None else int(device_of(min(zones)))
+    zone_node_data(pgs, lists, exchange,
+                   device="cpu" if isinstance(exchange, LocalExchange) else
+                   torch.device("cuda", dev0))
+    streams, held = {}, {}
+    for z in sorted(zones):
+        dev = 0 if device_of is None else int(device_of(z))
+        if dev not in streams:
+            streams[dev] = torch.cuda.Stream(device=dev)
+        held[z] = HaloPart(pgs[z], params, lists[z], streams[dev])
+    return held
 
 
 # ---- iteration -------------------------------------------------------------

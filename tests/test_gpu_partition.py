@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from helpers import assert_bitwise
-from minifs_b200 import _lib, grid as gr, meshgen
+from minifs_b200 import _lib, flowstar, grid as gr, meshgen
 from minifs_b200 import partition as pa
 from minifs_b200.compare import state_rel_err
 from minifs_b200.solver import Solver
@@ -132,6 +132,37 @@ def test_parts_converge_to_the_whole_mesh_state(world, how, live):
     # the parts did not follow the single mesh's path (block Jacobi across cuts)
     assert not np.allclose(nd[5], nr[5], rtol=1e-6)
     d.close()
+
+
+def test_zones_from_their_own_files(tmp_path):
+    """Each zone written as a FlowStar grid with its interface block and its
+    bc.para, read back and set up from that alone (node data combined over
+    the zones by exchange), against the zones set up from the whole mesh."""
+    m, p = _box(), _params()
+    world = 3
+    parts, whole, held = pa.build_parts(m, p, world, part_of=pa.rcb_parts(m, world), **BUMP)
+    ref = pa.Decomposed(held)
+    zones = {}
+    for pt in parts:
+        g, b = tmp_path / f"zone{pt.rank}.mfl", tmp_path / f"zone{pt.rank}.bc"
+        flowstar.write_grid(pt.mesh, g, pt.interfaces)
+        flowstar.write_bc(pt.mesh.patches, b)
+        mesh, itf = flowstar.read_grid(g)
+        mesh.patches = flowstar.read_bc(b)
+        zones[pt.rank] = (mesh, itf)
+    d = pa.Decomposed(pa.build_zones(zones, p, **BUMP))
+    C = whole.n_cell
+    for f in ("dqdx", "dqdy", "dqdz"):
+        a, b = _cells(parts, d, f, C), _cells(parts, ref, f, C)
+        for v in range(5):
+            np.testing.assert_allclose(a[v], b[v], rtol=0, atol=1e-11 * np.abs(b[v]).max())
+    na, nb = d.iterate(40), ref.iterate(40)
+    np.testing.assert_allclose(na, nb, rtol=1e-9)
+    qa, qb = _cells(parts, d, "q", C), _cells(parts, ref, "q", C)
+    for v in range(5):
+        np.testing.assert_allclose(qa[v], qb[v], rtol=1e-10, atol=1e-10 * np.abs(qb[v]).max())
+    d.close()
+    ref.close()
 
 
 def test_halo_refusals_and_checks():

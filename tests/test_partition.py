@@ -166,6 +166,41 @@ def test_part_preprocessing_matches_whole_mesh():
         assert np.array_equal(A["nmark"], W["nmark"][pt.nodes])
 
 
+def _zone_case(world, how, seed=7):
+    m = _mesh()
+    params = gr.make_params(mach=0.6, alpha=3.0, cfl_start=10.0)
+    part_of = {"slab": lambda: pa.slab_parts(m.n_cell, world),
+               "scatter": lambda: _scatter(m.n_cell, world, seed),
+               "rcb": lambda: pa.rcb_parts(m, world)}[how]()
+    parts = pa.split(m, part_of, world)
+    return m, params, parts
+
+
+def _compare_node_data(pt, A, W):
+    # marks and flags exactly; sums to round-off (a cell next to a cut has
+    # its faces in another order, so its centroid and weights may differ in
+    # the last bit)
+    assert np.array_equal(A["nmark"], W["nmark"])
+    assert np.array_equal(A["nodesymm"], W["nodesymm"])
+    np.testing.assert_allclose(A["wnode"], W["wnode"], rtol=1e-14)
+    for k in ("xfn_n_symm", "yfn_n_symm", "zfn_n_symm"):
+        np.testing.assert_allclose(A[k], W[k], rtol=1e-14, atol=1e-15)
+
+
+@pytest.mark.parametrize("world,how", [(2, "slab"), (3, "scatter"), (4, "rcb")])
+def test_zone_node_data_from_zone_grids_alone(world, how):
+    m, params, parts = _zone_case(world, how)
+    _, restricted = pa.prepare_parts(m, params, parts, bump_amp=0.05, bump_sigma=0.2)
+    pgs = {p.rank: gr.prepare(p.mesh, params, bump_amp=0.05, bump_sigma=0.2) for p in parts}
+    lists = {p.rank: pa.halo_lists(p.mesh, p.interfaces, p.rank) for p in parts}
+    # on its own a zone misses the other zones' shares of its shared nodes
+    assert all(not np.allclose(pgs[p.rank].arrays["wnode"], restricted[p.rank].arrays["wnode"])
+               for p in parts)
+    pa.zone_node_data(pgs, lists, pa.LocalExchange())
+    for p in parts:
+        _compare_node_data(p, pgs[p.rank].arrays, restricted[p.rank].arrays)
+
+
 # ---- the exchanges on host buffers ------------------------------------------
 
 def _fill(pt, buf, rank):
@@ -252,6 +287,38 @@ def _rank_main(rank, world, port, out_dir):
             np.concatenate([buf.ext.numpy().astype(np.float64), hist.numpy().reshape(-1)]))
     dist.barrier()
     dist.destroy_process_group()
+
+
+def _zone_rank_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    m, params, parts = _zone_case(world, "rcb")
+    p = parts[rank]
+    pg = gr.prepare(p.mesh, params)
+    pa.zone_node_data({rank: pg}, {rank: pa.halo_lists(p.mesh, p.interfaces, rank)},
+                      pa.DistExchange())
+    np.savez(os.path.join(out_dir, f"z{rank}.npz"),
+             **{k: pg.arrays[k] for k in ("wnode", "nmark", "nodesymm", "xfn_n_symm",
+                                          "yfn_n_symm", "zfn_n_symm")})
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_zone_node_data_two_gloo_ranks(tmp_path):
+    import torch.multiprocessing as mp
+    world = 2
+    mp.spawn(_zone_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+             join=True)
+    m, params, parts = _zone_case(world, "rcb")
+    _, restricted = pa.prepare_parts(m, params, parts)
+    for p in parts:
+        got = dict(np.load(tmp_path / f"z{p.rank}.npz"))
+        _compare_node_data(p, got, restricted[p.rank].arrays)
 
 
 def test_dist_exchange_two_gloo_ranks(tmp_path):
