@@ -179,6 +179,12 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
  * Returns MFG_ERR_TIMEOUT and leaves the context's state unchanged and
  * usable (MFG_ERR_UNSUPPORTED when the grid has a single chunk). */
 int mfg_selftest_sweep_timeout(mfg_ctx *ctx, int64_t spin_cycles);
+/* Self-test of the sweeps' division by a precomputed reciprocal (no
+ * counterpart in the reference): n pseudo-random dividend/divisor pairs
+ * (seeded, exponents across [-600, 600]) divided both ways on the current
+ * device; *mismatches receives the number of results whose bits differ
+ * from the division's (0 expected). */
+int mfg_selftest_division(int64_t n, uint64_t seed, int64_t *mismatches);
 
 /* ---- the iteration path (reference routine replaced in brackets) -------- */
 /* [ZeroResiduals, cal_flux.cpp:54-72] */

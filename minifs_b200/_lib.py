@@ -139,6 +139,8 @@ def load(build_if_missing: bool = True):
         "mfg_set_sweep_lanes": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_autotune_sweeps": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
         "mfg_selftest_sweep_timeout": (ct.c_int, [ctxp, ct.c_int64]),
+        "mfg_selftest_division": (ct.c_int, [ct.c_int64, ct.c_uint64,
+                                             ct.POINTER(ct.c_int64)]),
         "mfg_zero_residuals": (ct.c_int, [ctxp]),
         "mfg_inviscid_flux": (ct.c_int, [ctxp]),
         "mfg_compute_timestep": (ct.c_int, [ctxp, ct.c_int32]),

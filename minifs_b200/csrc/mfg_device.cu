@@ -941,6 +941,12 @@ __device__ __forceinline__ void sweep_cell(
   const int32_t c = o.cell;
   const int32_t cse = case_of(cs, c);
   const Params P = params_of(P0, cs, c);
+  // what the cell's own staged data give, formed while its neighbours'
+  // increments are still awaited: the reciprocal of the diagonal term the
+  // increment is divided by, and the velocity square of the limiter
+  const double den = FWD ? st.diag : 2.0 * st.diag;
+  const double rden = 1.0 / den;
+  const double vv = st.qc[1] * st.qc[1] + st.qc[2] * st.qc[2] + st.qc[3] * st.qc[3];
   // record j = lane + L r < ns: w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j)
 #pragma unroll
   for (int r = 0; r < W / L; r++) {
@@ -1024,11 +1030,12 @@ __device__ __forceinline__ void sweep_cell(
         }
       }
     }
-    const double tmp = 2.0 * st.diag;
 #pragma unroll
     for (int i = 0; i < kC; i++) {
       const int k = lane + L * i;
-      if (k < 5) sh[W * 5 + k] = FWD ? acc[i] / dg : st.in5[k] - acc[i] / tmp;
+      if (k < 5)
+        sh[W * 5 + k] = FWD ? (clamped ? acc[i] / dg : div_by_recip(acc[i], den, rden))
+                            : st.in5[k] - div_by_recip(acc[i], den, rden);
     }
   }
   __syncwarp(gmask);
@@ -1038,7 +1045,7 @@ __device__ __forceinline__ void sweep_cell(
   for (int k = 0; k < 5; k++) d[k] = sh[W * 5 + k];
 #pragma unroll
   for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
-  if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit(qc, d, P);
+  if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit_vv(qc, vv, d, P);
   if (lane == 0) {
     if (FWD && clamped) {
       dt[c] = lim;
@@ -1560,6 +1567,40 @@ __global__ void k_norm_seg_final(int32_t nparts, const double *__restrict__ part
 }
 
 __global__ void k_counter_inc(int32_t *__restrict__ counter) { *counter += 1; }
+
+// Self-test of div_by_recip against the division: n dividend/divisor pairs
+// from a splitmix64 stream, significands uniform, exponents uniform in
+// [-600, 600] (both sides of div_by_recip's window) and random signs; every
+// fourth divisor has an all-ones significand.  Counts the pairs whose bits
+// differ.
+__device__ __forceinline__ uint64_t splitmix64(uint64_t &x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double draw_double(uint64_t &x, bool all_ones) {
+  const uint64_t r = splitmix64(x), e = splitmix64(x);
+  const uint64_t mant = all_ones ? 0xFFFFFFFFFFFFFull : (r & 0xFFFFFFFFFFFFFull);
+  const uint64_t expo = (uint64_t)(1023 - 600 + (int64_t)(e % 1201));
+  return __longlong_as_double((long long)(((r >> 63) << 63) | (expo << 52) | mant));
+}
+
+__global__ void k_selftest_division(int64_t n, uint64_t seed,
+                                    unsigned long long *__restrict__ bad) {
+  unsigned long long local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t x = seed ^ ((uint64_t)i * 0xD1B54A32D192ED03ull);
+    const double a = draw_double(x, false);
+    const double b = draw_double(x, (i & 3) == 3);
+    const double y = 1.0 / b;
+    const double q = div_by_recip(a, b, y), ref = a / b;
+    if (__double_as_longlong(q) != __double_as_longlong(ref)) local++;
+  }
+  if (local) atomicAdd(bad, local);
+}
 
 // ---- one part of a partitioned mesh (the reference's MPI mode) ------------
 
@@ -4438,6 +4479,27 @@ std::mutex g_scratch_mu;
 double *g_scratch_dev[kMaxDevices] = {};
 
 }  // namespace
+
+extern "C" int mfg_selftest_division(int64_t n, uint64_t seed, int64_t *mismatches) {
+  if (n < 0 || !mismatches) return MFG_ERR_INVALID;
+  unsigned long long *d = nullptr;
+  MFG_CUDA(cudaMalloc(&d, sizeof(unsigned long long)));
+  cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
+  if (e == cudaSuccess) {
+    k_selftest_division<<<4 * 148, kBlock>>>(n, seed, d);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  unsigned long long h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    g_cuda_error = std::string("division self-test: ") + cudaGetErrorString(e);
+    return MFG_ERR_CUDA;
+  }
+  *mismatches = (int64_t)h;
+  return MFG_OK;
+}
 
 extern "C" int mfg_residual_norm_static(const double *res, int32_t n_cell, double *norms,
                                         void *stream) {

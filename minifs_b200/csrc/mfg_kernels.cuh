@@ -444,9 +444,32 @@ __device__ __forceinline__ void flux_lusgs_diff(const float *q, const float *DQ,
   flux[4] = H * dvn + dH * vnn - eig * DQ[4];
 }
 
-// DQ_limit == 2 positivity limiter (forward_lusgs.cpp:939-973, :1184-1218).
-__device__ __forceinline__ void dq_limit(const double *q, double *d, const Params &P) {
-  const double vv = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+// Correctly rounded a / b from y = RN(1 / b), for a divisor known before
+// the dividend (the LU-SGS diagonal): the quotient's dependent chain is one
+// product and four fused multiply-adds instead of a division.  Markstein's
+// theorem (P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): for y within
+// half an ulp of 1/b and q within one ulp of a/b, r = a - b q is exact and
+// RN(q + r y) = RN(a / b).  q0 = RN(a y) is within two ulps; one correction
+// step makes it faithful, the second rounds correctly.  Exponents outside
+// [2^-500, 2^500] (zeros, subnormals, overflow risks, non-finite values)
+// take the division itself.
+__device__ __forceinline__ double div_by_recip(double a, double b, double y) {
+  const int ea = (__double2hiint(a) >> 20) & 0x7FF;
+  const int eb = (__double2hiint(b) >> 20) & 0x7FF;
+  if (ea < 523 || ea > 1523 || eb < 523 || eb > 1523) return a / b;
+  const double q0 = __dmul_rn(a, y);
+  const double r0 = __fma_rn(-b, q0, a);
+  const double q1 = __fma_rn(r0, y, q0);
+  const double r1 = __fma_rn(-b, q1, a);
+  return __fma_rn(r1, y, q1);
+}
+
+// DQ_limit == 2 positivity limiter (forward_lusgs.cpp:939-973, :1184-1218);
+// vv = u^2 + v^2 + w^2 of the cell, which the sweeps form before the
+// increment is known.
+__device__ __forceinline__ void dq_limit_vv(const double *q, double vv, double *d,
+                                            const Params &P) {
 #pragma unroll
   for (int stage = 0; stage < 3; stage++) {
     double dp = d[4] + 0.5 * d[0] * vv - (d[1] * q[1] + d[2] * q[2] + d[3] * q[3]);
@@ -464,6 +487,10 @@ __device__ __forceinline__ void dq_limit(const double *q, double *d, const Param
       break;  // d unchanged: the later stages repeat this test and pass too
     }
   }
+}
+
+__device__ __forceinline__ void dq_limit(const double *q, double *d, const Params &P) {
+  dq_limit_vv(q, q[1] * q[1] + q[2] * q[2] + q[3] * q[3], d, P);
 }
 
 // UpdateFlowField3D_CFL3d (forward_lusgs.cpp:1335-1488) for one cell; q is
