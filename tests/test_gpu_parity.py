@@ -1,7 +1,7 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle and
-the reference's golden outputs.  FP64 form: bit-for-bit, with the north-star
-tolerances (1e-12 relative per residual entry, 1e-10 in state after 100
-iterations) asserted as well for the record."""
+the reference's golden outputs.  FP64 form: bit-for-bit, with the stated
+floating-point tolerances of the path (1e-12 relative per residual entry,
+1e-10 in state after 100 iterations) asserted as well for the record."""
 import numpy as np
 import pytest
 
