@@ -318,14 +318,21 @@ int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min);
  * Before the first iteration: MFG_HALO_PACK_Q (current states of the sent
  * cells -> send_rows), exchange, then MFG_HALO_NODES and MFG_HALO_GRADIENT
  * for the gradient of the initial state.  MFG_HALO_CHECK synchronises and
- * reports a sweep timeout (MFG_ERR_TIMEOUT).  The LU-SGS sweeps of a part
+ * reports a sweep timeout (MFG_ERR_TIMEOUT).  At second order (mfg_set_order
+ * >= 2, the halo registered with grad_send/grad_recv) each iteration starts
+ * with MFG_HALO_LIMIT (the limiter of the part's cells; their gradient,
+ * limiter and centroid rows -> grad_send), the caller moves each
+ * neighbour's grad_send to grad_recv, and MFG_HALO_FACE first places the
+ * received rows in the interface ghosts, whose face states are then
+ * reconstructed as the neighbouring cells' own (other ghosts stay first
+ * order).  The LU-SGS sweeps of a part
  * see a neighbour's increment only through the ghost DQ of the backward
  * sweep, as in the reference, so several parts converge along another
  * path than one mesh does; one part with no neighbours gives mfg_iterate's
  * bits.  The node weights, marks and symmetry normals of the part's mesh
  * must be those of the whole mesh (the reference sums them over parts,
- * grid_polyhedra_auxiliary_functions.cpp:951-1047).  FP64, first order,
- * single-case contexts only (MFG_ERR_UNSUPPORTED otherwise); a context with
+ * grid_polyhedra_auxiliary_functions.cpp:951-1047).  FP64, single-case
+ * contexts only (MFG_ERR_UNSUPPORTED otherwise); a context with
  * a halo refuses mfg_iterate, mfg_iterate_host, mfg_forward_lusgs,
  * mfg_calculate_gradient, mfg_profile_phases and mfg_autotune_sweeps. */
 typedef struct mfg_halo {
@@ -346,6 +353,10 @@ typedef struct mfg_halo {
   int64_t *ext;               /* device [2]: dt_max, dt_min as the bits of positive
                                  doubles (their order is that of the int64 values) */
   double *norm_sq;            /* device [5]: the part's sums of squared residuals */
+  double *grad_send;          /* device [n_send][24] (second order only, else NULL): the
+                                 sent cells' gradients (x, y, z of rho,u,v,w,p), limiter
+                                 (1 when unlimited) and centroid (x, y, z, vol^(1/3)) */
+  double *grad_recv;          /* device [n_recv][24] */
 } mfg_halo;
 #define MFG_HALO_PACK_Q 0
 #define MFG_HALO_FACE 1
@@ -354,6 +365,7 @@ typedef struct mfg_halo {
 #define MFG_HALO_NODES 4
 #define MFG_HALO_GRADIENT 5
 #define MFG_HALO_CHECK 6
+#define MFG_HALO_LIMIT 7
 /* Registers the exchange lists (copied) and the caller's device buffers
  * (kept; on the context's device, alive while the context is), once per
  * context.  MFG_ERR_INVALID for an index out of range or a received row

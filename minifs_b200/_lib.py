@@ -88,12 +88,13 @@ class Halo(ct.Structure):
                 ("recv_bfaces", i32p), ("n_node", ct.c_int32), ("nodes", i32p),
                 ("send_rows", ct.c_void_p), ("recv_rows", ct.c_void_p),
                 ("node_send", ct.c_void_p), ("node_recv", ct.c_void_p),
-                ("ext", ct.c_void_p), ("norm_sq", ct.c_void_p)]
+                ("ext", ct.c_void_p), ("norm_sq", ct.c_void_p),
+                ("grad_send", ct.c_void_p), ("grad_recv", ct.c_void_p)]
 
 
 # mfg_halo_phase phases
 HALO = {"pack_q": 0, "face": 1, "forward": 2, "backward": 3, "nodes": 4, "gradient": 5,
-        "check": 6}
+        "check": 6, "limit": 7}
 
 
 class MfgError(RuntimeError):

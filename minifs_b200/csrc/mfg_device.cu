@@ -449,20 +449,24 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
 // `order`, para_field_global.cpp:100, has no implementation behind it, so
 // this is this library's own reconstruction: linear from the Green-Gauss
 // gradient of the state the face kernel reads, limited per cell).
+// gflag (a partitioned mesh at second order): the ghosts that hold another
+// part's cell, with that cell's gradient, limiter and centroid, reconstruct
+// as the cell would; other ghosts stay first order.
 __device__ __forceinline__ void reconstruct(double *q, int32_t c, int32_t C, int64_t n,
                                             const Cen &fc, const Cen *__restrict__ ccen,
                                             const double *__restrict__ dqdx,
                                             const double *__restrict__ dqdy,
                                             const double *__restrict__ dqdz,
-                                            const double *__restrict__ phi) {
-  if (c >= C) return;
+                                            const double *__restrict__ phi,
+                                            const int32_t *__restrict__ gflag) {
+  if (c >= C && !(gflag && gflag[c - C])) return;
   const Cen cc = ccen[c];
   const double rx = fc.x - cc.x, ry = fc.y - cc.y, rz = fc.z - cc.z;
 #pragma unroll
   for (int v = 0; v < 5; v++) {
     const int64_t k = (int64_t)v * n + c;
     const double d = dqdx[k] * rx + dqdy[k] * ry + dqdz[k] * rz;
-    q[v] += (phi ? phi[(int64_t)v * C + c] : 1.0) * d;
+    q[v] += (phi ? phi[(int64_t)v * n + c] : 1.0) * d;
   }
 }
 
@@ -481,7 +485,8 @@ k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restri
             Params P0, Cases cs, double *__restrict__ fflux, int32_t C, int64_t n,
             const Cen *__restrict__ fcen, const Cen *__restrict__ ccen,
             const double *__restrict__ dqdx, const double *__restrict__ dqdy,
-            const double *__restrict__ dqdz, const double *__restrict__ phi) {
+            const double *__restrict__ dqdz, const double *__restrict__ phi,
+            const int32_t *__restrict__ gflag) {
   const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= F) return;
   const FaceRec fr = faces[f];
@@ -497,8 +502,8 @@ k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restri
       ar[v] = qr[v];
     }
     const Cen fc = fcen[f];
-    reconstruct(al, fr.c1, C, n, fc, ccen, dqdx, dqdy, dqdz, phi);
-    reconstruct(ar, fr.c2, C, n, fc, ccen, dqdx, dqdy, dqdz, phi);
+    reconstruct(al, fr.c1, C, n, fc, ccen, dqdx, dqdy, dqdz, phi, gflag);
+    reconstruct(ar, fr.c2, C, n, fc, ccen, dqdx, dqdy, dqdz, phi, gflag);
     if (al[0] > 0.0 && ar[0] > 0.0 && al[4] + P.p_bar > 0.0 && ar[4] + P.p_bar > 0.0) {
       cell_props(al, P);
       cell_props(ar, P);
@@ -570,7 +575,7 @@ k_limiter(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
       lim[v] = fmin(lim[v], psi);
     }
   }
-  for (int v = 0; v < 5; v++) phi[(int64_t)v * C + c] = fmax(0.0, fmin(1.0, lim[v]));
+  for (int v = 0; v < 5; v++) phi[(int64_t)v * n + c] = fmax(0.0, fmin(1.0, lim[v]));
 }
 
 // Centroids for the reconstruction: faces and cells (with h = vol^(1/3)).
@@ -1648,6 +1653,49 @@ __global__ void k_halo_scatter(int32_t n, int32_t width, const int32_t *__restri
   if (b) b[o] = v;
 }
 
+// Second order across parts: a sent cell's gradient rows (x, y, z of the
+// five variables), limiter (1 without one) and centroid into a packed row of
+// kGradRow doubles, and a received row into the ghost's places.
+constexpr int kGradRow = 24;
+
+__global__ void k_halo_pack_grad(int32_t m, const int32_t *__restrict__ cells, int64_t n,
+                                 const double *__restrict__ dqdx, const double *__restrict__ dqdy,
+                                 const double *__restrict__ dqdz, const double *__restrict__ phi,
+                                 const Cen *__restrict__ ccen, double *__restrict__ out) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int64_t c = cells[i];
+  double *o = out + (int64_t)i * kGradRow;
+  for (int v = 0; v < 5; v++) {
+    o[v] = dqdx[(int64_t)v * n + c];
+    o[5 + v] = dqdy[(int64_t)v * n + c];
+    o[10 + v] = dqdz[(int64_t)v * n + c];
+    o[15 + v] = phi ? phi[(int64_t)v * n + c] : 1.0;
+  }
+  const Cen cc = ccen[c];
+  o[20] = cc.x;
+  o[21] = cc.y;
+  o[22] = cc.z;
+  o[23] = cc.h;
+}
+
+__global__ void k_halo_unpack_grad(int32_t m, const int32_t *__restrict__ rows, int64_t n,
+                                   const double *__restrict__ in, double *__restrict__ dqdx,
+                                   double *__restrict__ dqdy, double *__restrict__ dqdz,
+                                   double *__restrict__ phi, Cen *__restrict__ ccen) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int64_t g = rows[i];
+  const double *r = in + (int64_t)i * kGradRow;
+  for (int v = 0; v < 5; v++) {
+    dqdx[(int64_t)v * n + g] = r[v];
+    dqdy[(int64_t)v * n + g] = r[5 + v];
+    dqdz[(int64_t)v * n + g] = r[10 + v];
+    if (phi) phi[(int64_t)v * n + g] = r[15 + v];
+  }
+  ccen[g] = Cen{r[20], r[21], r[22], r[23]};
+}
+
 // Shared nodes: the local partial sums plus each neighbour's (in entry
 // order, RecvSendVarNeighbor_Node, parallel_mpi.cpp:1997-2004), then the
 // division and projection of every node (cal_gradient.cpp:2314-2350).
@@ -1789,6 +1837,7 @@ struct mfg_ctx {
   int32_t *h_nodes = nullptr;           // local node of each node entry
   int32_t *h_unodes = nullptr, *h_eptr = nullptr, *h_eidx = nullptr;  // entries per shared node
   int32_t h_nu = 0;
+  int32_t *h_gflag = nullptr;  // [G] 1 for the ghosts received rows fill (second order)
 };
 
 namespace {
@@ -3417,17 +3466,21 @@ static int launch_gradient(mfg_ctx *ctx);
 
 int mfg_set_order(mfg_ctx *ctx, int32_t order, double venkat_k) {
   if (!ctx || order < 1 || order > 4 || !(venkat_k > 0.0)) return MFG_ERR_INVALID;
-  if (ctx->halo && order != 1) return MFG_ERR_UNSUPPORTED;  // first order across parts
+  // across parts, second order needs the gradient rows' exchange buffers
+  if (ctx->halo && order != 1 && ctx->hb.n_send + ctx->hb.n_recv > 0 &&
+      (!ctx->hb.grad_send || !ctx->hb.grad_recv))
+    return MFG_ERR_UNSUPPORTED;
   MFG_CUDA(cudaSetDevice(ctx->device));
   int rc;
-  if (order >= 3 && !ctx->phi && (rc = dalloc(ctx, &ctx->phi, (size_t)5 * ctx->C))) return rc;
+  if (order >= 3 && !ctx->phi && (rc = dalloc(ctx, &ctx->phi, (size_t)5 * ctx->n))) return rc;
   if (order != ctx->order) drop_graphs(ctx);
   ctx->order = order;
   ctx->venkat_k = venkat_k;
   if (order >= 3)
-    MFG_CUDA(cudaMemsetAsync(ctx->phi, 0, sizeof(double) * 5 * ctx->C, ctx->stream));
-  // the next flux reads the gradient of the current state
-  return order >= 2 ? launch_gradient(ctx) : MFG_OK;
+    MFG_CUDA(cudaMemsetAsync(ctx->phi, 0, sizeof(double) * 5 * ctx->n, ctx->stream));
+  // the next flux reads the gradient of the current state (a part's comes
+  // from its GRADIENT phase)
+  return order >= 2 && !ctx->halo ? launch_gradient(ctx) : MFG_OK;
 }
 
 int mfg_set_live_bc(mfg_ctx *ctx, int32_t on) {
@@ -3480,7 +3533,7 @@ int mfg_zero_residuals(mfg_ctx *ctx) {
 }
 
 static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
-                       bool use_table) {
+                       bool use_table, bool limiter = true) {
   cudaStream_t st = ctx->stream;
   const int g = grid_for(ctx->C);
   const double *q = ctx->q8[ctx->cur];
@@ -3491,7 +3544,7 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
   if (flux) {  // each face's Roe flux once, then gathered per cell
     const bool recon = ctx->order >= 2;
     const double *phi = ctx->order >= 3 ? ctx->phi : nullptr;
-    if (ctx->order >= 3) {
+    if (ctx->order >= 3 && limiter) {
       if (ctx->order == 4)
         k_limiter<true><<<g, kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots, q,
                                               ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->fcen,
@@ -3505,7 +3558,7 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
 #define MFG_FLUX(MX_, R_)                                                                     \
   k_face_flux<MX_, R_><<<grid_for(ctx->F), kBlock, 0, st>>>(                                   \
       ctx->F, ctx->faces, q, ctx->P, cs, ctx->fflux, ctx->C, ctx->n, ctx->fcen, ctx->ccen,     \
-      ctx->dqdx, ctx->dqdy, ctx->dqdz, phi)
+      ctx->dqdx, ctx->dqdy, ctx->dqdz, phi, ctx->halo ? ctx->h_gflag : nullptr)
     const bool fmx = mx && !ctx->flux_fp64;
     if (fmx && recon)
       MFG_FLUX(true, true);
@@ -4277,11 +4330,13 @@ int mfg_download(mfg_ctx *ctx, int32_t field, double *host) {
       break;
     case MFG_FIELD_DT: src = ctx->dt; count = C; break;
     case MFG_FIELD_DIAG: src = ctx->diag; count = C; break;
-    case MFG_FIELD_LIMITER:
+    case MFG_FIELD_LIMITER:  // [5][n] on the device: the cells' rows
       if (!ctx->phi) return MFG_ERR_INVALID;
-      src = ctx->phi;
-      count = 5 * C;
-      break;
+      for (int v = 0; v < 5; v++)
+        MFG_CUDA(cudaMemcpyAsync(host + (int64_t)v * C, ctx->phi + (int64_t)v * n,
+                                 sizeof(double) * C, cudaMemcpyDeviceToHost, st));
+      MFG_CUDA(cudaStreamSynchronize(st));
+      return MFG_OK;
     case MFG_FIELD_DQDX: src = ctx->dqdx; count = 5 * n; break;
     case MFG_FIELD_DQDY: src = ctx->dqdy; count = 5 * n; break;
     case MFG_FIELD_DQDZ: src = ctx->dqdz; count = 5 * n; break;
@@ -4318,8 +4373,9 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
 int mfg_halo_set(mfg_ctx *ctx, const mfg_halo *h) {
   if (!ctx || !h) return MFG_ERR_INVALID;
   if (ctx->halo) return MFG_ERR_INVALID;  // once per context
-  if (ctx->ncase != 1 || ctx->precision != MFG_PREC_FP64 || ctx->order != 1)
-    return MFG_ERR_UNSUPPORTED;
+  if (ctx->ncase != 1 || ctx->precision != MFG_PREC_FP64) return MFG_ERR_UNSUPPORTED;
+  if (ctx->order != 1 && h->n_send + h->n_recv > 0 && (!h->grad_send || !h->grad_recv))
+    return MFG_ERR_UNSUPPORTED;  // second order needs the gradient rows' buffers
   if (h->n_send < 0 || h->n_recv < 0 || h->n_node < 0 || !h->ext || !h->norm_sq)
     return MFG_ERR_INVALID;
   if ((h->n_send && (!h->send_cells || !h->send_rows)) ||
@@ -4365,6 +4421,9 @@ int mfg_halo_set(mfg_ctx *ctx, const mfg_halo *h) {
   if ((rc = dupload(ctx, &ctx->h_unodes, unodes))) return rc;
   if ((rc = dupload(ctx, &ctx->h_eptr, eptr))) return rc;
   if ((rc = dupload(ctx, &ctx->h_eidx, eidx))) return rc;
+  std::vector<int32_t> gflag(std::max(ctx->G, 1), 0);
+  for (int32_t i = 0; i < h->n_recv; i++) gflag[h->recv_bfaces[i]] = 1;
+  if ((rc = dupload(ctx, &ctx->h_gflag, gflag))) return rc;
   // shared nodes keep their partial sums in k_node_values (info bit 4)
   std::vector<int32_t> info(ctx->N);
   MFG_CUDA(cudaMemcpy(info.data(), ctx->ninfo, sizeof(int32_t) * ctx->N, cudaMemcpyDeviceToHost));
@@ -4405,9 +4464,40 @@ int mfg_halo_phase(mfg_ctx *ctx, int32_t phase, int32_t iter_done) {
     case MFG_HALO_PACK_Q:
       halo_gather(ctx, h.n_send, Q_STRIDE, ctx->h_send, ctx->q8[ctx->cur], h.send_rows);
       break;
+    case MFG_HALO_LIMIT: {  // second order: the limiter, then the gradient rows out
+      if (ctx->order < 2) return MFG_ERR_INVALID;
+      if (ctx->order >= 3) {
+        const int g = grid_for(ctx->C);
+        if (ctx->order == 4)
+          k_limiter<true><<<g, kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,
+                                                ctx->q8[ctx->cur], ctx->dqdx, ctx->dqdy,
+                                                ctx->dqdz, ctx->fcen, ctx->ccen, ctx->venkat_k,
+                                                ctx->phi);
+        else
+          k_limiter<false><<<g, kBlock, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,
+                                                 ctx->q8[ctx->cur], ctx->dqdx, ctx->dqdy,
+                                                 ctx->dqdz, ctx->fcen, ctx->ccen, ctx->venkat_k,
+                                                 ctx->phi);
+        count_launch();
+      }
+      if (h.n_send) {
+        k_halo_pack_grad<<<grid_for(h.n_send), kBlock, 0, st>>>(
+            h.n_send, ctx->h_send, ctx->n, ctx->dqdx, ctx->dqdy, ctx->dqdz,
+            ctx->order >= 3 ? ctx->phi : nullptr, ctx->ccen, h.grad_send);
+        count_launch();
+      }
+      break;
+    }
     case MFG_HALO_FACE: {
+      const bool second = ctx->order >= 2;
+      if (second && h.n_recv) {  // the neighbours' rows from MFG_HALO_LIMIT
+        k_halo_unpack_grad<<<grid_for(h.n_recv), kBlock, 0, st>>>(
+            h.n_recv, ctx->h_recv, ctx->n, h.grad_recv, ctx->dqdx, ctx->dqdy, ctx->dqdz,
+            ctx->order >= 3 ? ctx->phi : nullptr, ctx->ccen);
+        count_launch();
+      }
       ctx->res_zero = true;
-      rc = launch_face(ctx, true, true, true, cfl_for(ctx->hp, iter_done), false);
+      rc = launch_face(ctx, true, true, true, cfl_for(ctx->hp, iter_done), false, !second);
       if (rc) return rc;
       k_norm_sums<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, h.norm_sq);
       count_launch();

@@ -456,6 +456,9 @@ class HaloBuffers:
 
         self.send_rows, self.recv_rows = buf(ns), buf(nr)
         self.node_send, self.node_recv = buf(nn), buf(nn)
+        # second order: gradient, limiter and centroid rows of 24 doubles
+        self.grad_send = torch.zeros((max(ns, 1), 24), dtype=torch.float64, device=self.device)
+        self.grad_recv = torch.zeros((max(nr, 1), 24), dtype=torch.float64, device=self.device)
         self.ext = torch.zeros(2, dtype=torch.int64, device=self.device)
         self.norm_sq = torch.zeros(5, dtype=torch.float64, device=self.device)
 
@@ -487,7 +490,8 @@ class HaloPart(HaloBuffers):
                 (lists.send_cells, lists.recv_bfaces, lists.nodes)]
         h.n_send, h.n_recv, h.n_node = (int(a.size) for a in keep)
         h.send_cells, h.recv_bfaces, h.nodes = (_lib.ptr(a, _lib.i32p) for a in keep)
-        for name in ("send_rows", "recv_rows", "node_send", "node_recv", "ext", "norm_sq"):
+        for name in ("send_rows", "recv_rows", "node_send", "node_recv", "ext", "norm_sq",
+                     "grad_send", "grad_recv"):
             setattr(h, name, ct.c_void_p(getattr(self, name).data_ptr()))
         lib = self.solver.lib
         _lib.check("mfg_set_stream", lib.mfg_set_stream(self.solver.ctx,
@@ -536,6 +540,9 @@ class LocalExchange:
 
     def nodes(self, parts: dict):
         self._pairs(parts, "node_send", "node_recv")
+
+    def grads(self, parts: dict):
+        self._pairs(parts, "grad_send", "grad_recv")
 
     @staticmethod
     def _pairs(parts, src, dst):
@@ -588,6 +595,9 @@ class DistExchange:
     def nodes(self, parts: dict):
         self._p2p(parts, "node_send", "node_recv")
 
+    def grads(self, parts: dict):
+        self._p2p(parts, "grad_send", "grad_recv")
+
     def extrema(self, parts: dict):
         import torch
         import torch.distributed as dist
@@ -615,6 +625,7 @@ class Decomposed:
         self.parts = dict(sorted(parts.items()))
         self.ex = exchange if exchange is not None else LocalExchange()
         self.iter_done = 0
+        self.order = 1
         self.streams = []
         for hp in self.parts.values():
             if all(hp.stream is not s for s in self.streams):
@@ -647,6 +658,14 @@ class Decomposed:
         self.ex.nodes(self.parts)
         self._each(_lib.HALO["gradient"])
 
+    def set_order(self, order: int, venkat_k: float = 5.0):
+        """The reference's `order` switch on every part (``mfg_set_order``):
+        second order reconstructs the interface ghosts' face states from the
+        neighbouring cells' gradients, limiters and centroids."""
+        for hp in self.parts.values():
+            hp.solver.set_order(order, venkat_k)
+        self.order = int(order)
+
     def iterate(self, n: int) -> np.ndarray:
         """n iterations; returns the residual norms of every iteration over
         all parts, [n][5]."""
@@ -658,6 +677,9 @@ class Decomposed:
         with self._on_streams():
             hist = torch.zeros((max(n, 1), 5), dtype=torch.float64, device=first.device)
             for i in range(n):
+                if self.order >= 2:
+                    self._each(H["limit"])
+                    self.ex.grads(self.parts)
                 self._each(H["face"])
                 self.ex.extrema(self.parts)
                 self._each(H["forward"])
