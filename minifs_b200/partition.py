@@ -115,6 +115,8 @@ def split(mesh: RawMesh, part_of, world: int) -> list[Part]:
         raise ValueError("part_of needs one entry per cell")
     if world < 1 or part_of.min(initial=0) < 0 or part_of.max(initial=0) >= world:
         raise ValueError("part numbers must lie in [0, world)")
+    if np.any(np.bincount(part_of, minlength=world) == 0):
+        raise ValueError("every part needs at least one cell")
     f2c = np.asarray(mesh.f2c, np.int64).reshape(-1, 2)
     nnpf = np.asarray(mesh.nnpf, np.int64)
     fptr = np.concatenate([[0], np.cumsum(nnpf)])

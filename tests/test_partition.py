@@ -90,6 +90,8 @@ def test_split_rejects_bad_maps():
         pa.split(m, np.full(m.n_cell, 2, np.int32), 2)
     with pytest.raises(ValueError):
         pa.slab_parts(10, 0)
+    with pytest.raises(ValueError):  # an empty part
+        pa.split(m, np.zeros(m.n_cell, np.int32), 2)
 
 
 @pytest.mark.parametrize("world,how", [(2, "slab"), (3, "scatter")])
