@@ -331,8 +331,8 @@ int mfg_set_dt_extrema(mfg_ctx *ctx, double dt_max, double dt_min);
  * path than one mesh does; one part with no neighbours gives mfg_iterate's
  * bits.  The node weights, marks and symmetry normals of the part's mesh
  * must be those of the whole mesh (the reference sums them over parts,
- * grid_polyhedra_auxiliary_functions.cpp:951-1047).  FP64, single-case
- * contexts only (MFG_ERR_UNSUPPORTED otherwise); a context with
+ * grid_polyhedra_auxiliary_functions.cpp:951-1047).  Single-case contexts
+ * only, FP64 or mixed (MFG_ERR_UNSUPPORTED for a batch); a context with
  * a halo refuses mfg_iterate, mfg_iterate_host, mfg_forward_lusgs,
  * mfg_calculate_gradient, mfg_profile_phases and mfg_autotune_sweeps. */
 typedef struct mfg_halo {

@@ -1372,6 +1372,26 @@ k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
                   q8, vol, dqdx, dqdy, dqdz);
 }
 
+// Mixed form of node_finish: the sums (deviations from the freestream) times
+// the reciprocal of the weight, then the symmetry-plane projection of the
+// velocity (of value = freestream + deviation).
+__device__ __forceinline__ void node_finish_mx(int32_t nd, int32_t info,
+                                               const double *__restrict__ wnode,
+                                               const double *__restrict__ nsym, const Params &P,
+                                               float acc[5]) {
+  const float rden = __fdividef(1.0f, (float)(wnode[nd] + kTiny));
+  for (int v = 0; v < 5; v++) acc[v] *= rden;
+  if (info & 2) {
+    const float xs = (float)nsym[3 * nd], ys = (float)nsym[3 * nd + 1], zs = (float)nsym[3 * nd + 2];
+    const float vn = acc[1] * xs + acc[2] * ys + acc[3] * zs +
+                     (float)(P.ref[1] * nsym[3 * nd] + P.ref[2] * nsym[3 * nd + 1] +
+                             P.ref[3] * nsym[3 * nd + 2]);
+    acc[1] -= vn * xs;
+    acc[2] -= vn * ys;
+    acc[3] -= vn * zs;
+  }
+}
+
 // Mixed form of the gradient: node values and Green-Gauss face sums in FP32
 // over the same loops as the FP64 kernels above, carried as deviations from
 // the freestream state (formed in FP64 from the FP64 records): the reference
@@ -1409,17 +1429,8 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
       for (int v = 0; v < 5; v++) acc[v] += (float)(qa[v] - P.ref[v]) * w;
     }
   }
-  const float rden = __fdividef(1.0f, (float)(wnode[nd] + kTiny));
-  for (int v = 0; v < 5; v++) acc[v] *= rden;
-  if (info & 2) {  // symmetry plane: remove the normal velocity (of value = ref + deviation)
-    const float xs = (float)nsym[3 * nd], ys = (float)nsym[3 * nd + 1], zs = (float)nsym[3 * nd + 2];
-    const float vn = acc[1] * xs + acc[2] * ys + acc[3] * zs +
-                     (float)(P.ref[1] * nsym[3 * nd] + P.ref[2] * nsym[3 * nd + 1] +
-                             P.ref[3] * nsym[3 * nd + 2]);
-    acc[1] -= vn * xs;
-    acc[2] -= vn * ys;
-    acc[3] -= vn * zs;
-  }
+  // a node shared with other parts keeps its partial sum (k_halo_nodes_mx)
+  if (!(info & 4)) node_finish_mx(nd, info, wnode, nsym, P, acc);
   float4 *o = reinterpret_cast<float4 *>(qn4 + (int64_t)nd * Q_STRIDE);
   o[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
   o[1] = make_float4(acc[4], 0.f, 0.f, 0.f);
@@ -1640,9 +1651,11 @@ __global__ void k_halo_gather(int32_t n, int32_t width, const int32_t *__restric
 
 // A packed buffer [n][8] into the listed rows of one or two arrays (words
 // below `width`).
+// (the mixed form's state records: also the single-precision mirrors fa, fb)
 __global__ void k_halo_scatter(int32_t n, int32_t width, const int32_t *__restrict__ rows,
                                const double *__restrict__ src, double *__restrict__ a,
-                               double *__restrict__ b) {
+                               double *__restrict__ b, float *__restrict__ fa,
+                               float *__restrict__ fb) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)n * Q_STRIDE) return;
   const int32_t i = (int32_t)(t / Q_STRIDE), k = (int32_t)(t % Q_STRIDE);
@@ -1651,6 +1664,17 @@ __global__ void k_halo_scatter(int32_t n, int32_t width, const int32_t *__restri
   const double v = src[t];
   a[o] = v;
   if (b) b[o] = v;
+  if (fa) fa[o] = (float)v;
+  if (fb) fb[o] = (float)v;
+}
+
+// Mixed form: single-precision node rows into a packed double buffer.
+__global__ void k_halo_gather_f(int32_t n, int32_t width, const int32_t *__restrict__ idx,
+                                const float *__restrict__ src, double *__restrict__ dst) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)n * Q_STRIDE) return;
+  const int32_t i = (int32_t)(t / Q_STRIDE), k = (int32_t)(t % Q_STRIDE);
+  dst[t] = k < width ? (double)src[(int64_t)idx[i] * Q_STRIDE + k] : 0.0;
 }
 
 // Second order across parts: a sent cell's gradient rows (x, y, z of the
@@ -1715,6 +1739,28 @@ __global__ void k_halo_nodes(int32_t nu, const int32_t *__restrict__ unodes,
     for (int v = 0; v < 5; v++) acc[v] += r[v];
   }
   node_finish(nd, ninfo[nd], wnode, nsym, acc);
+  for (int v = 0; v < 5; v++) o[v] = acc[v];
+}
+
+// Mixed form of k_halo_nodes (partial sums in single precision).
+__global__ void k_halo_nodes_mx(int32_t nu, const int32_t *__restrict__ unodes,
+                                const int32_t *__restrict__ eptr,
+                                const int32_t *__restrict__ eidx, const double *__restrict__ recv,
+                                const int32_t *__restrict__ ninfo,
+                                const double *__restrict__ wnode,
+                                const double *__restrict__ nsym, Params P,
+                                float *__restrict__ qn4) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nu) return;
+  const int32_t nd = unodes[i];
+  float *o = qn4 + (int64_t)nd * Q_STRIDE;
+  float acc[5];
+  for (int v = 0; v < 5; v++) acc[v] = o[v];
+  for (int32_t e = eptr[i]; e < eptr[i + 1]; e++) {
+    const double *r = recv + (int64_t)eidx[e] * Q_STRIDE;
+    for (int v = 0; v < 5; v++) acc[v] += (float)r[v];
+  }
+  node_finish_mx(nd, ninfo[nd], wnode, nsym, P, acc);
   for (int v = 0; v < 5; v++) o[v] = acc[v];
 }
 
@@ -4373,7 +4419,7 @@ int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host) {
 int mfg_halo_set(mfg_ctx *ctx, const mfg_halo *h) {
   if (!ctx || !h) return MFG_ERR_INVALID;
   if (ctx->halo) return MFG_ERR_INVALID;  // once per context
-  if (ctx->ncase != 1 || ctx->precision != MFG_PREC_FP64) return MFG_ERR_UNSUPPORTED;
+  if (ctx->ncase != 1) return MFG_ERR_UNSUPPORTED;
   if (ctx->order != 1 && h->n_send + h->n_recv > 0 && (!h->grad_send || !h->grad_recv))
     return MFG_ERR_UNSUPPORTED;  // second order needs the gradient rows' buffers
   if (h->n_send < 0 || h->n_recv < 0 || h->n_node < 0 || !h->ext || !h->norm_sq)
@@ -4446,10 +4492,10 @@ static void halo_gather(mfg_ctx *ctx, int32_t n, int32_t width, const int32_t *i
 }
 
 static void halo_scatter(mfg_ctx *ctx, int32_t n, int32_t width, const double *src, double *a,
-                         double *b) {
+                         double *b, float *fa = nullptr, float *fb = nullptr) {
   if (n == 0) return;
   k_halo_scatter<<<grid_for((int64_t)n * Q_STRIDE), kBlock, 0, ctx->stream>>>(
-      n, width, ctx->h_recv, src, a, b);
+      n, width, ctx->h_recv, src, a, b, fa, fb);
   count_launch();
 }
 
@@ -4520,13 +4566,28 @@ int mfg_halo_phase(mfg_ctx *ctx, int32_t phase, int32_t iter_done) {
       if (ctx->live_bc && (rc = launch_ghost_bc(ctx, st))) return rc;
       halo_gather(ctx, h.n_send, Q_STRIDE, ctx->h_send, ctx->q8[ctx->cur], h.send_rows);
       break;
-    case MFG_HALO_NODES:
-      halo_scatter(ctx, h.n_recv, Q_STRIDE, h.recv_rows, ctx->q8[0], ctx->q8[1]);
+    case MFG_HALO_NODES: {
+      const bool mx = ctx->precision == MFG_PREC_MIXED;
+      halo_scatter(ctx, h.n_recv, Q_STRIDE, h.recv_rows, ctx->q8[0], ctx->q8[1],
+                   mx ? ctx->q4[0] : nullptr, mx ? ctx->q4[1] : nullptr);
       launch_node_values(ctx, st);
-      halo_gather(ctx, h.n_node, 5, ctx->h_nodes, ctx->qn8, h.node_send);
+      if (!h.n_node) break;
+      if (mx) {
+        k_halo_gather_f<<<grid_for((int64_t)h.n_node * Q_STRIDE), kBlock, 0, st>>>(
+            h.n_node, 5, ctx->h_nodes, ctx->qn4, h.node_send);
+        count_launch();
+      } else {
+        halo_gather(ctx, h.n_node, 5, ctx->h_nodes, ctx->qn8, h.node_send);
+      }
       break;
+    }
     case MFG_HALO_GRADIENT:
-      if (ctx->h_nu) {
+      if (ctx->h_nu && ctx->precision == MFG_PREC_MIXED) {
+        k_halo_nodes_mx<<<grid_for(ctx->h_nu), kBlock, 0, st>>>(
+            ctx->h_nu, ctx->h_unodes, ctx->h_eptr, ctx->h_eidx, h.node_recv, ctx->ninfo,
+            ctx->wnode, ctx->nsym, ctx->P, ctx->qn4);
+        count_launch();
+      } else if (ctx->h_nu) {
         k_halo_nodes<<<grid_for(ctx->h_nu), kBlock, 0, st>>>(
             ctx->h_nu, ctx->h_unodes, ctx->h_eptr, ctx->h_eidx, h.node_recv, ctx->ninfo,
             ctx->wnode, ctx->nsym, ctx->qn8);

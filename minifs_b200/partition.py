@@ -511,7 +511,7 @@ class HaloPart(HaloBuffers):
 
 
 def build_parts(mesh: RawMesh, params, world: int, part_of=None, zones=None, device_of=None,
-                **bump) -> tuple:
+                precision: str = "fp64", **bump) -> tuple:
     """Split `mesh` (slabs unless `part_of` is given), prepare every part and
     create the contexts of `zones` (default: all), zone z on CUDA device
     ``device_of(z)`` (default 0).  Returns (parts, whole-mesh grid,
@@ -529,7 +529,8 @@ def build_parts(mesh: RawMesh, params, world: int, part_of=None, zones=None, dev
         if dev not in streams:
             streams[dev] = torch.cuda.Stream(device=dev)
         pt = parts[z]
-        held[z] = HaloPart(pgs[z], params, halo_lists(pt.mesh, pt.interfaces, z), streams[dev])
+        held[z] = HaloPart(pgs[z], params, halo_lists(pt.mesh, pt.interfaces, z), streams[dev],
+                           precision=precision)
     return parts, whole, held
 
 

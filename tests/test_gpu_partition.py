@@ -201,6 +201,39 @@ def test_second_order_across_parts(order):
     d.close()
 
 
+def test_mixed_form_across_parts():
+    """The mixed form (single-precision dissipation, gradient and off-diagonal
+    LU-SGS products; node partial sums exchanged in single precision): one
+    part is the fused mixed iteration bit for bit; 3 parts stay within the
+    mixed form's own rounding of the whole mesh's mixed iterations."""
+    m, p = _box(), _params()
+    _, _, held1 = pa.build_parts(m, p, 1, precision="mixed", **BUMP)
+    hp = held1[0]
+    d1 = pa.Decomposed(held1)
+    ref = Solver(gr.prepare(m, p, **BUMP), p, precision="mixed")
+    nr = ref.iterate(6)
+    n1 = d1.iterate(6)
+    for f in ("q", "res", "dq", "dqdx"):
+        assert_bitwise(hp.solver.download(f), ref.download(f), f"mixed one part {f}")
+    assert_bitwise(n1.reshape(-1), nr.reshape(-1), "mixed norms")
+    d1.close()
+    world = 3
+    parts, whole, held = pa.build_parts(m, p, world, part_of=pa.rcb_parts(m, world),
+                                        precision="mixed", **BUMP)
+    d = pa.Decomposed(held)
+    ref = Solver(gr.prepare(m, p, **BUMP), p, precision="mixed")
+    ref.calculate_gradient()
+    C = whole.n_cell
+    g, r = _cells(parts, d, "dqdx", C), ref.download("dqdx").reshape(5, -1)[:, :C]
+    for v in range(5):
+        np.testing.assert_allclose(g[v], r[v], rtol=0, atol=1e-5 * np.abs(r[v]).max())
+    nd, nr = d.iterate(1), ref.iterate(1)
+    np.testing.assert_allclose(nd, nr, rtol=1e-6)
+    nd, it_d = _to_drop(d.iterate, 1e-6, 3000)
+    assert np.all(np.isfinite(nd)) and nd[-1, 0] < 1e-6 * nd[0, 0], it_d
+    d.close()
+
+
 def test_halo_refusals_and_checks():
     m, p = _box(6), _params()
     parts, whole, d = _decomposed(m, p, 2)
@@ -232,7 +265,8 @@ def test_halo_refusals_and_checks():
     rb2 = np.array([parts[0].n_own_bface], np.int32)
     h.recv_bfaces = _lib.ptr(rb2, _lib.i32p)
     assert lib.mfg_halo_set(second.ctx, ct.byref(h)) == -6
-    mixed = Solver(gr.prepare(m, p, **BUMP), p, precision="mixed")
+    from minifs_b200.solver import BatchSolver
+    batch = BatchSolver([gr.prepare(m, p, **BUMP)] * 2, [p, p])
     h.n_recv = 0
-    assert lib.mfg_halo_set(mixed.ctx, ct.byref(h)) == -6
+    assert lib.mfg_halo_set(batch.ctx, ct.byref(h)) == -6  # one case per context
     d.close()
