@@ -137,72 +137,77 @@ def split(mesh: RawMesh, part_of, world: int) -> list[Part]:
         inner = fidx[interior & (p1 == p) & (p2 == p)]
         sides.append((own_b, cut_p, inner))
     # local boundary-face index of each cut face in each of its two parts
-    cut_local = {}
+    cut_local = np.full((world, F), -1, np.int64)
     for p, (own_b, cut_p, _) in enumerate(sides):
-        for k, f in enumerate(cut_p.tolist()):
-            cut_local[(p, f)] = own_b.size + k
+        cut_local[p, cut_p] = own_b.size + np.arange(cut_p.size)
     parts = []
     for p, (own_b, cut_p, inner) in enumerate(sides):
         cells = np.nonzero(part_of == p)[0]
         local = np.full(mesh.n_cell, -1, np.int64)
         local[cells] = np.arange(cells.size)
         faces = np.concatenate([own_b, cut_p, inner])
+        turned = np.zeros(faces.size, bool)
+        ncut = cut_p.size
+        cs = slice(own_b.size, own_b.size + ncut)
+        turned[cs] = p1[cut_p] != p  # inner cell on the right: turned round
+        inner_c = np.where(turned[cs], c2[cut_p], c1[cut_p])
+        outer_c = np.where(turned[cs], c1[cut_p], c2[cut_p])
         lf2c = np.empty((faces.size, 2), np.int64)
-        nodes_of = []
-        nbz, nbf, ocell = [], [], []
-        for i, f in enumerate(faces.tolist()):
-            nd = f2n[fptr[f]:fptr[f + 1]]
-            a, b = int(c1[f]), int(c2[f])
-            if f < G:
-                lf2c[i] = (local[a], b)
-            elif p1[f] == p and p2[f] == p:
-                lf2c[i] = (local[a], local[b])
-            else:
-                other = int(p2[f]) if p1[f] == p else int(p1[f])
-                if p1[f] != p:  # inner cell on the right: turned round
-                    nd = np.concatenate([nd[:1], nd[1:][::-1]])
-                    a, b = b, a
-                lf2c[i] = (local[a], -iface_patch)
-                nbz.append(other)
-                nbf.append(cut_local[(other, f)])
-                ocell.append(b)
-            nodes_of.append(nd)
-        allnodes = np.concatenate(nodes_of) if nodes_of else np.zeros(0, np.int64)
+        lf2c[:own_b.size, 0] = local[c1[own_b]]
+        lf2c[:own_b.size, 1] = c2[own_b]
+        lf2c[cs, 0] = local[inner_c]
+        lf2c[cs, 1] = -iface_patch
+        lf2c[own_b.size + ncut:, 0] = local[c1[inner]]
+        lf2c[own_b.size + ncut:, 1] = local[c2[inner]]
+        other = np.where(turned[cs], p1[cut_p], p2[cut_p])
+        # node lists: each face's nodes, a turned face's after its first node
+        # reversed
+        cnt = nnpf[faces]
+        start = fptr[faces]
+        optr = np.concatenate([[0], np.cumsum(cnt)])
+        pos = np.arange(optr[-1]) - np.repeat(optr[:-1], cnt)   # position within the face
+        rev = np.where(pos == 0, 0, np.repeat(cnt, cnt) - pos)  # reversed position
+        src = np.repeat(start, cnt) + np.where(np.repeat(turned, cnt), rev, pos)
+        allnodes = f2n[src]
         used = np.unique(allnodes)
         nmap = np.full(mesh.n_node, -1, np.int64)
         nmap[used] = np.arange(used.size)
         raw = RawMesh(x=np.ascontiguousarray(mesh.x[used], np.float64),
                       y=np.ascontiguousarray(mesh.y[used], np.float64),
                       z=np.ascontiguousarray(mesh.z[used], np.float64),
-                      nnpf=np.array([v.size for v in nodes_of], np.int32),
+                      nnpf=cnt.astype(np.int32),
                       f2n=nmap[allnodes].astype(np.int32),
                       f2c=lf2c.reshape(-1).astype(np.int32),
-                      n_cell=int(cells.size), n_bface=int(own_b.size + cut_p.size),
+                      n_cell=int(cells.size), n_bface=int(own_b.size + ncut),
                       patches=list(mesh.patches) + [(iface_patch, INTERFACE)])
-        parts.append(Part(mesh=raw, interfaces=Interfaces(nbz=np.array(nbz, np.int32),
-                                                          nbf=np.array(nbf, np.int32)),
+        parts.append(Part(mesh=raw,
+                          interfaces=Interfaces(nbz=other.astype(np.int32),
+                                                nbf=cut_local[other, cut_p].astype(np.int32)),
                           rank=p, cells=cells.astype(np.int32), nodes=used.astype(np.int32),
-                          bfaces=own_b.astype(np.int32), iface_cells=np.array(ocell, np.int32),
+                          bfaces=own_b.astype(np.int32), iface_cells=outer_c.astype(np.int32),
                           n_own_bface=int(own_b.size)))
     # the node half of the interface block: every node shared with another
-    # part, once per such part, with its index there
-    holders = {}
+    # part, once per such part, with its index there, ordered by (zone,
+    # own index, index there)
+    zone = np.concatenate([np.full(pt.nodes.size, pt.rank, np.int64) for pt in parts])
+    lidx = np.concatenate([np.arange(pt.nodes.size, dtype=np.int64) for pt in parts])
+    glob = np.concatenate([pt.nodes.astype(np.int64) for pt in parts])
+    order = np.lexsort((zone, glob))  # by node, then zone
+    glob, zone, lidx = glob[order], zone[order], lidx[order]
+    first = np.concatenate([[0], np.nonzero(np.diff(glob))[0] + 1])
+    mult = np.diff(np.concatenate([first, [glob.size]]))
+    ent = [[] for _ in range(world)]
+    for f0, m in zip(first[mult > 1].tolist(), mult[mult > 1].tolist()):
+        zs, ls = zone[f0:f0 + m].tolist(), lidx[f0:f0 + m].tolist()
+        for a_ in range(m):
+            for b_ in range(m):
+                if a_ != b_:
+                    ent[zs[a_]].append((zs[b_], ls[a_], ls[b_]))
     for pt in parts:
-        for i, g in enumerate(pt.nodes.tolist()):
-            holders.setdefault(g, []).append((pt.rank, i))
-    sn = [[] for _ in range(world)]
-    for g, hs in holders.items():
-        if len(hs) < 2:
-            continue
-        for p, i in hs:
-            for r, j in hs:
-                if r != p:
-                    sn[p].append((r, i, j))
-    for pt in parts:
-        e = sorted(sn[pt.rank])
-        pt.interfaces.nbsn = np.array([i for _, i, _ in e], np.int32)
-        pt.interfaces.nbzn = np.array([r for r, _, _ in e], np.int32)
-        pt.interfaces.nbrn = np.array([j for _, _, j in e], np.int32)
+        e = np.array(sorted(ent[pt.rank]), np.int64).reshape(-1, 3)
+        pt.interfaces.nbsn = e[:, 1].astype(np.int32)
+        pt.interfaces.nbzn = e[:, 0].astype(np.int32)
+        pt.interfaces.nbrn = e[:, 2].astype(np.int32)
     return parts
 
 
@@ -337,19 +342,19 @@ def zone_node_data(pgs: dict, lists: dict, exchange, device="cpu") -> None:
         fptr = np.concatenate([[0], np.cumsum(nnpf)])
         f2n = np.asarray(A["f2n"], np.int64)
         kind = _face_kinds(A["bctype"][:G])
+        # per boundary-face node: its face (faces and their nodes in order)
+        bface = np.repeat(np.arange(G), nnpf[:G])
+        bnode = f2n[:fptr[G]]
         has = np.zeros((N, 3))
+        k = kind[bface]
+        has[bnode[k > 0], k[k > 0] - 1] = 1.0
         sym = np.zeros((N, 5))  # flag, sums of the normals, face count
-        for i in range(G):
-            nodes = f2n[fptr[i]:fptr[i + 1]]
-            if kind[i]:
-                has[nodes, kind[i] - 1] = 1.0
-            if A["bctype"][i] == 4:
-                for nd in nodes.tolist():  # FindNodeSYMM's loop order
-                    sym[nd, 0] = 1.0
-                    sym[nd, 1] += A["xfn"][i]
-                    sym[nd, 2] += A["yfn"][i]
-                    sym[nd, 3] += A["zfn"][i]
-                    sym[nd, 4] += 1.0
+        s4 = np.asarray(A["bctype"][:G])[bface] == 4
+        sym[bnode[s4], 0] = 1.0
+        # np.add.at adds in index order: FindNodeSYMM's loop order
+        for col, name in ((1, "xfn"), (2, "yfn"), (3, "zfn")):
+            np.add.at(sym[:, col], bnode[s4], np.asarray(A[name])[bface[s4]])
+        np.add.at(sym[:, 4], bnode[s4], 1.0)
         geo[z] = (fptr, f2n, kind, has, sym)
     recv = swap({z: np.concatenate([g[3], g[4]], 1)[lists[z].nodes] for z, g in geo.items()})
     marks = {}
@@ -383,16 +388,18 @@ def zone_node_data(pgs: dict, lists: dict, exchange, device="cpu") -> None:
         mark = marks[z]
         w = np.zeros(pg.n_node)
         wb = np.asarray(A["wbface"])
+        G = pg.n_bface
+        bface = np.repeat(np.arange(G), np.diff(fptr[:G + 1]))
+        bnode = f2n[:fptr[G]]
+        # the passes' order: wall faces, far-field faces, the others, each in
+        # face order; a node takes the faces of its mark's kind only
         for kd in (1, 2, 3):
-            for i in np.nonzero(kind == kd)[0].tolist():
-                for j in range(fptr[i], fptr[i + 1]):
-                    nd = f2n[j]
-                    if mark[nd] == _KIND_MARK[kd]:
-                        w[nd] += wb[j]
+            sel = (kind[bface] == kd) & (mark[bnode] == _KIND_MARK[kd])
+            np.add.at(w, bnode[sel], wb[:fptr[G]][sel])
         c2n = np.asarray(A["c2n"], np.int64)
         wc = np.asarray(A["wc2n"])
-        for k in np.nonzero(mark[c2n] == 0)[0].tolist():
-            w[c2n[k]] += wc[k]
+        sel = mark[c2n] == 0
+        np.add.at(w, c2n[sel], wc[sel])
         part[z] = w
     recv = swap({z: part[z][lists[z].nodes][:, None] for z in pgs})
     for z, pg in pgs.items():
