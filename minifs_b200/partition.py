@@ -41,11 +41,6 @@ class Part:
     iface_cells: np.ndarray  # whole-mesh cell on the other side of each interface face
     n_own_bface: int = 0     # boundary faces before the interface faces
 
-    @property
-    def iface_bfaces(self) -> np.ndarray:
-        """Local boundary-face index of each interface face."""
-        return np.arange(self.n_own_bface, self.mesh.n_bface, dtype=np.int32)
-
 
 def slab_parts(n_cell: int, world: int) -> np.ndarray:
     """Part of every cell: `world` contiguous, balanced ranges of the cell
