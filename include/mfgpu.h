@@ -468,6 +468,19 @@ int mfg_bc_read(const char *path, int32_t cap, int32_t *n_patch, int32_t *patch_
 int mfg_bc_write(const char *path, int32_t n_patch, const int32_t *patch_id,
                  const int32_t *type);
 
+/* Checkpoint of a run (no counterpart in the reference, which has none):
+ * the whole solver state between iterations -- the states of cells and
+ * ghosts q [5n] (mfg_download of MFG_FIELD_Q), the iteration count that
+ * sets the CFL ramp, and the running dt extrema (mfg_get_dt_extrema).  A
+ * context restored from it (mfg_upload, mfg_set_dt_extrema, the count
+ * passed on) continues with the bits of the uninterrupted run.  Read checks
+ * the magic word, the sizes against n_cell / n (MFG_ERR_INVALID for
+ * another grid) and the length (MFG_ERR_IO). */
+int mfg_checkpoint_write(const char *path, int64_t n_cell, int64_t n, int32_t iter_done,
+                         double dt_max, double dt_min, const double *q);
+int mfg_checkpoint_read(const char *path, int64_t n_cell, int64_t n, int32_t *iter_done,
+                        double *dt_max, double *dt_min, double *q);
+
 /* ---- the same preprocessing on a GPU ------------------------------------ */
 /* ComputeMetrics, CalnNPC/CalC2N, ComputeWeight3D_Node and FindNodeSYMM run
  * on `device`: every output is bit-identical to mfg_prep_metrics,

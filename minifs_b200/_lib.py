@@ -191,6 +191,10 @@ def load(build_if_missing: bool = True):
         "mfg_mfl_free": (ct.c_int, [ct.POINTER(Mfl)]),
         "mfg_bc_read": (ct.c_int, [ct.c_char_p, ct.c_int32, i32p, i32p, i32p]),
         "mfg_bc_write": (ct.c_int, [ct.c_char_p, ct.c_int32, i32p, i32p]),
+        "mfg_checkpoint_write": (ct.c_int, [ct.c_char_p, ct.c_int64, ct.c_int64, ct.c_int32,
+                                            ct.c_double, ct.c_double, f64p]),
+        "mfg_checkpoint_read": (ct.c_int, [ct.c_char_p, ct.c_int64, ct.c_int64,
+                                           ct.POINTER(ct.c_int32), f64p, f64p, f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -204,6 +204,48 @@ int mfg_bc_read(const char *path, int32_t cap, int32_t *n_patch, int32_t *patch_
   return MFG_OK;
 }
 
+// Checkpoint file: "MFGCKPT1", int64 n_cell, int64 n (cells + ghosts), int32
+// iter_done, int32 0, double dt_max, double dt_min, double q[5 n].
+static const char kCkptMagic[8] = {'M', 'F', 'G', 'C', 'K', 'P', 'T', '1'};
+
+int mfg_checkpoint_write(const char *path, int64_t n_cell, int64_t n, int32_t iter_done,
+                         double dt_max, double dt_min, const double *q) {
+  if (!path || n_cell < 0 || n < n_cell || iter_done < 0 || (n > 0 && !q))
+    return MFG_ERR_INVALID;
+  File f(fopen(path, "wb"));
+  if (!f.fp) return MFG_ERR_IO;
+  const int32_t pad = 0;
+  if (!write_n(f.fp, kCkptMagic, 8) || !write_n(f.fp, &n_cell, 1) || !write_n(f.fp, &n, 1) ||
+      !write_n(f.fp, &iter_done, 1) || !write_n(f.fp, &pad, 1) || !write_n(f.fp, &dt_max, 1) ||
+      !write_n(f.fp, &dt_min, 1) || !write_n(f.fp, q, 5 * n))
+    return MFG_ERR_IO;
+  if (fflush(f.fp) != 0) return MFG_ERR_IO;
+  return MFG_OK;
+}
+
+int mfg_checkpoint_read(const char *path, int64_t n_cell, int64_t n, int32_t *iter_done,
+                        double *dt_max, double *dt_min, double *q) {
+  if (!path || n_cell < 0 || n < n_cell || !iter_done || !dt_max || !dt_min || (n > 0 && !q))
+    return MFG_ERR_INVALID;
+  File f(fopen(path, "rb"));
+  if (!f.fp) return MFG_ERR_IO;
+  char magic[8];
+  int64_t fc = -1, fn = -1;
+  int32_t it = -1, pad = 0;
+  double mx = 0.0, mn = 0.0;
+  if (!read_n(f.fp, magic, 8) || std::memcmp(magic, kCkptMagic, 8) != 0 ||
+      !read_n(f.fp, &fc, 1) || !read_n(f.fp, &fn, 1) || !read_n(f.fp, &it, 1) ||
+      !read_n(f.fp, &pad, 1) || !read_n(f.fp, &mx, 1) || !read_n(f.fp, &mn, 1))
+    return MFG_ERR_IO;
+  if (fc != n_cell || fn != n || it < 0) return MFG_ERR_INVALID;  // another grid
+  if (remaining(f.fp) != 40 * n) return MFG_ERR_IO;
+  if (!read_n(f.fp, q, 5 * n)) return MFG_ERR_IO;
+  *iter_done = it;
+  *dt_max = mx;
+  *dt_min = mn;
+  return MFG_OK;
+}
+
 int mfg_bc_write(const char *path, int32_t n_patch, const int32_t *patch_id,
                  const int32_t *type) {
   if (!path || n_patch < 0 || (n_patch > 0 && (!patch_id || !type))) return MFG_ERR_INVALID;

@@ -207,6 +207,30 @@ class Solver:
         self._call("mfg_download", _lib.FIELD[field], _lib.ptr(out))
         return out
 
+    def save_checkpoint(self, path):
+        """The solver state between iterations (state, iteration count, dt
+        extrema) to `path` (``mfg_checkpoint_write``)."""
+        import os
+        q = self.download("q")
+        mx, mn = self.dt_extrema()
+        _lib.check("mfg_checkpoint_write", self.lib.mfg_checkpoint_write(
+            os.fsencode(os.fspath(path)), self.grid.n_cell, self.grid.n, int(self.iter_done),
+            float(mx), float(mn), _lib.ptr(q)))
+
+    def load_checkpoint(self, path):
+        """Restore a state saved by ``save_checkpoint`` on the same grid: the
+        run continues with the bits it would have had uninterrupted."""
+        import os
+        q = np.empty(5 * self.grid.n)
+        it = ct.c_int32(0)
+        mx, mn = ct.c_double(0.0), ct.c_double(0.0)
+        _lib.check("mfg_checkpoint_read", self.lib.mfg_checkpoint_read(
+            os.fsencode(os.fspath(path)), self.grid.n_cell, self.grid.n, ct.byref(it),
+            ct.byref(mx), ct.byref(mn), _lib.ptr(q)))
+        self.upload_q(q)
+        self._call("mfg_set_dt_extrema", mx.value, mn.value)
+        self.iter_done = int(it.value)
+
     def upload_q(self, q: np.ndarray):
         q = np.ascontiguousarray(q, np.float64)
         self._call("mfg_upload", _lib.FIELD["q"], _lib.ptr(q))
