@@ -46,3 +46,10 @@ def test_error_strings_and_host_only_calls():
         assert abs(getattr(p, k) - v) <= 5e-6 * abs(v), (k, getattr(p, k), v)
     assert lib.mfg_destroy(None) == -1
     assert lib.mfg_create(None, None, None, 0, 0, None) == -1
+    # the allocation-free norm validates its arguments before any device call
+    # (the address below is never dereferenced)
+    assert lib.mfg_residual_norm_static(None, 10, None, None) == -1
+    addr = ctypes.c_void_p(256)
+    assert lib.mfg_residual_norm_static(addr, -1, addr, None) == -1
+    assert lib.mfg_residual_norm_static(addr, (1 << 24) + 1, addr, None) == -1
+    assert b"exceeds the static scratch limit" in lib.mfg_last_cuda_error()
