@@ -8,11 +8,15 @@
 //
 //   minifs_kat roe   <in> <out>   RoeFlux_noprec (cal_flux.cpp:301-834)
 //   minifs_kat lusgs <in> <out>   FluxLUSGS3D (forward_lusgs.cpp:1271-1324)
+//   minifs_kat update <in> <out>  UpdateFlowField3D_CFL3d (forward_lusgs.cpp:1335-1488)
 //
 // <in> is raw float64.  roe: len, gam, p_bar, alf_l, then ql[5][len],
 // qr[5][len], xfn[len], yfn[len], zfn[len], area[len] (SoA, as the
 // reference's face chunks); <out> is flux[5][len].  lusgs: len, gam, p_bar,
 // lhs_omga, then per case q[5], dq[5], n[3]; <out> is flux[5] per case.
+// update: len (cells), gam, p_bar, unused, then rho_s, rho_min, rho_max,
+// p_min, p_max, q[5][len] (primitive), DQ[5][len]; <out> is the updated
+// q[5][len] (a grid of len cells and no ghosts).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -85,6 +89,33 @@ int main(int argc, char **argv) {
       FluxLUSGS3D(flux, q, dq, n, gam, p_bar, lhs);
       for (int k = 0; k < 5; k++) out[5 * i + k] = flux[k];
     }
+  } else if (!strcmp(argv[1], "update")) {
+    if (in.size() != 9 + 10 * (size_t)len) { fprintf(stderr, "bad update input size\n"); return 2; }
+    rho_s = d[0];
+    rho_min = d[1];
+    rho_max = d[2];
+    p_min = d[3];
+    p_max = d[4];
+    const double *q = d + 5, *dq = d + 5 + 5 * len;
+    // the grid owns its state arrays (new[]); never freed: the process ends
+    PolyGrid *grid = new PolyGrid();
+    grid->SetNTCell((IntType)len);
+    grid->SetNBFace(0);
+    RealFlow *prim[5], *DQ[5];
+    for (int k = 0; k < 5; k++) {
+      prim[k] = new RealFlow[len];
+      DQ[k] = new RealFlow[len];
+      memcpy(prim[k], q + k * len, len * sizeof(double));
+      memcpy(DQ[k], dq + k * len, len * sizeof(double));
+    }
+    grid->SetRho(prim[0]);
+    grid->SetU(prim[1]);
+    grid->SetV(prim[2]);
+    grid->SetW(prim[3]);
+    grid->SetP(prim[4]);
+    UpdateFlowField3D_CFL3d(grid, DQ);
+    out.resize(5 * len);
+    for (int k = 0; k < 5; k++) memcpy(out.data() + k * len, prim[k], len * sizeof(double));
   } else {
     fprintf(stderr, "unknown mode %s\n", argv[1]);
     return 2;

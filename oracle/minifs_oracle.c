@@ -394,8 +394,15 @@ void mfo_forward_lusgs(const mfo_grid *g, const mfo_params *p, mfo_state *s) {
   free(ptr);
   free(c2f);
 
-  /* UpdateFlowField3D_CFL3d */
-  double *qr = s->q, *qu = s->q + n, *qv = s->q + 2 * n, *qw = s->q + 3 * n, *qp = s->q + 4 * n;
+  mfo_update_flow(p, C, n, s->q, DQ);
+}
+
+/* UpdateFlowField3D_CFL3d (forward_lusgs.cpp:1335-1488): the conservative
+ * update of the C cells of q [5][n] by DQ [5][n], with the density and
+ * pressure relaxation and the clamps; ghosts untouched. */
+void mfo_update_flow(const mfo_params *p, int32_t C, int64_t n, double *q,
+                     const double *DQ) {
+  double *qr = q, *qu = q + n, *qv = q + 2 * n, *qw = q + 3 * n, *qp = q + 4 * n;
   const double gam1 = p->gam - 1.;
   const double p00 = p->p_bar;
   const double alpq = -0.2, phiq = 1. / 0.5;

@@ -72,6 +72,9 @@ void mfo_iterate(const mfo_grid *g, const mfo_params *p, mfo_state *s, int32_t n
 /* One matrix-free LU-SGS flux (forward_lusgs.cpp:1271-1324), for unit tests. */
 void mfo_flux_lusgs(double flux[5], const double q[5], const double dq[5], const double n[3],
                     double gam, double p_bar, double lhs_omga);
+/* UpdateFlowField3D_CFL3d (forward_lusgs.cpp:1335-1488) on the first C cells
+ * of q [5][n] (primitive) with DQ [5][n] (conservative), for unit tests. */
+void mfo_update_flow(const mfo_params *p, int32_t C, int64_t n, double *q, const double *DQ);
 /* One Roe face flux with the 1/2*area factor (cal_flux.cpp:676-834). */
 void mfo_roe_flux(double flux[5], const double ql[5], const double qr[5], double nx, double ny,
                   double nz, double area, double gam, double gamm1, double p_bar, double alf_l);

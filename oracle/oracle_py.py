@@ -67,6 +67,8 @@ def load():
     lib.mfo_flux_lusgs.argtypes = [_f64p, _f64p, _f64p, _f64p, ct.c_double, ct.c_double,
                                    ct.c_double]
     lib.mfo_roe_flux.argtypes = [_f64p, _f64p, _f64p] + [ct.c_double] * 8
+    lib.mfo_update_flow.argtypes = [ct.POINTER(_Params), ct.c_int32, ct.c_int64, _f64p, _f64p]
+    lib.mfo_update_flow.restype = None
     _lib = lib
     return lib
 
@@ -178,4 +180,19 @@ def flux_lusgs(q, dq, n, gam, p_bar, lhs_omga):
     nn = np.ascontiguousarray(n, np.float64)
     lib.mfo_flux_lusgs(_p(out, _f64p), _p(q, _f64p), _p(dq, _f64p), _p(nn, _f64p), gam, p_bar,
                        lhs_omga)
+    return out
+
+
+def update_flow(q, dq, params):
+    """UpdateFlowField3D_CFL3d on every cell of q [5][C] (primitive, no
+    ghosts) with dq [5][C]; ``params`` maps gam, p_bar, rho_min, rho_max,
+    p_min, p_max to values.  Returns the updated copy of q."""
+    lib = load()
+    pr = _Params()
+    for k, v in params.items():
+        setattr(pr, k, v)
+    out = np.array(q, np.float64, order="C", copy=True)
+    dq = np.ascontiguousarray(dq, np.float64)
+    C = out.shape[1]
+    lib.mfo_update_flow(ct.byref(pr), C, C, _p(out, _f64p), _p(dq, _f64p))
     return out

@@ -4,8 +4,9 @@ functions on inputs chosen to reach each of their branches.
 Runs ``oracle/_ref/minifs_kat`` (oracle/kat_harness.cpp linked with the
 unmodified MiniFS sources, built by ``make -C oracle ref``), which calls
 ``RoeFlux_noprec`` (cal_flux.cpp:301-834) on a chunk of faces and
-``FluxLUSGS3D`` (forward_lusgs.cpp:1271-1324) case by case, and stores the
-inputs with the reference's outputs.  Usage:  python tests/golden/make_kats.py
+``FluxLUSGS3D`` (forward_lusgs.cpp:1271-1324) case by case and
+``UpdateFlowField3D_CFL3d`` (forward_lusgs.cpp:1335-1488) on a grid of
+loose cells, and stores the inputs with the reference's outputs.  Usage:  python tests/golden/make_kats.py
 
 Face groups of the Roe cases (each with random unit normals unless noted):
   random      subsonic states with moderate jumps
@@ -17,6 +18,9 @@ Face groups of the Roe cases (each with random unit normals unless noted):
   jump        density ratio up to 5, pressure ratio up to 10 across the face
   equal       identical states on both sides
   axis        normals along +-x, +-y, +-z (zero components)
+Cell groups of the update cases: small increments, density drops and
+pressure drops beyond 20% (the relaxation branches), both at once, and
+increments past rho_max and p_max (the clamps).
 Two parameter sets: Mach 0.5 with the reference's epsa_r = 0.1, and Mach
 0.8395 with epsa_r = 0 (no entropy fix at all).
 """
@@ -105,6 +109,35 @@ def lusgs_inputs(rng, p, n=600):
     return np.column_stack([q, dq, nh])
 
 
+UPDATE_GROUPS = ("small", "rho_drop", "p_drop", "both_drop", "rho_high", "p_high")
+
+
+def update_inputs(rng, p, per=100):
+    """q [5][C] primitive states and DQ [5][C] conservative increments."""
+    G = len(UPDATE_GROUPS)
+    C = per * G
+    grp = np.repeat(np.arange(G, dtype=np.int32), per)
+    rho = p.rho_s * rng.uniform(0.5, 2.0, C)
+    pa = p.p_bar * rng.uniform(0.5, 2.0, C)
+    vel = 0.8 * p.ainf * rng.uniform(-1, 1, (C, 3))
+    e = pa / (p.gam - 1) + 0.5 * rho * (vel ** 2).sum(1)
+    cons = np.column_stack([rho, rho[:, None] * vel, e])
+    dq = cons * 1e-3 * rng.uniform(-1, 1, (C, 5))
+    drop = rng.uniform(0.25, 0.95, C)
+    for g, name in enumerate(UPDATE_GROUPS):
+        s = grp == g
+        if name in ("rho_drop", "both_drop"):
+            dq[s, 0] = -drop[s] * rho[s]
+        if name in ("p_drop", "both_drop"):
+            dq[s, 4] = -drop[s] * pa[s] / (p.gam - 1)
+        if name == "rho_high":
+            dq[s, 0] = (p.rho_max / rho[s]) * rng.uniform(1.5, 3.0, s.sum()) * rho[s]
+        if name == "p_high":
+            dq[s, 4] = (p.p_max + p.p_bar) * rng.uniform(1.5, 3.0, s.sum()) / (p.gam - 1)
+    q = np.vstack([rho, vel.T, pa - p.p_bar])
+    return q, np.ascontiguousarray(dq.T), grp
+
+
 def run(mode, head, body):
     with tempfile.TemporaryDirectory() as d:
         fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
@@ -127,6 +160,13 @@ def main():
         flux = run("roe", [F, p.gam, p.p_bar, epsa_r], body).reshape(5, F)
         cases = lusgs_inputs(rng, p)
         lflux = run("lusgs", [len(cases), p.gam, p.p_bar, lhs], cases).reshape(-1, 5)
+        uq, udq, ugrp = update_inputs(rng, p)
+        C = uq.shape[1]
+        lim = [p.rho_s, p.rho_min, p.rho_max, p.p_min, p.p_max]
+        uq_out = run("update", [C, p.gam, p.p_bar, 0.0],
+                     np.concatenate([lim, uq.ravel(), udq.ravel()])).reshape(5, C)
+        out.update({f"s{s}_update_q": uq, f"s{s}_update_dq": udq, f"s{s}_update_group": ugrp,
+                    f"s{s}_update_limits": np.array(lim), f"s{s}_update_out": uq_out})
         out.update({f"s{s}_params": np.array([mach, epsa_r, lhs, p.gam, p.p_bar]),
                     f"s{s}_ql": ql, f"s{s}_qr": qr, f"s{s}_normal": nrm, f"s{s}_area": area,
                     f"s{s}_group": grp, f"s{s}_roe_flux": flux,

@@ -1,9 +1,11 @@
 """Known answers of single reference functions (tests/golden/make_kats.py:
-RoeFlux_noprec, cal_flux.cpp:301-834, and FluxLUSGS3D,
-forward_lusgs.cpp:1271-1324, called directly on inputs chosen to reach the
+RoeFlux_noprec, cal_flux.cpp:301-834, FluxLUSGS3D,
+forward_lusgs.cpp:1271-1324, and UpdateFlowField3D_CFL3d,
+forward_lusgs.cpp:1335-1488, called directly on inputs chosen to reach the
 entropy fix's branches, sonic and supersonic faces, strong jumps, equal
-states, axis-aligned normals and zero increments) against the CPU oracle's
-per-face functions: bit for bit."""
+states, axis-aligned normals, zero increments, the update's density and
+pressure relaxation and its clamps) against the CPU oracle's functions:
+bit for bit."""
 import os
 
 import numpy as np
@@ -56,3 +58,26 @@ def test_flux_lusgs_matches_reference(kats, s):
     assert np.isfinite(ref).all()
     assert (np.abs(cases[:, 5:10]).sum(1) == 0).any()  # zero increments are among the cases
     assert_bitwise(got.ravel(), ref.ravel(), f"set {s} FluxLUSGS3D")
+
+
+UPDATE_GROUPS = ("small", "rho_drop", "p_drop", "both_drop", "rho_high", "p_high")
+
+
+@pytest.mark.parametrize("s", [0, 1])
+def test_update_flow_matches_reference(kats, s):
+    from oracle import oracle_py
+    _, _, _, gam, p_bar = kats[f"s{s}_params"]
+    rho_s, rho_min, rho_max, p_min, p_max = kats[f"s{s}_update_limits"]
+    q, dq, grp = kats[f"s{s}_update_q"], kats[f"s{s}_update_dq"], kats[f"s{s}_update_group"]
+    ref = kats[f"s{s}_update_out"]
+    got = oracle_py.update_flow(q, dq, dict(gam=gam, p_bar=p_bar, rho_s=rho_s, rho_min=rho_min,
+                                            rho_max=rho_max, p_min=p_min, p_max=p_max))
+    for g, name in enumerate(UPDATE_GROUPS):
+        sel = grp == g
+        assert_bitwise(got[:, sel].ravel(), ref[:, sel].ravel(), f"set {s} update {name}")
+    # the groups reach their branches: relaxed density drops are smaller
+    # than the raw increment, and the high groups end on the clamps
+    sel = (grp == 1) | (grp == 3)
+    assert (ref[0, sel] > q[0, sel] + dq[0, sel]).all()
+    assert (ref[0, grp == 4] == rho_max).all()
+    assert (ref[4, grp == 5] == p_max).all()
