@@ -212,7 +212,7 @@ class Solver:
         extrema) to `path` (``mfg_checkpoint_write``)."""
         import os
         q = self.download("q")
-        mx, mn = self.dt_extrema()
+        mx, mn = self.dt_extrema
         _lib.check("mfg_checkpoint_write", self.lib.mfg_checkpoint_write(
             os.fsencode(os.fspath(path)), self.grid.n_cell, self.grid.n, int(self.iter_done),
             float(mx), float(mn), _lib.ptr(q)))

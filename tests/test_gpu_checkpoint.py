@@ -30,4 +30,4 @@ def test_resume_is_bit_identical(tmp_path, precision):
     for f in ("q", "res", "dq", "dqdx"):
         assert_bitwise(resumed.download(f), straight.download(f), f"{precision} {f}")
     assert_bitwise(n_rest.reshape(-1), n_all[4:].reshape(-1), f"{precision} norms")
-    assert resumed.dt_extrema() == straight.dt_extrema()
+    assert resumed.dt_extrema == straight.dt_extrema
