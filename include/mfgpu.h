@@ -113,6 +113,12 @@ typedef struct mfg_info {
   int32_t sweep_chunks;             /* persistent sweeps: chunks (= resident blocks) */
   int32_t sweep_lanes;              /* persistent sweeps: lanes per cell */
   int32_t sweep_records;            /* persistent sweeps: record slots per cell (4 or 8) */
+  int32_t sweep_chunking;           /* persistent sweeps: chunk assignment (MFG_CHUNK_*) */
+  /* records of the [forward, backward] sweep whose neighbour increment is
+   * read from the block's shared-memory ring, from global memory (same
+   * chunk, older than the ring) and from another chunk (polled in L2) */
+  int32_t sweep_ring_records[2], sweep_global_records[2], sweep_cross_records[2];
+  double sweep_model_us[2];         /* modelled duration of each sweep with its chunks */
 } mfg_info;
 
 /* ---- parameters -------------------------------------------------------- */
@@ -163,10 +169,24 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info);
  * waits, with a bounded spin, for that neighbour's ready flag.  Both modes
  * give identical results. */
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode);
-/* Persistent sweeps: lanes per cell, either the record slots per cell W
- * (shortest latency per cell) or W / 2 (twice the cells per pass over a
- * wide level).  Results are identical either way. */
+/* Persistent sweeps: lanes per cell; the record slots per cell W is the
+ * only value the current kernels take (others: MFG_ERR_UNSUPPORTED). */
 int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes);
+/* Chunk assignments of the persistent sweeps (one chunk per block).
+ * MFG_CHUNK_VOTE: level by level a cell joins the chunk most of its
+ * dependencies are in, up to its share of the level (every level spread
+ * evenly, many dependencies between chunks).  MFG_CHUNK_TRANSVERSE_*: a
+ * grid of chunks over two centroid axes, each cell's label the maximum of
+ * its own bucket and its dependencies' labels, so that any dependency path
+ * crosses few chunk boundaries.  By default each context takes, per sweep,
+ * the assignment with the shortest modelled sweep; mfg_set_chunking(kind)
+ * forces one for contexts created afterwards (-1 restores the default).
+ * Results are identical with every assignment. */
+#define MFG_CHUNK_VOTE 0
+#define MFG_CHUNK_TRANSVERSE_XY 1
+#define MFG_CHUNK_TRANSVERSE_XZ 2
+#define MFG_CHUNK_TRANSVERSE_YZ 3
+int mfg_set_chunking(int32_t kind);
 /* Times n_trial fused iterations with each lane count on this context's own
  * grid and keeps the faster (ms_out[2], optional, receives the ms per
  * iteration of W and W / 2 lanes).  The state and the dt extrema are
@@ -185,6 +205,30 @@ int mfg_selftest_sweep_timeout(mfg_ctx *ctx, int64_t spin_cycles);
  * device; *mismatches receives the number of results whose bits differ
  * from the division's (0 expected). */
 int mfg_selftest_division(int64_t n, uint64_t seed, int64_t *mismatches);
+/* Known-answer self-test of the device arithmetic (test hook; the inputs
+ * are the reference functions' own arguments): runs the device functions
+ * the iteration kernels use on n given inputs, one GPU thread each, and
+ * copies the results back to the host.  consts = {gam, p_bar, alf_l
+ * (= epsa_r), lhs_omga, rho_min, rho_max, p_min, p_max}; in/out are host
+ * arrays.
+ *   mode 0 [RoeFlux_noprec, cal_flux.cpp:676-834]: in = ql[5][n], qr[5][n],
+ *          nx[n], ny[n], nz[n], area[n]; out = flux[5][n]
+ *   mode 1 [FluxLUSGS3D, forward_lusgs.cpp:1271-1324]: in = [n][13]
+ *          (q[5], dq[5], normal[3]); out = [n][5]
+ *   mode 2 [UpdateFlowField3D_CFL3d, forward_lusgs.cpp:1335-1488]: in =
+ *          q[5][n], dq[5][n]; out = updated q[5][n]
+ *   mode 3 as mode 1, in the persistent sweeps' form with branch-free
+ *          divisions (mfg_selftest_division_fast) */
+int mfg_selftest_functions(int32_t mode, int32_t n, const double *consts, const double *in,
+                           double *out);
+/* Self-test of the persistent sweeps' branch-free reciprocal and quotient
+ * (a single-precision seed, Newton-Raphson steps on the FMA and Markstein's
+ * correction steps; no counterpart in the reference): n pseudo-random
+ * divisor/dividend pairs (seeded; divisor exponents across [-130, 130],
+ * every eighth significand all ones) on the current device.  counts[0]:
+ * reciprocals, counts[1]: quotients whose bits differ from the division's
+ * (0 expected); counts[2]: divisors the fast path leaves to the division. */
+int mfg_selftest_division_fast(int64_t n, uint64_t seed, int64_t *counts);
 
 /* ---- the iteration path (reference routine replaced in brackets) -------- */
 /* [ZeroResiduals, cal_flux.cpp:54-72] */
@@ -276,8 +320,18 @@ int mfg_residual_norm(mfg_ctx *ctx, double out[5]);
  *     library holds it until the process exits.  Larger n_cell is rejected
  *     with MFG_ERR_INVALID (message in mfg_last_cuda_error).
  *   - The first call on a device resolves the array's device address
- *     (cudaGetSymbolAddress, once per device); make that first call before
- *     any stream capture.
+ *     (cudaGetSymbolAddress, once per device and context); make that first
+ *     call before any stream capture.  Under CUDA's lazy module loading
+ *     (the default since CUDA 12) that first call may also be the one that
+ *     loads this library's device code onto the device and reserves the
+ *     2.5 MiB array there, so it can fail with an out-of-memory error when
+ *     the device is already full: a caller whose memory is managed by
+ *     another allocator should make it early (e.g. once at start-up with
+ *     n_cell = 0) while there is room.
+ *   - The address is cached per device with the id of the context it was
+ *     resolved in; after cudaDeviceReset, or with another context current
+ *     (a caller's own driver-API context), the next call resolves it again
+ *     in the new context -- make that call outside stream capture too.
  *   - All calls on a device share the one array: calls that overlap on the
  *     GPU (different streams, no ordering between them) race and may return
  *     wrong norms.  Every partial read is written by the same call first, so

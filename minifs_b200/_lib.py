@@ -66,7 +66,9 @@ class Info(ct.Structure):
                 ("device_bytes", ct.c_int64), ("sweep_mode", ct.c_int32),
                 ("graph_ready", ct.c_int32), ("ncase", ct.c_int32),
                 ("sweep_chunks", ct.c_int32), ("sweep_lanes", ct.c_int32),
-                ("sweep_records", ct.c_int32)]
+                ("sweep_records", ct.c_int32), ("sweep_chunking", ct.c_int32),
+                ("sweep_ring_records", ct.c_int32 * 2), ("sweep_global_records", ct.c_int32 * 2),
+                ("sweep_cross_records", ct.c_int32 * 2), ("sweep_model_us", ct.c_double * 2)]
 
 
 class RawGrid(ct.Structure):
@@ -138,10 +140,14 @@ def load(build_if_missing: bool = True):
         "mfg_info_get": (ct.c_int, [ctxp, ct.POINTER(Info)]),
         "mfg_set_sweep_mode": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_sweep_lanes": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_set_chunking": (ct.c_int, [ct.c_int32]),
         "mfg_autotune_sweeps": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
         "mfg_selftest_sweep_timeout": (ct.c_int, [ctxp, ct.c_int64]),
         "mfg_selftest_division": (ct.c_int, [ct.c_int64, ct.c_uint64,
                                              ct.POINTER(ct.c_int64)]),
+        "mfg_selftest_functions": (ct.c_int, [ct.c_int32, ct.c_int32, f64p, f64p, f64p]),
+        "mfg_selftest_division_fast": (ct.c_int, [ct.c_int64, ct.c_uint64,
+                                                  ct.POINTER(ct.c_int64)]),
         "mfg_zero_residuals": (ct.c_int, [ctxp]),
         "mfg_inviscid_flux": (ct.c_int, [ctxp]),
         "mfg_compute_timestep": (ct.c_int, [ctxp, ct.c_int32]),

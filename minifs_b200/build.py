@@ -67,14 +67,21 @@ SHIM = os.path.join(HERE, "shim")
 DROPIN = os.path.join(SHIM, "_build", "minifs_dropin")
 
 
-def build_dropin(ref: str = "/root/reference", verbose: bool = False) -> str | None:
+def reference_root() -> str:
+    """The MiniFS source tree the oracle and the drop-in shim build against:
+    the environment variable MINIFS_REF, else /root/reference."""
+    return os.environ.get("MINIFS_REF", "/root/reference")
+
+
+def build_dropin(ref: str | None = None, verbose: bool = False) -> str | None:
     """The reference's driver sequence on libmfgpu through the shim
     (``shim/mfgpu_shim.cpp`` in place of the reference's four kernel files,
     ``shim/dropin_main.cpp`` for main.cpp's hard-coded set-up), linked with
     the reference's unmodified ``src/Base`` and ``load_grid.cpp`` read in
-    place.  Built only where the reference sources exist; the binary finds
-    libmfgpu.so next to the package through its run path."""
-    src = os.path.join(ref, "src")
+    place (``ref``, default ``reference_root()``).  Built only where the
+    reference sources exist; the binary finds libmfgpu.so next to the
+    package through its run path."""
+    src = os.path.join(ref or reference_root(), "src")
     if not os.path.isdir(src):
         return None
     os.makedirs(os.path.dirname(DROPIN), exist_ok=True)

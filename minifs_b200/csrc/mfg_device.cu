@@ -711,26 +711,35 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
 }
 
 // ---------------------------------------------------------------------------
-// Persistent chunked sweeps.  Cells are split into chunks, one per resident
-// block (cooperative launch), so that every LU-SGS level is shared evenly by
-// the chunks and most dependencies stay inside a chunk (a cell joins the
-// chunk of most of the cells it depends on).  A block walks the levels of its
-// chunk in increasing order, all its threads sharing one level, with
-// __syncthreads between levels: a dependency inside the chunk is then
-// resolved through the SM's own L1.  A dependency on another chunk is
-// resolved by polling the neighbour's increment in L2 until it is no longer
-// the sentinel (bounded wait).  Progress: a cell waits only for cells of
-// lower levels, each block visits its levels in increasing order, and every
-// block is resident, so by induction over the levels every cell completes.
+// Persistent chunked sweeps, warp-specialised.
+//
+// The cells are split into chunks, one per block and one block per SM
+// (cooperative launch).  A block walks the levels of its chunk in increasing
+// order; a level with more cells than the block has lane groups takes several
+// passes, and every (level, pass) is one work item.  The block's warps have
+// two roles:
+//
+//  * producer warps, in kWsTeams teams taking the items in turn, read what an
+//    item's cells need that no sweep writes -- the cell's state, Diag and
+//    right-hand side, and for each of its neighbour records the neighbour's
+//    state and the face -- and evaluate the neighbour-state half of
+//    FluxLUSGS3D (flux_lusgs_pre), the reciprocal of the diagonal term and
+//    the limiter's velocity square into the team's shared-memory stage slot
+//    (an mbarrier pair per slot hands it over and back);
+//  * consumer warps take an item from its stage into registers, wait at the
+//    level barrier (a named barrier over the consumer warps alone) and run
+//    only the dependent chain: the neighbours' increments, the rest of
+//    FluxLUSGS3D, the ordered sums, the division, the limiter and the stores.
+//
+// A dependency inside the chunk is read from the block's shared-memory ring
+// of its last kRing positions (or, when older, from global memory); a
+// dependency on another chunk is polled in L2 until it is no longer the
+// sentinel (bounded wait).  Progress: a cell waits only for cells of lower
+// levels, each block visits its levels in increasing order, and every block
+// is resident, so by induction over the levels every cell completes.  Every
+// wait is bounded; one that gives up sets the error word, after which every
+// other wait returns at once and the kernel runs to its end.
 // ---------------------------------------------------------------------------
-// Threads per persistent block and resident blocks per SM (tuning).
-#ifndef MFG_PERSIST_BLOCK
-#define MFG_PERSIST_BLOCK 64
-#endif
-#ifndef MFG_PERSIST_MINB
-#define MFG_PERSIST_MINB 6
-#endif
-constexpr int kPersistBlock = MFG_PERSIST_BLOCK;
 constexpr uint32_t kMark = 0x80000000u;    // neighbour flag: in another chunk (wait in L2)
 constexpr uint32_t kInRing = 0x40000000u;  // neighbour flag: increment in the block's ring
 constexpr uint32_t kIdMask = 0x3FFFFFFFu;  // neighbour id bits
@@ -738,51 +747,43 @@ constexpr int kMinChunk = 64;              // no chunk smaller than this many ce
 // Increments of the last kRing positions of a chunk stay in shared memory, so
 // that a dependency inside the chunk is read on the SM instead of from L2.
 #ifndef MFG_SWEEP_RING
-#define MFG_SWEEP_RING 128
+#define MFG_SWEEP_RING 512
 #endif
 constexpr int kRing = MFG_SWEEP_RING;
 static_assert((kRing & (kRing - 1)) == 0, "ring size must be a power of two");
 
-// Position-major sweep tables.  Position p (chunk-major, level-sorted) holds
-// one cell; its records sit at [p * W, p * W + ns), so every index a thread
-// needs for a future level follows from the position alone and can be loaded
-// levels ahead.  W = 4 (tetrahedra) or 8 (any cell with at most 8 lower or
-// upper neighbours).
-struct __align__(8) PosCell {
-  int32_t cell, ns;
-};
-
-// A cell is swept by a group of L lanes (L = W or W / 2, chosen per context):
-// lane l computes the fluxes of the cell's records j = l, l + L, ..., owns the
-// components k = l, l + L, ... < 5 of the increment (the ordered sum over the
-// records and the division), and lane 0 applies the limiter to the whole
-// increment and stores it.  The operations and their order per component are
-// those of the one-thread form, so the results are the same bits.  Wider
-// groups shorten a cell's latency; narrower ones let a block take more cells
-// of a wide level per pass.
-
+constexpr int kWsTeams = 4;  // producer teams; team t fills stage slot t
 // Segment starts of a chunk kept in shared memory (longer chunks read the
 // rest from global memory).
 constexpr int kSegCache = 512;
 // Cases whose LimitTimeStep clamp state is kept in shared memory.
 constexpr int kCaseCache = 128;
 
-// What a lane knows about its group's position on a future level: the
-// position, its ring slot, the cell, the record count, this lane's
-// neighbours (flags kMark / kInRing) and their ring slots; cell < 0 = none.
-template <int R>
-struct LaneRegs {
-  int32_t p, slot, cell, ns;
-  uint32_t nb[R];
-  int32_t nslot[R];
+// Position-major sweep tables.  Position p (chunk-major, level-sorted) holds
+// one cell; its records sit at [p * W, p * W + ns).  W = 4 (tetrahedra) or 8
+// (any cell with at most 8 lower or upper neighbours).
+struct __align__(8) PosCell {
+  int32_t cell, ns;
 };
 
-// Everything a group reads for one cell that no sweep writes, staged into
-// shared memory by cp.async one item ahead: neighbour states and records
-// (by the lane of the record), the cell's state and Diag (lane 0), and res
-// (forward) or the cell's forward increment (backward), component k by the
-// lane that owns it.  The mixed form (MX) stages the single-precision
-// neighbour records.
+// A cell is swept by a pair of consumer lanes: lane h of the pair owns the
+// records [h W / 2, (h + 1) W / 2), whose products are independent
+// (instruction-level parallelism); lane 0 sums its records into the
+// right-hand side in record order and hands the partial sums to lane 1,
+// which adds its own in order, divides, limits and stores -- the operations
+// and order of the reference's loop, so the same bits.  An item holds
+// kGroups cells: 64 (four consumer warps, one per SM sub-partition) for W =
+// 4, 32 for W = 8, whose stage records are twice the size; a producer
+// thread stages one cell.
+template <int W>
+struct WsGeom {
+  static constexpr int kGroups = W == 8 ? 32 : 64;      // cells per item
+  static constexpr int kRh = W / 2;                     // records per consumer lane
+  static constexpr int kConsumers = 2 * kGroups;        // consumer threads
+  static constexpr int kTeamThreads = kGroups;          // producer threads per team
+  static constexpr int kThreads = kConsumers + kWsTeams * kTeamThreads;
+};
+
 template <bool MX>
 struct SweepTypes {
   using Q = double;
@@ -793,111 +794,94 @@ struct SweepTypes<true> {
   using Q = float;
   using Rec = SweepRecF;
 };
-// Padding of a stage so that consecutive groups' stages start 16 bytes
-// apart modulo 128: the groups of a warp then read their records from
-// different shared-memory banks (without it every group's record k sits in
-// the same bank and a warp's stage reads are 4- to 8-way conflicts).
-constexpr int stage_pad_bytes(int raw) {
-  const int a16 = (raw + 15) / 16 * 16;
-  return a16 - raw + ((16 - a16 % 128) % 128 + 128) % 128;
-}
+
+// One stage slot: what the producers stage for the cells of one item, each
+// field an array over the item's G cells, so that the consumer warps (one
+// thread per cell) read 32 consecutive words per field without bank
+// conflicts.  A record's fields -- FP64: the neighbour-state half of
+// FluxLUSGS3D (LusgsPre, 11 values), the face normal and the weight;
+// mixed: the neighbour's single-precision state record (8 values), the
+// normal and the weight.  A cell's: its state record, the right-hand side
+// (res, forward; the forward increment, backward), the diagonal term it
+// divides by with its reciprocal, the limiter's velocity square, and the
+// indices.
 template <int W, bool MX>
-struct __align__(16) Stage {
-  typename SweepTypes<MX>::Q qn[W][Q_STRIDE];
-  typename SweepTypes<MX>::Rec rec[W];
-  double qc[Q_STRIDE];
-  double in5[5];
-  double diag;
-  char pad[stage_pad_bytes(int(sizeof(typename SweepTypes<MX>::Q)) * W * Q_STRIDE +
-                           int(sizeof(typename SweepTypes<MX>::Rec)) * W + 8 * (Q_STRIDE + 6))];
+struct WsSlot {
+  static constexpr int G = WsGeom<W>::kGroups;
+  static constexpr int kRF = MX ? Q_STRIDE + 4 : 15;
+  typename SweepTypes<MX>::Q rec[W][kRF][G];
+  double qc[Q_STRIDE][G];
+  double in5[5][G];
+  double den[G], rden[G], vv[G];
+  int32_t cell[G], ns[G], first[G], pos[G];
+  uint32_t nb[W][G];
+  int32_t nslot[W][G];
 };
-static_assert(sizeof(Stage<4, false>) % 128 == 16 && sizeof(Stage<4, true>) % 128 == 16 &&
-                  sizeof(Stage<8, false>) % 128 == 16 && sizeof(Stage<8, true>) % 128 == 16,
-              "stage stride");
 
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+template <int W, bool MX>
+constexpr size_t ws_smem_bytes() {
+  return sizeof(WsSlot<W, MX>) * kWsTeams + sizeof(double) * kRing * 5 +
+         sizeof(int32_t) * (kSegCache + 2) + sizeof(double) * kCaseCache +
+         sizeof(uint64_t) * 2 * kWsTeams;
 }
-__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
+static_assert(sizeof(WsSlot<4, false>) % 16 == 0 && sizeof(WsSlot<8, false>) % 16 == 0 &&
+                  sizeof(WsSlot<4, true>) % 16 == 0 && sizeof(WsSlot<8, true>) % 16 == 0,
+              "slot alignment");
+static_assert(ws_smem_bytes<4, false>() <= 227 * 1024 && ws_smem_bytes<8, false>() <= 227 * 1024,
+              "stage fits in shared memory");
 
-template <int W, int L>
-__device__ __forceinline__ void fetch_lane(const int32_t *s_segs, const int32_t *__restrict__ segs,
-                                           int32_t sg0, int32_t sg, int32_t sg1, int32_t pbase,
-                                           int32_t pos_in_level, int32_t lane,
-                                           const PosCell *__restrict__ pcs,
-                                           const int32_t *__restrict__ pnb,
-                                           const int32_t *__restrict__ pslot,
-                                           LaneRegs<W / L> &o) {
-  o.cell = -1;
-  o.ns = 0;
-#pragma unroll
-  for (int r = 0; r < W / L; r++) {
-    o.nb[r] = 0;
-    o.nslot[r] = 0;
-  }
-  if (sg >= sg1) return;
-  const int32_t i = sg - sg0;
-  const int32_t a = i < kSegCache ? s_segs[i] : segs[sg];
-  const int32_t b = i + 1 <= kSegCache ? s_segs[i + 1] : segs[sg + 1];
-  const int32_t p = a + pos_in_level;
-  if (p >= b) return;
-  const PosCell x = pcs[p];
-  o.p = p;
-  o.slot = (p - pbase) & (kRing - 1);
-  o.cell = x.cell;
-  o.ns = x.ns;
-#pragma unroll
-  for (int r = 0; r < W / L; r++) {  // padding reads 0
-    o.nb[r] = (uint32_t)pnb[(int64_t)p * W + lane + L * r];
-    o.nslot[r] = pslot[(int64_t)p * W + lane + L * r];
-  }
+// mbarrier hand-off between the producer teams and the consumer warps.
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
 }
-
-template <int W, int L, bool FWD, bool MX>
-__device__ __forceinline__ void stage_copy(const LaneRegs<W / L> &o, int32_t lane,
-                                           Stage<W, MX> &st, const double *q8,
-                                           const typename SweepTypes<MX>::Q *qnb,
-                                           const typename SweepTypes<MX>::Rec *prec,
-                                           const double *res, const double *diag,
-                                           const double *dqf, int32_t C) {
-  if (o.cell < 0) return;
-  // 16-byte pieces of the neighbour record (64 B FP64, 32 B FP32) and of the
-  // sweep record (32 B, 16 B)
-  constexpr int kQ = sizeof(st.qn[0]) / 16, kR = sizeof(st.rec[0]) / 16;
-#pragma unroll
-  for (int r = 0; r < W / L; r++) {
-    const int j = lane + L * r;
-    if (j < o.ns) {
-      const char *qs =
-          reinterpret_cast<const char *>(qnb + (int64_t)(o.nb[r] & kIdMask) * Q_STRIDE);
-      char *qd = reinterpret_cast<char *>(&st.qn[j][0]);
-#pragma unroll
-      for (int i = 0; i < kQ; i++) cp_async16(qd + 16 * i, qs + 16 * i);
-      const char *rs = reinterpret_cast<const char *>(prec + (int64_t)o.p * W + j);
-      char *rd = reinterpret_cast<char *>(&st.rec[j]);
-#pragma unroll
-      for (int i = 0; i < kR; i++) cp_async16(rd + 16 * i, rs + 16 * i);
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+                   smem_addr(b))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the completion of the phase of the given parity; gives up
+// (setting *err) after `spin` cycles, or soon after another wait gave up.
+// The error word and the clock are read every 64th try only, and a waiter
+// with slack (the producers) sleeps between tries, so that waiting warps
+// take neither issue slots nor L2 requests from the ones that compute.
+__device__ __forceinline__ void mbar_wait(uint64_t *b, unsigned parity, int *err,
+                                          long long spin, unsigned sleep_ns) {
+  if (mbar_test(b, parity)) return;
+  const long long t0 = clock64();
+  for (unsigned tries = 1;; tries++) {
+    if (sleep_ns) __nanosleep(sleep_ns);
+    if (mbar_test(b, parity)) return;
+    if ((tries & 63) == 0) {
+      if (ld_relaxed(err)) return;
+      if (clock64() - t0 > spin) {
+        atomicExch(err, 1);
+        return;
+      }
     }
   }
-  if (lane == 0) {
-    const double *qs = q8 + (int64_t)o.cell * Q_STRIDE;
-#pragma unroll
-    for (int i = 0; i < 4; i++) cp_async16(&st.qc[2 * i], qs + 2 * i);
-    cp_async8(&st.diag, diag + o.cell);
-  }
-  for (int k = lane; k < 5; k += L)
-    cp_async8(&st.in5[k], FWD ? res + (int64_t)k * C + o.cell : dqf + (int64_t)o.cell * Q_STRIDE + k);
+}
+// The level barrier of the consumer warps (named barrier 1; the producers
+// never take part).
+template <int N>
+__device__ __forceinline__ void consumers_sync() {
+  if (N > 32)
+    asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory");
+  else
+    __syncwarp();
 }
 
 // Diag of a cell whose dt LimitTimeStep clamps to lim (compute_timestep.cpp
@@ -925,178 +909,325 @@ __device__ __forceinline__ double clamp_limit(const Params &P,
   return (dt_max / dt_min > P.ratio_dtmax) ? P.ratio_dtmax * dt_min : -1.0;
 }
 
-// One cell of one sweep level on a lane group, from its stage (the group's
-// lanes only wait for one another: a cell is stored as soon as its own
-// inputs are in).  sh: the group's scratch (W * 5 + 5 doubles); ring: the
-// block's increments of its last kRing positions.  FWD: DQ* = (res - sum_j
-// 0.5 area_j F_j) / Diag, limited except for the first cell (SolveLUSGS3D
-// forward, forward_lusgs.cpp:799-870); backward: DQ = DQ* - (sum_j area_j
-// F_j) / (2 Diag), limited (:871-940).
-template <int W, int L, bool FWD, bool MX>
-__device__ __forceinline__ void sweep_cell(
-    const LaneRegs<W / L> &o, int32_t lane, const Stage<W, MX> &st, double *sh, double *ring,
-    const double (*pre)[5],
-    const double *src, double *dst, double *rearm, int32_t first_cell, const Params &P0,
-    const double *s_lim, int clamp_check, double *__restrict__ dt, double *__restrict__ diag,
-    const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
-    const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err,
-    long long spin, const Cases &cs) {
-  if (o.cell < 0) return;  // the whole group
-  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
-  const int32_t c = o.cell;
-  const int32_t cse = case_of(cs, c);
-  const Params P = params_of(P0, cs, c);
-  // what the cell's own staged data give, formed while its neighbours'
-  // increments are still awaited: the reciprocal of the diagonal term the
-  // increment is divided by, and the velocity square of the limiter
-  const double den = FWD ? st.diag : 2.0 * st.diag;
-  const double rden = 1.0 / den;
-  const double vv = st.qc[1] * st.qc[1] + st.qc[2] * st.qc[2] + st.qc[3] * st.qc[3];
-  // record j = lane + L r < ns: w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j)
+// Producer: one item's cells into a stage slot; thread g of the team stages
+// cell g of the item.
+template <int W, bool FWD, bool MX>
+__device__ __forceinline__ void ws_produce(
+    WsSlot<W, MX> &S, int32_t g, int32_t p0, int32_t pend, const PosCell *__restrict__ pcs,
+    const typename SweepTypes<MX>::Rec *__restrict__ prec, const int32_t *__restrict__ pnb,
+    const int32_t *__restrict__ pslot, const double *__restrict__ q8,
+    const typename SweepTypes<MX>::Q *__restrict__ qnb, const double *__restrict__ res,
+    const double *__restrict__ dqf_own, int32_t C, const double *__restrict__ diag,
+    int32_t first_cell, const Params &P0, const Cases &cs) {
+  const int32_t p = p0 + g;
+  if (p >= pend) {
+    S.cell[g] = -1;
+    return;
+  }
+  const PosCell x = pcs[p];
+  const Params P = params_of(P0, cs, x.cell);
+  // the records' indices beside the position's own (a position's W slots
+  // all exist; padding reads neighbour 0), then the states, then the
+  // products
+  uint32_t e[W];
+  int32_t sl[W];
+  typename SweepTypes<MX>::Rec rc[W];
 #pragma unroll
-  for (int r = 0; r < W / L; r++) {
-    const int j = lane + L * r;
-    if (j < o.ns) {
-      const uint32_t b = o.nb[r];
-      // FP64: the part of the product the neighbour's state and the face
-      // give, before the increment is waited for
-      LusgsPre<double> a{};
-      if constexpr (!MX) {
-        double qn[Q_STRIDE];
+  for (int j = 0; j < W; j++) {
+    const int64_t o = (int64_t)p * W + j;
+    e[j] = (uint32_t)pnb[o];
+    sl[j] = pslot[o];
+    rc[j] = prec[o];
+  }
+  {
+    double qc[Q_STRIDE];
+    load_q(q8, x.cell, qc);
+    const double dg = diag[x.cell];
+    double in5[5];
 #pragma unroll
-        for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[j][k];
-        a = flux_lusgs_pre(qn, st.rec[j].nx, st.rec[j].ny, st.rec[j].nz, flux_params<double>(P));
-      }
-      double dn[5];
-      if (b & kInRing) {
+    for (int k = 0; k < 5; k++)
+      in5[k] = FWD ? res[(int64_t)k * C + x.cell] : dqf_own[(int64_t)x.cell * Q_STRIDE + k];
+    const double den = FWD ? dg : 2.0 * dg;
 #pragma unroll
-        for (int k = 0; k < 5; k++) dn[k] = ring[o.nslot[r] * 5 + k];
-      } else if ((b & kMark) && !rec5_ready(pre[r])) {
-        wait_rec(src + (int64_t)(b & kIdMask) * Q_STRIDE, dn, err, spin);
-      } else {  // read at the start of the item (see sweep_chunk)
+    for (int k = 0; k < Q_STRIDE; k++) S.qc[k][g] = qc[k];
 #pragma unroll
-        for (int k = 0; k < 5; k++) dn[k] = pre[r][k];
-      }
-      if constexpr (MX) {
-        // off-diagonal product in FP32, accumulated in FP64 below
-        float qf[Q_STRIDE], df[5], ff[5];
+    for (int k = 0; k < 5; k++) S.in5[k][g] = in5[k];
+    S.den[g] = den;
+    S.rden[g] = 1.0 / den;
+    S.vv[g] = qc[1] * qc[1] + qc[2] * qc[2] + qc[3] * qc[3];
+    S.cell[g] = x.cell;
+    S.ns[g] = x.ns;
+    S.first[g] = FWD && x.cell == (cs.P ? cs.first[case_of(cs, x.cell)] : first_cell);
+    S.pos[g] = p;
+  }
 #pragma unroll
-        for (int k = 0; k < Q_STRIDE; k++) qf[k] = st.qn[j][k];
+  for (int j = 0; j < W; j++) {
+    if (j >= x.ns) continue;
+    S.nb[j][g] = e[j];
+    S.nslot[j][g] = sl[j];
+    const int64_t nb = (int64_t)(e[j] & kIdMask);
+    if constexpr (MX) {
+      const float4 *qs = reinterpret_cast<const float4 *>(qnb + nb * Q_STRIDE);
+      const float4 a = __ldg(qs), b = __ldg(qs + 1);
+      const float v[Q_STRIDE] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-        for (int k = 0; k < 5; k++) df[k] = (float)dn[k];
-        const SweepRecF rr = st.rec[j];
-        flux_lusgs_diff(qf, df, rr.nx, rr.ny, rr.nz, flux_params<float>(P), ff);
+      for (int k = 0; k < Q_STRIDE; k++) S.rec[j][k][g] = v[k];
+      S.rec[j][Q_STRIDE][g] = rc[j].nx;
+      S.rec[j][Q_STRIDE + 1][g] = rc[j].ny;
+      S.rec[j][Q_STRIDE + 2][g] = rc[j].nz;
+      S.rec[j][Q_STRIDE + 3][g] = rc[j].w;
+    } else {
+      double qn[Q_STRIDE];
+      load_q(qnb, nb, qn);
+      const LusgsPre<double> a =
+          flux_lusgs_pre(qn, rc[j].nx, rc[j].ny, rc[j].nz, flux_params<double>(P));
+      const double v[15] = {a.Q0, a.Q1, a.Q2, a.Q3, a.Q4, a.vq, a.eig, a.f1,
+                            a.f2, a.f3, a.f4, rc[j].nx, rc[j].ny, rc[j].nz, rc[j].w};
 #pragma unroll
-        for (int k = 0; k < 5; k++) sh[j * 5 + k] = (double)(rr.w * ff[k]);
-      } else {
-        double f[5];
-        const SweepRec rr = st.rec[j];
-        flux_lusgs_fin(a, dn, rr.nx, rr.ny, rr.nz, flux_params<double>(P), f);
-#pragma unroll
-        for (int k = 0; k < 5; k++) sh[j * 5 + k] = rr.w * f[k];
-      }
+      for (int k = 0; k < 15; k++) S.rec[j][k][g] = v[k];
     }
   }
-  // LimitTimeStep's clamp (fused forward sweep, and only when some case's
-  // dt ratio exceeds its limit): every component lane reads dt[c] before
-  // lane 0 may write it below
-  double dg = st.diag, lim = -1.0;
+}
+
+// Consumer: the dependent chain of one cell on its lane pair (lane h, see
+// WsGeom), c < 0 when the pair has no cell in this item.  e[u]: the
+// neighbour word of the lane's record u, dn[u]: its increment as read when
+// the item was taken (unless it is in the ring).  FWD: DQ* = (res - sum_j
+// 0.5 area_j F_j) / Diag, limited except for the first cell (SolveLUSGS3D
+// forward, forward_lusgs.cpp:803-1014); backward: DQ = DQ* - (sum_j area_j
+// F_j) / (2 Diag), limited (:1060-1249).
+template <int W, bool FWD, bool MX>
+__device__ __forceinline__ void ws_cell(
+    const WsSlot<W, MX> &S, int32_t g, int32_t h, int32_t c, int32_t ns, const uint32_t *e,
+    double (*dn)[5], int32_t pbase, double *ring, const double *src, double *dst,
+    double *rearm, const Params &P0, const double *s_lim, int clamp_check,
+    double *__restrict__ dt, double *__restrict__ diag,
+    const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
+    const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err, long long spin,
+    const Cases &cs) {
+  constexpr int R = WsGeom<W>::kRh;
+  const bool live = c >= 0;
+  // the neighbour increments: from the ring, else as read when the item was
+  // taken, polled again in L2 while one is the sentinel.  The warp polls in
+  // one converged, bounded loop.
+  bool have[R];
+#pragma unroll
+  for (int u = 0; u < R; u++) {
+    const int j = h * R + u;
+    have[u] = true;
+    if (!live || j >= ns) continue;
+    if (e[u] & kInRing) {
+      const int32_t sl = S.nslot[j][g];
+#pragma unroll
+      for (int k = 0; k < 5; k++) dn[u][k] = ring[sl * 5 + k];
+    } else {
+      have[u] = rec5_ready(dn[u]);
+    }
+  }
+  bool all = true;
+#pragma unroll
+  for (int u = 0; u < R; u++) all = all && have[u];
+  if (__any_sync(0xffffffffu, !all)) {
+    const long long t0 = clock64();
+    for (int polls = 1;; polls++) {
+      if (polls > 64) __nanosleep(64);
+      if (!all) {
+        const int gave_up = ld_relaxed(err);
+        all = true;
+#pragma unroll
+        for (int u = 0; u < R; u++) {
+          if (have[u]) continue;
+          load_rec5_l2(src + (int64_t)(e[u] & kIdMask) * Q_STRIDE, dn[u]);
+          have[u] = rec5_ready(dn[u]);
+          all = all && have[u];
+        }
+        if (!all && (gave_up || clock64() - t0 > spin)) {
+          if (!gave_up) atomicExch(err, 1);
+          all = true;  // results invalid; the host reports MFG_ERR_TIMEOUT
+        }
+      }
+      if (!__any_sync(0xffffffffu, !all)) break;
+    }
+  }
+  const int32_t cse = live ? case_of(cs, c) : 0;
+  const Params P = live ? params_of(P0, cs, c) : P0;
+  // w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j) of the lane's records, their
+  // products overlapping (FP64: branch-free divisions, the exact form redone
+  // for the lane's records when one is out of its window)
+  double wf[R][5];
+  if constexpr (!MX) {
+    auto pre_of = [&](int j) {
+      LusgsPre<double> a;
+      a.Q0 = S.rec[j][0][g];
+      a.Q1 = S.rec[j][1][g];
+      a.Q2 = S.rec[j][2][g];
+      a.Q3 = S.rec[j][3][g];
+      a.Q4 = S.rec[j][4][g];
+      a.vq = S.rec[j][5][g];
+      a.eig = S.rec[j][6][g];
+      a.f1 = S.rec[j][7][g];
+      a.f2 = S.rec[j][8][g];
+      a.f3 = S.rec[j][9][g];
+      a.f4 = S.rec[j][10][g];
+      return a;
+    };
+    bool ok = true;
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int j = h * R + u;
+      if (!live || j >= ns) continue;
+      double f[5];
+      bool oku;
+      flux_lusgs_fin_fast(pre_of(j), dn[u], S.rec[j][11][g], S.rec[j][12][g], S.rec[j][13][g],
+                          flux_params<double>(P), f, oku);
+      ok = ok && oku;
+      const double w = S.rec[j][14][g];
+#pragma unroll
+      for (int k = 0; k < 5; k++) wf[u][k] = w * f[k];
+    }
+    if (!ok) {
+#pragma unroll
+      for (int u = 0; u < R; u++) {
+        const int j = h * R + u;
+        if (!live || j >= ns) continue;
+        double f[5];
+        flux_lusgs_fin(pre_of(j), dn[u], S.rec[j][11][g], S.rec[j][12][g], S.rec[j][13][g],
+                       flux_params<double>(P), f);
+        const double w = S.rec[j][14][g];
+#pragma unroll
+        for (int k = 0; k < 5; k++) wf[u][k] = w * f[k];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int j = h * R + u;
+      if (!live || j >= ns) continue;
+      // off-diagonal product in FP32, accumulated in FP64
+      float qf[Q_STRIDE], df[5], ff[5];
+#pragma unroll
+      for (int k = 0; k < Q_STRIDE; k++) qf[k] = S.rec[j][k][g];
+#pragma unroll
+      for (int k = 0; k < 5; k++) df[k] = (float)dn[u][k];
+      flux_lusgs_diff(qf, df, S.rec[j][Q_STRIDE][g], S.rec[j][Q_STRIDE + 1][g],
+                      S.rec[j][Q_STRIDE + 2][g], flux_params<float>(P), ff);
+      const float w = S.rec[j][Q_STRIDE + 3][g];
+#pragma unroll
+      for (int k = 0; k < 5; k++) wf[u][k] = (double)(w * ff[k]);
+    }
+  }
+  // the sum over the records in record order: lane 0 from the right-hand
+  // side through its records, lane 1 on from lane 0's partial sums
+  double part[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) part[k] = (FWD && h == 0 && live) ? S.in5[k][g] : 0.0;
+#pragma unroll
+  for (int u = 0; u < R; u++) {
+    const int j = h * R + u;
+    if (!live || j >= ns || h != 0) continue;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      if (FWD)
+        part[k] -= wf[u][k];
+      else
+        part[k] += wf[u][k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 5; k++) part[k] = __shfl_sync(0xffffffffu, part[k], threadIdx.x & ~1);
+#pragma unroll
+  for (int u = 0; u < R; u++) {
+    const int j = h * R + u;
+    if (!live || j >= ns || h != 1) continue;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      if (FWD)
+        part[k] -= wf[u][k];
+      else
+        part[k] += wf[u][k];
+    }
+  }
+  if (!live || h != 1) return;
+  double qc[Q_STRIDE];
+#pragma unroll
+  for (int k = 0; k < Q_STRIDE; k++) qc[k] = S.qc[k][g];
+  const double den = S.den[g], rden = S.rden[g];
+  // LimitTimeStep's clamp (forward sweep of a fused iteration, only when some
+  // case's dt ratio exceeds its limit)
+  double dg = den, lim = -1.0;  // forward: den is Diag itself
   bool clamped = false;
-  if (FWD && clamp_check && lane < 5) {
+  if (FWD && clamp_check) {
     lim = (cse < kCaseCache) ? s_lim[cse] : clamp_limit(P, dt_ext + 2 * cse);
     if (lim > 0.0 && dt[c] > lim) {
-      double qc[Q_STRIDE];
-#pragma unroll
-      for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
       dg = clamped_diag(c, qc, P, lim, cptr, slots, vol);
       clamped = true;
     }
   }
-  __syncwarp(gmask);
-  // components k = lane, lane + L, ... < 5 (at most two per lane, as two
-  // independent chains); records summed in order
-  {
-    constexpr int kC = (5 + L - 1) / L;
-    double acc[kC];
+  // the five quotients overlapping (branch-free; div_by_recip for all when
+  // one of them is out of its window)
+  double d[5];
+  bool okq = true;
 #pragma unroll
-    for (int i = 0; i < kC; i++) {
-      const int k = lane + L * i;
-      acc[i] = (FWD && k < 5) ? st.in5[k] : 0.0;
-    }
-    for (int32_t j = 0; j < o.ns; j++) {
-#pragma unroll
-      for (int i = 0; i < kC; i++) {
-        const int k = lane + L * i;
-        if (k < 5) {
-          if (FWD)
-            acc[i] -= sh[j * 5 + k];
-          else
-            acc[i] += sh[j * 5 + k];
-        }
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < kC; i++) {
-      const int k = lane + L * i;
-      if (k < 5)
-        sh[W * 5 + k] = FWD ? (clamped ? acc[i] / dg : div_by_recip(acc[i], den, rden))
-                            : st.in5[k] - div_by_recip(acc[i], den, rden);
-    }
+  for (int k = 0; k < 5; k++) {
+    bool okk;
+    const double qk = div_recip_fast(part[k], den, rden, okk);
+    okq = okq && okk;
+    d[k] = FWD ? qk : S.in5[k][g] - qk;
   }
-  __syncwarp(gmask);
-  // the limiter on every lane (same values), the stores spread over the lanes
-  double d[5], qc[Q_STRIDE];
+  if (!okq)
 #pragma unroll
-  for (int k = 0; k < 5; k++) d[k] = sh[W * 5 + k];
-#pragma unroll
-  for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
-  if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit_vv(qc, vv, d, P);
-  if (lane == 0) {
-    if (FWD && clamped) {
-      dt[c] = lim;
-      diag[c] = dg;
+    for (int k = 0; k < 5; k++) {
+      const double qk = div_by_recip(part[k], den, rden);
+      d[k] = FWD ? qk : S.in5[k][g] - qk;
     }
-    store_dq(dst, c, d);
-  }
-  if (lane == (L > 1 ? 1 : 0)) store_sentinel(rearm, c);  // armed for the other sweep
+  if (FWD && clamped)
 #pragma unroll
-  for (int k = 0; k < 5; k++)
-    if (k % L == lane) ring[o.slot * 5 + k] = d[k];
-  __syncwarp(gmask);  // sh is free for the group's next cell
+    for (int k = 0; k < 5; k++) d[k] = part[k] / dg;
+  if (!FWD || !S.first[g]) dq_limit_vv(qc, S.vv[g], d, P);
+  if (FWD && clamped) {
+    dt[c] = lim;
+    diag[c] = dg;
+  }
+  store_dq(dst, c, d);
+  store_sentinel(rearm, c);  // armed for the other sweep
+  const int32_t slot = (S.pos[g] - pbase) & (kRing - 1);
+#pragma unroll
+  for (int k = 0; k < 5; k++) ring[slot * 5 + k] = d[k];
 }
 
-// One persistent sweep: block b walks chunk b level by level.  A level of
-// more cells than the block has groups takes several passes; the group's
-// work items (level, pass) form one sequence, pipelined as a whole: indices
-// loaded two items ahead, read-only data staged into shared memory one item
-// ahead (cp.async), so that an item's critical path holds the increments it
-// depends on and one cell's arithmetic.  Blocks synchronise only between
-// levels.
-template <int W, int L, bool FWD, bool MX>
-__device__ __forceinline__ void sweep_chunk(
+// One persistent sweep over chunk blockIdx.x (see the section comment).
+template <int W, bool FWD, bool MX>
+__device__ __forceinline__ void ws_sweep(
     const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
     const PosCell *__restrict__ pcs, const typename SweepTypes<MX>::Rec *__restrict__ prec,
     const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
     const double *__restrict__ q8, const typename SweepTypes<MX>::Q *__restrict__ qnb,
-    const double *src, double *dst, double *rearm,
-    const double *__restrict__ res, const double *__restrict__ dqf_own, int32_t C,
-    double *__restrict__ diag, int32_t first_cell, const Params &P0, int clamp_check,
-    double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
-    const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
-    const double *__restrict__ vol, int *err, long long spin, const Cases &cs) {
-  constexpr int kGroups = kPersistBlock / L;
-  __shared__ Stage<W, MX> stg[2][kGroups];
-  __shared__ double shm[kGroups][W * 5 + 5];
-  __shared__ double ring[kRing * 5];
-  __shared__ int32_t s_segs[kSegCache + 1];
-  __shared__ double s_lim[FWD ? kCaseCache : 1];
+    const double *src, double *dst, double *rearm, const double *__restrict__ res,
+    const double *__restrict__ dqf_own, int32_t C, double *__restrict__ diag, int32_t first_cell,
+    const Params &P0, int clamp_check, double *__restrict__ dt,
+    const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
+    const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err, long long spin,
+    const Cases &cs) {
+  using Geo = WsGeom<W>;
+  constexpr int G = Geo::kGroups;
+  extern __shared__ __align__(16) unsigned char ws_smem[];
+  WsSlot<W, MX> *stage = reinterpret_cast<WsSlot<W, MX> *>(ws_smem);  // [kWsTeams]
+  double *ring = reinterpret_cast<double *>(stage + kWsTeams);         // [kRing][5]
+  int32_t *s_segs = reinterpret_cast<int32_t *>(ring + kRing * 5);       // [kSegCache + 1]
+  double *s_lim = reinterpret_cast<double *>(s_segs + kSegCache + 2);    // [kCaseCache]
+  uint64_t *full = reinterpret_cast<uint64_t *>(s_lim + kCaseCache);     // [kWsTeams]
+  uint64_t *empty = full + kWsTeams;                                      // [kWsTeams]
+  __shared__ int s_clamp_any;
   const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
-  const int32_t lane = threadIdx.x & (L - 1);
-  const int32_t grp = threadIdx.x / L;
   for (int32_t i = threadIdx.x; i <= sg1 - sg0 && i <= kSegCache; i += blockDim.x)
     s_segs[i] = segs[sg0 + i];
-  __shared__ int s_clamp_any;
-  if (threadIdx.x == 0) s_clamp_any = 0;
+  if (threadIdx.x == 0) {
+    s_clamp_any = 0;
+    for (int t = 0; t < kWsTeams; t++) {
+      mbar_init(&full[t], Geo::kTeamThreads);
+      mbar_init(&empty[t], Geo::kConsumers / 32);
+    }
+  }
   __syncthreads();
   if (FWD && clamp_check)
     for (int32_t k = threadIdx.x; k < cs.ncase && k < kCaseCache; k += blockDim.x) {
@@ -1107,76 +1238,73 @@ __device__ __forceinline__ void sweep_chunk(
   __syncthreads();
   // the per-cell clamp test only when some case needs it
   clamp_check = (FWD && clamp_check && s_clamp_any) ? 1 : 0;
-  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
-  double *sh = shm[grp];
   const int32_t pbase = sg1 > sg0 ? s_segs[0] : 0;
-  // work items (level sg, pass): the same sequence in every thread of the block
   auto seg_at = [&](int32_t sg) {
     const int32_t i = sg - sg0;
     return i <= kSegCache ? s_segs[i] : segs[sg];
   };
-  auto advance = [&](int32_t &sg, int32_t &pass) {
-    if (sg >= sg1) return;
-    const int32_t np = (seg_at(sg + 1) - seg_at(sg) + kGroups - 1) / kGroups;
-    if (++pass >= np) {
-      ++sg;
-      pass = 0;
+  if (threadIdx.x >= Geo::kConsumers) {
+    // producer team t: items t, t + kWsTeams, ... into stage slot t
+    const int32_t t = (threadIdx.x - Geo::kConsumers) / Geo::kTeamThreads;
+    const int32_t r = (threadIdx.x - Geo::kConsumers) % Geo::kTeamThreads;
+    WsSlot<W, MX> &S = stage[t];
+    int32_t item = 0;
+    for (int32_t sg = sg0; sg < sg1; sg++) {
+      const int32_t a = seg_at(sg), b = seg_at(sg + 1);
+      const int32_t np = (b - a + G - 1) / G;
+      for (int32_t pass = 0; pass < np; pass++, item++) {
+        if (item % kWsTeams != t) continue;
+        const int32_t use = item / kWsTeams;
+        if (use >= 1) mbar_wait(&empty[t], (unsigned)((use - 1) & 1), err, spin, 256);
+        ws_produce<W, FWD, MX>(S, r, a + pass * G, b, pcs, prec, pnb, pslot, q8, qnb, res,
+                               dqf_own, C, diag, first_cell, P0, cs);
+        mbar_arrive(&full[t]);
+      }
     }
-  };
-  auto fetch = [&](int32_t sg, int32_t pass, LaneRegs<W / L> &o) {
-    fetch_lane<W, L>(s_segs, segs, sg0, sg, sg1, pbase, grp + pass * kGroups, lane, pcs, pnb,
-                     pslot, o);
-  };
-  int32_t sg = sg0, pass = 0;              // this item
-  int32_t sgn = sg, passn = pass;          // the next
-  advance(sgn, passn);
-  int32_t sgf = sgn, passf = passn;        // the one after
-  advance(sgf, passf);
-  LaneRegs<W / L> cur, nxt, far;
-  fetch(sg, pass, cur);
-  fetch(sgn, passn, nxt);
-  stage_copy<W, L, FWD, MX>(cur, lane, stg[0][grp], q8, qnb, prec, res, diag, dqf_own, C);
-  cp_async_commit();
-  int par = 0;
-  while (sg < sg1) {
-    // increments this item reads from L2 (older than the ring, or produced by
-    // another chunk): requested first, so that their round trip overlaps the
-    // staging of the next items; one that still holds the sentinel is waited
-    // for in sweep_cell
-    double pre[W / L][5];
-#pragma unroll
-    for (int r = 0; r < W / L; r++) {
-      const int j = lane + L * r;
-      if (cur.cell >= 0 && j < cur.ns && !(cur.nb[r] & kInRing))
-        load_rec5_l2(src + (int64_t)(cur.nb[r] & kIdMask) * Q_STRIDE, pre[r]);
-    }
-    fetch(sgf, passf, far);
-    stage_copy<W, L, FWD, MX>(nxt, lane, stg[par ^ 1][grp], q8, qnb, prec, res, diag, dqf_own,
-                              C);
-    cp_async_commit();
-    cp_async_wait<1>();  // this item's stage
-    __syncwarp(gmask);
-    sweep_cell<W, L, FWD, MX>(cur, lane, stg[par][grp], sh, ring, pre, src, dst, rearm, first_cell,
-                              P0, s_lim, clamp_check, dt, diag, dt_ext, cptr, slots, vol, err,
-                              spin, cs);
-    if (sgn != sg) __syncthreads();  // end of a level
-    sg = sgn;
-    pass = passn;
-    sgn = sgf;
-    passn = passf;
-    advance(sgf, passf);
-    cur = nxt;
-    nxt = far;
-    par ^= 1;
+    return;
   }
-  cp_async_wait<0>();
+  // consumers: lane pair g takes cell g of every item
+  constexpr int R = Geo::kRh;
+  const int32_t g = threadIdx.x >> 1, h = threadIdx.x & 1;
+  int32_t item = 0;
+  for (int32_t sg = sg0; sg < sg1; sg++) {
+    const int32_t a = seg_at(sg), b = seg_at(sg + 1);
+    const int32_t np = (b - a + G - 1) / G;
+    for (int32_t pass = 0; pass < np; pass++, item++) {
+      const int32_t t = item % kWsTeams;
+      mbar_wait(&full[t], (unsigned)((item / kWsTeams) & 1), err, spin, 0);
+      const WsSlot<W, MX> &S = stage[t];
+      const int32_t c = S.cell[g];
+      const int32_t ns = c >= 0 ? S.ns[g] : 0;
+      uint32_t e[R];
+      double dn[R][5];
+      // increments read from L2 (older than the ring, or produced by another
+      // chunk) are requested now, so that their round trips overlap the
+      // level barrier; one still holding the sentinel is polled in ws_cell
+#pragma unroll
+      for (int u = 0; u < R; u++) {
+        const int j = h * R + u;
+        e[u] = j < ns ? S.nb[j][g] : kInRing;
+        if (!(e[u] & kInRing)) load_rec5_l2(src + (int64_t)(e[u] & kIdMask) * Q_STRIDE, dn[u]);
+      }
+      if (pass == 0 && item > 0) consumers_sync<Geo::kConsumers>();  // the previous level is stored
+      ws_cell<W, FWD, MX>(S, g, h, c, ns, e, dn, pbase, ring, src, dst, rearm, P0, s_lim, clamp_check,
+                          dt, diag, dt_ext, cptr, slots, vol, err, spin, cs);
+      __syncwarp();
+      if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[t]);  // the slot is free again
+    }
+  }
 }
+
+#ifndef MFG_PERSIST_MINB
+#define MFG_PERSIST_MINB 1
+#endif
 
 // Forward sweep.  chunk_skip > 0 withholds the first chunk_skip chunks
 // (failure-detection self-test only: the cells that depend on them wait
 // until the bound runs out).
-template <int W, int L, bool MX>
-__global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
+template <int W, bool MX>
+__global__ void __launch_bounds__(WsGeom<W>::kThreads, MFG_PERSIST_MINB)
 k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
                   const PosCell *__restrict__ pcs,
                   const typename SweepTypes<MX>::Rec *__restrict__ prec,
@@ -1190,15 +1318,15 @@ k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
                   const double *__restrict__ vol, int *err, long long spin,
                   int32_t chunk_skip, Cases cs) {
   if ((int32_t)blockIdx.x < chunk_skip) return;
-  sweep_chunk<W, L, true, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqf, dqf, dqb, res,
-                              nullptr, C, diag, first_cell, P0, clamp_check, dt, dt_ext, cptr,
-                              slots, vol, err, spin, cs);
+  ws_sweep<W, true, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqf, dqf, dqb, res,
+                        nullptr, C, diag, first_cell, P0, clamp_check, dt, dt_ext, cptr, slots,
+                        vol, err, spin, cs);
 }
 
 // Backward sweep.  The state update of a cell is not needed by any later
 // level, so it runs after the block has swept its whole chunk.
-template <int W, int L, bool MX>
-__global__ void __launch_bounds__(kPersistBlock, MFG_PERSIST_MINB)
+template <int W, bool MX>
+__global__ void __launch_bounds__(WsGeom<W>::kThreads, MFG_PERSIST_MINB)
 k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
                   const PosCell *__restrict__ pcs,
                   const typename SweepTypes<MX>::Rec *__restrict__ prec,
@@ -1209,9 +1337,9 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
                   double *__restrict__ dqf, double *dqb, const double *__restrict__ diag,
                   Params P0, int *err, long long spin, Cases cs) {
   const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
-  sweep_chunk<W, L, false, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqb, dqb, dqf,
-                               nullptr, dqf, 0, const_cast<double *>(diag), 0, P0, 0, nullptr,
-                               nullptr, nullptr, nullptr, nullptr, err, spin, cs);
+  ws_sweep<W, false, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqb, dqb, dqf, nullptr,
+                         dqf, 0, const_cast<double *>(diag), 0, P0, 0, nullptr, nullptr, nullptr,
+                         nullptr, nullptr, err, spin, cs);
   __syncthreads();  // the chunk's increments are final
   // UpdateFlowField3D_CFL3d for the chunk's cells
   if (sg1 > sg0) {
@@ -1618,6 +1746,93 @@ __global__ void k_selftest_division(int64_t n, uint64_t seed,
   if (local) atomicAdd(bad, local);
 }
 
+// Known-answer self-test of the device arithmetic: the device functions the
+// iteration kernels call (roe_flux, flux_lusgs through its pre/fin split,
+// update_cell with cell_props before each) on caller-given inputs, one
+// thread per input.  mode 0: RoeFlux_noprec, in = ql[5][n], qr[5][n],
+// nx[n], ny[n], nz[n], area[n] -> out[5][n]; mode 1: FluxLUSGS3D, in =
+// [n][13] (q[5], dq[5], normal[3]) -> out[n][5]; mode 2:
+// UpdateFlowField3D_CFL3d, in = q[5][n], dq[5][n] -> out[5][n].
+__global__ void k_selftest_functions(int mode, int32_t n, Params P, const double *__restrict__ in,
+                                     double *__restrict__ out) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t m = n;
+  if (mode == 0) {
+    double ql[Q_STRIDE], qr[Q_STRIDE], f[5];
+    for (int k = 0; k < 5; k++) {
+      ql[k] = in[k * m + i];
+      qr[k] = in[(5 + k) * m + i];
+    }
+    cell_props(ql, P);
+    cell_props(qr, P);
+    roe_flux(ql, qr, in[10 * m + i], in[11 * m + i], in[12 * m + i], in[13 * m + i], P, f);
+    for (int k = 0; k < 5; k++) out[k * m + i] = f[k];
+  } else if (mode == 1 || mode == 3) {
+    const double *c = in + 13 * (int64_t)i;
+    double q[Q_STRIDE], dq[5], f[5];
+    for (int k = 0; k < 5; k++) {
+      q[k] = c[k];
+      dq[k] = c[5 + k];
+    }
+    cell_props(q, P);
+    const FluxP<double> fp = flux_params<double>(P);
+    const LusgsPre<double> a = flux_lusgs_pre(q, c[10], c[11], c[12], fp);
+    bool ok = false;
+    if (mode == 3) flux_lusgs_fin_fast(a, dq, c[10], c[11], c[12], fp, f, ok);
+    if (!ok) flux_lusgs_fin(a, dq, c[10], c[11], c[12], fp, f);
+    for (int k = 0; k < 5; k++) out[5 * (int64_t)i + k] = f[k];
+  } else {
+    double q[Q_STRIDE], dq[5];
+    for (int k = 0; k < 5; k++) {
+      q[k] = in[k * m + i];
+      dq[k] = in[(5 + k) * m + i];
+    }
+    cell_props(q, P);
+    update_cell(q, dq, P);
+    for (int k = 0; k < 5; k++) out[k * m + i] = q[k];
+  }
+}
+
+// Self-test of the branch-free reciprocal and quotient against the division:
+// divisors with exponents across [-130, 130] (both sides of rcp_rn_fast's
+// window), significands uniform, and every eighth one all ones (routed to
+// the division), every eighth + 1 all ones but the last bit, every eighth +
+// 2 a power of two.  Counts bad[0] reciprocals and bad[1] quotients (both
+// fast forms taken) whose bits differ from the division's, bad[2] divisors
+// outside the fast path.
+__global__ void k_selftest_division_fast(int64_t n, uint64_t seed,
+                                         unsigned long long *__restrict__ bad) {
+  unsigned long long b0 = 0, b1 = 0, b2 = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t x = seed ^ ((uint64_t)i * 0xD1B54A32D192ED03ull);
+    const uint64_t r = splitmix64(x), e = splitmix64(x), ra = splitmix64(x), ea = splitmix64(x);
+    uint64_t mant = r & 0xFFFFFFFFFFFFFull;
+    if ((i & 7) == 0) mant = 0xFFFFFFFFFFFFFull;
+    if ((i & 7) == 1) mant = 0xFFFFFFFFFFFFEull;
+    if ((i & 7) == 2) mant = 0;
+    const uint64_t expo = (uint64_t)(1023 - 130 + (int64_t)(e % 261));
+    const double b = __longlong_as_double((long long)(((r >> 63) << 63) | (expo << 52) | mant));
+    const uint64_t expa = (uint64_t)(1023 - 400 + (int64_t)(ea % 801));
+    const double a = __longlong_as_double(
+        (long long)(((ra >> 63) << 63) | (expa << 52) | (ra & 0xFFFFFFFFFFFFFull)));
+    bool ok;
+    const double y = rcp_rn_fast(b, ok);
+    if (!ok) {
+      b2++;
+      continue;
+    }
+    if (__double_as_longlong(y) != __double_as_longlong(1.0 / b)) b0++;
+    bool okq;
+    const double q = div_recip_fast(a, b, y, okq);
+    if (okq && __double_as_longlong(q) != __double_as_longlong(a / b)) b1++;
+  }
+  if (b0) atomicAdd(bad, b0);
+  if (b1) atomicAdd(bad + 1, b1);
+  if (b2) atomicAdd(bad + 2, b2);
+}
+
 // ---- one part of a partitioned mesh (the reference's MPI mode) ------------
 
 // The partials of k_norm_final, summed in its order, left squared: a part's
@@ -1770,20 +1985,24 @@ __global__ void k_halo_nodes_mx(int32_t nu, const int32_t *__restrict__ unodes,
 // context
 // ---------------------------------------------------------------------------
 
-// The persistent sweep kernel for (W, lanes per cell, precision).
-static const void *sweep_kernel(bool fwd, int w, int lanes, bool mx) {
-#define MFG_SK(W_, L_)                                                                       \
-  if (w == W_ && lanes == L_)                                                                \
-    return fwd ? (mx ? (const void *)k_sweep_fwd_chunk<W_, L_, true>                           \
-                     : (const void *)k_sweep_fwd_chunk<W_, L_, false>)                         \
-               : (mx ? (const void *)k_sweep_bwd_chunk<W_, L_, true>                           \
-                     : (const void *)k_sweep_bwd_chunk<W_, L_, false>);
-  MFG_SK(4, 4)
-  MFG_SK(4, 2)
-  MFG_SK(8, 8)
-  MFG_SK(8, 4)
+// The persistent sweep kernel for (W, precision) and its dynamic shared
+// memory.
+static const void *sweep_kernel(bool fwd, int w, bool mx) {
+#define MFG_SK(W_)                                                                           \
+  if (w == W_)                                                                               \
+    return fwd ? (mx ? (const void *)k_sweep_fwd_chunk<W_, true>                               \
+                     : (const void *)k_sweep_fwd_chunk<W_, false>)                             \
+               : (mx ? (const void *)k_sweep_bwd_chunk<W_, true>                               \
+                     : (const void *)k_sweep_bwd_chunk<W_, false>);
+  MFG_SK(4)
+  MFG_SK(8)
 #undef MFG_SK
   return nullptr;
+}
+static int sweep_threads(int w) { return w == 8 ? WsGeom<8>::kThreads : WsGeom<4>::kThreads; }
+static size_t sweep_smem(int w, bool mx) {
+  if (w == 8) return mx ? ws_smem_bytes<8, true>() : ws_smem_bytes<8, false>();
+  return mx ? ws_smem_bytes<4, true>() : ws_smem_bytes<4, false>();
 }
 
 struct ChunkSweep {
@@ -1852,9 +2071,14 @@ struct mfg_ctx {
   int *sweep_err = nullptr;
   int persist_grid = 0;
   int sweep_w = 0;               // records per position of the persistent sweeps (4 or 8)
-  int sweep_lanes = 0;           // lanes per cell of the persistent sweeps (W or W / 2)
-  int persist_occ[2][2] = {{0, 0}, {0, 0}};  // resident blocks per SM: [W = 4, 8][W, W / 2 lanes]
-  bool lanes_ok[2] = {false, false};         // lane counts [W, W / 2] usable with the chunk grid
+  int sweep_lanes = 0;           // lanes per cell of the persistent sweeps (= W)
+  int persist_occ[2] = {0, 0};   // resident blocks per SM of the persistent sweeps [W = 4, 8]
+  int chunking = 0;              // chunk assignment of the forward sweep (MFG_CHUNK_*)
+  double chunk_est_us[2] = {0.0, 0.0};  // modelled duration of each sweep with its chunks
+  // records of each sweep [forward, backward] whose increment comes from the
+  // block's ring, from global memory (same chunk, older than the ring), or
+  // from another chunk
+  int32_t sweep_stats[2][3] = {{0, 0, 0}, {0, 0, 0}};
   int n_sm = 0;
   unsigned long long *dt_ext = nullptr;
   double *norm_part = nullptr, *norm_out = nullptr, *norm_hist = nullptr, *cfl_tab = nullptr;
@@ -2220,7 +2444,7 @@ __global__ void k_dev_pack(int32_t C, int32_t W, int with_recs, const int32_t *_
                            const SweepRec *__restrict__ recs, PosCell *__restrict__ packed,
                            int32_t *__restrict__ cnbs, SweepRec *__restrict__ crecs,
                            SweepRecF *__restrict__ crecs_f, int32_t *__restrict__ cslot,
-                           int32_t *__restrict__ chunk0_exported) {
+                           int32_t *__restrict__ chunk0_exported, int32_t *__restrict__ stats) {
   const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= C) return;
   const int32_t gi = order[k];
@@ -2238,9 +2462,13 @@ __global__ void k_dev_pack(int32_t C, int32_t W, int with_recs, const int32_t *_
     uint32_t e = (uint32_t)nb;
     if (cross) {
       e |= kMark;
+      atomicAdd(&stats[2], 1);
     } else if (nb < C && posof[nb] >= seg_end - kRing) {
       e |= kInRing;
       cslot[o] = (posof[nb] - chunk_ptr[p]) & (kRing - 1);
+      atomicAdd(&stats[0], 1);
+    } else if (nb < C) {
+      atomicAdd(&stats[1], 1);
     }
     cnbs[o] = (int32_t)e;
     const SweepRec r = recs[s0 + j];
@@ -2377,6 +2605,26 @@ int mfg_destroy(mfg_ctx *ctx) {
   return MFG_OK;
 }
 
+// Lane groups (cells per item) of the persistent sweeps with W records.
+static int32_t sweep_groups(int w) { return w == 8 ? WsGeom<8>::kGroups : WsGeom<4>::kGroups; }
+
+// Chunk assignment forced for contexts created from now on (-1: chosen by
+// the model), set by mfg_set_chunking.
+static std::atomic<int> g_chunking{-1};
+
+// Records per position (W), persistent-sweep grid and chunk count of a new
+// context: one chunk per resident block, no chunk under kMinChunk cells.
+static void setup_sweep_grid(mfg_ctx *ctx, int32_t maxns) {
+  const int32_t C = ctx->C;
+  ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
+  if (ctx->n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
+  const int per_sm = ctx->sweep_w ? ctx->persist_occ[ctx->sweep_w == 8 ? 1 : 0] : 0;
+  ctx->persist_grid = per_sm * ctx->n_sm;
+  ctx->nchunks = std::max(1, std::min(ctx->persist_grid, (C + kMinChunk - 1) / kMinChunk));
+  ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
+  ctx->sweep_lanes = ctx->sweep_w;
+}
+
 // Chunks for the persistent sweeps, one per resident block.  Level by level
 // (lptr over the level-sorted cells, sptr/nbs their dependencies), a cell
 // joins the chunk that most of its dependencies are in, unless that chunk
@@ -2421,6 +2669,194 @@ static void assign_chunks(int32_t C, int32_t P, const std::vector<int32_t> &lptr
       load[pp]++;
     }
   }
+}
+
+// Chunks across the level sets, monotone along the dependencies.  Every
+// cell gets a label (la, lb) on a Pa x Pb grid: its seed is the equal-count
+// bucket of its centroid along two axes, and per axis the label is the
+// maximum of the seed and the labels of the cells it depends on (cells in
+// level order, so those are labelled first) -- the minimum instead along an
+// axis on which a sweep's dependencies lie mostly above the cell (the
+// backward sweep's).  Labels are therefore monotone along every dependency:
+// a dependency path crosses at most Pa + Pb - 2 chunk boundaries, and where
+// the level sets run across the two axes (the levels of a lexicographically
+// numbered box follow its slowest axis) every level spreads over all the
+// chunks.
+// rank: each cell's position in the centroid order along an axis.
+static void assign_chunks_transverse(int32_t C, int32_t Pa, int32_t Pb, int ax, int bx,
+                                     const std::vector<int32_t> &lptr, const int32_t *cells,
+                                     const int32_t *sptr, const int32_t *nbs,
+                                     const double *const xyz[3],
+                                     const std::vector<int32_t> *rank,
+                                     std::vector<int32_t> &assign) {
+  const double *ca = xyz[ax], *cb = xyz[bx];
+  std::vector<int32_t> la(C), lb(C);
+  for (int32_t c = 0; c < C; c++) {
+    la[c] = (int32_t)((int64_t)rank[ax][c] * Pa / C);
+    lb[c] = (int32_t)((int64_t)rank[bx][c] * Pb / C);
+  }
+  const int32_t L = (int32_t)lptr.size() - 1;
+  // per axis: do the dependencies lie mostly above (then labels take the
+  // minimum) or below the cell (the maximum)?
+  int64_t up_a = 0, up_b = 0;
+  for (int32_t i = 0; i < lptr[L]; i++) {
+    const int32_t c = cells[i];
+    for (int32_t s0 = sptr[i]; s0 < sptr[i + 1]; s0++) {
+      const int32_t d = nbs[s0];
+      if (d >= C) continue;
+      up_a += (ca[d] > ca[c]) - (ca[d] < ca[c]);
+      up_b += (cb[d] > cb[c]) - (cb[d] < cb[c]);
+    }
+  }
+  for (int32_t i = 0; i < lptr[L]; i++) {
+    const int32_t c = cells[i];
+    for (int32_t s0 = sptr[i]; s0 < sptr[i + 1]; s0++) {
+      const int32_t d = nbs[s0];
+      if (d >= C) continue;
+      la[c] = up_a > 0 ? std::min(la[c], la[d]) : std::max(la[c], la[d]);
+      lb[c] = up_b > 0 ? std::min(lb[c], lb[d]) : std::max(lb[c], lb[d]);
+    }
+  }
+  assign.resize(C);
+  for (int32_t c = 0; c < C; c++) assign[c] = la[c] + Pa * lb[c];
+}
+
+// Modelled duration (SM cycles) of a persistent sweep over the chunks
+// `assign`: per level, a chunk starts after its previous level plus a
+// barrier; its k-th cell of the level waits k / G lane-group passes; a cell
+// waits for each dependency in another chunk until that one is done plus the
+// L2 round trip; a cell takes one dependent chain.  Used to choose between
+// chunk assignments.
+static double model_sweep_cycles(int32_t C, int32_t P, int32_t G,
+                                 const std::vector<int32_t> &lptr, const int32_t *cells,
+                                 const int32_t *sptr, const int32_t *nbs,
+                                 const std::vector<int32_t> &assign) {
+  const double kChain = 800.0, kCross = 1500.0, kBarrier = 60.0;
+  std::vector<double> done(C, 0.0), tch(P, 0.0), nxt(P, 0.0);
+  std::vector<int32_t> cnt(P, 0);
+  const int32_t L = (int32_t)lptr.size() - 1;
+  double tmax = 0.0;
+  for (int32_t l = 0; l < L; l++) {
+    for (int32_t i = lptr[l]; i < lptr[l + 1]; i++) {
+      const int32_t c = cells[i], ch = assign[c];
+      double t = tch[ch] + kBarrier + (double)(cnt[ch]++ / G) * kChain;
+      for (int32_t s0 = sptr[i]; s0 < sptr[i + 1]; s0++) {
+        const int32_t d = nbs[s0];
+        if (d < C && assign[d] != ch) t = std::max(t, done[d] + kCross);
+      }
+      done[c] = t + kChain;
+      nxt[ch] = std::max(nxt[ch], done[c]);
+      tmax = std::max(tmax, done[c]);
+    }
+    for (int32_t i = lptr[l]; i < lptr[l + 1]; i++) {
+      const int32_t ch = assign[cells[i]];
+      tch[ch] = nxt[ch];
+      cnt[ch] = 0;
+    }
+  }
+  return tmax;
+}
+
+// Most cells any chunk holds on any level (more than the block's lane
+// groups take two passes over that level).
+static int32_t max_chunk_level(int32_t P, const std::vector<int32_t> &lptr, const int32_t *cells,
+                               const std::vector<int32_t> &assign) {
+  std::vector<int32_t> cnt(P, 0);
+  int32_t mx = 0;
+  const int32_t L = (int32_t)lptr.size() - 1;
+  for (int32_t l = 0; l < L; l++) {
+    for (int32_t i = lptr[l]; i < lptr[l + 1]; i++) mx = std::max(mx, ++cnt[assign[cells[i]]]);
+    for (int32_t i = lptr[l]; i < lptr[l + 1]; i++) cnt[assign[cells[i]]] = 0;
+  }
+  return mx;
+}
+
+// The chunk assignment of a sweep: the balanced vote (assign_chunks) and the
+// transverse monotone one over each pair of axes and each Pa x Pb <= P grid
+// whose aspect is within a factor two of the pair's extents.  Grids that
+// keep every level of every chunk within one pass of the lane groups come
+// first (else the fewest cells per chunk and level); among those the
+// shortest modelled sweep is kept.  Returns the choice (MFG_CHUNK_VOTE or
+// MFG_CHUNK_TRANSVERSE_*) and its modelled duration in microseconds at
+// 1.9 GHz.
+static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int32_t> &lptr,
+                         const int32_t *cells, const int32_t *sptr, const int32_t *nbs,
+                         const double *const xyz[3], int force, std::vector<int32_t> &assign,
+                         double *est_us) {
+  std::vector<int32_t> best, cand;
+  double tbest = 1e300;
+  int32_t lbest = INT32_MAX;
+  int choice = MFG_CHUNK_VOTE;
+  if (force < 0 || force == MFG_CHUNK_VOTE) {
+    assign_chunks(C, P, lptr, cells, sptr, nbs, cand);
+    lbest = std::max(max_chunk_level(P, lptr, cells, cand), G);  // <= G: one pass
+    tbest = model_sweep_cycles(C, P, G, lptr, cells, sptr, nbs, cand);
+    choice = MFG_CHUNK_VOTE;
+    best.swap(cand);
+  }
+  const bool geo = xyz[0] && xyz[1] && xyz[2] &&
+                   (force < 0 || force >= MFG_CHUNK_TRANSVERSE_XY);
+  if (geo) {
+    // each axis's centroid order once; the axis pairs on threads of their own
+    std::vector<int32_t> rank[3];
+    double ext[3];
+    for (int a = 0; a < 3; a++) {
+      std::vector<int32_t> idx(C);
+      for (int32_t c = 0; c < C; c++) idx[c] = c;
+      std::stable_sort(idx.begin(), idx.end(),
+                       [&](int32_t x, int32_t y) { return xyz[a][x] < xyz[a][y]; });
+      rank[a].resize(C);
+      for (int32_t r = 0; r < C; r++) rank[a][idx[r]] = r;
+      ext[a] = std::max(C ? xyz[a][idx[C - 1]] - xyz[a][idx[0]] : 0.0, 1e-300);
+    }
+    struct Best {
+      int32_t load = INT32_MAX;
+      double t = 1e300;
+      std::vector<int32_t> assign;
+    } pb[3];
+    auto pair_search = [&](int kind) {
+      const int ax = kind == MFG_CHUNK_TRANSVERSE_YZ ? 1 : 0;
+      const int bx = kind == MFG_CHUNK_TRANSVERSE_XY ? 1 : 2;
+      Best &b = pb[kind - MFG_CHUNK_TRANSVERSE_XY];
+      std::vector<int32_t> a;
+      for (int32_t Pa = 1; Pa <= P; Pa++) {
+        const int32_t Pb = P / Pa;
+        if (Pb < 1 || (Pa > 1 && P / (Pa - 1) == Pb)) continue;  // the largest Pa per Pb
+        const double r = (double)Pa / Pb / (ext[ax] / ext[bx]);
+        if (r > 2.0 || r < 0.5) continue;
+        assign_chunks_transverse(C, Pa, Pb, ax, bx, lptr, cells, sptr, nbs, xyz, rank, a);
+        const int32_t load = std::max(max_chunk_level(P, lptr, cells, a), G);
+        if (load > b.load) continue;
+        const double t = model_sweep_cycles(C, P, G, lptr, cells, sptr, nbs, a);
+        if (load < b.load || t < b.t) {
+          b.load = load;
+          b.t = t;
+          b.assign.swap(a);
+        }
+      }
+    };
+    std::vector<std::thread> th;
+    for (int kind = MFG_CHUNK_TRANSVERSE_XY; kind <= MFG_CHUNK_TRANSVERSE_YZ; kind++)
+      if (force < 0 || force == kind) th.emplace_back(pair_search, kind);
+    for (auto &t : th) t.join();
+    for (int kind = MFG_CHUNK_TRANSVERSE_XY; kind <= MFG_CHUNK_TRANSVERSE_YZ; kind++) {
+      Best &b = pb[kind - MFG_CHUNK_TRANSVERSE_XY];
+      if (b.assign.empty() || b.load > lbest || (b.load == lbest && b.t >= tbest)) continue;
+      lbest = b.load;
+      tbest = b.t;
+      choice = kind;
+      best.swap(b.assign);
+    }
+  }
+  if (best.empty()) {  // a forced transverse assignment without centroids
+    assign_chunks(C, P, lptr, cells, sptr, nbs, best);
+    tbest = model_sweep_cycles(C, P, G, lptr, cells, sptr, nbs, best);
+    choice = MFG_CHUNK_VOTE;
+  }
+  (void)lbest;
+  assign.swap(best);
+  if (est_us) *est_us = tbest / 1900.0;
+  return choice;
 }
 
 static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32_t> &cptr,
@@ -2474,24 +2910,7 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
   {
     int32_t maxns = 0;
     for (int32_t c = 0; c < C; c++) maxns = std::max(maxns, std::max(fw_cnt[c], bw_cnt[c]));
-    ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
-    if (n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
-    const int wi = ctx->sweep_w == 8 ? 1 : 0;
-    const int occ_w = ctx->sweep_w ? ctx->persist_occ[wi][0] : 0;
-    const int occ_h = ctx->sweep_w ? ctx->persist_occ[wi][1] : 0;
-    auto chunks_for = [&](int per_sm) {
-      return std::max(1, std::min(per_sm * ctx->n_sm, (C + kMinChunk - 1) / kMinChunk));
-    };
-    // the grid of the W-lane kernels (measured faster than a smaller grid
-    // shared with the W/2-lane ones); W/2 lanes where they fit it too, for
-    // mfg_autotune_sweeps to try
-    const int per_sm = occ_w;
-    ctx->persist_grid = per_sm * ctx->n_sm;
-    ctx->nchunks = chunks_for(per_sm);
-    ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
-    ctx->lanes_ok[0] = occ_w >= per_sm && per_sm > 0;
-    ctx->lanes_ok[1] = occ_h >= per_sm && per_sm > 0;
-    ctx->sweep_lanes = ctx->sweep_w;
+    setup_sweep_grid(ctx, maxns);
   }
   const int W = std::max(ctx->sweep_w, 1);
   auto make = [&](const std::vector<int32_t> &lv, const std::vector<int32_t> &cnt, bool fwd,
@@ -2532,7 +2951,13 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     }
     const int32_t P = ctx->nchunks;
     std::vector<int32_t> assign, chunk_cnt(P, 0);
-    assign_chunks(C, P, lptr, cells.data(), sptr.data(), nbs.data(), assign);
+    {
+      const double *xyz[3] = {m->xcc, m->ycc, m->zcc};
+      const int kind = choose_chunks(C, P, sweep_groups(ctx->sweep_w), lptr, cells.data(),
+                                     sptr.data(), nbs.data(), xyz, g_chunking.load(), assign,
+                                     &ctx->chunk_est_us[fwd ? 0 : 1]);
+      if (fwd) ctx->chunking = kind;
+    }
     // chunk-major, level-sorted cell lists (the level order is already sorted)
     for (int32_t c = 0; c < C; c++) chunk_cnt[assign[c]]++;
     std::vector<int32_t> chunk_ptr(P + 1, 0);
@@ -2573,13 +2998,18 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
           const bool cross = nb < C && assign[nb] != p;
           if (cross && assign[nb] == 0) chunk0_exported = true;
           uint32_t e = (uint32_t)nb;
+          int32_t *stat = ctx->sweep_stats[fwd ? 0 : 1];
           if (cross) {
             e |= kMark;
+            stat[2]++;
           } else if (nb < C && posof[nb] >= seg_end - kRing) {
             // still in the ring when this level reads it: overwritten only by
             // position posof[nb] + kRing, which lies in a later level
             e |= kInRing;
             cslot[o] = (posof[nb] - chunk_ptr[p]) & (kRing - 1);
+            stat[0]++;
+          } else if (nb < C) {
+            stat[1]++;  // in the chunk, older than the ring: read from global memory
           }
           cnbs[o] = (int32_t)e;
           crecs[o] = recs[s0];
@@ -2770,21 +3200,26 @@ static int ctx_begin(int32_t n_node, int32_t n_face, int32_t n_cell, int32_t n_b
     // most as many blocks as the occupancy of the heavier kernel allows
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
-    // resident blocks per SM of each kernel pair (both sweeps)
+    // resident blocks per SM of each kernel pair (both sweeps), with the
+    // stage's dynamic shared memory allowed first
     const bool mx = precision == MFG_PREC_MIXED;
-    for (int wi = 0; wi < 2; wi++)
-      for (int li = 0; li < 2; li++) {
-        const int w = wi ? 8 : 4, lanes = li ? w / 2 : w;
-        int per_sm = 1 << 30;
-        for (bool fwd : {true, false}) {
-          int b = 0;
-          if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, sweep_kernel(fwd, w, lanes, mx),
-                                                            kPersistBlock, 0) != cudaSuccess)
-            return fail(MFG_ERR_CUDA);
-          per_sm = std::min(per_sm, b);
-        }
-        ctx->persist_occ[wi][li] = coop ? per_sm : 0;
+    for (int wi = 0; wi < 2; wi++) {
+      const int w = wi ? 8 : 4;
+      int per_sm = 1 << 30;
+      for (bool fwd : {true, false}) {
+        const void *fn = sweep_kernel(fwd, w, mx);
+        const size_t smem = sweep_smem(w, mx);
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+          return fail(MFG_ERR_CUDA);
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, sweep_threads(w), smem) !=
+            cudaSuccess)
+          return fail(MFG_ERR_CUDA);
+        per_sm = std::min(per_sm, b);
       }
+      ctx->persist_occ[wi] = coop ? per_sm : 0;
+    }
     ctx->n_sm = prop.multiProcessorCount;
   }
   *out = ctx;
@@ -3211,12 +3646,12 @@ int dev_pack(mfg_ctx *ctx, DevScratch &sc, DevSweep &d) {
       (rc = sc.get(&chunk_cnt, (int64_t)P + 1)) || (rc = sc.get(&chunk_ptr, (int64_t)P + 1)) ||
       (rc = sc.get(&ccells, C)) || (rc = sc.get(&posof, C)) ||
       (rc = sc.get(&head, (int64_t)C + 1)) || (rc = sc.get(&hscan, (int64_t)C + 1)) ||
-      (rc = sc.get(&exported, 1)))
+      (rc = sc.get(&exported, 4)))
     return rc;
   MFG_CUDA(cudaMemcpyAsync(assign, d.h_assign.data(), sizeof(int32_t) * C,
                            cudaMemcpyHostToDevice, st));
   MFG_CUDA(cudaMemsetAsync(chunk_cnt, 0, sizeof(int32_t) * ((size_t)P + 1), st));
-  MFG_CUDA(cudaMemsetAsync(exported, 0, sizeof(int32_t), st));
+  MFG_CUDA(cudaMemsetAsync(exported, 0, 4 * sizeof(int32_t), st));
   const int32_t *cells = d.fwd ? ctx->fw_cells : ctx->bw_cells;
   const int32_t *sptr = d.fwd ? ctx->fw_sptr : ctx->bw_sptr;
   const int32_t *nbs = d.fwd ? ctx->fw_nb : ctx->bw_nb;
@@ -3256,16 +3691,18 @@ int dev_pack(mfg_ctx *ctx, DevScratch &sc, DevSweep &d) {
   if (mx)
     k_dev_pack<true><<<grid_for(C), kBlock, 0, st>>>(
         C, W, with_recs, order, ccells, pchunk, head, hscan, cs.segs, chunk_ptr, posof, assign,
-        sptr, nbs, recs, cs.cells, cs.nbs, nullptr, cs.recs_f, cs.nslots, exported);
+        sptr, nbs, recs, cs.cells, cs.nbs, nullptr, cs.recs_f, cs.nslots, exported, exported + 1);
   else
     k_dev_pack<false><<<grid_for(C), kBlock, 0, st>>>(
         C, W, with_recs, order, ccells, pchunk, head, hscan, cs.segs, chunk_ptr, posof, assign,
-        sptr, nbs, recs, cs.cells, cs.nbs, cs.recs, nullptr, cs.nslots, exported);
+        sptr, nbs, recs, cs.cells, cs.nbs, cs.recs, nullptr, cs.nslots, exported, exported + 1);
   count_launch();
   MFG_CUDA(cudaGetLastError());
-  int32_t ex = 0;
-  if ((rc = dev_read_i32(exported, &ex, st))) return rc;
-  if (d.fwd) ctx->chunk0_exported = ex != 0;
+  int32_t ex[4] = {0, 0, 0, 0};
+  MFG_CUDA(cudaMemcpyAsync(ex, exported, sizeof(ex), cudaMemcpyDeviceToHost, st));
+  MFG_CUDA(cudaStreamSynchronize(st));
+  if (d.fwd) ctx->chunk0_exported = ex[0] != 0;
+  for (int k = 0; k < 3; k++) ctx->sweep_stats[d.fwd ? 0 : 1][k] = ex[1 + k];
   (d.fwd ? ctx->fw_lptr : ctx->bw_lptr) = d.lptr;
   return MFG_OK;
 }
@@ -3331,19 +3768,7 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
   if (h_flags[0]) return fail(MFG_ERR_BADMESH);
   {
     // the choices of build_levels
-    const int32_t maxns = h_flags[1];
-    ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
-    if (n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
-    const int wi = ctx->sweep_w == 8 ? 1 : 0;
-    const int occ_w = ctx->sweep_w ? ctx->persist_occ[wi][0] : 0;
-    const int occ_h = ctx->sweep_w ? ctx->persist_occ[wi][1] : 0;
-    const int per_sm = occ_w;
-    ctx->persist_grid = per_sm * ctx->n_sm;
-    ctx->nchunks = std::max(1, std::min(per_sm * ctx->n_sm, (C + kMinChunk - 1) / kMinChunk));
-    ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
-    ctx->lanes_ok[0] = occ_w >= per_sm && per_sm > 0;
-    ctx->lanes_ok[1] = occ_h >= per_sm && per_sm > 0;
-    ctx->sweep_lanes = ctx->sweep_w;
+    setup_sweep_grid(ctx, h_flags[1]);
     ctx->first_cell = 0;
   }
   {
@@ -3353,15 +3778,24 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
     if ((rc = dev_levels(ctx, sc, fw, front, next, counter))) return fail(rc);
     if ((rc = dev_levels(ctx, sc, bw, front, next, counter))) return fail(rc);
   }
-  // the chunk assignment runs on the host, both sweeps at once
+  // the chunk assignment runs on the host, both sweeps at once, from the
+  // cell centroids
   {
     const int32_t P = ctx->nchunks;
+    std::vector<double> cx, cy, cz;
+    if ((rc = d2h(cx, pp->xcc, C, st)) || (rc = d2h(cy, pp->ycc, C, st)) ||
+        (rc = d2h(cz, pp->zcc, C, st)))
+      return fail(rc);
+    MFG_CUDA_OR(cudaStreamSynchronize(st));
+    const double *xyz[3] = {cx.data(), cy.data(), cz.data()};
+    const int force = g_chunking.load();
+    const int32_t G = sweep_groups(ctx->sweep_w);
     std::thread tb([&] {
-      assign_chunks(C, P, bw.lptr, bw.h_cells.data(), bw.h_sptr.data(), bw.h_nbs.data(),
-                    bw.h_assign);
+      choose_chunks(C, P, G, bw.lptr, bw.h_cells.data(), bw.h_sptr.data(), bw.h_nbs.data(), xyz,
+                    force, bw.h_assign, &ctx->chunk_est_us[1]);
     });
-    assign_chunks(C, P, fw.lptr, fw.h_cells.data(), fw.h_sptr.data(), fw.h_nbs.data(),
-                  fw.h_assign);
+    ctx->chunking = choose_chunks(C, P, G, fw.lptr, fw.h_cells.data(), fw.h_sptr.data(),
+                                  fw.h_nbs.data(), xyz, force, fw.h_assign, &ctx->chunk_est_us[0]);
     tb.join();
   }
   if ((rc = dev_pack(ctx, sc, fw))) return fail(rc);
@@ -3470,6 +3904,19 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
   info->sweep_chunks = ctx->sweep_mode == 1 ? ctx->nchunks : 0;
   info->sweep_lanes = ctx->sweep_mode == 1 ? ctx->sweep_lanes : 0;
   info->sweep_records = ctx->sweep_w;
+  info->sweep_chunking = ctx->chunking;
+  for (int k = 0; k < 2; k++) {
+    info->sweep_ring_records[k] = ctx->sweep_stats[k][0];
+    info->sweep_global_records[k] = ctx->sweep_stats[k][1];
+    info->sweep_cross_records[k] = ctx->sweep_stats[k][2];
+    info->sweep_model_us[k] = ctx->chunk_est_us[k];
+  }
+  return MFG_OK;
+}
+
+int mfg_set_chunking(int32_t kind) {
+  if (kind < -1 || kind > MFG_CHUNK_TRANSVERSE_YZ) return MFG_ERR_INVALID;
+  g_chunking.store(kind);
   return MFG_OK;
 }
 
@@ -3540,10 +3987,7 @@ int mfg_set_live_bc(mfg_ctx *ctx, int32_t on) {
 
 int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes) {
   if (!ctx) return MFG_ERR_INVALID;
-  if (!ctx->sweep_w || ctx->sweep_mode != 1 ||
-      !((lanes == ctx->sweep_w && ctx->lanes_ok[0]) ||
-        (lanes == ctx->sweep_w / 2 && ctx->lanes_ok[1])))
-    return MFG_ERR_UNSUPPORTED;
+  if (!ctx->sweep_w || ctx->sweep_mode != 1 || lanes != ctx->sweep_w) return MFG_ERR_UNSUPPORTED;
   ctx->sweep_lanes = lanes;
   for (int k = 0; k < 2; k++)
     if (ctx->graph[k]) {
@@ -3679,11 +4123,12 @@ int mfg_compute_timestep(mfg_ctx *ctx, int32_t iter_done) {
   return check_kernel();
 }
 
-static int launch_coop(const void *fn, int blocks, cudaStream_t st, void **args) {
+static int launch_coop(const void *fn, int blocks, int threads, size_t smem, cudaStream_t st,
+                       void **args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
-  cfg.blockDim = dim3(kPersistBlock);
-  cfg.dynamicSmemBytes = 0;
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -3710,9 +4155,10 @@ static int launch_fwd_persist(mfg_ctx *ctx, bool clamp_check, int32_t chunk_skip
                   (void *)&qnb, &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P,
                   &clamp, &ctx->dt, &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol,
                   &ctx->sweep_err, &spin, &skip, &cs};
-  const void *fn = sweep_kernel(true, ctx->sweep_w, ctx->sweep_lanes, mx);
+  const void *fn = sweep_kernel(true, ctx->sweep_w, mx);
   if (!fn) return MFG_ERR_UNSUPPORTED;
-  return launch_coop(fn, ctx->nchunks, ctx->stream, args);
+  return launch_coop(fn, ctx->nchunks, sweep_threads(ctx->sweep_w), sweep_smem(ctx->sweep_w, mx),
+                     ctx->stream, args);
 }
 
 static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
@@ -3728,9 +4174,10 @@ static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
   void *args[] = {&w.seg_begin, &w.segs, &w.cells, &recs, &w.nbs, &w.nslots, (void *)&q,
                   (void *)&qnb, &qn, &q4n, &ctx->dqf, &ctx->dq8, &ctx->diag, &P,
                   &ctx->sweep_err, &spin, &cs};
-  const void *fn = sweep_kernel(false, ctx->sweep_w, ctx->sweep_lanes, mx);
+  const void *fn = sweep_kernel(false, ctx->sweep_w, mx);
   if (!fn) return MFG_ERR_UNSUPPORTED;
-  return launch_coop(fn, ctx->nchunks, ctx->stream, args);
+  return launch_coop(fn, ctx->nchunks, sweep_threads(ctx->sweep_w), sweep_smem(ctx->sweep_w, mx),
+                     ctx->stream, args);
 }
 
 // Reads the sweeps' error word; on a timeout, re-arms the flags so that the
@@ -4132,8 +4579,8 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
   double ms_best = 1e300;
   int best = ctx->sweep_lanes;
   for (int k = 0; k < 2 && rc == MFG_OK; k++) {
-    ms[k] = -1.0;  // not usable with this context's chunk grid
-    if (!ctx->lanes_ok[k]) continue;
+    ms[k] = -1.0;  // not usable with this context's kernels
+    if (cand[k] != ctx->sweep_w) continue;
     if ((rc = mfg_set_sweep_lanes(ctx, cand[k]))) break;
     if ((rc = mfg_iterate(ctx, 2, iter_done, nullptr))) break;  // builds the graphs
     cudaEventRecord(e0, st);
@@ -4627,7 +5074,48 @@ __device__ __align__(256) double g_norm_scratch[kStaticNormBlocks * 5];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-double *g_scratch_dev[kMaxDevices] = {};
+// The array's device address as resolved in one CUDA context: a context
+// has its own copy of the module, so the address is cached per device
+// together with the unique id of the context it was resolved in (the
+// driver never reuses a context id within a process).  A device reset or a
+// different current context (a caller's own driver-API context) changes the
+// id, and the address is resolved again there.
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;
+  double *ptr = nullptr;
+};
+ScratchAddr g_scratch_dev[kMaxDevices];
+
+// Driver entry points for the current context and its id, fetched through
+// the runtime (the library does not link libcuda itself).
+using CtxGetCurrentFn = int (*)(void **);
+using CtxGetIdFn = int (*)(void *, unsigned long long *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Id of the context current on this thread, 0 where none can be had.  With
+// no context current yet, the device's primary context is made current
+// first (cudaSetDevice on the current device; it allocates nothing).
+unsigned long long current_context_id(int dev) {
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qb != cudaDriverEntryPointSuccess)
+      return 0;
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+    g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(b);
+  }
+  void *ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != 0) return 0;
+  if (!ctx) {
+    if (cudaSetDevice(dev) != cudaSuccess || g_ctx_get_current(&ctx) != 0 || !ctx) return 0;
+  }
+  unsigned long long id = 0;
+  return g_ctx_get_id(ctx, &id) == 0 ? id : 0;
+}
 
 }  // namespace
 
@@ -4652,6 +5140,62 @@ extern "C" int mfg_selftest_division(int64_t n, uint64_t seed, int64_t *mismatch
   return MFG_OK;
 }
 
+extern "C" int mfg_selftest_division_fast(int64_t n, uint64_t seed, int64_t *counts) {
+  if (n < 0 || !counts) return MFG_ERR_INVALID;
+  unsigned long long *d = nullptr;
+  MFG_CUDA(cudaMalloc(&d, 3 * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemset(d, 0, 3 * sizeof(unsigned long long));
+  if (e == cudaSuccess) {
+    k_selftest_division_fast<<<8 * 148, kBlock>>>(n, seed, d);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  unsigned long long h[3] = {0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    g_cuda_error = std::string("division self-test: ") + cudaGetErrorString(e);
+    return MFG_ERR_CUDA;
+  }
+  for (int k = 0; k < 3; k++) counts[k] = (int64_t)h[k];
+  return MFG_OK;
+}
+
+extern "C" int mfg_selftest_functions(int32_t mode, int32_t n, const double *consts,
+                                      const double *in, double *out) {
+  if (mode < 0 || mode > 3 || n < 0 || !consts || (n > 0 && (!in || !out)))
+    return MFG_ERR_INVALID;
+  if (n == 0) return MFG_OK;
+  Params P{};
+  P.gam = consts[0];
+  P.p_bar = consts[1];
+  P.gamm1 = P.gam - 1.0;
+  P.alf_l = consts[2];
+  P.lhs_omga = consts[3];
+  P.peff = P.gam * P.p_bar / (P.gam - 1.);  // forward_lusgs.cpp:1295
+  P.rho_min = consts[4];
+  P.rho_max = consts[5];
+  P.p_min = consts[6];
+  P.p_max = consts[7];
+  const size_t nin = (size_t)n * (mode == 0 ? 14 : (mode == 1 || mode == 3) ? 13 : 10);
+  const size_t nout = (size_t)n * 5;
+  double *d = nullptr;
+  MFG_CUDA(cudaMalloc(&d, sizeof(double) * (nin + nout)));
+  cudaError_t e = cudaMemcpy(d, in, sizeof(double) * nin, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_selftest_functions<<<grid_for(n), kBlock>>>(mode, n, P, d, d + nin);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + nin, sizeof(double) * nout, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    g_cuda_error = std::string("function self-test: ") + cudaGetErrorString(e);
+    return MFG_ERR_CUDA;
+  }
+  return MFG_OK;
+}
+
 extern "C" int mfg_residual_norm_static(const double *res, int32_t n_cell, double *norms,
                                         void *stream) {
   if (!res || !norms || n_cell < 0) return MFG_ERR_INVALID;
@@ -4667,18 +5211,27 @@ extern "C" int mfg_residual_norm_static(const double *res, int32_t n_cell, doubl
   double *scratch = nullptr;
   {
     // Host code cannot use the symbol itself (it names a host-side shadow),
-    // so resolve its device address once per device, with it current.
+    // so resolve its device address at the first call on a device, with it
+    // current, and again only if the current context has changed since.
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_dev[dev]) {
+    const unsigned long long id = current_context_id(dev);
+    if (!id) {
+      g_cuda_error = "mfg_residual_norm_static: no CUDA context current on device " +
+                     std::to_string(dev);
+      return MFG_ERR_CUDA;
+    }
+    ScratchAddr &a = g_scratch_dev[dev];
+    if (!a.ptr || a.ctx_id != id) {
       void *p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
       if (e != cudaSuccess) {
         g_cuda_error = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
         return MFG_ERR_CUDA;
       }
-      g_scratch_dev[dev] = static_cast<double *>(p);
+      a.ptr = static_cast<double *>(p);
+      a.ctx_id = id;
     }
-    scratch = g_scratch_dev[dev];
+    scratch = a.ptr;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int nblocks = grid_for(n_cell);  // <= kStaticNormBlocks by the check above

@@ -272,6 +272,70 @@ __device__ __forceinline__ void roe_flux(const double *ql, const double *qr, dou
   roe_flux_t<double>(ql, qr, areax, areay, areaz, area, flux_params<double>(P), flux);
 }
 
+// Correctly rounded a / b from y = RN(1 / b), for a divisor known before
+// the dividend (the LU-SGS diagonal): the quotient's dependent chain is one
+// product and four fused multiply-adds instead of a division.  Markstein's
+// theorem (P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): for y within
+// half an ulp of 1/b and q within one ulp of a/b, r = a - b q is exact and
+// RN(q + r y) = RN(a / b).  q0 = RN(a y) is within two ulps; one correction
+// step makes it faithful, the second rounds correctly.  Exponents outside
+// [2^-500, 2^500] (zeros, subnormals, overflow risks, non-finite values)
+// take the division itself.
+__device__ __forceinline__ double div_by_recip(double a, double b, double y) {
+  const int ea = (__double2hiint(a) >> 20) & 0x7FF;
+  const int eb = (__double2hiint(b) >> 20) & 0x7FF;
+  if (ea < 523 || ea > 1523 || eb < 523 || eb > 1523) return a / b;
+  const double q0 = __dmul_rn(a, y);
+  const double r0 = __fma_rn(-b, q0, a);
+  const double q1 = __fma_rn(r0, y, q0);
+  const double r1 = __fma_rn(-b, q1, a);
+  return __fma_rn(r1, y, q1);
+}
+
+// Branch-free forms of the correctly rounded reciprocal and quotient, so
+// that the divisions of a cell's several records (and the five components'
+// quotients) can overlap instead of running one after another.
+//
+// rcp_rn_fast(b) = RN(1 / b) without a division: a single-precision seed
+// (hardware approximate reciprocal of b rounded to single, relative error
+// below 2^-22) refined by Newton-Raphson steps on the FMA -- e = 1 - b y is
+// exact once y is close, y' = y + y e squares the relative error (2^-44,
+// then below half an ulp) -- and a final step of the same form, which for a
+// reciprocal within one ulp rounds correctly (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990) except when the significand of b is all ones.  ok is
+// false for that significand and outside the window 2^+-120 (zeros,
+// subnormals, non-finite values): the caller then takes 1 / b.
+__device__ __forceinline__ double rcp_rn_fast(double b, bool &ok) {
+  const int hb = __double2hiint(b);
+  const int eb = (hb >> 20) & 0x7FF;
+  ok = eb > 1023 - 120 && eb < 1023 + 120 &&
+       !((hb & 0xFFFFF) == 0xFFFFF && (unsigned)__double2loint(b) == 0xFFFFFFFFu);
+  const float bf = __double2float_rn(b);
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(bf));
+  double y = (double)r;
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  return __fma_rn(y, e, y);
+}
+// The quotient steps of div_by_recip without its branch: ok is false when
+// an exponent lies outside [2^-500, 2^500]; the caller then takes a / b.
+__device__ __forceinline__ double div_recip_fast(double a, double b, double y, bool &ok) {
+  const int ea = (__double2hiint(a) >> 20) & 0x7FF;
+  const int eb = (__double2hiint(b) >> 20) & 0x7FF;
+  ok = ea >= 523 && ea <= 1523 && eb >= 523 && eb <= 1523;
+  const double q0 = __dmul_rn(a, y);
+  const double r0 = __fma_rn(-b, q0, a);
+  const double q1 = __fma_rn(r0, y, q0);
+  const double r1 = __fma_rn(-b, q1, a);
+  return __fma_rn(r1, y, q1);
+}
+
 // FluxLUSGS3D (forward_lusgs.cpp:1271-1324) with the neighbour's sound speed
 // and conserved energy taken from its record (same expressions), in two
 // parts: what the neighbour's state and the face give, which an LU-SGS sweep
@@ -325,6 +389,40 @@ __device__ __forceinline__ void flux_lusgs_fin(const LusgsPre<T> &a, const T *DQ
   const T f2 = a.f2 + (Q2 * v_n + p * ny);
   const T f3 = a.f3 + (Q3 * v_n + p * nz);
   const T f4 = a.f4 + ((Q4 + p + peff) * v_n);
+  flux[0] = f0 - a.eig * DQ[0];
+  flux[1] = f1 - a.eig * DQ[1];
+  flux[2] = f2 - a.eig * DQ[2];
+  flux[3] = f3 - a.eig * DQ[3];
+  flux[4] = f4 - a.eig * DQ[4];
+}
+
+// flux_lusgs_fin<double> with its two divisions by Q0 as rcp_rn_fast +
+// div_recip_fast: the same bits when ok comes back true (else the caller
+// takes flux_lusgs_fin).
+__device__ __forceinline__ void flux_lusgs_fin_fast(const LusgsPre<double> &a, const double *DQ,
+                                                    double nx, double ny, double nz,
+                                                    const FluxP<double> &P, double *flux,
+                                                    bool &ok) {
+  const double gam1 = P.gamm1;
+  const double peff = P.peff;
+  const double Q0 = a.Q0 + DQ[0];
+  const double Q1 = a.Q1 + DQ[1];
+  const double Q2 = a.Q2 + DQ[2];
+  const double Q3 = a.Q3 + DQ[3];
+  const double Q4 = a.Q4 + DQ[4];
+  bool ok0, ok1, ok2;
+  const double y = rcp_rn_fast(Q0, ok0);
+  const double rv2 = div_recip_fast(0.5 * (Q1 * Q1 + Q2 * Q2 + Q3 * Q3), Q0, y, ok1);
+  const double p = gam1 * (Q4 - rv2);
+  const double f0 = DQ[1] * nx + DQ[2] * ny + DQ[3] * nz;
+  double v_n = a.vq;
+  v_n += f0;
+  v_n = div_recip_fast(v_n, Q0, y, ok2);
+  ok = ok0 && ok1 && ok2;
+  const double f1 = a.f1 + (Q1 * v_n + p * nx);
+  const double f2 = a.f2 + (Q2 * v_n + p * ny);
+  const double f3 = a.f3 + (Q3 * v_n + p * nz);
+  const double f4 = a.f4 + ((Q4 + p + peff) * v_n);
   flux[0] = f0 - a.eig * DQ[0];
   flux[1] = f1 - a.eig * DQ[1];
   flux[2] = f2 - a.eig * DQ[2];
@@ -442,27 +540,6 @@ __device__ __forceinline__ void flux_lusgs_diff(const float *q, const float *DQ,
   flux[2] = rho * v * dvn + DQ[2] * vnn + dp * ny - eig * DQ[2];
   flux[3] = rho * w * dvn + DQ[3] * vnn + dp * nz - eig * DQ[3];
   flux[4] = H * dvn + dH * vnn - eig * DQ[4];
-}
-
-// Correctly rounded a / b from y = RN(1 / b), for a divisor known before
-// the dividend (the LU-SGS diagonal): the quotient's dependent chain is one
-// product and four fused multiply-adds instead of a division.  Markstein's
-// theorem (P. Markstein, "Computation of elementary functions on the IBM
-// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): for y within
-// half an ulp of 1/b and q within one ulp of a/b, r = a - b q is exact and
-// RN(q + r y) = RN(a / b).  q0 = RN(a y) is within two ulps; one correction
-// step makes it faithful, the second rounds correctly.  Exponents outside
-// [2^-500, 2^500] (zeros, subnormals, overflow risks, non-finite values)
-// take the division itself.
-__device__ __forceinline__ double div_by_recip(double a, double b, double y) {
-  const int ea = (__double2hiint(a) >> 20) & 0x7FF;
-  const int eb = (__double2hiint(b) >> 20) & 0x7FF;
-  if (ea < 523 || ea > 1523 || eb < 523 || eb > 1523) return a / b;
-  const double q0 = __dmul_rn(a, y);
-  const double r0 = __fma_rn(-b, q0, a);
-  const double q1 = __fma_rn(r0, y, q0);
-  const double r1 = __fma_rn(-b, q1, a);
-  return __fma_rn(r1, y, q1);
 }
 
 // DQ_limit == 2 positivity limiter (forward_lusgs.cpp:939-973, :1184-1218);
@@ -605,8 +682,9 @@ __device__ __forceinline__ bool wait_rec(const double *rec, double *d, int *err,
     if (polls > 64) __nanosleep(64);
     ++polls;
     load_rec5_l2(rec, d);
+    const int gave_up = ld_relaxed(err);  // in flight beside the record's words
     if (rec5_ready(d)) return true;
-    if (ld_relaxed(err)) return false;  // another lane gave up: finish quickly
+    if (gave_up) return false;  // another lane gave up: finish quickly
     if (clock64() - t0 > max_cycles) {
       atomicExch(err, 1);
       return false;

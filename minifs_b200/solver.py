@@ -166,7 +166,7 @@ class Solver:
         self._call("mfg_set_sweep_mode", int(mode))
 
     def set_sweep_lanes(self, lanes: int):
-        """Persistent sweeps: lanes per cell (W or W / 2)."""
+        """Persistent sweeps: lanes per cell (the record slots per cell W)."""
         self._call("mfg_set_sweep_lanes", int(lanes))
 
     def autotune_sweeps(self, n_trial: int = 3) -> dict:
@@ -241,7 +241,8 @@ class Solver:
     def info(self) -> dict:
         inf = _lib.Info()
         self._call("mfg_info_get", ct.byref(inf))
-        return {k: getattr(inf, k) for k, _ in inf._fields_}
+        return {k: (list(getattr(inf, k)) if isinstance(getattr(inf, k), ct.Array)
+                    else getattr(inf, k)) for k, _ in inf._fields_}
 
 
 class BatchSolver(Solver):

@@ -5,8 +5,12 @@ holds device pointers and has no mfgpu context (creating one allocates), or
 an application whose device memory is owned by another allocator.  For them
 the norm's block partials live in a static device array instead of a
 context buffer.  This checks, through the C ABI, that two calls in a row
-give the norms of the context-based entry point, and that a residual larger
-than the static limit is refused.
+give the norms of the context-based entry point, that a residual larger
+than the static limit is refused, that a call on a 64^3 x 6-sized residual
+(1,572,864 cells: more blocks than the context-based norm's fixed grid, so
+a different reduction order) matches the norms summed on the host, that
+n_cell = 0 gives zeros, and that repeated calls leave the device's free
+memory unchanged.
 
 Kept in its own file, collected last, so that a failure here comes after
 every other test has run.
@@ -56,3 +60,42 @@ def test_static_norm_matches_context_norm_twice():
     assert rc == -1
     assert b"exceeds the static scratch limit" in lib.mfg_last_cuda_error()
     s.close()
+
+
+def test_static_norm_large_zero_and_no_allocation():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from minifs_b200 import _lib
+
+    lib = _lib.load()
+    stream = torch.cuda.current_stream()
+    out = torch.full((5,), -1.0, dtype=torch.float64, device="cuda")
+
+    def call(res, n):
+        rc = lib.mfg_residual_norm_static(ct.c_void_p(res.data_ptr()), n,
+                                          ct.c_void_p(out.data_ptr()),
+                                          ct.c_void_p(stream.cuda_stream))
+        assert rc == 0, lib.mfg_last_cuda_error()
+        torch.cuda.synchronize()
+        return out.cpu().numpy().copy()
+
+    n = 6 * 64 ** 3
+    rng = np.random.default_rng(11)
+    host = rng.standard_normal((5, n)) * np.array([1e-3, 1e-1, 1e-2, 1e-2, 1e2])[:, None]
+    res = torch.from_numpy(host.ravel()).to("cuda")
+    expected = np.sqrt(np.sum(host * host, axis=1))
+    for _ in range(2):
+        np.testing.assert_allclose(call(res, n), expected, rtol=1e-12, atol=0)
+
+    # no cells: the norms are zero
+    np.testing.assert_array_equal(call(res, 0), np.zeros(5))
+
+    # nothing is allocated on the device by further calls (the first calls
+    # above have loaded the module and resolved the scratch address)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        call(res, n)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
