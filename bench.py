@@ -84,7 +84,21 @@ def parse():
     ap.add_argument("--impl", default="mfgpu", choices=["mfgpu", "reference"])
     ap.add_argument("--size", type=int, default=64, help="hexes per cube edge (64 = 1.57M tets)")
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the reference's CPU runs (baseline and parity)")
+    ap.add_argument("--parity-iters", type=int, default=10,
+                    help="iterations of the parity check against the reference's serial build")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="fp64 form only: skip the mixed, channel and batched legs")
+    ap.add_argument("--form-iters", type=int, default=1500,
+                    help="iteration cap of the mixed form's run to its drop (x3 for the channel)")
+    ap.add_argument("--form-batch-steps", type=int, default=10,
+                    help="timed iterations of the batched form and of its sequential runs")
+    ap.add_argument("--form-cpu-iters", type=int, default=2,
+                    help="iteration cap of the reference's CPU sample on the channel workload")
+    ap.add_argument("--form-cpu", default="serial", choices=["serial", "tdtree"],
+                    help="the reference build timed on the 128^3 mixed workload (its TDTree "
+                         "set-up takes minutes there)")
     ap.add_argument("--form", default="fp64",
                     choices=["fp64", "batched", "mixed", "channel", "partition"],
                     help="fp64: the single-grid workload; batched: 64 uneven cases in one "
@@ -228,13 +242,14 @@ class ClockSampler:
 # CPU baseline: the reference's own code (oracle/_ref), else the C oracle
 # ---------------------------------------------------------------------------
 
-def cpu_reference_run(mesh, wl, iters, threads=None):
+def cpu_reference_run(mesh, wl, iters, threads=None, tdtree=True):
     from oracle import refrun
+    x0, y0, z0 = wl.get("bump_center", (0.5, 0.5, 0.5))
     flow = dict(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"], cfl_end=wl["cfl"],
                 n_steps=iters, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
-                bump_x0=0.5, bump_y0=0.5, bump_z0=0.5)
+                bump_x0=x0, bump_y0=y0, bump_z0=z0)
     threads = threads or os.cpu_count()
-    if refrun.available(tdtree=True):
+    if tdtree and refrun.available(tdtree=True):
         r = refrun.run(mesh, flow, tdtree=True, threads=threads, light=True, dump=False)
         kind, desc = "reference", f"reference TDTree build (OpenMP, {threads} threads)"
     elif refrun.available():
@@ -257,26 +272,72 @@ def cpu_port_run(pg, params, iters):
     return dict(iter_times=times, threads=1, kind="port", desc="C restatement (1 thread)")
 
 
-def cpu_baseline(mesh, pg, params, wl, iters=2):
+def ref_flow(wl, iters):
+    return dict(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"], cfl_end=wl["cfl"],
+                n_steps=iters, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
+                bump_x0=0.5, bump_y0=0.5, bump_z0=0.5)
+
+
+def cpu_baseline(mesh, pg, params, wl, iters=16):
+    """The reference's threaded build on all host cores over `iters` full
+    iterations (a sample of a few seconds at 64^3), timed per iteration."""
     r = cpu_reference_run(mesh, wl, iters)
     if r is None:
-        r = cpu_port_run(pg, params, iters)
+        r = cpu_port_run(pg, params, max(2, iters // 8))
     t = sum(r["iter_times"])
-    out = {"value": pg.n_cell * len(r["iter_times"]) / t, "unit": UNIT, "cores": r["threads"],
-           "kind": r["kind"],
-           "sample": f"{wl['name']}, {len(r['iter_times'])} full iterations after setup, "
-                     f"{r['desc']}, {t:.2f} s"}
-    # the serial build on one core beside the threaded one, same sample
+    return {"value": pg.n_cell * len(r["iter_times"]) / t, "unit": UNIT, "cores": r["threads"],
+            "kind": r["kind"],
+            "sample": f"{wl['name']}, {len(r['iter_times'])} full iterations after setup, "
+                      f"{r['desc']}, {t:.2f} s"}
+
+
+def parity_vs_reference(mesh, pg, params, wl, device, iters):
+    """The bench's own workload run `iters` iterations by the reference's
+    serial build (oracle/_ref/minifs_ref, the unmodified kernels on one core)
+    and by a fresh GPU context from the same seeded mesh and initial state:
+    entries of the final state, residual, gradient and dt extrema that
+    differ, and the largest relative difference of the per-iteration
+    residual norms (a reduction of its own order on the GPU).  The serial
+    run's iteration times are the one-core baseline."""
     from oracle import refrun
-    if r["kind"] == "reference" and r["threads"] > 1 and refrun.available():
-        flow = dict(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"], cfl_end=wl["cfl"],
-                    n_steps=iters, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
-                    bump_x0=0.5, bump_y0=0.5, bump_z0=0.5)
-        rs = refrun.run(mesh, flow, light=True, dump=False)
-        ts = sum(rs["iter_times"])
-        out["serial_1core"] = {"value": pg.n_cell * len(rs["iter_times"]) / ts, "unit": UNIT,
-                               "cores": 1, "sample": f"reference serial build, {ts:.2f} s"}
-    return out
+    from minifs_b200.solver import Solver
+    if not refrun.available():
+        return None, None
+    t0 = time.perf_counter()
+    ref = refrun.run(mesh, ref_flow(wl, iters), dump=True, dump_iters="-1")
+    ref_s = time.perf_counter() - t0
+    s = Solver(pg, params, device=device)
+    s.calculate_gradient()
+    norms = s.iterate(iters)
+    fields = {"q": ("final.q", s.download("q")), "res": ("final.res", s.download("res")),
+              "dqdx": ("final.dqdx", s.download("dqdx")),
+              "dqdy": ("final.dqdy", s.download("dqdy")),
+              "dqdz": ("final.dqdz", s.download("dqdz"))}
+    ext = np.array(s.dt_extrema)
+    s.close()
+    out = {"against": "reference serial build (oracle/_ref/minifs_ref: the unmodified MiniFS "
+                      "kernels), same seeded mesh, parameters and initial state",
+           "iterations": iters, "fields": {}}
+    total = 0
+    for name, (key, got) in fields.items():
+        want = ref[key]
+        diff = got.view(np.int64) != want.view(np.int64)
+        nd = int(np.count_nonzero(diff))
+        total += nd
+        out["fields"][name] = {"entries": int(want.size), "differing": nd,
+                               "max_abs_diff": float(np.max(np.abs(got - want))) if nd else 0.0}
+    dex = int(np.count_nonzero(ext.view(np.int64) != ref["final.dt_extrema"].view(np.int64)))
+    out["fields"]["dt_extrema"] = {"entries": 2, "differing": dex}
+    total += dex
+    rn = ref["norms"].reshape(iters, 5)
+    out["norms_max_rel_diff"] = float(np.max(np.abs(norms - rn) / np.abs(rn)))
+    out["differing_total"] = total
+    out["bitwise_equal"] = total == 0
+    ts = float(sum(ref["iter_times"]))
+    serial = {"value": pg.n_cell * iters / ts, "unit": UNIT, "cores": 1,
+              "sample": f"reference serial build, {iters} iterations, {ts:.2f} s "
+                        f"(run with its set-up and dumps {ref_s:.1f} s)"}
+    return out, serial
 
 
 # ---------------------------------------------------------------------------
@@ -559,12 +620,19 @@ def run_single(args, rank, world, local, stream, dist):
     r["roofline"]["traffic"] = read_traffic(r["roofline"]["kernel"], wl["name"])
     norms = s.residual_norm()
     info = r["info"]
-    cpu = None
+    s.close()
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cpu = cpu_baseline(mesh, pg, params, wl)
         except Exception as e:  # reported, never silently replaced
             cpu = {"error": str(e)[:200]}
+        try:
+            parity, serial = parity_vs_reference(mesh, pg, params, wl, local, args.parity_iters)
+            if serial is not None and isinstance(cpu, dict) and "value" in cpu:
+                cpu["serial_1core"] = serial
+        except Exception as e:
+            parity = {"error": str(e)[:300]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
@@ -585,14 +653,201 @@ def run_single(args, rank, world, local, stream, dist):
             "flux_plus_gradient": r["flux_plus_gradient"],
             "phases": r["phases"],
             "cpu_baseline": cpu,
+            "parity": parity,
             "e2e": r["e2e"],
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
             "residual_norm": [float(x) for x in norms],
             "prep": prep,
         }
+        if world == 1 and not args.no_forms:
+            line["forms"] = run_forms(args, local, stream, not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
-    s.close()
+
+
+# ---------------------------------------------------------------------------
+# the metric's other legs in the default run: mixed precision, batched cases
+# and the channel, each to its residual drop (bounded) with clocks sampled
+# ---------------------------------------------------------------------------
+
+def _drop_runs(prep, q0, params, C, stream, drop, max_iter, precisions, fp64_flux_below):
+    """Each precision from the same device-prepared grid and initial state to
+    `drop` (at most max_iter iterations): iterations, device ms, throughput,
+    final state."""
+    from minifs_b200.solver import Solver
+    out, states = {}, {}
+    for prec in precisions:
+        s = Solver.from_device_prep(prep, params, q0, precision=prec)
+        s.set_stream(stream.cuda_stream)
+        s.calculate_gradient()
+        tail = fp64_flux_below if prec == "mixed" else None
+        it, ms, reached, switched = to_drop(s, stream, drop, max_iter, fp64_flux_below=tail)
+        info = s.info()
+        out[prec] = {"iterations": it, "ms": ms, "drop": reached, "reached": reached <= drop,
+                     "cell_updates_per_s": C * it / (ms / 1e3),
+                     "sweep_chunking": info["sweep_chunking"],
+                     "sweep_model_us": info["sweep_model_us"]}
+        if tail is not None:
+            out[prec]["fp64_flux_from_iteration"] = switched
+        states[prec] = s.download("q")
+        s.close()
+    return out, states
+
+
+def _form_errors(states, n, p_bar):
+    from minifs_b200.compare import state_component_err, state_rel_err
+    return {"physical_scales": state_rel_err(states["mixed"], states["fp64"], n, p_bar),
+            "per_component": state_component_err(states["mixed"], states["fp64"], n)}
+
+
+def form_mixed(args, local, stream, with_cpu):
+    """Configuration 3: the 128^3 x 6 cube (Mach 0.8, alpha 1.25 deg, CFL 20),
+    FP64 and mixed forms each to a 1e-6 residual drop."""
+    from minifs_b200 import grid as gr, meshgen
+    wl = mixed_workload(args.mixed_size)
+    mesh = meshgen.cube_mesh(wl["n"], jitter=wl["jitter"], seed=wl["seed"])
+    params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+    prep = gr.DevicePrep(mesh, device=local)
+    q0 = prep.init_flow(params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"])
+    C, n = prep.n_cell, prep.n
+    with ClockSampler(local) as clk:
+        runs, states = _drop_runs(prep, q0, params, C, stream, 1e-6, args.form_iters,
+                                  ("fp64", "mixed"), None)
+    prep.close()
+    f, m = runs["fp64"], runs["mixed"]
+    out = {"workload": wl["name"], "cells": C, "drop_target": 1e-6, "fp64": f, "mixed": m,
+           "mixed_over_fp64": m["cell_updates_per_s"] / f["cell_updates_per_s"],
+           "time_to_drop_ratio": f["ms"] / m["ms"] if m["reached"] and f["reached"] else None,
+           "state_rel_err_vs_fp64_at_drop": _form_errors(states, n, params.p_bar),
+           "clocks": clk.summary()}
+    if with_cpu:
+        # the TDTree build's own set-up (METIS on the cell graph) takes minutes
+        # at 12.6M cells: the serial build by default, the threaded one on
+        # request
+        out["cpu_baseline"] = _cpu_sample(mesh, wl, 1, tdtree=args.form_cpu == "tdtree")
+    return out
+
+
+def form_channel(args, local, stream, with_cpu):
+    """Configuration 5: the 4x1x1 channel with a wall bump (Mach 0.7, CFL 30),
+    FP64 and mixed forms each to a 1e-8 residual drop (the mixed form's flux
+    goes FP64 below a 1e-6 drop), and the mixed wall pressure against FP64."""
+    from minifs_b200 import grid as gr, meshgen
+    wl = channel_workload()
+    mesh = meshgen.channel_mesh(jitter=wl["jitter"], seed=wl["seed"])
+    params = gr.make_params(mach=wl["mach"], alpha=wl["alpha"], cfl_start=wl["cfl"])
+    prep = gr.DevicePrep(mesh, device=local)
+    q0 = prep.init_flow(params, bump_amp=wl["bump_amp"], bump_sigma=wl["bump_sigma"],
+                        bump_center=wl["bump_center"])
+    C, n, G = prep.n_cell, prep.n, prep.n_bface
+    with ClockSampler(local) as clk:
+        runs, states = _drop_runs(prep, q0, params, C, stream, wl["drop"], args.form_iters * 3,
+                                  ("fp64", "mixed"), 1e-6)
+    bct = np.asarray(prep.bctype)[:G]
+    prep.close()
+    wf = np.nonzero(bct == 3)[0]
+    c1 = np.asarray(mesh.f2c).reshape(-1, 2)[wf, 0]
+    pa, pb = states["mixed"][4 * n + c1], states["fp64"][4 * n + c1]
+    d = np.abs(pa - pb) / (np.abs(pb) + params.p_bar)
+    f, m = runs["fp64"], runs["mixed"]
+    out = {"workload": wl["name"], "cells": C, "drop_target": wl["drop"], "fp64": f, "mixed": m,
+           "mixed_over_fp64": m["cell_updates_per_s"] / f["cell_updates_per_s"],
+           "time_to_drop_ratio": f["ms"] / m["ms"] if m["reached"] and f["reached"] else None,
+           "state_rel_err_vs_fp64_at_drop": _form_errors(states, n, params.p_bar),
+           "wall_pressure_rel_err_vs_fp64": {"max": float(d.max()),
+                                             "rms": float(np.sqrt(np.mean(d * d))),
+                                             "faces": int(wf.size),
+                                             "scale": "p + p_bar"},
+           "clocks": clk.summary()}
+    if with_cpu:
+        out["cpu_baseline"] = _cpu_sample(mesh, wl, args.form_cpu_iters, tdtree=True)
+    return out
+
+
+def _cpu_sample(mesh, wl, iters, tdtree):
+    """The reference's threaded build on all host cores (tdtree) or its serial
+    build on one core, capped at `iters` iterations of the form's workload
+    (its set-up time stated apart)."""
+    t0 = time.perf_counter()
+    r = cpu_reference_run(mesh, wl, iters, tdtree=tdtree)
+    if r is None:
+        return None
+    t = sum(r["iter_times"])
+    return {"value": mesh.n_cell * len(r["iter_times"]) / t, "unit": UNIT, "cores": r["threads"],
+            "kind": r["kind"],
+            "sample": f"{wl['name']}: {len(r['iter_times'])} full iterations (iteration-capped) "
+                      f"after set-up, {r['desc']}, {t:.2f} s; run with its set-up "
+                      f"{time.perf_counter() - t0:.1f} s"}
+
+
+def form_batched(args, local, stream):
+    """Configuration 4: 64 cube cases (n uniform in 8..48, Mach U(0.3, 0.8),
+    alpha U(-5, 5) deg, jitter U(0, 0.2)h) in one context against the same
+    cases one after another in their own contexts, FP64 and mixed, each over
+    the same timed iterations."""
+    import torch
+    from minifs_b200.solver import BatchSolver, Solver
+    bw = batched_workload(args.ncase)
+    grids, params = build_batched(bw)
+    cells = int(sum(g.n_cell for g in grids))
+    steps = args.form_batch_steps
+    out = {"workload": bw["name"], "ncase": len(grids), "cells": cells, "steps": steps}
+    with ClockSampler(local) as clk:
+        for prec in ("fp64", "mixed"):
+            seq_ms = 0.0
+            for pg, p in zip(grids, params):
+                s = Solver(pg, p, device=local, precision=prec)
+                s.set_stream(stream.cuda_stream)
+                s.calculate_gradient()
+                s.iterate(3, norms=False)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                s.iterate(steps, norms=False)
+                e1.record(stream)
+                e1.synchronize()
+                seq_ms += e0.elapsed_time(e1)
+                s.close()
+            b = BatchSolver(grids, params, device=local, precision=prec)
+            b.set_stream(stream.cuda_stream)
+            b.calculate_gradient()
+            b.iterate(3, norms=False)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.iterate(steps, norms=False)
+            e1.record(stream)
+            e1.synchronize()
+            bms = e0.elapsed_time(e1)
+            info = b.info()
+            b.close()
+            bv, sv = cells * steps / (bms / 1e3), cells * steps / (seq_ms / 1e3)
+            out[prec] = {"value": bv, "unit": UNIT, "ms_per_step": bms / steps,
+                         "sequential": {"value": sv, "ms_per_step": seq_ms / steps,
+                                        "how": "each case in its own context, graph-captured "
+                                               "fused iterations, one after another; device "
+                                               "time summed"},
+                         "batched_over_sequential": bv / sv,
+                         "sweep_chunks": info["sweep_chunks"],
+                         "sweep_chunking": info["sweep_chunking"],
+                         "sweep_model_us": info["sweep_model_us"]}
+    out["clocks"] = clk.summary()
+    return out
+
+
+def run_forms(args, local, stream, with_cpu):
+    """The metric's mixed, batched and channel legs (configurations 3-5)."""
+    forms = {}
+    for name, fn in (("mixed", lambda: form_mixed(args, local, stream, with_cpu)),
+                     ("channel", lambda: form_channel(args, local, stream, with_cpu)),
+                     ("batched", lambda: form_batched(args, local, stream))):
+        t0 = time.perf_counter()
+        try:
+            forms[name] = fn()
+        except Exception as e:  # reported, never silently replaced
+            forms[name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
+        forms[name]["wall_s"] = time.perf_counter() - t0
+    return forms
 
 
 def run_partition(args, rank, world, local, dist):
