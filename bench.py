@@ -43,8 +43,9 @@ MPI-mode exchanges between them: device copies between the parts of one
 process, NCCL point-to-point and all-reduce between processes (part z on
 rank z mod N).  Strong scaling: the whole mesh's cells per step.
 
-Before the warm-up the sweep launch parameters are chosen by measurement
-on the workload's own grid (mfg_autotune_sweeps) and reported.
+Before the warm-up the launch parameters (sweep kernels, chunk assignment,
+sweep mode, face-kernel register caps, gradient block sizes) are chosen by
+measurement on the workload's own grid (mfg_autotune) and reported.
 
 With --gpus N > 1 (one process per GPU under torchrun) every rank runs its
 own replica of the workload (the path has no exchange step) and rank 0
@@ -112,6 +113,8 @@ def parse():
                     help="mixed form: also iterate both forms to a 1e-6 residual drop "
                          "(at most this many iterations) and time it")
     ap.add_argument("--ncase", type=int, default=64)
+    ap.add_argument("--tune-trials", type=int, default=3,
+                    help="timed iterations per autotuner trial (0: no autotuning)")
     ap.add_argument("--parts", type=int, default=0,
                     help="partition form: parts of the mesh (default: one per GPU)")
     ap.add_argument("--profile-region", action="store_true",
@@ -475,10 +478,10 @@ def measure(s, counts, args, stream, dist, world, local, total_cells=None):
     def max_over_ranks(ms):
         return shard.reduce_max(ms, dist, "cuda")
 
-    # launch parameters of the sweeps chosen by measurement on this grid
-    # (the state is left as it was), then the warm-up (builds the CUDA graphs)
+    # launch parameters chosen by measurement on this grid (the state is left
+    # as it was), then the warm-up (builds the CUDA graphs)
     s.calculate_gradient()
-    tuned = s.autotune_sweeps(2) if info["sweep_mode"] == 1 else None
+    tuned = s.autotune(args.tune_trials) if args.tune_trials > 0 else None
     info = s.info()
     s.iterate(max(args.warmup, 3), norms=False)
     barrier()
@@ -500,9 +503,9 @@ def measure(s, counts, args, stream, dist, world, local, total_cells=None):
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     out = {"ms": ms, "value": total * args.steps / (ms / 1e3), "launches": int(launches),
            "clocks": clk.summary(), "info": info,
-           "autotuned": None if tuned is None else {
-               "sweep_lanes_per_cell": tuned["lanes_per_cell"], "sweep_chunks": tuned["chunks"],
-               "sweep_block_threads": 64, "trial_ms_per_iter": tuned["ms_per_iter"]}}
+           "autotuned": None if tuned is None else dict(
+               tuned, sweep_chunks=info["sweep_chunks"], sweep_kernel=info["sweep_kernel"],
+               sweep_chunking=info["sweep_chunking"], sweep_model_us=info["sweep_model_us"])}
 
     # phase breakdown with CUDA events on the same stream (same fused kernels)
     phase_iters = max(3, min(args.steps, 10))
@@ -811,6 +814,9 @@ def form_batched(args, local, stream):
             b = BatchSolver(grids, params, device=local, precision=prec)
             b.set_stream(stream.cuda_stream)
             b.calculate_gradient()
+            # the batch's sweep kernels and chunks as chosen at creation (a
+            # rebuild of 12M cells takes seconds); the other knobs timed
+            tuned = b.autotune(2, rebuild=False) if args.tune_trials > 0 else None
             b.iterate(3, norms=False)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -828,6 +834,8 @@ def form_batched(args, local, stream):
                                                "fused iterations, one after another; device "
                                                "time summed"},
                          "batched_over_sequential": bv / sv,
+                         "autotuned": tuned,
+                         "sweep_kernel": info["sweep_kernel"],
                          "sweep_chunks": info["sweep_chunks"],
                          "sweep_chunking": info["sweep_chunking"],
                          "sweep_model_us": info["sweep_model_us"]}

@@ -119,6 +119,7 @@ typedef struct mfg_info {
    * chunk, older than the ring) and from another chunk (polled in L2) */
   int32_t sweep_ring_records[2], sweep_global_records[2], sweep_cross_records[2];
   double sweep_model_us[2];         /* modelled duration of each sweep with its chunks */
+  int32_t sweep_kernel;             /* persistent sweep kernels (MFG_SWEEP_*) */
 } mfg_info;
 
 /* ---- parameters -------------------------------------------------------- */
@@ -186,13 +187,68 @@ int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes);
 #define MFG_CHUNK_TRANSVERSE_XY 1
 #define MFG_CHUNK_TRANSVERSE_XZ 2
 #define MFG_CHUNK_TRANSVERSE_YZ 3
+#define MFG_CHUNK_TRANSVERSE_ANY 4 /* the best transverse grid over any axis pair */
 int mfg_set_chunking(int32_t kind);
+/* The persistent sweep kernels.  MFG_SWEEP_DEEP: one block per SM, producer
+ * warps staging each cell's static terms ahead for consumer lane pairs that
+ * run only the dependent chain -- short per-level latency, for levels of up
+ * to about 128 cells per SM.  MFG_SWEEP_WIDE: many 64-thread blocks per SM
+ * with small chunks -- for wider levels, whose latency one block hides
+ * behind another's work.  A context takes WIDE when its widest level would
+ * give a DEEP block more than two passes per level; mfg_set_sweep_kernel
+ * forces a kind for contexts created afterwards (-1 restores the default).
+ * Identical results either way. */
+#define MFG_SWEEP_DEEP 0
+#define MFG_SWEEP_WIDE 1
+int mfg_set_sweep_kernel(int32_t kind);
 /* Times n_trial fused iterations with each lane count on this context's own
  * grid and keeps the faster (ms_out[2], optional, receives the ms per
  * iteration of W and W / 2 lanes).  The state and the dt extrema are
  * restored afterwards; res, dt, Diag, DQ and the gradient hold the last
  * trial iteration's values.  iter_done: the CFL ramp position to time at. */
 int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double *ms_out);
+/* Launch parameters chosen by measurement on the context's own grid (the
+ * reference's counterpart is TDTree's fixed partition sizes,
+ * grid_polyhedra.cpp:380,405): one pass of coordinate descent over the
+ * knobs below, each candidate timed over n_trial fused iterations after two
+ * warm-up ones, the fastest kept.  The state and the dt extrema are restored
+ * after every trial; res, dt, Diag, DQ and the gradient hold the last
+ * trial's values.  iter_done: the CFL ramp position to time at.  rep
+ * (optional) receives every trial.  Knobs:
+ *   MFG_KNOB_SWEEP_KERNEL  persistent sweep kernels (MFG_SWEEP_*; the
+ *                          chunk tables are rebuilt for each)
+ *   MFG_KNOB_CHUNKING      chunk assignment: MFG_CHUNK_VOTE or
+ *                          MFG_CHUNK_TRANSVERSE_ANY (tables rebuilt)
+ * (flags & MFG_TUNE_NO_REBUILD leaves these two as the context has them:
+ * a rebuild of a grid of many millions of cells takes seconds)
+ *   MFG_KNOB_SWEEP_MODE    1 persistent, 0 one launch per level (FP64 only)
+ *   MFG_KNOB_GATHER_BLOCKS resident blocks per SM the fused face gather is
+ *                          compiled for (its register cap): 2, 3, 4
+ *   MFG_KNOB_FLUX_BLOCKS   the same for the per-face Roe flux
+ *   MFG_KNOB_NODE_BLOCK    threads per block of the node values
+ *   MFG_KNOB_GRAD_BLOCK    threads per block of the gradient face sums
+ * Results are identical with every choice. */
+#define MFG_KNOB_SWEEP_KERNEL 0
+#define MFG_KNOB_CHUNKING 1
+#define MFG_KNOB_SWEEP_MODE 2
+#define MFG_KNOB_GATHER_BLOCKS 3
+#define MFG_KNOB_FLUX_BLOCKS 4
+#define MFG_KNOB_NODE_BLOCK 5
+#define MFG_KNOB_GRAD_BLOCK 6
+#define MFG_TUNE_KNOBS 8
+#define MFG_TUNE_CANDS 4
+typedef struct mfg_tune_report {
+  int32_t n_knobs;
+  int32_t knob[MFG_TUNE_KNOBS];                 /* MFG_KNOB_* of each row */
+  int32_t n_cand[MFG_TUNE_KNOBS];
+  int32_t cand[MFG_TUNE_KNOBS][MFG_TUNE_CANDS]; /* candidate values */
+  double ms[MFG_TUNE_KNOBS][MFG_TUNE_CANDS];    /* ms per fused iteration; < 0: not usable */
+  int32_t chosen[MFG_TUNE_KNOBS];               /* the value kept */
+  double ms_initial, ms_final;                  /* before and after */
+} mfg_tune_report;
+#define MFG_TUNE_NO_REBUILD 1
+int mfg_autotune(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, int32_t flags,
+                 mfg_tune_report *rep);
 /* Failure-detection self-test of the bounded waits: runs a forward sweep
  * whose first chunk is withheld, so the cells that depend on it wait for
  * flags that are never set; each wait gives up after spin_cycles SM cycles.

@@ -68,7 +68,22 @@ class Info(ct.Structure):
                 ("sweep_chunks", ct.c_int32), ("sweep_lanes", ct.c_int32),
                 ("sweep_records", ct.c_int32), ("sweep_chunking", ct.c_int32),
                 ("sweep_ring_records", ct.c_int32 * 2), ("sweep_global_records", ct.c_int32 * 2),
-                ("sweep_cross_records", ct.c_int32 * 2), ("sweep_model_us", ct.c_double * 2)]
+                ("sweep_cross_records", ct.c_int32 * 2), ("sweep_model_us", ct.c_double * 2),
+                ("sweep_kernel", ct.c_int32)]
+
+
+TUNE_KNOBS, TUNE_CANDS = 8, 4
+KNOBS = {0: "sweep_kernel", 1: "sweep_chunking", 2: "sweep_mode", 3: "face_gather_blocks_per_sm",
+         4: "face_flux_blocks_per_sm", 5: "node_values_block", 6: "grad_faces_block"}
+
+
+class TuneReport(ct.Structure):
+    _fields_ = [("n_knobs", ct.c_int32), ("knob", ct.c_int32 * TUNE_KNOBS),
+                ("n_cand", ct.c_int32 * TUNE_KNOBS),
+                ("cand", (ct.c_int32 * TUNE_CANDS) * TUNE_KNOBS),
+                ("ms", (ct.c_double * TUNE_CANDS) * TUNE_KNOBS),
+                ("chosen", ct.c_int32 * TUNE_KNOBS), ("ms_initial", ct.c_double),
+                ("ms_final", ct.c_double)]
 
 
 class RawGrid(ct.Structure):
@@ -141,7 +156,10 @@ def load(build_if_missing: bool = True):
         "mfg_set_sweep_mode": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_sweep_lanes": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_chunking": (ct.c_int, [ct.c_int32]),
+        "mfg_set_sweep_kernel": (ct.c_int, [ct.c_int32]),
         "mfg_autotune_sweeps": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
+        "mfg_autotune": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, ct.c_int32,
+                                    ct.POINTER(TuneReport)]),
         "mfg_selftest_sweep_timeout": (ct.c_int, [ctxp, ct.c_int64]),
         "mfg_selftest_division": (ct.c_int, [ct.c_int64, ct.c_uint64,
                                              ct.POINTER(ct.c_int64)]),

@@ -46,6 +46,7 @@ constexpr int kBlock = 256;
 // from 128-thread ones (0.137 -> 0.117 and 0.250 -> 0.240 ms at 64^3).
 constexpr int kNodeBlock = 512;
 constexpr int kGradBlock = 128;
+constexpr int kGradBlockMax = 256;  // the largest block mfg_autotune tries
 constexpr int kNormBlocks = 1184;  // 8 x 148 SMs, fixed so the norm reduction order is fixed
 constexpr int kSegBlocks = 32;     // blocks per case of the batched norm reduction
 
@@ -349,8 +350,8 @@ __device__ __forceinline__ void face_gather_cell(
   gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
 }
 
-template <bool FLUX, bool DT, bool DIAG, bool PRE>
-__global__ void __launch_bounds__(kBlock, MFG_GATHER_MINB)
+template <bool FLUX, bool DT, bool DIAG, bool PRE, int MINB = MFG_GATHER_MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
 k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
               const double *__restrict__ q8, const double *__restrict__ vol,
               double *__restrict__ res, int res_zero, double *__restrict__ dt,
@@ -367,8 +368,8 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
 // local time step and its CellIsMG switch (a discrete decision, kept in FP64
 // so that both forms take it alike), the Diag terms and all sums in FP64 in
 // the same face order.
-template <bool FLUX, bool DT, bool DIAG, bool PRE>
-__global__ void __launch_bounds__(kBlock, MFG_GATHER_MINB)
+template <bool FLUX, bool DT, bool DIAG, bool PRE, int MINB = MFG_GATHER_MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
 k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
                  const double *__restrict__ q8, const double *__restrict__ vol,
                  double *__restrict__ res, int res_zero, double *__restrict__ dt,
@@ -479,8 +480,8 @@ __device__ __forceinline__ void reconstruct(double *q, int32_t c, int32_t C, int
 // the face states reconstructed to second order first (a face whose
 // reconstructed density or absolute pressure is not positive keeps its
 // first-order states).
-template <bool MX, bool RECON>
-__global__ void __launch_bounds__(kBlock, MFG_FLUX_MINB)
+template <bool MX, bool RECON, int MINB = MFG_FLUX_MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
 k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restrict__ q8,
             Params P0, Cases cs, double *__restrict__ fflux, int32_t C, int64_t n,
             const Cen *__restrict__ fcen, const Cen *__restrict__ ccen,
@@ -1360,6 +1361,455 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent chunked sweeps for wide levels.  The same tables with many
+// small chunks -- several blocks of 64 threads per SM, kWideRing positions
+// in each block's ring -- so that a level of many cells is spread over many
+// blocks and an SM hides one block's waits behind another's work.  A cell is
+// swept by a group of W lanes: lane j computes the flux of record j and owns
+// the components k = j, j + W, ... < 5 of the increment (the ordered sum over
+// the records and the division); every lane applies the limiter.  The
+// operations and their order per component are those of the one-thread
+// form, so the results are the same bits.  A block walks its chunk level by
+// level with __syncthreads between levels; a group's work items (level,
+// pass) are pipelined: indices loaded two items ahead, the read-only data
+// staged into shared memory by cp.async one item ahead.
+// ---------------------------------------------------------------------------
+constexpr int kWideBlock = 64;  // threads per block
+constexpr int kWideMinB = 6;    // resident blocks per SM (register cap)
+constexpr int kWideRing = 128;  // positions of a block's ring
+static_assert((kWideRing & (kWideRing - 1)) == 0, "ring size must be a power of two");
+
+// What a lane knows about its group's position on a future level: the
+// position, its ring slot, the cell, the record count, this lane's
+// neighbours (flags kMark / kInRing) and their ring slots; cell < 0 = none.
+template <int R>
+struct WideRegs {
+  int32_t p, slot, cell, ns;
+  uint32_t nb[R];
+  int32_t nslot[R];
+};
+
+// Everything a group reads for one cell that no sweep writes, staged into
+// shared memory by cp.async one item ahead: neighbour states and records
+// (by the lane of the record), the cell's state and Diag (lane 0), and res
+// (forward) or the cell's forward increment (backward), component k by the
+// lane that owns it.  The mixed form (MX) stages the single-precision
+// neighbour records.
+// Padding of a stage so that consecutive groups' stages start 16 bytes
+// apart modulo 128: the groups of a warp then read their records from
+// different shared-memory banks (without it every group's record k sits in
+// the same bank and a warp's stage reads are 4- to 8-way conflicts).
+constexpr int wide_pad_bytes(int raw) {
+  const int a16 = (raw + 15) / 16 * 16;
+  return a16 - raw + ((16 - a16 % 128) % 128 + 128) % 128;
+}
+template <int W, bool MX>
+struct __align__(16) WideStage {
+  typename SweepTypes<MX>::Q qn[W][Q_STRIDE];
+  typename SweepTypes<MX>::Rec rec[W];
+  double qc[Q_STRIDE];
+  double in5[5];
+  double diag;
+  char pad[wide_pad_bytes(int(sizeof(typename SweepTypes<MX>::Q)) * W * Q_STRIDE +
+                           int(sizeof(typename SweepTypes<MX>::Rec)) * W + 8 * (Q_STRIDE + 6))];
+};
+static_assert(sizeof(WideStage<4, false>) % 128 == 16 && sizeof(WideStage<4, true>) % 128 == 16 &&
+                  sizeof(WideStage<8, false>) % 128 == 16 && sizeof(WideStage<8, true>) % 128 == 16,
+              "stage stride");
+
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int W, int L>
+__device__ __forceinline__ void wide_fetch(const int32_t *s_segs, const int32_t *__restrict__ segs,
+                                           int32_t sg0, int32_t sg, int32_t sg1, int32_t pbase,
+                                           int32_t pos_in_level, int32_t lane,
+                                           const PosCell *__restrict__ pcs,
+                                           const int32_t *__restrict__ pnb,
+                                           const int32_t *__restrict__ pslot,
+                                           WideRegs<W / L> &o) {
+  o.cell = -1;
+  o.ns = 0;
+#pragma unroll
+  for (int r = 0; r < W / L; r++) {
+    o.nb[r] = 0;
+    o.nslot[r] = 0;
+  }
+  if (sg >= sg1) return;
+  const int32_t i = sg - sg0;
+  const int32_t a = i < kSegCache ? s_segs[i] : segs[sg];
+  const int32_t b = i + 1 <= kSegCache ? s_segs[i + 1] : segs[sg + 1];
+  const int32_t p = a + pos_in_level;
+  if (p >= b) return;
+  const PosCell x = pcs[p];
+  o.p = p;
+  o.slot = (p - pbase) & (kWideRing - 1);
+  o.cell = x.cell;
+  o.ns = x.ns;
+#pragma unroll
+  for (int r = 0; r < W / L; r++) {  // padding reads 0
+    o.nb[r] = (uint32_t)pnb[(int64_t)p * W + lane + L * r];
+    o.nslot[r] = pslot[(int64_t)p * W + lane + L * r];
+  }
+}
+
+template <int W, int L, bool FWD, bool MX>
+__device__ __forceinline__ void wide_stage_copy(const WideRegs<W / L> &o, int32_t lane,
+                                           WideStage<W, MX> &st, const double *q8,
+                                           const typename SweepTypes<MX>::Q *qnb,
+                                           const typename SweepTypes<MX>::Rec *prec,
+                                           const double *res, const double *diag,
+                                           const double *dqf, int32_t C) {
+  if (o.cell < 0) return;
+  // 16-byte pieces of the neighbour record (64 B FP64, 32 B FP32) and of the
+  // sweep record (32 B, 16 B)
+  constexpr int kQ = sizeof(st.qn[0]) / 16, kR = sizeof(st.rec[0]) / 16;
+#pragma unroll
+  for (int r = 0; r < W / L; r++) {
+    const int j = lane + L * r;
+    if (j < o.ns) {
+      const char *qs =
+          reinterpret_cast<const char *>(qnb + (int64_t)(o.nb[r] & kIdMask) * Q_STRIDE);
+      char *qd = reinterpret_cast<char *>(&st.qn[j][0]);
+#pragma unroll
+      for (int i = 0; i < kQ; i++) cp_async16(qd + 16 * i, qs + 16 * i);
+      const char *rs = reinterpret_cast<const char *>(prec + (int64_t)o.p * W + j);
+      char *rd = reinterpret_cast<char *>(&st.rec[j]);
+#pragma unroll
+      for (int i = 0; i < kR; i++) cp_async16(rd + 16 * i, rs + 16 * i);
+    }
+  }
+  if (lane == 0) {
+    const double *qs = q8 + (int64_t)o.cell * Q_STRIDE;
+#pragma unroll
+    for (int i = 0; i < 4; i++) cp_async16(&st.qc[2 * i], qs + 2 * i);
+    cp_async8(&st.diag, diag + o.cell);
+  }
+  for (int k = lane; k < 5; k += L)
+    cp_async8(&st.in5[k], FWD ? res + (int64_t)k * C + o.cell : dqf + (int64_t)o.cell * Q_STRIDE + k);
+}
+
+// One cell of one sweep level on a lane group, from its stage (the group's
+// lanes only wait for one another: a cell is stored as soon as its own
+// inputs are in).  sh: the group's scratch (W * 5 + 5 doubles); ring: the
+// block's increments of its last kWideRing positions.  FWD: DQ* = (res - sum_j
+// 0.5 area_j F_j) / Diag, limited except for the first cell (SolveLUSGS3D
+// forward, forward_lusgs.cpp:799-870); backward: DQ = DQ* - (sum_j area_j
+// F_j) / (2 Diag), limited (:871-940).
+template <int W, int L, bool FWD, bool MX>
+__device__ __forceinline__ void wide_cell(
+    const WideRegs<W / L> &o, int32_t lane, const WideStage<W, MX> &st, double *sh, double *ring,
+    const double (*pre)[5],
+    const double *src, double *dst, double *rearm, int32_t first_cell, const Params &P0,
+    const double *s_lim, int clamp_check, double *__restrict__ dt, double *__restrict__ diag,
+    const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
+    const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err,
+    long long spin, const Cases &cs) {
+  if (o.cell < 0) return;  // the whole group
+  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+  const int32_t c = o.cell;
+  const int32_t cse = case_of(cs, c);
+  const Params P = params_of(P0, cs, c);
+  // what the cell's own staged data give, formed while its neighbours'
+  // increments are still awaited: the reciprocal of the diagonal term the
+  // increment is divided by, and the velocity square of the limiter
+  const double den = FWD ? st.diag : 2.0 * st.diag;
+  const double rden = 1.0 / den;
+  const double vv = st.qc[1] * st.qc[1] + st.qc[2] * st.qc[2] + st.qc[3] * st.qc[3];
+  // record j = lane + L r < ns: w_j * FluxLUSGS3D(q[nb_j], DQ[nb_j], n_j)
+#pragma unroll
+  for (int r = 0; r < W / L; r++) {
+    const int j = lane + L * r;
+    if (j < o.ns) {
+      const uint32_t b = o.nb[r];
+      // FP64: the part of the product the neighbour's state and the face
+      // give, before the increment is waited for
+      LusgsPre<double> a{};
+      if constexpr (!MX) {
+        double qn[Q_STRIDE];
+#pragma unroll
+        for (int k = 0; k < Q_STRIDE; k++) qn[k] = st.qn[j][k];
+        a = flux_lusgs_pre(qn, st.rec[j].nx, st.rec[j].ny, st.rec[j].nz, flux_params<double>(P));
+      }
+      double dn[5];
+      if (b & kInRing) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) dn[k] = ring[o.nslot[r] * 5 + k];
+      } else if ((b & kMark) && !rec5_ready(pre[r])) {
+        wait_rec(src + (int64_t)(b & kIdMask) * Q_STRIDE, dn, err, spin);
+      } else {  // read at the start of the item (see wide_chunk)
+#pragma unroll
+        for (int k = 0; k < 5; k++) dn[k] = pre[r][k];
+      }
+      if constexpr (MX) {
+        // off-diagonal product in FP32, accumulated in FP64 below
+        float qf[Q_STRIDE], df[5], ff[5];
+#pragma unroll
+        for (int k = 0; k < Q_STRIDE; k++) qf[k] = st.qn[j][k];
+#pragma unroll
+        for (int k = 0; k < 5; k++) df[k] = (float)dn[k];
+        const SweepRecF rr = st.rec[j];
+        flux_lusgs_diff(qf, df, rr.nx, rr.ny, rr.nz, flux_params<float>(P), ff);
+#pragma unroll
+        for (int k = 0; k < 5; k++) sh[j * 5 + k] = (double)(rr.w * ff[k]);
+      } else {
+        double f[5];
+        const SweepRec rr = st.rec[j];
+        flux_lusgs_fin(a, dn, rr.nx, rr.ny, rr.nz, flux_params<double>(P), f);
+#pragma unroll
+        for (int k = 0; k < 5; k++) sh[j * 5 + k] = rr.w * f[k];
+      }
+    }
+  }
+  // LimitTimeStep's clamp (fused forward sweep, and only when some case's
+  // dt ratio exceeds its limit): every component lane reads dt[c] before
+  // lane 0 may write it below
+  double dg = st.diag, lim = -1.0;
+  bool clamped = false;
+  if (FWD && clamp_check && lane < 5) {
+    lim = (cse < kCaseCache) ? s_lim[cse] : clamp_limit(P, dt_ext + 2 * cse);
+    if (lim > 0.0 && dt[c] > lim) {
+      double qc[Q_STRIDE];
+#pragma unroll
+      for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
+      dg = clamped_diag(c, qc, P, lim, cptr, slots, vol);
+      clamped = true;
+    }
+  }
+  __syncwarp(gmask);
+  // components k = lane, lane + L, ... < 5 (at most two per lane, as two
+  // independent chains); records summed in order
+  {
+    constexpr int kC = (5 + L - 1) / L;
+    double acc[kC];
+#pragma unroll
+    for (int i = 0; i < kC; i++) {
+      const int k = lane + L * i;
+      acc[i] = (FWD && k < 5) ? st.in5[k] : 0.0;
+    }
+    for (int32_t j = 0; j < o.ns; j++) {
+#pragma unroll
+      for (int i = 0; i < kC; i++) {
+        const int k = lane + L * i;
+        if (k < 5) {
+          if (FWD)
+            acc[i] -= sh[j * 5 + k];
+          else
+            acc[i] += sh[j * 5 + k];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kC; i++) {
+      const int k = lane + L * i;
+      if (k < 5)
+        sh[W * 5 + k] = FWD ? (clamped ? acc[i] / dg : div_by_recip(acc[i], den, rden))
+                            : st.in5[k] - div_by_recip(acc[i], den, rden);
+    }
+  }
+  __syncwarp(gmask);
+  // the limiter on every lane (same values), the stores spread over the lanes
+  double d[5], qc[Q_STRIDE];
+#pragma unroll
+  for (int k = 0; k < 5; k++) d[k] = sh[W * 5 + k];
+#pragma unroll
+  for (int i = 0; i < Q_STRIDE; i++) qc[i] = st.qc[i];
+  if (!FWD || c != (cs.P ? cs.first[cse] : first_cell)) dq_limit_vv(qc, vv, d, P);
+  if (lane == 0) {
+    if (FWD && clamped) {
+      dt[c] = lim;
+      diag[c] = dg;
+    }
+    store_dq(dst, c, d);
+  }
+  if (lane == (L > 1 ? 1 : 0)) store_sentinel(rearm, c);  // armed for the other sweep
+#pragma unroll
+  for (int k = 0; k < 5; k++)
+    if (k % L == lane) ring[o.slot * 5 + k] = d[k];
+  __syncwarp(gmask);  // sh is free for the group's next cell
+}
+
+// One persistent sweep: block b walks chunk b level by level.  A level of
+// more cells than the block has groups takes several passes; the group's
+// work items (level, pass) form one sequence, pipelined as a whole: indices
+// loaded two items ahead, read-only data staged into shared memory one item
+// ahead (cp.async), so that an item's critical path holds the increments it
+// depends on and one cell's arithmetic.  Blocks synchronise only between
+// levels.
+template <int W, int L, bool FWD, bool MX>
+__device__ __forceinline__ void wide_chunk(
+    const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
+    const PosCell *__restrict__ pcs, const typename SweepTypes<MX>::Rec *__restrict__ prec,
+    const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
+    const double *__restrict__ q8, const typename SweepTypes<MX>::Q *__restrict__ qnb,
+    const double *src, double *dst, double *rearm,
+    const double *__restrict__ res, const double *__restrict__ dqf_own, int32_t C,
+    double *__restrict__ diag, int32_t first_cell, const Params &P0, int clamp_check,
+    double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
+    const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+    const double *__restrict__ vol, int *err, long long spin, const Cases &cs) {
+  constexpr int kGroups = kWideBlock / L;
+  __shared__ WideStage<W, MX> stg[2][kGroups];
+  __shared__ double shm[kGroups][W * 5 + 5];
+  __shared__ double ring[kWideRing * 5];
+  __shared__ int32_t s_segs[kSegCache + 1];
+  __shared__ double s_lim[FWD ? kCaseCache : 1];
+  const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
+  const int32_t lane = threadIdx.x & (L - 1);
+  const int32_t grp = threadIdx.x / L;
+  for (int32_t i = threadIdx.x; i <= sg1 - sg0 && i <= kSegCache; i += blockDim.x)
+    s_segs[i] = segs[sg0 + i];
+  __shared__ int s_clamp_any;
+  if (threadIdx.x == 0) s_clamp_any = 0;
+  __syncthreads();
+  if (FWD && clamp_check)
+    for (int32_t k = threadIdx.x; k < cs.ncase && k < kCaseCache; k += blockDim.x) {
+      s_lim[k] = clamp_limit(cs.P ? cs.P[k] : P0, dt_ext + 2 * k);
+      if (s_lim[k] > 0.0) s_clamp_any = 1;
+    }
+  if (FWD && clamp_check && cs.ncase > kCaseCache && threadIdx.x == 0) s_clamp_any = 1;
+  __syncthreads();
+  // the per-cell clamp test only when some case needs it
+  clamp_check = (FWD && clamp_check && s_clamp_any) ? 1 : 0;
+  const unsigned gmask = ((1u << L) - 1u) << ((threadIdx.x & 31) & ~(L - 1));
+  double *sh = shm[grp];
+  const int32_t pbase = sg1 > sg0 ? s_segs[0] : 0;
+  // work items (level sg, pass): the same sequence in every thread of the block
+  auto seg_at = [&](int32_t sg) {
+    const int32_t i = sg - sg0;
+    return i <= kSegCache ? s_segs[i] : segs[sg];
+  };
+  auto advance = [&](int32_t &sg, int32_t &pass) {
+    if (sg >= sg1) return;
+    const int32_t np = (seg_at(sg + 1) - seg_at(sg) + kGroups - 1) / kGroups;
+    if (++pass >= np) {
+      ++sg;
+      pass = 0;
+    }
+  };
+  auto fetch = [&](int32_t sg, int32_t pass, WideRegs<W / L> &o) {
+    wide_fetch<W, L>(s_segs, segs, sg0, sg, sg1, pbase, grp + pass * kGroups, lane, pcs, pnb,
+                     pslot, o);
+  };
+  int32_t sg = sg0, pass = 0;              // this item
+  int32_t sgn = sg, passn = pass;          // the next
+  advance(sgn, passn);
+  int32_t sgf = sgn, passf = passn;        // the one after
+  advance(sgf, passf);
+  WideRegs<W / L> cur, nxt, far;
+  fetch(sg, pass, cur);
+  fetch(sgn, passn, nxt);
+  wide_stage_copy<W, L, FWD, MX>(cur, lane, stg[0][grp], q8, qnb, prec, res, diag, dqf_own, C);
+  cp_async_commit();
+  int par = 0;
+  while (sg < sg1) {
+    // increments this item reads from L2 (older than the ring, or produced by
+    // another chunk): requested first, so that their round trip overlaps the
+    // staging of the next items; one that still holds the sentinel is waited
+    // for in wide_cell
+    double pre[W / L][5];
+#pragma unroll
+    for (int r = 0; r < W / L; r++) {
+      const int j = lane + L * r;
+      if (cur.cell >= 0 && j < cur.ns && !(cur.nb[r] & kInRing))
+        load_rec5_l2(src + (int64_t)(cur.nb[r] & kIdMask) * Q_STRIDE, pre[r]);
+    }
+    fetch(sgf, passf, far);
+    wide_stage_copy<W, L, FWD, MX>(nxt, lane, stg[par ^ 1][grp], q8, qnb, prec, res, diag, dqf_own,
+                              C);
+    cp_async_commit();
+    cp_async_wait<1>();  // this item's stage
+    __syncwarp(gmask);
+    wide_cell<W, L, FWD, MX>(cur, lane, stg[par][grp], sh, ring, pre, src, dst, rearm, first_cell,
+                              P0, s_lim, clamp_check, dt, diag, dt_ext, cptr, slots, vol, err,
+                              spin, cs);
+    if (sgn != sg) __syncthreads();  // end of a level
+    sg = sgn;
+    pass = passn;
+    sgn = sgf;
+    passn = passf;
+    advance(sgf, passf);
+    cur = nxt;
+    nxt = far;
+    par ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+// Forward sweep.  chunk_skip > 0 withholds the first chunk_skip chunks
+// (failure-detection self-test only: the cells that depend on them wait
+// until the bound runs out).
+template <int W, int L, bool MX>
+__global__ void __launch_bounds__(kWideBlock, kWideMinB)
+k_sweep_fwd_wide(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
+                  const PosCell *__restrict__ pcs,
+                  const typename SweepTypes<MX>::Rec *__restrict__ prec,
+                  const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
+                  const double *__restrict__ q8,
+                  const typename SweepTypes<MX>::Q *__restrict__ qnb, double *dqf,
+                  double *__restrict__ dqb, const double *__restrict__ res, int32_t C,
+                  double *__restrict__ diag, int32_t first_cell, Params P0, int clamp_check,
+                  double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
+                  const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+                  const double *__restrict__ vol, int *err, long long spin,
+                  int32_t chunk_skip, Cases cs) {
+  if ((int32_t)blockIdx.x < chunk_skip) return;
+  wide_chunk<W, L, true, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqf, dqf, dqb, res,
+                              nullptr, C, diag, first_cell, P0, clamp_check, dt, dt_ext, cptr,
+                              slots, vol, err, spin, cs);
+}
+
+// Backward sweep.  The state update of a cell is not needed by any later
+// level, so it runs after the block has swept its whole chunk.
+template <int W, int L, bool MX>
+__global__ void __launch_bounds__(kWideBlock, kWideMinB)
+k_sweep_bwd_wide(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
+                  const PosCell *__restrict__ pcs,
+                  const typename SweepTypes<MX>::Rec *__restrict__ prec,
+                  const int32_t *__restrict__ pnb, const int32_t *__restrict__ pslot,
+                  const double *__restrict__ q8,
+                  const typename SweepTypes<MX>::Q *__restrict__ qnb,
+                  double *__restrict__ q8_new, float *__restrict__ q4_new,
+                  double *__restrict__ dqf, double *dqb, const double *__restrict__ diag,
+                  Params P0, int *err, long long spin, Cases cs) {
+  const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
+  wide_chunk<W, L, false, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqb, dqb, dqf,
+                               nullptr, dqf, 0, const_cast<double *>(diag), 0, P0, 0, nullptr,
+                               nullptr, nullptr, nullptr, nullptr, err, spin, cs);
+  __syncthreads();  // the chunk's increments are final
+  // UpdateFlowField3D_CFL3d for the chunk's cells
+  if (sg1 > sg0) {
+    const int32_t a = segs[sg0], b = segs[sg1];
+    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+      const int32_t c = pcs[i].cell;
+      double d[5], qc[Q_STRIDE];
+      const double2 *pp = reinterpret_cast<const double2 *>(dqb + (int64_t)c * Q_STRIDE);
+      const double2 x = pp[0], y = pp[1], z = pp[2];
+      d[0] = x.x; d[1] = x.y; d[2] = y.x; d[3] = y.y; d[4] = z.x;
+      load_q(q8, c, qc);
+      const Params P = params_of(P0, cs, c);
+      update_cell(qc, d, P);
+      cell_props(qc, P);
+      store_q(q8_new, c, qc);
+      if (MX) store_q4(q4_new, c, qc);
+    }
+  }
+}
+
 // A node's weighted sums divided by its weight (cal_gradient.cpp:2314-2324),
 // then the symmetry-plane projection of the velocity (:2330-2350).
 __device__ __forceinline__ void node_finish(int32_t nd, int32_t info,
@@ -1490,7 +1940,7 @@ __device__ __forceinline__ void grad_faces_cell(
   }
 }
 
-__global__ void __launch_bounds__(kGradBlock)
+__global__ void __launch_bounds__(kGradBlockMax)
 k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
              const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
              const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
@@ -1564,7 +2014,7 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
   o[1] = make_float4(acc[4], 0.f, 0.f, 0.f);
 }
 
-__global__ void __launch_bounds__(kGradBlock)
+__global__ void __launch_bounds__(kGradBlockMax)
 k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
                 const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
                 const int32_t *__restrict__ fnodes, const float *__restrict__ qn4,
@@ -1987,23 +2437,41 @@ __global__ void k_halo_nodes_mx(int32_t nu, const int32_t *__restrict__ unodes,
 
 // The persistent sweep kernel for (W, precision) and its dynamic shared
 // memory.
-static const void *sweep_kernel(bool fwd, int w, bool mx) {
+// kind MFG_SWEEP_DEEP: the warp-specialised kernels (one block per SM);
+// MFG_SWEEP_WIDE: the many-block kernels for wide levels.
+static const void *sweep_kernel(bool fwd, int w, bool mx, int kind = MFG_SWEEP_DEEP) {
 #define MFG_SK(W_)                                                                           \
-  if (w == W_)                                                                               \
+  if (w == W_ && kind == MFG_SWEEP_DEEP)                                                     \
     return fwd ? (mx ? (const void *)k_sweep_fwd_chunk<W_, true>                               \
                      : (const void *)k_sweep_fwd_chunk<W_, false>)                             \
                : (mx ? (const void *)k_sweep_bwd_chunk<W_, true>                               \
-                     : (const void *)k_sweep_bwd_chunk<W_, false>);
+                     : (const void *)k_sweep_bwd_chunk<W_, false>);                            \
+  if (w == W_ && kind == MFG_SWEEP_WIDE)                                                     \
+    return fwd ? (mx ? (const void *)k_sweep_fwd_wide<W_, W_, true>                            \
+                     : (const void *)k_sweep_fwd_wide<W_, W_, false>)                          \
+               : (mx ? (const void *)k_sweep_bwd_wide<W_, W_, true>                            \
+                     : (const void *)k_sweep_bwd_wide<W_, W_, false>);
   MFG_SK(4)
   MFG_SK(8)
 #undef MFG_SK
   return nullptr;
 }
-static int sweep_threads(int w) { return w == 8 ? WsGeom<8>::kThreads : WsGeom<4>::kThreads; }
-static size_t sweep_smem(int w, bool mx) {
+static int sweep_threads(int w, int kind = MFG_SWEEP_DEEP) {
+  if (kind == MFG_SWEEP_WIDE) return kWideBlock;
+  return w == 8 ? WsGeom<8>::kThreads : WsGeom<4>::kThreads;
+}
+static size_t sweep_smem(int w, bool mx, int kind = MFG_SWEEP_DEEP) {
+  if (kind == MFG_SWEEP_WIDE) return 0;
   if (w == 8) return mx ? ws_smem_bytes<8, true>() : ws_smem_bytes<8, false>();
   return mx ? ws_smem_bytes<4, true>() : ws_smem_bytes<4, false>();
 }
+// Cells per work item (lane groups of a block) and ring positions of a
+// kernel kind.
+static int32_t sweep_groups(int w, int kind = MFG_SWEEP_DEEP) {
+  if (kind == MFG_SWEEP_WIDE) return kWideBlock / std::max(w, 1);
+  return w == 8 ? WsGeom<8>::kGroups : WsGeom<4>::kGroups;
+}
+static int32_t sweep_ring(int kind) { return kind == MFG_SWEEP_WIDE ? kWideRing : kRing; }
 
 struct ChunkSweep {
   int32_t *seg_begin = nullptr, *segs = nullptr, *nbs = nullptr, *nslots = nullptr;
@@ -2072,7 +2540,14 @@ struct mfg_ctx {
   int persist_grid = 0;
   int sweep_w = 0;               // records per position of the persistent sweeps (4 or 8)
   int sweep_lanes = 0;           // lanes per cell of the persistent sweeps (= W)
-  int persist_occ[2] = {0, 0};   // resident blocks per SM of the persistent sweeps [W = 4, 8]
+  int persist_occ[2][2] = {{0, 0}, {0, 0}};  // resident blocks per SM [kind][W = 4, 8]
+  int sweep_kind = MFG_SWEEP_DEEP;  // persistent sweep kernels in use (MFG_SWEEP_*)
+  // launch knobs of the other kernels (mfg_autotune): resident blocks per SM
+  // the fused face gather and the face flux are compiled for (their register
+  // caps), and the block sizes of the two gradient kernels
+  int gather_minb = MFG_GATHER_MINB, flux_minb = MFG_FLUX_MINB;
+  int node_block = kNodeBlock, grad_block = kGradBlock;
+  int ring = kRing;                 // ring positions the tables were built for
   int chunking = 0;              // chunk assignment of the forward sweep (MFG_CHUNK_*)
   double chunk_est_us[2] = {0.0, 0.0};  // modelled duration of each sweep with its chunks
   // records of each sweep [forward, backward] whose increment comes from the
@@ -2444,7 +2919,8 @@ __global__ void k_dev_pack(int32_t C, int32_t W, int with_recs, const int32_t *_
                            const SweepRec *__restrict__ recs, PosCell *__restrict__ packed,
                            int32_t *__restrict__ cnbs, SweepRec *__restrict__ crecs,
                            SweepRecF *__restrict__ crecs_f, int32_t *__restrict__ cslot,
-                           int32_t *__restrict__ chunk0_exported, int32_t *__restrict__ stats) {
+                           int32_t *__restrict__ chunk0_exported, int32_t *__restrict__ stats,
+                           int32_t ring) {
   const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= C) return;
   const int32_t gi = order[k];
@@ -2463,9 +2939,9 @@ __global__ void k_dev_pack(int32_t C, int32_t W, int with_recs, const int32_t *_
     if (cross) {
       e |= kMark;
       atomicAdd(&stats[2], 1);
-    } else if (nb < C && posof[nb] >= seg_end - kRing) {
+    } else if (nb < C && posof[nb] >= seg_end - ring) {
       e |= kInRing;
-      cslot[o] = (posof[nb] - chunk_ptr[p]) & (kRing - 1);
+      cslot[o] = (posof[nb] - chunk_ptr[p]) & (ring - 1);
       atomicAdd(&stats[0], 1);
     } else if (nb < C) {
       atomicAdd(&stats[1], 1);
@@ -2605,21 +3081,36 @@ int mfg_destroy(mfg_ctx *ctx) {
   return MFG_OK;
 }
 
-// Lane groups (cells per item) of the persistent sweeps with W records.
-static int32_t sweep_groups(int w) { return w == 8 ? WsGeom<8>::kGroups : WsGeom<4>::kGroups; }
-
-// Chunk assignment forced for contexts created from now on (-1: chosen by
-// the model), set by mfg_set_chunking.
+// Chunk assignment and persistent sweep kernels forced for contexts created
+// from now on (-1: chosen by the model), set by mfg_set_chunking and
+// mfg_set_sweep_kernel.
 static std::atomic<int> g_chunking{-1};
+static std::atomic<int> g_sweep_kind{-1};
 
-// Records per position (W), persistent-sweep grid and chunk count of a new
-// context: one chunk per resident block, no chunk under kMinChunk cells.
-static void setup_sweep_grid(mfg_ctx *ctx, int32_t maxns) {
+// Records per position (W), persistent-sweep kernel kind, grid and chunk
+// count of a new context: one chunk per resident block, no chunk under
+// kMinChunk cells.  The kind follows the widest level (max_level_cells,
+// both sweeps): where it would give a deep block more than two passes of
+// its lane groups per level, the many small blocks of the wide kernels.
+static void setup_sweep_grid(mfg_ctx *ctx, int32_t maxns, int force_kind = -1) {
   const int32_t C = ctx->C;
   ctx->sweep_w = maxns <= 4 ? 4 : (maxns <= 8 ? 8 : 0);
   if (ctx->n > (int64_t)kIdMask) ctx->sweep_w = 0;  // neighbour ids share their word with flags
-  const int per_sm = ctx->sweep_w ? ctx->persist_occ[ctx->sweep_w == 8 ? 1 : 0] : 0;
-  ctx->persist_grid = per_sm * ctx->n_sm;
+  const int wi = ctx->sweep_w == 8 ? 1 : 0;
+  auto grid_of = [&](int kind) {
+    return ctx->sweep_w ? ctx->persist_occ[kind][wi] * ctx->n_sm : 0;
+  };
+  int kind = force_kind >= 0 ? force_kind : g_sweep_kind.load();
+  if (kind < 0) {
+    const int32_t pdeep = std::max(1, std::min(grid_of(MFG_SWEEP_DEEP), (C + kMinChunk - 1) / kMinChunk));
+    kind = (int64_t)ctx->max_level_cells > 2LL * sweep_groups(ctx->sweep_w) * pdeep
+               ? MFG_SWEEP_WIDE
+               : MFG_SWEEP_DEEP;
+  }
+  if (grid_of(kind) <= 0) kind = kind == MFG_SWEEP_WIDE ? MFG_SWEEP_DEEP : MFG_SWEEP_WIDE;
+  ctx->sweep_kind = kind;
+  ctx->ring = sweep_ring(kind);
+  ctx->persist_grid = grid_of(kind);
   ctx->nchunks = std::max(1, std::min(ctx->persist_grid, (C + kMinChunk - 1) / kMinChunk));
   ctx->sweep_mode = ctx->persist_grid > 0 ? 1 : 0;
   ctx->sweep_lanes = ctx->sweep_w;
@@ -2787,7 +3278,10 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
   double tbest = 1e300;
   int32_t lbest = INT32_MAX;
   int choice = MFG_CHUNK_VOTE;
-  if (force < 0 || force == MFG_CHUNK_VOTE) {
+  // MFG_CHUNK_TRANSVERSE_ANY: the transverse grids of every axis pair, no vote
+  const bool any_t = force == MFG_CHUNK_TRANSVERSE_ANY;
+  if (any_t) force = -1;
+  if ((force < 0 && !any_t) || force == MFG_CHUNK_VOTE) {
     assign_chunks(C, P, lptr, cells, sptr, nbs, cand);
     lbest = std::max(max_chunk_level(P, lptr, cells, cand), G);  // <= G: one pass
     tbest = model_sweep_cycles(C, P, G, lptr, cells, sptr, nbs, cand);
@@ -2818,6 +3312,9 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
       const int ax = kind == MFG_CHUNK_TRANSVERSE_YZ ? 1 : 0;
       const int bx = kind == MFG_CHUNK_TRANSVERSE_XY ? 1 : 2;
       Best &b = pb[kind - MFG_CHUNK_TRANSVERSE_XY];
+      // the grids' balance first (one pass over the cells each), the model
+      // on the best-balanced three
+      std::vector<std::pair<int32_t, int32_t>> grids;  // (load, Pa)
       std::vector<int32_t> a;
       for (int32_t Pa = 1; Pa <= P; Pa++) {
         const int32_t Pb = P / Pa;
@@ -2825,8 +3322,13 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
         const double r = (double)Pa / Pb / (ext[ax] / ext[bx]);
         if (r > 2.0 || r < 0.5) continue;
         assign_chunks_transverse(C, Pa, Pb, ax, bx, lptr, cells, sptr, nbs, xyz, rank, a);
-        const int32_t load = std::max(max_chunk_level(P, lptr, cells, a), G);
-        if (load > b.load) continue;
+        grids.push_back({std::max(max_chunk_level(P, lptr, cells, a), G), Pa});
+      }
+      std::sort(grids.begin(), grids.end());
+      for (size_t i = 0; i < grids.size() && i < 3; i++) {
+        const int32_t load = grids[i].first, Pa = grids[i].second, Pb = P / Pa;
+        if (load > b.load) break;
+        assign_chunks_transverse(C, Pa, Pb, ax, bx, lptr, cells, sptr, nbs, xyz, rank, a);
         const double t = model_sweep_cycles(C, P, G, lptr, cells, sptr, nbs, a);
         if (load < b.load || t < b.t) {
           b.load = load;
@@ -2910,6 +3412,13 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
   {
     int32_t maxns = 0;
     for (int32_t c = 0; c < C; c++) maxns = std::max(maxns, std::max(fw_cnt[c], bw_cnt[c]));
+    for (const std::vector<int32_t> *lv : {&lvl, &blvl}) {
+      std::vector<int32_t> width;
+      for (int32_t c = 0; c < C; c++) {
+        if ((int32_t)width.size() <= (*lv)[c]) width.resize((*lv)[c] + 1, 0);
+        ctx->max_level_cells = std::max(ctx->max_level_cells, ++width[(*lv)[c]]);
+      }
+    }
     setup_sweep_grid(ctx, maxns);
   }
   const int W = std::max(ctx->sweep_w, 1);
@@ -2953,7 +3462,8 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
     std::vector<int32_t> assign, chunk_cnt(P, 0);
     {
       const double *xyz[3] = {m->xcc, m->ycc, m->zcc};
-      const int kind = choose_chunks(C, P, sweep_groups(ctx->sweep_w), lptr, cells.data(),
+      const int kind = choose_chunks(C, P, sweep_groups(ctx->sweep_w, ctx->sweep_kind), lptr,
+                                     cells.data(),
                                      sptr.data(), nbs.data(), xyz, g_chunking.load(), assign,
                                      &ctx->chunk_est_us[fwd ? 0 : 1]);
       if (fwd) ctx->chunking = kind;
@@ -3002,11 +3512,11 @@ static int build_levels(mfg_ctx *ctx, const mfg_mesh *m, const std::vector<int32
           if (cross) {
             e |= kMark;
             stat[2]++;
-          } else if (nb < C && posof[nb] >= seg_end - kRing) {
+          } else if (nb < C && posof[nb] >= seg_end - ctx->ring) {
             // still in the ring when this level reads it: overwritten only by
-            // position posof[nb] + kRing, which lies in a later level
+            // position posof[nb] + ring, which lies in a later level
             e |= kInRing;
-            cslot[o] = (posof[nb] - chunk_ptr[p]) & (kRing - 1);
+            cslot[o] = (posof[nb] - chunk_ptr[p]) & (ctx->ring - 1);
             stat[0]++;
           } else if (nb < C) {
             stat[1]++;  // in the chunk, older than the ring: read from global memory
@@ -3203,23 +3713,25 @@ static int ctx_begin(int32_t n_node, int32_t n_face, int32_t n_cell, int32_t n_b
     // resident blocks per SM of each kernel pair (both sweeps), with the
     // stage's dynamic shared memory allowed first
     const bool mx = precision == MFG_PREC_MIXED;
-    for (int wi = 0; wi < 2; wi++) {
-      const int w = wi ? 8 : 4;
-      int per_sm = 1 << 30;
-      for (bool fwd : {true, false}) {
-        const void *fn = sweep_kernel(fwd, w, mx);
-        const size_t smem = sweep_smem(w, mx);
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-          return fail(MFG_ERR_CUDA);
-        int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, sweep_threads(w), smem) !=
-            cudaSuccess)
-          return fail(MFG_ERR_CUDA);
-        per_sm = std::min(per_sm, b);
+    for (int kind = 0; kind < 2; kind++)
+      for (int wi = 0; wi < 2; wi++) {
+        const int w = wi ? 8 : 4;
+        int per_sm = 1 << 30;
+        for (bool fwd : {true, false}) {
+          const void *fn = sweep_kernel(fwd, w, mx, kind);
+          const size_t smem = sweep_smem(w, mx, kind);
+          if (smem &&
+              cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                  cudaSuccess)
+            return fail(MFG_ERR_CUDA);
+          int b = 0;
+          if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, sweep_threads(w, kind),
+                                                            smem) != cudaSuccess)
+            return fail(MFG_ERR_CUDA);
+          per_sm = std::min(per_sm, b);
+        }
+        ctx->persist_occ[kind][wi] = coop ? per_sm : 0;
       }
-      ctx->persist_occ[wi] = coop ? per_sm : 0;
-    }
     ctx->n_sm = prop.multiProcessorCount;
   }
   *out = ctx;
@@ -3691,11 +4203,13 @@ int dev_pack(mfg_ctx *ctx, DevScratch &sc, DevSweep &d) {
   if (mx)
     k_dev_pack<true><<<grid_for(C), kBlock, 0, st>>>(
         C, W, with_recs, order, ccells, pchunk, head, hscan, cs.segs, chunk_ptr, posof, assign,
-        sptr, nbs, recs, cs.cells, cs.nbs, nullptr, cs.recs_f, cs.nslots, exported, exported + 1);
+        sptr, nbs, recs, cs.cells, cs.nbs, nullptr, cs.recs_f, cs.nslots, exported, exported + 1,
+        ctx->ring);
   else
     k_dev_pack<false><<<grid_for(C), kBlock, 0, st>>>(
         C, W, with_recs, order, ccells, pchunk, head, hscan, cs.segs, chunk_ptr, posof, assign,
-        sptr, nbs, recs, cs.cells, cs.nbs, cs.recs, nullptr, cs.nslots, exported, exported + 1);
+        sptr, nbs, recs, cs.cells, cs.nbs, cs.recs, nullptr, cs.nslots, exported, exported + 1,
+        ctx->ring);
   count_launch();
   MFG_CUDA(cudaGetLastError());
   int32_t ex[4] = {0, 0, 0, 0};
@@ -3767,10 +4281,11 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
   MFG_CUDA_OR(cudaStreamSynchronize(st));
   if (h_flags[0]) return fail(MFG_ERR_BADMESH);
   {
-    // the choices of build_levels
+    // the choices of build_levels (the kernel kind once the levels are known)
     setup_sweep_grid(ctx, h_flags[1]);
     ctx->first_cell = 0;
   }
+  const int32_t maxns_dev = h_flags[1];
   {
     int32_t *front = nullptr, *next = nullptr, *counter = nullptr;
     if ((rc = sc.get(&front, C)) || (rc = sc.get(&next, C)) || (rc = sc.get(&counter, 1)))
@@ -3778,6 +4293,7 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
     if ((rc = dev_levels(ctx, sc, fw, front, next, counter))) return fail(rc);
     if ((rc = dev_levels(ctx, sc, bw, front, next, counter))) return fail(rc);
   }
+  setup_sweep_grid(ctx, maxns_dev);
   // the chunk assignment runs on the host, both sweeps at once, from the
   // cell centroids
   {
@@ -3789,7 +4305,7 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
     MFG_CUDA_OR(cudaStreamSynchronize(st));
     const double *xyz[3] = {cx.data(), cy.data(), cz.data()};
     const int force = g_chunking.load();
-    const int32_t G = sweep_groups(ctx->sweep_w);
+    const int32_t G = sweep_groups(ctx->sweep_w, ctx->sweep_kind);
     std::thread tb([&] {
       choose_chunks(C, P, G, bw.lptr, bw.h_cells.data(), bw.h_sptr.data(), bw.h_nbs.data(), xyz,
                     force, bw.h_assign, &ctx->chunk_est_us[1]);
@@ -3905,6 +4421,7 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
   info->sweep_lanes = ctx->sweep_mode == 1 ? ctx->sweep_lanes : 0;
   info->sweep_records = ctx->sweep_w;
   info->sweep_chunking = ctx->chunking;
+  info->sweep_kernel = ctx->sweep_kind;
   for (int k = 0; k < 2; k++) {
     info->sweep_ring_records[k] = ctx->sweep_stats[k][0];
     info->sweep_global_records[k] = ctx->sweep_stats[k][1];
@@ -3915,8 +4432,14 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info) {
 }
 
 int mfg_set_chunking(int32_t kind) {
-  if (kind < -1 || kind > MFG_CHUNK_TRANSVERSE_YZ) return MFG_ERR_INVALID;
+  if (kind < -1 || kind > MFG_CHUNK_TRANSVERSE_ANY) return MFG_ERR_INVALID;
   g_chunking.store(kind);
+  return MFG_OK;
+}
+
+int mfg_set_sweep_kernel(int32_t kind) {
+  if (kind < -1 || kind > MFG_SWEEP_WIDE) return MFG_ERR_INVALID;
+  g_sweep_kind.store(kind);
   return MFG_OK;
 }
 
@@ -4045,35 +4568,51 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
                                                ctx->ccen, ctx->venkat_k, ctx->phi);
       count_launch();
     }
-#define MFG_FLUX(MX_, R_)                                                                     \
-  k_face_flux<MX_, R_><<<grid_for(ctx->F), kBlock, 0, st>>>(                                   \
+#define MFG_FLUX(MX_, R_, M_)                                                                 \
+  k_face_flux<MX_, R_, M_><<<grid_for(ctx->F), kBlock, 0, st>>>(                               \
       ctx->F, ctx->faces, q, ctx->P, cs, ctx->fflux, ctx->C, ctx->n, ctx->fcen, ctx->ccen,     \
       ctx->dqdx, ctx->dqdy, ctx->dqdz, phi, ctx->halo ? ctx->h_gflag : nullptr)
     const bool fmx = mx && !ctx->flux_fp64;
+    const int fm = ctx->flux_minb;
     if (fmx && recon)
-      MFG_FLUX(true, true);
-    else if (fmx)
-      MFG_FLUX(true, false);
+      MFG_FLUX(true, true, MFG_FLUX_MINB);
     else if (recon)
-      MFG_FLUX(false, true);
+      MFG_FLUX(false, true, MFG_FLUX_MINB);
+    else if (fmx && fm == 2)
+      MFG_FLUX(true, false, 2);
+    else if (fmx && fm == 4)
+      MFG_FLUX(true, false, 4);
+    else if (fmx)
+      MFG_FLUX(true, false, 3);
+    else if (fm == 2)
+      MFG_FLUX(false, false, 2);
+    else if (fm == 4)
+      MFG_FLUX(false, false, 4);
     else
-      MFG_FLUX(false, false);
+      MFG_FLUX(false, false, 3);
 #undef MFG_FLUX
     count_launch();
   }
-#define MFG_FACE(F_, D_, G_)                                                                  \
+#define MFG_FACE_M(F_, D_, G_, M_)                                                            \
   if (mx)                                                                                     \
-    k_face_gather_mx<F_, D_, G_, F_><<<g, kBlock, 0, st>>>(                                   \
+    k_face_gather_mx<F_, D_, G_, F_, M_><<<g, kBlock, 0, st>>>(                               \
         ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
         ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
         ctx->F);                                                                              \
   else                                                                                        \
-    k_face_gather<F_, D_, G_, F_><<<g, kBlock, 0, st>>>(                                      \
+    k_face_gather<F_, D_, G_, F_, M_><<<g, kBlock, 0, st>>>(                                  \
         ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
         ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
         ctx->F)
+#define MFG_FACE(F_, D_, G_) MFG_FACE_M(F_, D_, G_, MFG_GATHER_MINB)
   if (flux && dtp && diag) {
-    MFG_FACE(true, true, true);
+    if (ctx->gather_minb == 2) {
+      MFG_FACE_M(true, true, true, 2);
+    } else if (ctx->gather_minb == 4) {
+      MFG_FACE_M(true, true, true, 4);
+    } else {
+      MFG_FACE_M(true, true, true, 3);
+    }
   } else if (flux && !dtp && !diag) {
     MFG_FACE(true, false, false);
   } else if (!flux && dtp && !diag) {
@@ -4084,6 +4623,7 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
     return MFG_ERR_INVALID;
   }
 #undef MFG_FACE
+#undef MFG_FACE_M
   count_launch();
   if (flux) ctx->res_zero = false;
   return check_kernel();
@@ -4155,10 +4695,10 @@ static int launch_fwd_persist(mfg_ctx *ctx, bool clamp_check, int32_t chunk_skip
                   (void *)&qnb, &ctx->dqf, &ctx->dq8, &ctx->res, &C, &ctx->diag, &first, &P,
                   &clamp, &ctx->dt, &ctx->dt_ext, &ctx->cptr, &ctx->slots, &ctx->vol,
                   &ctx->sweep_err, &spin, &skip, &cs};
-  const void *fn = sweep_kernel(true, ctx->sweep_w, mx);
+  const void *fn = sweep_kernel(true, ctx->sweep_w, mx, ctx->sweep_kind);
   if (!fn) return MFG_ERR_UNSUPPORTED;
-  return launch_coop(fn, ctx->nchunks, sweep_threads(ctx->sweep_w), sweep_smem(ctx->sweep_w, mx),
-                     ctx->stream, args);
+  return launch_coop(fn, ctx->nchunks, sweep_threads(ctx->sweep_w, ctx->sweep_kind),
+                     sweep_smem(ctx->sweep_w, mx, ctx->sweep_kind), ctx->stream, args);
 }
 
 static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
@@ -4174,10 +4714,10 @@ static int launch_bwd_persist(mfg_ctx *ctx, long long spin) {
   void *args[] = {&w.seg_begin, &w.segs, &w.cells, &recs, &w.nbs, &w.nslots, (void *)&q,
                   (void *)&qnb, &qn, &q4n, &ctx->dqf, &ctx->dq8, &ctx->diag, &P,
                   &ctx->sweep_err, &spin, &cs};
-  const void *fn = sweep_kernel(false, ctx->sweep_w, mx);
+  const void *fn = sweep_kernel(false, ctx->sweep_w, mx, ctx->sweep_kind);
   if (!fn) return MFG_ERR_UNSUPPORTED;
-  return launch_coop(fn, ctx->nchunks, sweep_threads(ctx->sweep_w), sweep_smem(ctx->sweep_w, mx),
-                     ctx->stream, args);
+  return launch_coop(fn, ctx->nchunks, sweep_threads(ctx->sweep_w, ctx->sweep_kind),
+                     sweep_smem(ctx->sweep_w, mx, ctx->sweep_kind), ctx->stream, args);
 }
 
 // Reads the sweeps' error word; on a timeout, re-arms the flags so that the
@@ -4279,24 +4819,26 @@ int mfg_selftest_sweep_timeout(mfg_ctx *ctx, int64_t spin_cycles) {
 }
 
 static void launch_node_values(mfg_ctx *ctx, cudaStream_t st) {
+  const int nb = ctx->node_block;
   if (ctx->precision == MFG_PREC_MIXED)
-    k_node_values_mx<<<grid_for(ctx->N, kNodeBlock), kNodeBlock, 0, st>>>(
+    k_node_values_mx<<<grid_for(ctx->N, nb), nb, 0, st>>>(
         ctx->N, ctx->C, ctx->nptr, ctx->nsrc, ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
         ctx->bface_c1, ctx->q8[ctx->cur], ctx->qn4, ctx->P, cases_of(ctx));
   else
-    k_node_values<<<grid_for(ctx->N, kNodeBlock), kNodeBlock, 0, st>>>(
+    k_node_values<<<grid_for(ctx->N, nb), nb, 0, st>>>(
         ctx->N, ctx->C, ctx->nptr, ctx->nsrc, ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
         ctx->bface_c1, ctx->q8[ctx->cur], ctx->qn8);
   count_launch();
 }
 
 static void launch_grad_faces(mfg_ctx *ctx, cudaStream_t st) {
+  const int gb = ctx->grad_block;
   if (ctx->precision == MFG_PREC_MIXED)
-    k_grad_faces_mx<<<grid_for(ctx->C, kGradBlock), kGradBlock, 0, st>>>(
+    k_grad_faces_mx<<<grid_for(ctx->C, gb), gb, 0, st>>>(
         ctx->C, ctx->n, ctx->cptr, ctx->slots, ctx->fnptr, ctx->fnodes, ctx->qn4,
         ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->P, cases_of(ctx));
   else
-    k_grad_faces<<<grid_for(ctx->C, kGradBlock), kGradBlock, 0, st>>>(
+    k_grad_faces<<<grid_for(ctx->C, gb), gb, 0, st>>>(
         ctx->C, ctx->n, ctx->cptr, ctx->slots, ctx->fnptr, ctx->fnodes, ctx->qn8,
         ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
   count_launch();
@@ -4531,6 +5073,231 @@ int mfg_iterate(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *norms) 
   }
   MFG_CUDA(cudaGetLastError());
   return check_sweep_error(ctx);
+}
+
+}  // extern "C"
+
+// Rebuild the persistent sweeps' chunk tables of a context with another
+// kernel kind and chunk assignment (-1: the model's), for mfg_autotune's
+// trials: the level order and records of both sweeps stay on the device;
+// the assignment is chosen on the host from them and the cell centroids,
+// then packed on the device as at creation.
+static int rechunk(mfg_ctx *ctx, int kind, int chunking) {
+  if (!ctx->sweep_w || !ctx->fw_cells || !ctx->bw_cells || ctx->halo) return MFG_ERR_UNSUPPORTED;
+  cudaStream_t st = ctx->stream;
+  const int32_t C = ctx->C, W = ctx->sweep_w;
+  int rc;
+  std::vector<Cen> cc;
+  if ((rc = d2h(cc, ctx->ccen, C, st))) return rc;
+  DevSweep d[2];
+  d[0].fwd = true;
+  d[1].fwd = false;
+  for (int k = 0; k < 2; k++) {
+    d[k].lptr = k ? ctx->bw_lptr : ctx->fw_lptr;
+    if ((rc = d2h(d[k].h_cells, (const int32_t *)(k ? ctx->bw_cells : ctx->fw_cells), C, st)) ||
+        (rc = d2h(d[k].h_sptr, (const int32_t *)(k ? ctx->bw_sptr : ctx->fw_sptr), (int64_t)C + 1,
+                  st)))
+      return rc;
+  }
+  MFG_CUDA(cudaStreamSynchronize(st));
+  for (int k = 0; k < 2; k++)
+    if ((rc = d2h(d[k].h_nbs, (const int32_t *)(k ? ctx->bw_nb : ctx->fw_nb), d[k].h_sptr[C], st)))
+      return rc;
+  MFG_CUDA(cudaStreamSynchronize(st));
+  std::vector<double> xyz3[3];
+  for (int a = 0; a < 3; a++) xyz3[a].resize(C);
+  for (int32_t c = 0; c < C; c++) {
+    xyz3[0][c] = cc[c].x;
+    xyz3[1][c] = cc[c].y;
+    xyz3[2][c] = cc[c].z;
+  }
+  const double *xyz[3] = {xyz3[0].data(), xyz3[1].data(), xyz3[2].data()};
+  const int old_kind = ctx->sweep_kind;
+  const int32_t old_chunks = ctx->nchunks;
+  setup_sweep_grid(ctx, W, kind);
+  if (ctx->persist_grid <= 0 || ctx->sweep_kind != kind) {
+    setup_sweep_grid(ctx, W, old_kind);
+    return MFG_ERR_UNSUPPORTED;
+  }
+  const int32_t P = ctx->nchunks, G = sweep_groups(W, ctx->sweep_kind);
+  for (int k = 0; k < 2; k++) {
+    const int ch = choose_chunks(C, P, G, d[k].lptr, d[k].h_cells.data(), d[k].h_sptr.data(),
+                                 d[k].h_nbs.data(), xyz, chunking, d[k].h_assign,
+                                 &ctx->chunk_est_us[k]);
+    if (k == 0) ctx->chunking = ch;
+  }
+  // the previous tables go; the new ones are packed as at creation
+  auto dfree = [&](void *ptr, size_t bytes) {
+    if (!ptr) return;
+    auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), ptr);
+    if (it != ctx->allocs.end()) {
+      ctx->allocs.erase(it);
+      ctx->device_bytes -= (int64_t)std::max<size_t>(bytes, 1);
+    }
+    cudaFree(ptr);
+  };
+  MFG_CUDA(cudaStreamSynchronize(st));
+  for (ChunkSweep *cs : {&ctx->fwc, &ctx->bwc}) {
+    const size_t nrec = (size_t)C * W;
+    dfree(cs->seg_begin, sizeof(int32_t) * ((size_t)old_chunks + 1));
+    dfree(cs->segs, sizeof(int32_t) * ((size_t)cs->nseg + 1));
+    dfree(cs->cells, sizeof(PosCell) * C);
+    dfree(cs->nbs, sizeof(int32_t) * nrec);
+    dfree(cs->nslots, sizeof(int32_t) * nrec);
+    dfree(cs->recs, sizeof(SweepRec) * nrec);
+    dfree(cs->recs_f, sizeof(SweepRecF) * nrec);
+    *cs = ChunkSweep{};
+  }
+  DevScratch sc;
+  for (int k = 0; k < 2; k++) {
+    std::vector<int32_t> lv(C, 0);
+    for (size_t l = 0; l + 1 < d[k].lptr.size(); l++)
+      for (int32_t i = d[k].lptr[l]; i < d[k].lptr[l + 1]; i++) lv[d[k].h_cells[i]] = (int32_t)l;
+    if ((rc = sc.get(&d[k].lvl, C))) return rc;
+    MFG_CUDA(cudaMemcpyAsync(d[k].lvl, lv.data(), sizeof(int32_t) * C, cudaMemcpyHostToDevice, st));
+    for (int a = 0; a < 2; a++) ctx->sweep_stats[k][a] = 0;
+    ctx->sweep_stats[k][2] = 0;
+    if ((rc = dev_pack(ctx, sc, d[k]))) return rc;
+  }
+  MFG_CUDA(cudaStreamSynchronize(st));
+  drop_graphs(ctx);
+  return MFG_OK;
+}
+
+extern "C" {
+
+int mfg_autotune(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, int32_t flags,
+                 mfg_tune_report *rep) {
+  if (!ctx || n_trial <= 0) return MFG_ERR_INVALID;
+  if (ctx->halo) return MFG_ERR_UNSUPPORTED;  // a part iterates through mfg_halo_phase
+  MFG_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const size_t qbytes = sizeof(double) * ctx->n * Q_STRIDE;
+  const size_t q4bytes = sizeof(float) * ctx->n * Q_STRIDE;
+  // every trial leaves the state as it was: the current records and the
+  // running dt extrema are saved once and restored after each
+  void *save = nullptr;
+  if (cudaMalloc(&save, qbytes + (mx ? q4bytes : 0)) != cudaSuccess) {
+    g_cuda_error = "cudaMalloc: autotune scratch";
+    return MFG_ERR_NOMEM;
+  }
+  std::vector<unsigned long long> ext(2 * ctx->ncase);
+  cudaMemcpyAsync(save, ctx->q8[ctx->cur], qbytes, cudaMemcpyDeviceToDevice, st);
+  if (mx)
+    cudaMemcpyAsync((char *)save + qbytes, ctx->q4[ctx->cur], q4bytes, cudaMemcpyDeviceToDevice,
+                    st);
+  cudaMemcpyAsync(ext.data(), ctx->dt_ext, sizeof(unsigned long long) * ext.size(),
+                  cudaMemcpyDeviceToHost, st);
+  const int cur0 = ctx->cur;
+  const bool res_zero0 = ctx->res_zero;
+  int rc = cudaStreamSynchronize(st) == cudaSuccess ? MFG_OK : MFG_ERR_CUDA;
+  auto restore = [&]() {
+    ctx->cur = cur0;
+    cudaMemcpyAsync(ctx->q8[ctx->cur], save, qbytes, cudaMemcpyDeviceToDevice, st);
+    if (mx)
+      cudaMemcpyAsync(ctx->q4[ctx->cur], (char *)save + qbytes, q4bytes, cudaMemcpyDeviceToDevice,
+                      st);
+    cudaMemcpyAsync(ctx->dt_ext, ext.data(), sizeof(unsigned long long) * ext.size(),
+                    cudaMemcpyHostToDevice, st);
+    return cudaStreamSynchronize(st) == cudaSuccess ? MFG_OK : MFG_ERR_CUDA;
+  };
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (rc == MFG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    rc = MFG_ERR_CUDA;
+  // ms per fused iteration of the context as it stands (-1: it cannot run)
+  auto trial = [&]() -> double {
+    if (mfg_iterate(ctx, 2, iter_done, nullptr) != MFG_OK) {  // builds the graphs
+      restore();
+      return -1.0;
+    }
+    cudaEventRecord(e0, st);
+    const int r = mfg_iterate(ctx, n_trial, iter_done + 2, nullptr);
+    cudaEventRecord(e1, st);
+    float t = 0.f;
+    const bool ok = r == MFG_OK && cudaEventSynchronize(e1) == cudaSuccess &&
+                    cudaEventElapsedTime(&t, e0, e1) == cudaSuccess;
+    if (restore() != MFG_OK) return -1.0;
+    return ok ? (double)t / n_trial : -1.0;
+  };
+  mfg_tune_report local{};
+  mfg_tune_report &R = rep ? *rep : local;
+  R = mfg_tune_report{};
+  if (rc == MFG_OK) R.ms_initial = trial();
+  // knob k: candidates, how to apply one, how to read the current value
+  struct Knob {
+    int id;
+    std::vector<int> cand;
+  };
+  std::vector<Knob> knobs;
+  if (ctx->sweep_w && ctx->sweep_mode == 1 && !(flags & MFG_TUNE_NO_REBUILD)) {
+    knobs.push_back({MFG_KNOB_SWEEP_KERNEL, {MFG_SWEEP_DEEP, MFG_SWEEP_WIDE}});
+    knobs.push_back({MFG_KNOB_CHUNKING, {MFG_CHUNK_VOTE, MFG_CHUNK_TRANSVERSE_ANY}});
+  }
+  if (!mx && ctx->sweep_w) knobs.push_back({MFG_KNOB_SWEEP_MODE, {1, 0}});
+  knobs.push_back({MFG_KNOB_GATHER_BLOCKS, {3, 2, 4}});
+  knobs.push_back({MFG_KNOB_FLUX_BLOCKS, {3, 2, 4}});
+  knobs.push_back({MFG_KNOB_NODE_BLOCK, {512, 256, 128}});
+  knobs.push_back({MFG_KNOB_GRAD_BLOCK, {128, 64, 256}});
+  auto current = [&](int id) {
+    switch (id) {
+      case MFG_KNOB_SWEEP_KERNEL: return ctx->sweep_kind;
+      case MFG_KNOB_CHUNKING:  // the transverse candidate stands for any axis pair
+        return ctx->chunking == MFG_CHUNK_VOTE ? MFG_CHUNK_VOTE : MFG_CHUNK_TRANSVERSE_ANY;
+      case MFG_KNOB_SWEEP_MODE: return ctx->sweep_mode;
+      case MFG_KNOB_GATHER_BLOCKS: return ctx->gather_minb;
+      case MFG_KNOB_FLUX_BLOCKS: return ctx->flux_minb;
+      case MFG_KNOB_NODE_BLOCK: return ctx->node_block;
+      default: return ctx->grad_block;
+    }
+  };
+  auto apply = [&](int id, int v) -> int {
+    switch (id) {
+      case MFG_KNOB_SWEEP_KERNEL:
+        return v == ctx->sweep_kind ? MFG_OK : rechunk(ctx, v, -1);
+      case MFG_KNOB_CHUNKING:
+        return v == current(MFG_KNOB_CHUNKING) ? MFG_OK : rechunk(ctx, ctx->sweep_kind, v);
+      case MFG_KNOB_SWEEP_MODE: return mfg_set_sweep_mode(ctx, v);
+      case MFG_KNOB_GATHER_BLOCKS: ctx->gather_minb = v; break;
+      case MFG_KNOB_FLUX_BLOCKS: ctx->flux_minb = v; break;
+      case MFG_KNOB_NODE_BLOCK: ctx->node_block = v; break;
+      default: ctx->grad_block = v; break;
+    }
+    drop_graphs(ctx);
+    return MFG_OK;
+  };
+  for (size_t k = 0; k < knobs.size() && k < MFG_TUNE_KNOBS && rc == MFG_OK; k++) {
+    const Knob &kb = knobs[k];
+    R.knob[k] = kb.id;
+    const int v0 = current(kb.id);
+    int best = v0;
+    double tbest = 1e300;
+    R.n_cand[k] = (int32_t)std::min<size_t>(kb.cand.size(), MFG_TUNE_CANDS);
+    for (int i = 0; i < R.n_cand[k]; i++) {
+      const int v = kb.cand[i];
+      R.cand[k][i] = v;
+      R.ms[k][i] = -1.0;
+      if (apply(kb.id, v) != MFG_OK) continue;
+      // a rebuild may settle on another value than asked (a kind without a
+      // grid): the trial is recorded under the value asked only when taken
+      if (current(kb.id) != v) continue;
+      R.ms[k][i] = trial();
+      if (R.ms[k][i] > 0.0 && R.ms[k][i] < tbest) {
+        tbest = R.ms[k][i];
+        best = v;
+      }
+    }
+    if (apply(kb.id, best) != MFG_OK) rc = MFG_ERR_CUDA;
+    R.chosen[k] = current(kb.id);
+    R.n_knobs = (int32_t)k + 1;
+  }
+  if (rc == MFG_OK) R.ms_final = trial();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(save);
+  ctx->res_zero = res_zero0;
+  drop_graphs(ctx);
+  return rc;
 }
 
 int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double *ms_out) {

@@ -179,6 +179,23 @@ class Solver:
         return {"lanes_per_cell": info["sweep_lanes"], "chunks": info["sweep_chunks"],
                 "ms_per_iter": {str(w): float(ms[0]), str(w // 2): float(ms[1])}}
 
+    def autotune(self, n_trial: int = 3, rebuild: bool = True) -> dict:
+        """mfg_autotune: every launch knob timed on this grid (coordinate
+        descent), the fastest kept, the state left as it was (rebuild=False:
+        the sweep kernels and chunk tables as they are).  Returns, per knob,
+        the ms per fused iteration of each candidate and the choice."""
+        rep = _lib.TuneReport()
+        self._call("mfg_autotune", int(n_trial), int(self.iter_done), 0 if rebuild else 1,
+                   ct.byref(rep))
+        knobs = {}
+        for k in range(rep.n_knobs):
+            name = _lib.KNOBS.get(rep.knob[k], str(rep.knob[k]))
+            knobs[name] = {"trial_ms_per_iter": {str(rep.cand[k][i]): float(rep.ms[k][i])
+                                                 for i in range(rep.n_cand[k])},
+                           "chosen": int(rep.chosen[k])}
+        return {"knobs": knobs, "ms_per_iter_before": float(rep.ms_initial),
+                "ms_per_iter_after": float(rep.ms_final)}
+
     def selftest_sweep_timeout(self, spin_cycles: int = 2_000_000) -> int:
         """Run the bounded-wait self-test; returns the status code."""
         return int(self.lib.mfg_selftest_sweep_timeout(self._ctx, int(spin_cycles)))

@@ -12,6 +12,8 @@ from helpers import assert_bitwise
 pytestmark = pytest.mark.gpu
 
 KINDS = {"vote": 0, "transverse_xy": 1, "transverse_xz": 2, "transverse_yz": 3}
+# transverse on any axis pair: the chunking the model finds best among them
+ANY_TRANSVERSE = 4
 
 
 @pytest.fixture(scope="module")
@@ -85,9 +87,15 @@ def test_wide_levels_reach_the_global_fallback_and_two_passes():
         p = gr.make_params(mach=0.4 + 0.01 * k, alpha=1.0, cfl_start=10.0)
         grids.append(gr.prepare(m, p, bump_amp=0.05, bump_sigma=0.1))
         params.append(p)
+    from minifs_b200 import _lib
+    lib = _lib.load()
     out = {}
     for mode in (1, 0):
-        b = BatchSolver(grids, params)
+        lib.mfg_set_sweep_kernel(0)  # one block per SM: wide chunk levels
+        try:
+            b = BatchSolver(grids, params)
+        finally:
+            lib.mfg_set_sweep_kernel(-1)
         info = b.info()
         if mode == 1:
             assert info["sweep_mode"] == 1, info
