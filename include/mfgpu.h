@@ -221,7 +221,7 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
  *                          MFG_CHUNK_TRANSVERSE_ANY (tables rebuilt)
  * (flags & MFG_TUNE_NO_REBUILD leaves these two as the context has them:
  * a rebuild of a grid of many millions of cells takes seconds)
- *   MFG_KNOB_SWEEP_MODE    1 persistent, 0 one launch per level (FP64 only)
+ *   MFG_KNOB_SWEEP_MODE    1 persistent, 0 one launch per level
  *   MFG_KNOB_GATHER_BLOCKS resident blocks per SM the fused face gather is
  *                          compiled for (its register cap): 2, 3, 4
  *   MFG_KNOB_FLUX_BLOCKS   the same for the per-face Roe flux

@@ -637,10 +637,40 @@ __device__ __forceinline__ void clamp_diag(int32_t c, const double *qc, double &
   }
 }
 
+// The mixed form (MX) evaluates each record's product as the persistent
+// sweeps' mixed form does: FluxLUSGS3D in difference form in FP32 from the
+// neighbour's single-precision state record q4 and the record's normal and
+// weight rounded to FP32, the weighted product widened to FP64 and summed in
+// record order.  Same operations, same bits as those sweeps.
+template <bool MX>
+__device__ __forceinline__ void level_rec_product(const SweepRec &r, int32_t nb,
+                                                  const double *__restrict__ q8,
+                                                  const float *__restrict__ q4, const double *dn,
+                                                  const Params &P, double *wf) {
+  if constexpr (MX) {
+    float qf[Q_STRIDE], df[5], ff[5];
+    load_q4(q4, nb, qf);
+#pragma unroll
+    for (int k = 0; k < 5; k++) df[k] = (float)dn[k];
+    flux_lusgs_diff(qf, df, (float)r.nx, (float)r.ny, (float)r.nz, flux_params<float>(P), ff);
+    const float w = (float)r.w;
+#pragma unroll
+    for (int k = 0; k < 5; k++) wf[k] = (double)(w * ff[k]);
+  } else {
+    double qn[Q_STRIDE], f[5];
+    load_q(q8, nb, qn);
+    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
+#pragma unroll
+    for (int k = 0; k < 5; k++) wf[k] = r.w * f[k];
+  }
+}
+
+template <bool MX>
 __global__ void __launch_bounds__(kBlock)
 k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
             const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
             const int32_t *__restrict__ nbs, const double *__restrict__ q8,
+            const float *__restrict__ q4,
             double *__restrict__ dqf, double *__restrict__ dqb, const double *__restrict__ res,
             int32_t C, double *__restrict__ diag, int32_t first_cell, Params P0, int clamp_check,
             double *__restrict__ dt, const unsigned long long *__restrict__ dt_ext,
@@ -658,11 +688,10 @@ k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
   for (int32_t s = sptr[i]; s < s1; s++) {
     const SweepRec r = recs[s];
     const int32_t nb = nbs[s];
-    double qn[Q_STRIDE], dn[5], f[5];
-    load_q(q8, nb, qn);
+    double dn[5], wf[5];
     load_dq_cg(dqf, nb, dn);
-    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
-    for (int k = 0; k < 5; k++) d[k] -= r.w * f[k];
+    level_rec_product<MX>(r, nb, q8, q4, dn, P, wf);
+    for (int k = 0; k < 5; k++) d[k] -= wf[k];
   }
   double dg = diag[c];
   double qc[Q_STRIDE];
@@ -677,11 +706,13 @@ k_sweep_fwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
 // Backward (upper) sweep of one level, fused with the state update: the new
 // state of the cell goes to the other buffer, so later levels of this sweep
 // still read the old state (the reference updates after the sweep).
+template <bool MX>
 __global__ void __launch_bounds__(kBlock)
 k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
             const int32_t *__restrict__ sptr, const SweepRec *__restrict__ recs,
             const int32_t *__restrict__ nbs, const double *__restrict__ q8,
-            double *__restrict__ q8_new, double *__restrict__ dqf, double *__restrict__ dqb,
+            const float *__restrict__ q4, double *__restrict__ q8_new,
+            float *__restrict__ q4_new, double *__restrict__ dqf, double *__restrict__ dqb,
             const double *__restrict__ diag, Params P0, Cases cs) {
   const int32_t i = l0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= l1) return;
@@ -693,11 +724,10 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
   for (int32_t s = sptr[i]; s < s1; s++) {
     const SweepRec r = recs[s];
     const int32_t nb = nbs[s];
-    double qn[Q_STRIDE], dn[5], f[5];
-    load_q(q8, nb, qn);
+    double dn[5], wf[5];
     load_dq_cg(dqb, nb, dn);
-    flux_lusgs(qn, dn, r.nx, r.ny, r.nz, P, f);
-    for (int k = 0; k < 5; k++) fs[k] += r.w * f[k];
+    level_rec_product<MX>(r, nb, q8, q4, dn, P, wf);
+    for (int k = 0; k < 5; k++) fs[k] += wf[k];
   }
   const double tmp = 2.0 * diag[c];
   for (int k = 0; k < 5; k++) d[k] -= fs[k] / tmp;
@@ -709,6 +739,7 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
   update_cell(qc, d, P);
   cell_props(qc, P);
   store_q(q8_new, c, qc);
+  if (MX) store_q4(q4_new, c, qc);
 }
 
 // ---------------------------------------------------------------------------
@@ -735,11 +766,18 @@ k_sweep_bwd(int32_t l0, int32_t l1, const int32_t *__restrict__ cells,
 // A dependency inside the chunk is read from the block's shared-memory ring
 // of its last kRing positions (or, when older, from global memory); a
 // dependency on another chunk is polled in L2 until it is no longer the
-// sentinel (bounded wait).  Progress: a cell waits only for cells of lower
-// levels, each block visits its levels in increasing order, and every block
-// is resident, so by induction over the levels every cell completes.  Every
-// wait is bounded; one that gives up sets the error word, after which every
-// other wait returns at once and the kernel runs to its end.
+// sentinel (bounded wait).  In the backward sweep the producers also apply
+// the state update of an item's cells (UpdateFlowField3D_CFL3d) once the
+// consumers have released its slot, from the slot's state record and the
+// ring: the update is off the dependent chain and reads nothing twice.  The
+// consumer warps are then at most kWsTeams - 1 items further (a slot is
+// refilled only after every consumer warp has released it), fewer than kRing
+// positions, so the item's ring entries are still there.  Progress: a cell
+// waits only for cells of lower levels, each block visits its levels in
+// increasing order, and every block is resident, so by induction over the
+// levels every cell completes.  Every wait is bounded; one that gives up
+// sets the error word, after which every other wait returns at once and the
+// kernel runs to its end.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kMark = 0x80000000u;    // neighbour flag: in another chunk (wait in L2)
 constexpr uint32_t kInRing = 0x40000000u;  // neighbour flag: increment in the block's ring
@@ -825,11 +863,32 @@ constexpr size_t ws_smem_bytes() {
          sizeof(int32_t) * (kSegCache + 2) + sizeof(double) * kCaseCache +
          sizeof(uint64_t) * 2 * kWsTeams;
 }
+// the producers' update reads an item's ring entries up to kWsTeams items on
+static_assert(kWsTeams * WsGeom<4>::kGroups < kRing && kWsTeams * WsGeom<8>::kGroups < kRing,
+              "ring longer than the stage");
 static_assert(sizeof(WsSlot<4, false>) % 16 == 0 && sizeof(WsSlot<8, false>) % 16 == 0 &&
                   sizeof(WsSlot<4, true>) % 16 == 0 && sizeof(WsSlot<8, true>) % 16 == 0,
               "slot alignment");
-static_assert(ws_smem_bytes<4, false>() <= 227 * 1024 && ws_smem_bytes<8, false>() <= 227 * 1024,
+static_assert(ws_smem_bytes<4, false>() <= 227 * 1024 && ws_smem_bytes<8, false>() <= 227 * 1024 &&
+                  ws_smem_bytes<4, true>() <= 227 * 1024 && ws_smem_bytes<8, true>() <= 227 * 1024,
               "stage fits in shared memory");
+
+// Asynchronous copies global -> shared (.cg: from L2, never a stale L1 line).
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // mbarrier hand-off between the producer teams and the consumer warps.
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
@@ -927,15 +986,15 @@ __device__ __forceinline__ void ws_produce(
   }
   const PosCell x = pcs[p];
   const Params P = params_of(P0, cs, x.cell);
-  // the records' indices beside the position's own (a position's W slots
-  // all exist; padding reads neighbour 0), then the states, then the
-  // products
+  // the records' indices, then the states, then the products (the padding
+  // slots past ns are not read)
   uint32_t e[W];
   int32_t sl[W];
   typename SweepTypes<MX>::Rec rc[W];
 #pragma unroll
   for (int j = 0; j < W; j++) {
     const int64_t o = (int64_t)p * W + j;
+    if (j >= x.ns) continue;
     e[j] = (uint32_t)pnb[o];
     sl[j] = pslot[o];
     rc[j] = prec[o];
@@ -1196,6 +1255,30 @@ __device__ __forceinline__ void ws_cell(
   for (int k = 0; k < 5; k++) ring[slot * 5 + k] = d[k];
 }
 
+// Backward sweep, producer thread g: UpdateFlowField3D_CFL3d of cell g of the
+// item whose slot the consumers have just released, from the slot's state
+// record and the cell's final increment in the ring (forward_lusgs.cpp:
+// 1335-1488); the new state goes to the other state buffer.
+template <int W, bool MX>
+__device__ __forceinline__ void ws_update(const WsSlot<W, MX> &S, int32_t g, int32_t pbase,
+                                          const double *ring, double *__restrict__ q8_new,
+                                          float *__restrict__ q4_new, const Params &P0,
+                                          const Cases &cs) {
+  const int32_t c = S.cell[g];
+  if (c < 0) return;
+  double qc[Q_STRIDE], d[5];
+#pragma unroll
+  for (int k = 0; k < Q_STRIDE; k++) qc[k] = S.qc[k][g];
+  const int32_t sl = (S.pos[g] - pbase) & (kRing - 1);
+#pragma unroll
+  for (int k = 0; k < 5; k++) d[k] = ring[sl * 5 + k];
+  const Params P = params_of(P0, cs, c);
+  update_cell(qc, d, P);
+  cell_props(qc, P);
+  store_q(q8_new, c, qc);
+  if (MX) store_q4(q4_new, c, qc);
+}
+
 // One persistent sweep over chunk blockIdx.x (see the section comment).
 template <int W, bool FWD, bool MX>
 __device__ __forceinline__ void ws_sweep(
@@ -1208,7 +1291,7 @@ __device__ __forceinline__ void ws_sweep(
     const Params &P0, int clamp_check, double *__restrict__ dt,
     const unsigned long long *__restrict__ dt_ext, const int32_t *__restrict__ cptr,
     const SlotRec *__restrict__ slots, const double *__restrict__ vol, int *err, long long spin,
-    const Cases &cs) {
+    const Cases &cs, double *__restrict__ q8_new, float *__restrict__ q4_new) {
   using Geo = WsGeom<W>;
   constexpr int G = Geo::kGroups;
   extern __shared__ __align__(16) unsigned char ws_smem[];
@@ -1249,18 +1332,26 @@ __device__ __forceinline__ void ws_sweep(
     const int32_t t = (threadIdx.x - Geo::kConsumers) / Geo::kTeamThreads;
     const int32_t r = (threadIdx.x - Geo::kConsumers) % Geo::kTeamThreads;
     WsSlot<W, MX> &S = stage[t];
-    int32_t item = 0;
+    int32_t item = 0, last_use = -1;
     for (int32_t sg = sg0; sg < sg1; sg++) {
       const int32_t a = seg_at(sg), b = seg_at(sg + 1);
       const int32_t np = (b - a + G - 1) / G;
       for (int32_t pass = 0; pass < np; pass++, item++) {
         if (item % kWsTeams != t) continue;
         const int32_t use = item / kWsTeams;
-        if (use >= 1) mbar_wait(&empty[t], (unsigned)((use - 1) & 1), err, spin, 256);
+        if (use >= 1) {
+          mbar_wait(&empty[t], (unsigned)((use - 1) & 1), err, spin, 256);
+          if (!FWD) ws_update<W, MX>(S, r, pbase, ring, q8_new, q4_new, P0, cs);
+        }
         ws_produce<W, FWD, MX>(S, r, a + pass * G, b, pcs, prec, pnb, pslot, q8, qnb, res,
                                dqf_own, C, diag, first_cell, P0, cs);
         mbar_arrive(&full[t]);
+        last_use = use;
       }
+    }
+    if (!FWD && last_use >= 0) {  // the slot's last item
+      mbar_wait(&empty[t], (unsigned)(last_use & 1), err, spin, 256);
+      ws_update<W, MX>(S, r, pbase, ring, q8_new, q4_new, P0, cs);
     }
     return;
   }
@@ -1289,7 +1380,8 @@ __device__ __forceinline__ void ws_sweep(
         if (!(e[u] & kInRing)) load_rec5_l2(src + (int64_t)(e[u] & kIdMask) * Q_STRIDE, dn[u]);
       }
       if (pass == 0 && item > 0) consumers_sync<Geo::kConsumers>();  // the previous level is stored
-      ws_cell<W, FWD, MX>(S, g, h, c, ns, e, dn, pbase, ring, src, dst, rearm, P0, s_lim, clamp_check,
+      ws_cell<W, FWD, MX>(S, g, h, c, ns, e, dn, pbase, ring, src, dst, rearm, P0, s_lim,
+                          clamp_check,
                           dt, diag, dt_ext, cptr, slots, vol, err, spin, cs);
       __syncwarp();
       if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[t]);  // the slot is free again
@@ -1321,11 +1413,11 @@ k_sweep_fwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
   if ((int32_t)blockIdx.x < chunk_skip) return;
   ws_sweep<W, true, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqf, dqf, dqb, res,
                         nullptr, C, diag, first_cell, P0, clamp_check, dt, dt_ext, cptr, slots,
-                        vol, err, spin, cs);
+                        vol, err, spin, cs, nullptr, nullptr);
 }
 
-// Backward sweep.  The state update of a cell is not needed by any later
-// level, so it runs after the block has swept its whole chunk.
+// Backward sweep with the state update (by the producers, see the section
+// comment).
 template <int W, bool MX>
 __global__ void __launch_bounds__(WsGeom<W>::kThreads, MFG_PERSIST_MINB)
 k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restrict__ segs,
@@ -1337,28 +1429,9 @@ k_sweep_bwd_chunk(const int32_t *__restrict__ seg_begin, const int32_t *__restri
                   double *__restrict__ q8_new, float *__restrict__ q4_new,
                   double *__restrict__ dqf, double *dqb, const double *__restrict__ diag,
                   Params P0, int *err, long long spin, Cases cs) {
-  const int32_t sg0 = seg_begin[blockIdx.x], sg1 = seg_begin[blockIdx.x + 1];
   ws_sweep<W, false, MX>(seg_begin, segs, pcs, prec, pnb, pslot, q8, qnb, dqb, dqb, dqf, nullptr,
                          dqf, 0, const_cast<double *>(diag), 0, P0, 0, nullptr, nullptr, nullptr,
-                         nullptr, nullptr, err, spin, cs);
-  __syncthreads();  // the chunk's increments are final
-  // UpdateFlowField3D_CFL3d for the chunk's cells
-  if (sg1 > sg0) {
-    const int32_t a = segs[sg0], b = segs[sg1];
-    for (int32_t i = a + threadIdx.x; i < b; i += blockDim.x) {
-      const int32_t c = pcs[i].cell;
-      double d[5], qc[Q_STRIDE];
-      const double2 *pp = reinterpret_cast<const double2 *>(dqb + (int64_t)c * Q_STRIDE);
-      const double2 x = pp[0], y = pp[1], z = pp[2];
-      d[0] = x.x; d[1] = x.y; d[2] = y.x; d[3] = y.y; d[4] = z.x;
-      load_q(q8, c, qc);
-      const Params P = params_of(P0, cs, c);
-      update_cell(qc, d, P);
-      cell_props(qc, P);
-      store_q(q8_new, c, qc);
-      if (MX) store_q4(q4_new, c, qc);
-    }
-  }
+                         nullptr, nullptr, err, spin, cs, q8_new, q4_new);
 }
 
 // ---------------------------------------------------------------------------
@@ -1417,22 +1490,6 @@ struct __align__(16) WideStage {
 static_assert(sizeof(WideStage<4, false>) % 128 == 16 && sizeof(WideStage<4, true>) % 128 == 16 &&
                   sizeof(WideStage<8, false>) % 128 == 16 && sizeof(WideStage<8, true>) % 128 == 16,
               "stage stride");
-
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 template <int W, int L>
 __device__ __forceinline__ void wide_fetch(const int32_t *s_segs, const int32_t *__restrict__ segs,
@@ -3746,8 +3803,6 @@ static int ctx_finish(mfg_ctx *ctx, const double *q0, const CaseLayout &cl) {
   const int32_t precision = ctx->precision;
   int rc;
   if (precision == MFG_PREC_MIXED) {
-    // the mixed form runs the persistent sweeps only
-    if (ctx->sweep_mode != 1) return MFG_ERR_UNSUPPORTED;
     for (int k = 0; k < 2; k++)
       if ((rc = dalloc(ctx, &ctx->q4[k], (size_t)n * Q_STRIDE))) return rc;
     if ((rc = dalloc(ctx, &ctx->qn4, (size_t)ctx->N * Q_STRIDE))) return rc;
@@ -4393,7 +4448,6 @@ int mfg_set_params(mfg_ctx *ctx, const mfg_params *p) {
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode) {
   if (!ctx || (mode != 0 && mode != 1)) return MFG_ERR_INVALID;
   if (mode == 1 && ctx->persist_grid <= 0) return MFG_ERR_UNSUPPORTED;
-  if (mode == 0 && ctx->precision == MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
   ctx->sweep_mode = mode;
   for (int k = 0; k < 2; k++)
     if (ctx->graph[k]) {
@@ -4739,34 +4793,45 @@ static int check_sweep_error(mfg_ctx *ctx) {
 
 // One LU-SGS sweep: forward (DQ* into dqf) or backward (DQ into dq8 and the
 // updated state into the other state buffer).
-static int launch_sweep(mfg_ctx *ctx, bool fwd, bool clamp_check) {
-  if (ctx->sweep_mode == 1)
-    return fwd ? launch_fwd_persist(ctx, clamp_check, 0, kSpinCycles)
-               : launch_bwd_persist(ctx, kSpinCycles);
-  if (ctx->precision == MFG_PREC_MIXED) return MFG_ERR_UNSUPPORTED;
-  cudaStream_t st = ctx->stream;
+// One sweep as one launch per level (cells with more records than the
+// persistent sweeps take, or sweep mode 0), either precision.
+static void launch_level_sweep(mfg_ctx *ctx, bool fwd, bool clamp_check, cudaStream_t st) {
   const double *q = ctx->q8[ctx->cur];
   double *qn = ctx->q8[ctx->cur ^ 1];
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const float *q4 = mx ? ctx->q4[ctx->cur] : nullptr;
+  float *q4n = mx ? ctx->q4[ctx->cur ^ 1] : nullptr;
+  const Cases cs = cases_of(ctx);
   if (fwd) {
     const int Lf = (int)ctx->fw_lptr.size() - 1;
+    auto kf = mx ? k_sweep_fwd<true> : k_sweep_fwd<false>;
     for (int l = 0; l < Lf; l++) {
       const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
-      k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
-          a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
-          ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, clamp_check ? 1 : 0, ctx->dt,
-          ctx->dt_ext, ctx->cptr, ctx->slots, ctx->vol, cases_of(ctx));
+      kf<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs,
+                                             ctx->fw_nb, q, q4, ctx->dqf, ctx->dq8, ctx->res,
+                                             ctx->C, ctx->diag, ctx->first_cell, ctx->P,
+                                             clamp_check ? 1 : 0, ctx->dt, ctx->dt_ext,
+                                             ctx->cptr, ctx->slots, ctx->vol, cs);
     }
     count_launch(Lf);
   } else {
     const int Lb = (int)ctx->bw_lptr.size() - 1;
+    auto kb = mx ? k_sweep_bwd<true> : k_sweep_bwd<false>;
     for (int l = 0; l < Lb; l++) {
       const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
-      k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
-                                                      ctx->bw_recs, ctx->bw_nb, q, qn, ctx->dqf,
-                                                      ctx->dq8, ctx->diag, ctx->P, cases_of(ctx));
+      kb<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr, ctx->bw_recs,
+                                             ctx->bw_nb, q, q4, qn, q4n, ctx->dqf, ctx->dq8,
+                                             ctx->diag, ctx->P, cs);
     }
     count_launch(Lb);
   }
+}
+
+static int launch_sweep(mfg_ctx *ctx, bool fwd, bool clamp_check) {
+  if (ctx->sweep_mode == 1)
+    return fwd ? launch_fwd_persist(ctx, clamp_check, 0, kSpinCycles)
+               : launch_bwd_persist(ctx, kSpinCycles);
+  launch_level_sweep(ctx, fwd, clamp_check, ctx->stream);
   return check_kernel();
 }
 
@@ -5234,7 +5299,7 @@ int mfg_autotune(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, int32_t flags
     knobs.push_back({MFG_KNOB_SWEEP_KERNEL, {MFG_SWEEP_DEEP, MFG_SWEEP_WIDE}});
     knobs.push_back({MFG_KNOB_CHUNKING, {MFG_CHUNK_VOTE, MFG_CHUNK_TRANSVERSE_ANY}});
   }
-  if (!mx && ctx->sweep_w) knobs.push_back({MFG_KNOB_SWEEP_MODE, {1, 0}});
+  if (ctx->sweep_w) knobs.push_back({MFG_KNOB_SWEEP_MODE, {1, 0}});
   knobs.push_back({MFG_KNOB_GATHER_BLOCKS, {3, 2, 4}});
   knobs.push_back({MFG_KNOB_FLUX_BLOCKS, {3, 2, 4}});
   knobs.push_back({MFG_KNOB_NODE_BLOCK, {512, 256, 128}});
@@ -5388,11 +5453,8 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
   for (auto &e : ev) MFG_CUDA(cudaEventCreate(&e));
   for (int k = 0; k < MFG_NPHASES; k++) phase_ms[k] = 0.0;
   int rc = MFG_OK;
-  const int Lf = (int)ctx->fw_lptr.size() - 1, Lb = (int)ctx->bw_lptr.size() - 1;
   for (int32_t it = 0; it < n_iter && rc == MFG_OK; it++) {
     ctx->res_zero = true;
-    const double *q = ctx->q8[ctx->cur];
-    double *qn = ctx->q8[ctx->cur ^ 1];
     cudaEventRecord(ev[0], st);
     rc = launch_face(ctx, true, true, true, 0.0, true);
     cudaEventRecord(ev[1], st);
@@ -5400,23 +5462,12 @@ int mfg_profile_phases(mfg_ctx *ctx, int32_t n_iter, int32_t iter_done, double *
       if (rc == MFG_OK) rc = launch_fwd_persist(ctx, true, 0, kSpinCycles);
       cudaEventRecord(ev[2], st);
       if (rc == MFG_OK) rc = launch_bwd_persist(ctx, kSpinCycles);
-    } else {
-      for (int l = 0; l < Lf && rc == MFG_OK; l++) {
-        const int32_t a = ctx->fw_lptr[l], b = ctx->fw_lptr[l + 1];
-        k_sweep_fwd<<<grid_for(b - a), kBlock, 0, st>>>(
-            a, b, ctx->fw_cells, ctx->fw_sptr, ctx->fw_recs, ctx->fw_nb, q, ctx->dqf, ctx->dq8,
-            ctx->res, ctx->C, ctx->diag, ctx->first_cell, ctx->P, 1, ctx->dt, ctx->dt_ext,
-            ctx->cptr, ctx->slots, ctx->vol, cases_of(ctx));
-      }
+    } else if (rc == MFG_OK) {
+      launch_level_sweep(ctx, true, true, st);
       cudaEventRecord(ev[2], st);
-      for (int l = 0; l < Lb; l++) {
-        const int32_t a = ctx->bw_lptr[l], b = ctx->bw_lptr[l + 1];
-        k_sweep_bwd<<<grid_for(b - a), kBlock, 0, st>>>(a, b, ctx->bw_cells, ctx->bw_sptr,
-                                                        ctx->bw_recs, ctx->bw_nb, q, qn,
-                                                        ctx->dqf, ctx->dq8, ctx->diag, ctx->P,
-                                                        cases_of(ctx));
-      }
-      count_launch(Lf + Lb);
+      launch_level_sweep(ctx, false, true, st);
+    } else {
+      cudaEventRecord(ev[2], st);
     }
     ctx->cur ^= 1;
     if (ctx->live_bc && rc == MFG_OK) rc = launch_ghost_bc(ctx, st);  // with the update

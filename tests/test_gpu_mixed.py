@@ -6,6 +6,8 @@ a state within 1e-6 (relative) of the FP64 one."""
 import numpy as np
 import pytest
 
+from helpers import assert_bitwise
+
 pytestmark = pytest.mark.gpu
 
 
@@ -114,16 +116,24 @@ def test_mixed_batched_and_per_routine():
     b.close()
 
 
-def test_mixed_requires_persistent_sweeps():
-    from minifs_b200 import _lib
+def test_mixed_per_level_sweeps_match_persistent():
+    """The mixed form's sweeps one launch per level give the persistent mixed
+    sweeps' bits (cube with far field and the LimitTimeStep clamp active)."""
     from minifs_b200 import grid as gr, meshgen
     from minifs_b200.solver import Solver
-    m = meshgen.cube_mesh(4, jitter=0.1, seed=1)
+    m = meshgen.cube_mesh(12, jitter=0.15, seed=3)
     p = gr.make_params(mach=0.5, alpha=2.0, cfl_start=10.0)
-    s = Solver(gr.prepare(m, p), p, precision="mixed")
-    with pytest.raises(_lib.MfgError):
-        s.set_sweep_mode(0)
-    s.close()
+    pg = gr.prepare(m, p, bump_amp=0.05, bump_sigma=0.1)
+    a = Solver(pg, p, precision="mixed")
+    b = Solver(pg, p, precision="mixed")
+    b.set_sweep_mode(0)
+    assert a.info()["sweep_mode"] == 1 and b.info()["sweep_mode"] == 0
+    a.iterate(6)
+    b.iterate(6)
+    for f in ("q", "res", "dq", "dqdx"):
+        assert_bitwise(b.download(f), a.download(f), f"mixed per level ({f})")
+    a.close()
+    b.close()
 
 
 def test_mixed_form_with_fp64_flux():

@@ -117,8 +117,34 @@ def test_merged_cells_lanes_mixed_and_device_context():
     c = Solver(pg, p, precision="mixed")
     c.iterate(ITERS)
     assert state_rel_err(c.download("q"), a.download("q"), pg.n, p.p_bar)["max_norm"] < 1e-6
-    # the mixed form needs the persistent sweeps, which 10-record cells rule out
+
+
+def test_mixed_form_on_cells_beyond_eight_records():
+    """Merged cells on the boundary have 10 sweep records: the mixed form
+    runs its sweeps one launch per level there.  Those per-level sweeps give
+    the persistent mixed sweeps' bits where both run (8-record cells), and
+    on the 10-record grid the mixed state stays within 1e-6 of FP64's."""
+    m, flow, p, pg = merged_case(False)
+    a = Solver(pg, p, precision="mixed")
+    b = Solver(pg, p, precision="mixed")
+    b.set_sweep_mode(0)
+    assert a.info()["sweep_mode"] == 1 and b.info()["sweep_mode"] == 0
+    for fused in (True, False):
+        if fused:
+            a.iterate(ITERS)
+            b.iterate(ITERS)
+        else:
+            a.step()
+            b.step()
+        for f in ("q", "res", "dqdx", "dq"):
+            assert_bitwise(b.download(f), a.download(f), f"mixed per level ({f})")
+    a.close()
+    b.close()
     m2, _, _, pg2 = merged_case(True)
-    with pytest.raises(_lib.MfgError) as e:
-        Solver(pg2, p, precision="mixed")
-    assert e.value.code == -6
+    f64 = Solver(pg2, p)
+    mx = Solver(pg2, p, precision="mixed")
+    assert mx.info()["sweep_mode"] == 0 and mx.info()["sweep_records"] == 0
+    f64.iterate(ITERS)
+    mx.iterate(ITERS)
+    err = state_rel_err(mx.download("q"), f64.download("q"), pg2.n, p.p_bar)["max_norm"]
+    assert 0.0 < err < 1e-6, err
