@@ -227,6 +227,10 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
  *   MFG_KNOB_FLUX_BLOCKS   the same for the per-face Roe flux
  *   MFG_KNOB_NODE_BLOCK    threads per block of the node values
  *   MFG_KNOB_GRAD_BLOCK    threads per block of the gradient face sums
+ *   MFG_KNOB_GATHER_LANES  lanes per cell of the face gather and the
+ *                          gradient face sums: one lane per face of a cell
+ *                          (4 or 8, as the grid's cells allow) or 0 (one
+ *                          thread per cell)
  * Results are identical with every choice. */
 #define MFG_KNOB_SWEEP_KERNEL 0
 #define MFG_KNOB_CHUNKING 1
@@ -235,6 +239,7 @@ int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double
 #define MFG_KNOB_FLUX_BLOCKS 4
 #define MFG_KNOB_NODE_BLOCK 5
 #define MFG_KNOB_GRAD_BLOCK 6
+#define MFG_KNOB_GATHER_LANES 7
 #define MFG_TUNE_KNOBS 8
 #define MFG_TUNE_CANDS 4
 typedef struct mfg_tune_report {

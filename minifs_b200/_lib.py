@@ -74,7 +74,8 @@ class Info(ct.Structure):
 
 TUNE_KNOBS, TUNE_CANDS = 8, 4
 KNOBS = {0: "sweep_kernel", 1: "sweep_chunking", 2: "sweep_mode", 3: "face_gather_blocks_per_sm",
-         4: "face_flux_blocks_per_sm", 5: "node_values_block", 6: "grad_faces_block"}
+         4: "face_flux_blocks_per_sm", 5: "node_values_block", 6: "grad_faces_block",
+         7: "gather_lanes_per_cell"}
 
 
 class TuneReport(ct.Structure):

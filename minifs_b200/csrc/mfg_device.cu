@@ -22,6 +22,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -71,6 +72,10 @@ constexpr int kSegBlocks = 32;     // blocks per case of the batched norm reduct
 
 inline int grid_for(int64_t n, int block = kBlock) {
   return (int)std::max<int64_t>(1, (n + block - 1) / block);
+}
+// Lanes per cell of the face gather for cells of at most max_slots faces.
+inline int gather_lanes_for(int32_t max_slots) {
+  return max_slots <= 4 ? 4 : (max_slots <= 8 ? 8 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -262,6 +267,15 @@ __device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double d
   }
 }
 
+// A face's row of the per-face flux array: the five fluxes and CellIsMG's
+// pressure test of its two cells (1.0 when |p2 - p1| / (p2 + p1 + 2 p_bar)
+// exceeds 0.1, compute_timestep.cpp:1009-1340; the expression is symmetric
+// in the two sides, so either cell's gather reads the same outcome).
+constexpr int kFluxRow = 6;
+// Cells per slice of the sliced slot records (one warp).
+constexpr int kSlice = 32;
+static_assert(kBlock % kSlice == 0, "blocks hold whole slices");
+
 // Per-cell face gather: Roe flux into the residual, local time step with
 // CellIsMG and LimitTimeStep, and the LU-SGS diagonal.  One thread per cell,
 // faces in ascending order (see the file header for why that is exact).
@@ -275,8 +289,8 @@ __device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double d
 
 template <bool FLUX, bool DT, bool DIAG, bool PRE>
 __device__ __forceinline__ void face_gather_cell(
-    int32_t c, int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
-    const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ res,
+    int32_t c, int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ sslots,
+    const int32_t *__restrict__ sptr32, const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ res,
     int res_zero, double *__restrict__ dt, double *__restrict__ diag,
     const double *__restrict__ cfl_tab, const int32_t *__restrict__ iter_counter, double cfl_arg,
     const Params &P0, unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part,
@@ -291,18 +305,25 @@ __device__ __forceinline__ void face_gather_cell(
     load_q(q8, c, qc);
     if (FLUX && !res_zero)
       for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
-    const int32_t s0 = __ldg(cptr + c), s1 = __ldg(cptr + c + 1);
+    const int32_t ns = __ldg(cptr + c + 1) - __ldg(cptr + c);
+    const SlotRec *sl = sslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
     double dtl = kBig;
     int det = 1;
-    for (int32_t s = s0; s < s1; s++) {
-      const SlotRec sr = slots[s];
+    for (int32_t j = 0; j < ns; j++) {
+      const SlotRec sr = sl[(int64_t)j * kSlice];
       if (FLUX || DT) {
-        double qn[Q_STRIDE];
-        load_q(q8, sr.nb, qn);
+        // the neighbour's state: its pressure for CellIsMG and, without the
+        // per-face rows, the flux; with them (PRE) the row holds both
+        double qn[Q_STRIDE], mgf = 0.0;
+        if (!PRE) load_q(q8, sr.nb, qn);
         if (FLUX) {
           double f[5];
           if (PRE) {  // the face's flux, computed once by k_face_flux
-            for (int k = 0; k < 5; k++) f[k] = fflux[(int64_t)k * F + sr.face];
+            const double2 *row =
+                reinterpret_cast<const double2 *>(fflux + (int64_t)sr.face * kFluxRow);
+            const double2 a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2);
+            f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y; f[4] = e.x;
+            mgf = e.y;
           } else if (sr.flags & SLOT_IS_C2) {
             roe_flux(qn, qc, sr.nx, sr.ny, sr.nz, sr.area, P, f);
           } else {
@@ -320,8 +341,12 @@ __device__ __forceinline__ void face_gather_cell(
           const double eigv = vn + qc[Q_A];
           dtl = smin(dtl, sr.dn / eigv);
           // CellIsMG: |p2-p1| and p2+p1 are symmetric in the two sides.
-          const double dp = fabs(qn[4] - qc[4]) / (qn[4] + qc[4] + P.p_bar + P.p_bar);
-          if (dp > 0.1) det = 0;
+          if (PRE) {
+            if (mgf != 0.0) det = 0;
+          } else {
+            const double dp = fabs(qn[4] - qc[4]) / (qn[4] + qc[4] + P.p_bar + P.p_bar);
+            if (dp > 0.1) det = 0;
+          }
         }
       }
     }
@@ -335,8 +360,8 @@ __device__ __forceinline__ void face_gather_cell(
     if (DIAG) {
       const double dtv = DT ? dtc : dt[c];
       double d = vol[c] / dtv;
-      for (int32_t s = s0; s < s1; s++) {
-        const SlotRec sr = slots[s];
+      for (int32_t j = 0; j < ns; j++) {
+        const SlotRec sr = sl[(int64_t)j * kSlice];
         double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
         vn = fabs(vn);
         const double eig = vn + qc[Q_A];
@@ -352,15 +377,16 @@ __device__ __forceinline__ void face_gather_cell(
 
 template <bool FLUX, bool DT, bool DIAG, bool PRE, int MINB = MFG_GATHER_MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
-k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
-              const double *__restrict__ q8, const double *__restrict__ vol,
+k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ sslots,
+              const int32_t *__restrict__ sptr32, const double *__restrict__ q8,
+              const double *__restrict__ vol,
               double *__restrict__ res, int res_zero, double *__restrict__ dt,
               double *__restrict__ diag, const double *__restrict__ cfl_tab,
               const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
               unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs,
               const double *__restrict__ fflux, int32_t F) {
-  face_gather_cell<FLUX, DT, DIAG, PRE>(blockIdx.x * blockDim.x + threadIdx.x, C, cptr, slots,
-                                        q8, vol, res, res_zero, dt, diag, cfl_tab, iter_counter,
+  face_gather_cell<FLUX, DT, DIAG, PRE>(blockIdx.x * blockDim.x + threadIdx.x, C, cptr, sslots,
+                                        sptr32, q8, vol, res, res_zero, dt, diag, cfl_tab, iter_counter,
                                         cfl_arg, P0, dt_ext, norm_part, cs, fflux, F);
 }
 
@@ -370,7 +396,8 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
 // the same face order.
 template <bool FLUX, bool DT, bool DIAG, bool PRE, int MINB = MFG_GATHER_MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
-k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ slots,
+k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
+                 const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
                  const double *__restrict__ q8, const double *__restrict__ vol,
                  double *__restrict__ res, int res_zero, double *__restrict__ dt,
                  double *__restrict__ diag, const double *__restrict__ cfl_tab,
@@ -389,18 +416,23 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
     load_q(q8, c, qd);
     if (FLUX && !res_zero)
       for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
-    const int32_t s0 = __ldg(cptr + c), s1 = __ldg(cptr + c + 1);
+    const int32_t ns = __ldg(cptr + c + 1) - __ldg(cptr + c);
+    const SlotRec *sl = sslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
     double dtl = kBig;
     int det = 1;
-    for (int32_t s = s0; s < s1; s++) {
-      const SlotRec sr = slots[s];
+    for (int32_t j = 0; j < ns; j++) {
+      const SlotRec sr = sl[(int64_t)j * kSlice];
       if (FLUX || DT) {
-        double qn[Q_STRIDE];
-        load_q(q8, sr.nb, qn);
+        double qn[Q_STRIDE], mgf = 0.0;
+        if (!PRE) load_q(q8, sr.nb, qn);
         if (FLUX) {
           double f[5];
           if (PRE) {  // the face's flux, computed once by k_face_flux
-            for (int k = 0; k < 5; k++) f[k] = fflux[(int64_t)k * F + sr.face];
+            const double2 *row =
+                reinterpret_cast<const double2 *>(fflux + (int64_t)sr.face * kFluxRow);
+            const double2 a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2);
+            f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y; f[4] = e.x;
+            mgf = e.y;
           } else if (sr.flags & SLOT_IS_C2) {
             roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
           } else {
@@ -417,8 +449,12 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
           vn = fabs(vn);
           const double eigv = vn + qd[Q_A];
           dtl = smin(dtl, sr.dn / eigv);
-          const double dp = fabs(qn[4] - qd[4]) / (qn[4] + qd[4] + P.p_bar + P.p_bar);
-          if (dp > 0.1) det = 0;
+          if (PRE) {
+            if (mgf != 0.0) det = 0;
+          } else {
+            const double dp = fabs(qn[4] - qd[4]) / (qn[4] + qd[4] + P.p_bar + P.p_bar);
+            if (dp > 0.1) det = 0;
+          }
         }
       }
     }
@@ -431,8 +467,8 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
     if (DIAG) {
       const double dtv = DT ? dtc : dt[c];
       double d = vol[c] / dtv;
-      for (int32_t s = s0; s < s1; s++) {
-        const SlotRec sr = slots[s];
+      for (int32_t j = 0; j < ns; j++) {
+        const SlotRec sr = sl[(int64_t)j * kSlice];
         double vn = qd[1] * sr.nx + qd[2] * sr.ny + qd[3] * sr.nz;
         vn = fabs(vn);
         d += 0.5 * sr.area * (vn + qd[Q_A]) * P.lhs_omga;
@@ -443,6 +479,141 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__r
       for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
   }
   gather_epilogue<FLUX, DT>(live, cse, dtc, r, dt_ext, norm_part);
+}
+
+// Face gather with one lane per (cell, face) slot: L lanes per cell (L at
+// least the cell's slot count), so that a cell's slot records and face rows
+// are loaded side by side instead of one after another.  The per-cell
+// results are folds over the slots in ascending face order passed from lane
+// to lane: the residual r := r - F_f (r + F_f where the cell is the face's
+// second cell; a difference is the sum with the negated term, exactly), the
+// time step min(dt, dn_f / eig_f), CellIsMG's switch, then Diag := vol / dt
+// + sum 0.5 area_f eig_f lhs_omga -- the operations and order of the
+// one-thread gather, so the same bits.  The flux comes from the per-face
+// rows (FLUX, either precision's flux kernel); without them (the time step
+// alone) CellIsMG reads the neighbour's pressure.
+template <int L>
+__device__ __forceinline__ double lane_prev(double x) {
+  return __shfl_up_sync(0xffffffffu, x, 1, L);
+}
+
+template <int L, bool FLUX, bool DT, bool DIAG, int MINB = MFG_GATHER_MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
+k_face_gather_lanes(int32_t C, const int32_t *__restrict__ cptr,
+                    const SlotRec *__restrict__ slots, const double *__restrict__ q8,
+                    const double *__restrict__ vol, double *__restrict__ res, int res_zero,
+                    double *__restrict__ dt, double *__restrict__ diag,
+                    const double *__restrict__ cfl_tab, const int32_t *__restrict__ iter_counter,
+                    double cfl_arg, Params P0, unsigned long long *__restrict__ dt_ext,
+                    double *__restrict__ norm_part, Cases cs, const double *__restrict__ fflux) {
+  static_assert((L & (L - 1)) == 0 && L >= 2 && L <= 32 && kBlock % L == 0, "lanes per cell");
+  const int64_t cl = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / L;
+  const bool live = cl < C;
+  const int32_t c = live ? (int32_t)cl : 0;
+  const int lane = threadIdx.x & (L - 1);
+  const bool last = lane == L - 1;
+  int32_t s0 = 0, ns = 0;
+  if (live) {
+    s0 = __ldg(cptr + c);
+    ns = __ldg(cptr + c + 1) - s0;
+  }
+  const bool has = live && lane < ns;
+  const int32_t cse = live ? case_of(cs, c) : 0;
+  const Params P = live ? params_of(P0, cs, c) : P0;
+  double qc[Q_STRIDE];
+  load_q(q8, c, qc);
+  // this lane's slot
+  double t[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double dtt = 0.0, dgt = 0.0;
+  int bad = 0;
+  if (has) {
+    const SlotRec sr = slots[s0 + lane];
+    if (FLUX) {
+      const double2 *row = reinterpret_cast<const double2 *>(fflux + (int64_t)sr.face * kFluxRow);
+      const double2 a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2);
+      const double f[5] = {a.x, a.y, b.x, b.y, e.x};
+      const bool plus = (sr.flags & SLOT_IS_C2) != 0;
+#pragma unroll
+      for (int k = 0; k < 5; k++) t[k] = plus ? f[k] : -f[k];
+      if (DT) bad = e.y != 0.0;
+    }
+    if (DT || DIAG) {
+      double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
+      vn = fabs(vn);
+      const double eig = vn + qc[Q_A];
+      if (DT) {
+        dtt = sr.dn / eig;
+        if (!FLUX) {
+          const double pn = __ldg(q8 + (int64_t)sr.nb * Q_STRIDE + 4);
+          const double dp = fabs(pn - qc[4]) / (pn + qc[4] + P.p_bar + P.p_bar);
+          bad = dp > 0.1;
+        }
+      }
+      if (DIAG) dgt = 0.5 * sr.area * eig * P.lhs_omga;
+    }
+  }
+  // the folds, lane 0 from the initial values
+  double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double dtl = kBig;
+  if (lane == 0) {
+    if (FLUX && live && !res_zero)
+#pragma unroll
+      for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
+    if (has) {
+      if (FLUX)
+#pragma unroll
+        for (int k = 0; k < 5; k++) r[k] += t[k];
+      if (DT) dtl = smin(dtl, dtt);
+    }
+  }
+#pragma unroll
+  for (int j = 1; j < L; j++) {
+    double pr[5], pd = 0.0;
+    if (FLUX)
+#pragma unroll
+      for (int k = 0; k < 5; k++) pr[k] = lane_prev<L>(r[k]);
+    if (DT) pd = lane_prev<L>(dtl);
+    if (lane == j) {
+      if (FLUX)
+#pragma unroll
+        for (int k = 0; k < 5; k++) r[k] = has ? pr[k] + t[k] : pr[k];
+      if (DT) dtl = has ? smin(pd, dtt) : pd;
+    }
+  }
+  double dtc = 0.0;
+  if (DT) {
+#pragma unroll
+    for (int o = 1; o < L; o <<= 1) bad |= __shfl_xor_sync(0xffffffffu, bad, o, L);
+    if (last && live) {
+      const double cfl =
+          cfl_tab ? cfl_tab[(int64_t)(*iter_counter) * max(cs.ncase, 1) + cse] : cfl_arg;
+      const double cfl_min = 0.5 * cfl;
+      dtc = dtl * local_cfl(qc[4], bad ? 0 : 1, cfl, cfl_min, P);
+      dt[c] = dtc;
+    }
+  }
+  if (DIAG) {
+    double dtv;
+    if (DT)
+      dtv = __shfl_sync(0xffffffffu, dtc, L - 1, L);
+    else
+      dtv = live ? dt[c] : 1.0;
+    double d = 0.0;
+    if (lane == 0 && live) {
+      d = vol[c] / dtv;
+      if (has) d += dgt;
+    }
+#pragma unroll
+    for (int j = 1; j < L; j++) {
+      const double pd = lane_prev<L>(d);
+      if (lane == j) d = has ? pd + dgt : pd;
+    }
+    if (last && live) diag[c] = d;
+  }
+  if (FLUX && last && live)
+#pragma unroll
+    for (int k = 0; k < 5; k++) res[(int64_t)k * C + c] = r[k];
+  gather_epilogue<FLUX, DT>(live && last, cse, dtc, r, dt_ext, norm_part);
 }
 
 // Second-order face state (RECON): q + phi * grad(q) . (x_f - x_c) for an
@@ -473,8 +644,8 @@ __device__ __forceinline__ void reconstruct(double *q, int32_t c, int32_t C, int
 
 // RoeFlux_noprec once per face (the reference's own face loop,
 // cal_flux.cpp:84-192), from q[c1] and q[c2] with the stored normal, into
-// fflux[5][F]; the face gathers then add each face's flux to its cells in
-// ascending face order.  The arguments are those the per-cell form passes
+// row f of fflux[F][kFluxRow]; the face gathers then add each face's flux to
+// its cells in ascending face order.  The arguments are those the per-cell form passes
 // from either side, so the sums are the same bits with half the flux work.
 // RECON:
 // the face states reconstructed to second order first (a face whose
@@ -495,6 +666,9 @@ k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restri
   double ql[Q_STRIDE], qr[Q_STRIDE], fl[5];
   load_q(q8, fr.c1, ql);
   load_q(q8, fr.c2, qr);
+  // CellIsMG's test of the two cells' states (first order, as the gathers)
+  const double dp = fabs(qr[4] - ql[4]) / (qr[4] + ql[4] + P.p_bar + P.p_bar);
+  const double mg = dp > 0.1 ? 1.0 : 0.0;
   if (RECON) {
     double al[Q_STRIDE], ar[Q_STRIDE];
 #pragma unroll
@@ -519,8 +693,10 @@ k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restri
     roe_flux_mx(ql, qr, fr.nx, fr.ny, fr.nz, fr.area, P, flux_params<float>(P), fl);
   else
     roe_flux(ql, qr, fr.nx, fr.ny, fr.nz, fr.area, P, fl);
-#pragma unroll
-  for (int k = 0; k < 5; k++) fflux[(int64_t)k * F + f] = fl[k];
+  double2 *row = reinterpret_cast<double2 *>(fflux + (int64_t)f * kFluxRow);
+  row[0] = make_double2(fl[0], fl[1]);
+  row[1] = make_double2(fl[2], fl[3]);
+  row[2] = make_double2(fl[4], mg);
 }
 
 // Per-cell limiter of the reconstruction, per variable: the minimum over the
@@ -1933,21 +2109,22 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
 // cal_gradient.cpp:1740-1897), divided by the volume.
 __device__ __forceinline__ void grad_faces_cell(
     int32_t c, int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-    const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+    const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+    const int32_t *__restrict__ fnptr,
     const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
     const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ dqdx,
     double *__restrict__ dqdy, double *__restrict__ dqdz) {
   if (c >= C) return;
   double gx[5] = {0., 0., 0., 0., 0.}, gy[5] = {0., 0., 0., 0., 0.},
          gz[5] = {0., 0., 0., 0., 0.};
-  double qc[Q_STRIDE];
-  load_q(q8, c, qc);
-  const int32_t s1 = cptr[c + 1];
-  for (int32_t s = cptr[c]; s < s1; s++) {
-    const SlotRec sr = slots[s];
+  const int32_t ns = cptr[c + 1] - cptr[c];
+  const SlotRec *sl = sslots + sptr32[c / kSlice] + c % kSlice;  // sliced
+  for (int32_t j = 0; j < ns; j++) {
+    const SlotRec sr = sl[(int64_t)j * kSlice];
     double qs[5];
     if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
-      double qg[Q_STRIDE];
+      double qc[Q_STRIDE], qg[Q_STRIDE];
+      load_q(q8, c, qc);
       load_q(q8, sr.nb, qg);
       for (int v = 0; v < 5; v++) qs[v] = 0.5 * (qc[v] + qg[v]);
     } else {
@@ -1999,12 +2176,13 @@ __device__ __forceinline__ void grad_faces_cell(
 
 __global__ void __launch_bounds__(kGradBlockMax)
 k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-             const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+             const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+             const int32_t *__restrict__ fnptr,
              const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
              const double *__restrict__ q8, const double *__restrict__ vol,
              double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz) {
-  grad_faces_cell(blockIdx.x * blockDim.x + threadIdx.x, C, n, cptr, slots, fnptr, fnodes, qn8,
-                  q8, vol, dqdx, dqdy, dqdz);
+  grad_faces_cell(blockIdx.x * blockDim.x + threadIdx.x, C, n, cptr, sslots, sptr32, fnptr,
+                  fnodes, qn8, q8, vol, dqdx, dqdy, dqdz);
 }
 
 // Mixed form of node_finish: the sums (deviations from the freestream) times
@@ -2073,7 +2251,8 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
 
 __global__ void __launch_bounds__(kGradBlockMax)
 k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-                const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+                const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+                const int32_t *__restrict__ fnptr,
                 const int32_t *__restrict__ fnodes, const float *__restrict__ qn4,
                 const double *__restrict__ q8, const double *__restrict__ vol,
                 double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz,
@@ -2083,14 +2262,14 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
   const Params P = params_of(P0, cs, c);
   float gx[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, gy[5] = {0.f, 0.f, 0.f, 0.f, 0.f},
         gz[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-  double qc[Q_STRIDE];
-  load_q(q8, c, qc);
-  const int32_t s1 = cptr[c + 1];
-  for (int32_t s = cptr[c]; s < s1; s++) {
-    const SlotRec sr = slots[s];
+  const int32_t ns = cptr[c + 1] - cptr[c];
+  const SlotRec *sl = sslots + sptr32[c / kSlice] + c % kSlice;  // sliced
+  for (int32_t j = 0; j < ns; j++) {
+    const SlotRec sr = sl[(int64_t)j * kSlice];
     float qs[5];
     if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
-      double qg[Q_STRIDE];
+      double qc[Q_STRIDE], qg[Q_STRIDE];
+      load_q(q8, c, qc);
       load_q(q8, sr.nb, qg);
       for (int v = 0; v < 5; v++) qs[v] = (float)(0.5 * ((qc[v] - P.ref[v]) + (qg[v] - P.ref[v])));
     } else {
@@ -2134,6 +2313,167 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
   }
 }
 
+// Green-Gauss face sums with one lane per (cell, face) slot (L lanes per
+// cell, L at least its face count): each lane forms its face's value (the
+// mean of the face's node values, or of the cell and ghost states) and its
+// area-weighted normal components; the 15 sums are folds over the slots in
+// ascending face order passed from lane to lane (a difference as the sum with
+// the negated term, exactly), so the same bits as grad_faces_cell (FP64) and
+// k_grad_faces_mx (mixed: FP32 sums of deviations from the freestream).
+template <int L, bool MX>
+__global__ void __launch_bounds__(kGradBlockMax)
+k_grad_faces_lanes(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
+                   const SlotRec *__restrict__ slots, const int32_t *__restrict__ fnptr,
+                   const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
+                   const float *__restrict__ qn4, const double *__restrict__ q8,
+                   const double *__restrict__ vol, double *__restrict__ dqdx,
+                   double *__restrict__ dqdy, double *__restrict__ dqdz, Params P0, Cases cs) {
+  using T = typename std::conditional<MX, float, double>::type;
+  static_assert((L & (L - 1)) == 0 && L >= 2 && L <= 32, "lanes per cell");
+  const int64_t cl = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / L;
+  const bool live = cl < C;
+  const int32_t c = live ? (int32_t)cl : 0;
+  const int lane = threadIdx.x & (L - 1);
+  int32_t s0 = 0, ns = 0;
+  if (live) {
+    s0 = __ldg(cptr + c);
+    ns = __ldg(cptr + c + 1) - s0;
+  }
+  const bool has = live && lane < ns;
+  // this lane's face: value qs and weight a n (sign folded in)
+  T qs[5] = {0, 0, 0, 0, 0};
+  T ax = 0, ay = 0, az = 0, aw = 0;
+  bool minus = false;
+  double dnx = 0.0, dny = 0.0, dnz = 0.0, darea = 0.0;
+  if (has) {
+    const SlotRec sr = slots[s0 + lane];
+    if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
+      double qc[Q_STRIDE], qg[Q_STRIDE];
+      load_q(q8, c, qc);
+      load_q(q8, sr.nb, qg);
+      if (MX) {
+        const Params P = params_of(P0, cs, c);
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+          qs[v] = (T)(0.5 * ((qc[v] - P.ref[v]) + (qg[v] - P.ref[v])));
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; v++) qs[v] = (T)(0.5 * (qc[v] + qg[v]));
+      }
+    } else {
+      auto add = [&](int32_t node) {
+        if (MX) {
+          const float4 *p = reinterpret_cast<const float4 *>(qn4 + (int64_t)node * Q_STRIDE);
+          const float4 a = __ldg(p), b = __ldg(p + 1);
+          qs[0] += (T)a.x;
+          qs[1] += (T)a.y;
+          qs[2] += (T)a.z;
+          qs[3] += (T)a.w;
+          qs[4] += (T)b.x;
+        } else {
+          const double2 *p = reinterpret_cast<const double2 *>(qn8 + (int64_t)node * Q_STRIDE);
+          const double2 a = __ldg(p), b = __ldg(p + 1), e = __ldg(p + 2);
+          qs[0] += (T)a.x;
+          qs[1] += (T)a.y;
+          qs[2] += (T)b.x;
+          qs[3] += (T)b.y;
+          qs[4] += (T)e.x;
+        }
+      };
+      int32_t nn = 3;
+      if (sr.flags & SLOT_TRI) {
+        add(sr.tri[0]);
+        add(sr.tri[1]);
+        add(sr.tri[2]);
+      } else {
+        const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+        for (int32_t j = j0; j < j1; j++) add(fnodes[j]);
+        nn = j1 - j0;
+      }
+      if (MX) {
+        const float rc = __fdividef(1.0f, (float)nn);
+#pragma unroll
+        for (int v = 0; v < 5; v++) qs[v] = (T)((float)qs[v] * rc);
+      } else {
+        const double cnt = (double)nn;
+#pragma unroll
+        for (int v = 0; v < 5; v++) qs[v] = (T)((double)qs[v] / cnt);
+      }
+    }
+    minus = (sr.flags & SLOT_IS_C2) != 0;
+    if (MX) {
+      aw = (T)(minus ? -(float)sr.area : (float)sr.area);
+      ax = (T)(float)sr.nx;
+      ay = (T)(float)sr.ny;
+      az = (T)(float)sr.nz;
+    } else {
+      darea = sr.area;
+      dnx = sr.nx;
+      dny = sr.ny;
+      dnz = sr.nz;
+    }
+  }
+  // this lane's 15 terms: FP64 (qs area) n, negated for the second cell;
+  // mixed (qs (+-area)) n
+  auto terms = [&](int v, T &tx, T &ty, T &tz) {
+    if (MX) {
+      const T qsum = qs[v] * aw;
+      tx = qsum * ax;
+      ty = qsum * ay;
+      tz = qsum * az;
+    } else {
+      const double qsum = (double)qs[v] * darea;
+      const double x = qsum * dnx, y = qsum * dny, z = qsum * dnz;
+      tx = (T)(minus ? -x : x);
+      ty = (T)(minus ? -y : y);
+      tz = (T)(minus ? -z : z);
+    }
+  };
+  T gx[5], gy[5], gz[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    T tx, ty, tz;
+    terms(v, tx, ty, tz);
+    gx[v] = (lane == 0 && has) ? (T)0 + tx : (T)0;
+    gy[v] = (lane == 0 && has) ? (T)0 + ty : (T)0;
+    gz[v] = (lane == 0 && has) ? (T)0 + tz : (T)0;
+  }
+#pragma unroll
+  for (int j = 1; j < L; j++) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const T px = __shfl_up_sync(0xffffffffu, gx[v], 1, L);
+      const T py = __shfl_up_sync(0xffffffffu, gy[v], 1, L);
+      const T pz = __shfl_up_sync(0xffffffffu, gz[v], 1, L);
+      if (lane == j) {
+        T tx, ty, tz;
+        terms(v, tx, ty, tz);
+        gx[v] = has ? px + tx : px;
+        gy[v] = has ? py + ty : py;
+        gz[v] = has ? pz + tz : pz;
+      }
+    }
+  }
+  if (lane != L - 1 || !live) return;
+  if (MX) {
+    const float rv = __fdividef(1.0f, (float)vol[c]);
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      dqdx[v * n + c] = (double)((float)gx[v] * rv);
+      dqdy[v * n + c] = (double)((float)gy[v] * rv);
+      dqdz[v * n + c] = (double)((float)gz[v] * rv);
+    }
+  } else {
+    const double vc = vol[c];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      dqdx[v * n + c] = (double)gx[v] / vc;
+      dqdy[v * n + c] = (double)gy[v] / vc;
+      dqdz[v * n + c] = (double)gz[v] / vc;
+    }
+  }
+}
+
 // Residual norm from res (main.cpp:294-317) as fixed-order block partials.
 __global__ void k_norm_partial(int32_t C, const double *__restrict__ res,
                                double *__restrict__ part) {
@@ -2157,21 +2497,35 @@ __global__ void k_norm_partial(int32_t C, const double *__restrict__ res,
 }
 
 // Final reduction of the partials; also advances the fused-loop counter.
-__global__ void k_norm_final(int32_t nparts, const double *__restrict__ part,
-                             double *__restrict__ out, int32_t *__restrict__ iter_counter,
-                             double *__restrict__ hist) {
-  __shared__ double sh[5][32];
-  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
-  if (k < 5) {
-    double acc = 0.0;
-    for (int32_t b = lane; b < nparts; b += 32) acc += part[(int64_t)b * 5 + k];
-    sh[k][lane] = acc;
-  }
+// The sums over b < nparts of part[b][k] (k < 5) in a fixed order: thread t
+// of the block (kNormThreads) adds b = t, t + kNormThreads, ... in turn, then
+// a tree over the threads halves them in fixed pairs.  sh[k][0] holds sum k.
+constexpr int kNormThreads = 256;
+__device__ __forceinline__ void norm_parts_sum(int32_t nparts, const double *__restrict__ part,
+                                               double (*sh)[kNormThreads]) {
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+  for (int32_t b = threadIdx.x; b < nparts; b += kNormThreads)
+#pragma unroll
+    for (int k = 0; k < 5; k++) acc[k] += part[(int64_t)b * 5 + k];
+#pragma unroll
+  for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = acc[k];
   __syncthreads();
+  for (int w = kNormThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int k = 0; k < 5; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + w];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kNormThreads)
+k_norm_final(int32_t nparts, const double *__restrict__ part, double *__restrict__ out,
+             int32_t *__restrict__ iter_counter, double *__restrict__ hist) {
+  __shared__ double sh[5][kNormThreads];
+  norm_parts_sum(nparts, part, sh);
   if (threadIdx.x < 5) {
-    double acc = 0.0;
-    for (int l = 0; l < 32; l++) acc += sh[threadIdx.x][l];
-    const double v = sqrt(acc);
+    const double v = sqrt(sh[threadIdx.x][0]);
     out[threadIdx.x] = v;
     if (hist) hist[(int64_t)(*iter_counter) * 5 + threadIdx.x] = v;
   }
@@ -2344,21 +2698,11 @@ __global__ void k_selftest_division_fast(int64_t n, uint64_t seed,
 
 // The partials of k_norm_final, summed in its order, left squared: a part's
 // share of main.cpp:311-312's MPI_Reduce.
-__global__ void k_norm_sums(int32_t nparts, const double *__restrict__ part,
-                            double *__restrict__ out) {
-  __shared__ double sh[5][32];
-  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
-  if (k < 5) {
-    double acc = 0.0;
-    for (int32_t b = lane; b < nparts; b += 32) acc += part[(int64_t)b * 5 + k];
-    sh[k][lane] = acc;
-  }
-  __syncthreads();
-  if (threadIdx.x < 5) {
-    double acc = 0.0;
-    for (int l = 0; l < 32; l++) acc += sh[threadIdx.x][l];
-    out[threadIdx.x] = acc;
-  }
+__global__ void __launch_bounds__(kNormThreads)
+k_norm_sums(int32_t nparts, const double *__restrict__ part, double *__restrict__ out) {
+  __shared__ double sh[5][kNormThreads];
+  norm_parts_sum(nparts, part, sh);
+  if (threadIdx.x < 5) out[threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // Rows (Q_STRIDE doubles) of the listed records into a packed buffer [n][8];
@@ -2569,8 +2913,13 @@ struct mfg_ctx {
   double *vol = nullptr, *staging = nullptr;
   int32_t *cptr = nullptr;
   SlotRec *slots = nullptr;
+  // the slots again, sliced: the cells in slices of kSlice (a warp), slot j
+  // of the slice's lane t at sptr32[slice] + j kSlice + t, so that a warp's
+  // one-thread-per-cell gathers read consecutive records
+  SlotRec *sslots = nullptr;
+  int32_t *sptr32 = nullptr;
   FaceRec *faces = nullptr;  // per-face flux: normal, area, cells
-  double *fflux = nullptr;   // per-face flux [5][F]
+  double *fflux = nullptr;   // per-face flux rows [F][kFluxRow]
   int32_t *bctype_d = nullptr;  // BC type of each boundary face [G]
   int32_t live_bc = 0;          // ghost states recomputed every iteration
   int32_t flux_fp64 = 0;        // mixed form: the Roe flux wholly in FP64
@@ -2603,6 +2952,10 @@ struct mfg_ctx {
   // the fused face gather and the face flux are compiled for (their register
   // caps), and the block sizes of the two gradient kernels
   int gather_minb = MFG_GATHER_MINB, flux_minb = MFG_FLUX_MINB;
+  // lanes per cell of the face gather and the gradient face sums (one lane
+  // per face; 0: one thread per cell), and the most the grid's cells allow
+  // (0 for cells of more than 8 faces)
+  int gather_lanes = 0, gather_lanes_fit = 0;
   int node_block = kNodeBlock, grad_block = kGradBlock;
   int ring = kRing;                 // ring positions the tables were built for
   int chunking = 0;              // chunk assignment of the forward sweep (MFG_CHUNK_*)
@@ -2778,9 +3131,10 @@ __global__ void k_dev_slots(int32_t C, int32_t B, const int32_t *__restrict__ cp
                             const double *__restrict__ yfc, const double *__restrict__ zfc,
                             const double *__restrict__ xcc, const double *__restrict__ ycc,
                             const double *__restrict__ zcc, SlotRec *__restrict__ slots,
-                            int32_t *__restrict__ bad) {
+                            int32_t *__restrict__ bad, int32_t *__restrict__ max_slots) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C) return;
+  atomicMax(max_slots, cptr[c + 1] - cptr[c]);
   const double cx = xcc[c], cy = ycc[c], cz = zcc[c];
   for (int32_t j = cptr[c]; j < cptr[c + 1]; j++) {
     const int32_t f = cf[j];
@@ -3795,6 +4149,18 @@ static int ctx_begin(int32_t n_node, int32_t n_face, int32_t n_cell, int32_t n_b
   return MFG_OK;
 }
 
+namespace {
+int build_sliced_slots(mfg_ctx *ctx);  // defined with the device-build helpers
+}  // namespace
+
+// Blocks of the face gather, each leaving one partial of the residual norm.
+static int gather_blocks(const mfg_ctx *ctx) {
+  return grid_for((int64_t)ctx->C * std::max(ctx->gather_lanes, 1));
+}
+static int gather_blocks_max(const mfg_ctx *ctx) {
+  return grid_for((int64_t)ctx->C * std::max(ctx->gather_lanes_fit, 1));
+}
+
 // Buffers of the iteration, their initial contents and the initial state:
 // the end of every context creation.
 static int ctx_finish(mfg_ctx *ctx, const double *q0, const CaseLayout &cl) {
@@ -3802,6 +4168,7 @@ static int ctx_finish(mfg_ctx *ctx, const double *q0, const CaseLayout &cl) {
   const int64_t n = ctx->n;
   const int32_t precision = ctx->precision;
   int rc;
+  if ((rc = build_sliced_slots(ctx))) return rc;
   if (precision == MFG_PREC_MIXED) {
     for (int k = 0; k < 2; k++)
       if ((rc = dalloc(ctx, &ctx->q4[k], (size_t)n * Q_STRIDE))) return rc;
@@ -3819,7 +4186,7 @@ static int ctx_finish(mfg_ctx *ctx, const double *q0, const CaseLayout &cl) {
   if ((rc = dalloc(ctx, &ctx->qn8, (size_t)ctx->N * Q_STRIDE))) return rc;
   if ((rc = dalloc(ctx, &ctx->staging, (size_t)5 * n))) return rc;
   if ((rc = dalloc(ctx, &ctx->dt_ext, (size_t)2 * cl.ncase))) return rc;
-  const int nparts = std::max(grid_for(C), kNormBlocks);
+  const int nparts = std::max(gather_blocks_max(ctx), kNormBlocks);
   if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return rc;
   if ((rc = dalloc(ctx, &ctx->norm_out, (size_t)5 * cl.ncase))) return rc;
   if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return rc;
@@ -3903,12 +4270,17 @@ static int create_impl(const mfg_mesh *m, const mfg_params *params, const CaseLa
   if ((rc = dupload(ctx, &ctx->cptr, cptr))) return fail(rc);
   if ((rc = dupload(ctx, &ctx->slots, slots))) return fail(rc);
   {
+    int32_t max_slots = 0;
+    for (int32_t c = 0; c < C; c++) max_slots = std::max(max_slots, cptr[c + 1] - cptr[c]);
+    ctx->gather_lanes_fit = gather_lanes_for(max_slots);
+  }
+  {
     std::vector<FaceRec> fr(m->n_face);
     for (int32_t f = 0; f < m->n_face; f++)
       fr[f] = FaceRec{m->xfn[f], m->yfn[f], m->zfn[f], m->area[f], m->f2c[2 * f],
                       m->f2c[2 * f + 1], 0, 0};
     if ((rc = dupload(ctx, &ctx->faces, fr))) return fail(rc);
-    if ((rc = dalloc(ctx, &ctx->fflux, (size_t)5 * m->n_face))) return fail(rc);
+    if ((rc = dalloc(ctx, &ctx->fflux, (size_t)kFluxRow * m->n_face))) return fail(rc);
     std::vector<int32_t> bt(m->bctype, m->bctype + m->n_bface);
     if ((rc = dupload(ctx, &ctx->bctype_d, bt))) return fail(rc);
   }
@@ -4121,6 +4493,51 @@ int dev_sort_pairs(DevScratch &sc, const int32_t *kin, int32_t *kout, const int3
   return MFG_OK;
 }
 
+// One thread per slice: kSlice times the most slots of its cells.
+__global__ void k_slice_width(int32_t C, const int32_t *__restrict__ cptr,
+                              int32_t *__restrict__ width) {
+  const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t nsl = (C + kSlice - 1) / kSlice;
+  if (b > nsl) return;
+  int32_t w = 0;
+  if (b < nsl)
+    for (int32_t c = b * kSlice; c < min(C, (b + 1) * kSlice); c++)
+      w = max(w, cptr[c + 1] - cptr[c]);
+  width[b] = w * kSlice;
+}
+
+__global__ void k_slice_fill(int32_t C, const int32_t *__restrict__ cptr,
+                             const SlotRec *__restrict__ slots, const int32_t *__restrict__ sptr32,
+                             SlotRec *__restrict__ sslots) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  SlotRec *o = sslots + sptr32[c / kSlice] + c % kSlice;
+  const int32_t s0 = cptr[c], ns = cptr[c + 1] - s0;
+  for (int32_t j = 0; j < ns; j++) o[(int64_t)j * kSlice] = slots[s0 + j];
+}
+
+// The sliced copy of the slot records (see mfg_ctx::sslots), from cptr and
+// slots on the device.
+int build_sliced_slots(mfg_ctx *ctx) {
+  const int32_t C = ctx->C, nsl = (C + kSlice - 1) / kSlice;
+  cudaStream_t st = ctx->stream;
+  DevScratch sc;
+  int32_t *width = nullptr;
+  int rc;
+  if ((rc = sc.get(&width, (int64_t)nsl + 1))) return rc;
+  if ((rc = dalloc(ctx, &ctx->sptr32, (size_t)nsl + 1))) return rc;
+  k_slice_width<<<grid_for((int64_t)nsl + 1), kBlock, 0, st>>>(C, ctx->cptr, width);
+  if ((rc = dev_scan(sc, width, ctx->sptr32, nsl + 1, st))) return rc;
+  int32_t total = 0;
+  if ((rc = dev_read_i32(ctx->sptr32 + nsl, &total, st))) return rc;
+  if ((rc = dalloc(ctx, &ctx->sslots, (size_t)std::max(total, 1)))) return rc;
+  k_slice_fill<<<grid_for(C), kBlock, 0, st>>>(C, ctx->cptr, ctx->slots, ctx->sptr32,
+                                                 ctx->sslots);
+  MFG_CUDA(cudaGetLastError());
+  MFG_CUDA(cudaStreamSynchronize(st));
+  return MFG_OK;
+}
+
 template <typename T>
 int d2h(std::vector<T> &h, const T *d, int64_t count, cudaStream_t st) {
   h.resize((size_t)std::max<int64_t>(count, 0));
@@ -4293,13 +4710,14 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
   const int64_t n = ctx->n;
   cudaStream_t st = ctx->stream;
   DevScratch sc;
-  int32_t *flags = nullptr;  // [0] bad slot, [1] most records of a cell, [2] bad node list
-  if ((rc = sc.get(&flags, 3))) return fail(rc);
-  MFG_CUDA_OR(cudaMemsetAsync(flags, 0, 3 * sizeof(int32_t), st));
+  // [0] bad slot, [1] most records of a cell, [2] bad node list, [3] most faces of a cell
+  int32_t *flags = nullptr;
+  if ((rc = sc.get(&flags, 4))) return fail(rc);
+  MFG_CUDA_OR(cudaMemsetAsync(flags, 0, 4 * sizeof(int32_t), st));
   // slots, faces, volumes, BC types
   ctx->S = pp->S;
   if ((rc = dalloc(ctx, &ctx->cptr, (size_t)C + 1)) || (rc = dalloc(ctx, &ctx->slots, pp->S)) ||
-      (rc = dalloc(ctx, &ctx->faces, F)) || (rc = dalloc(ctx, &ctx->fflux, (size_t)5 * F)) ||
+      (rc = dalloc(ctx, &ctx->faces, F)) || (rc = dalloc(ctx, &ctx->fflux, (size_t)kFluxRow * F)) ||
       (rc = dalloc(ctx, &ctx->bctype_d, G)) || (rc = dalloc(ctx, &ctx->vol, n)))
     return fail(rc);
   MFG_CUDA_OR(cudaMemcpyAsync(ctx->cptr, pp->cptr, sizeof(int32_t) * ((size_t)C + 1),
@@ -4313,7 +4731,7 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
                                               pp->f2c, pp->bctype,
                                               pp->xfn, pp->yfn, pp->zfn, pp->area, pp->xfc,
                                               pp->yfc, pp->zfc, pp->xcc, pp->ycc, pp->zcc,
-                                              ctx->slots, flags);
+                                              ctx->slots, flags, flags + 3);
   k_dev_faces<<<grid_for(F), kBlock, 0, st>>>(F, pp->f2c, pp->xfn, pp->yfn, pp->zfn, pp->area,
                                               ctx->faces);
   if ((rc = dalloc(ctx, &ctx->fcen, F)) || (rc = dalloc(ctx, &ctx->ccen, n))) return fail(rc);
@@ -4331,10 +4749,11 @@ int create_from_prep_impl(const mfg_prep_gpu *pp, const mfg_params *params, cons
                                                bw.deg, flags + 1);
   count_launch();
   MFG_CUDA_OR(cudaGetLastError());
-  int32_t h_flags[3] = {0, 0, 0};
+  int32_t h_flags[4] = {0, 0, 0, 0};
   MFG_CUDA_OR(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, st));
   MFG_CUDA_OR(cudaStreamSynchronize(st));
   if (h_flags[0]) return fail(MFG_ERR_BADMESH);
+  ctx->gather_lanes_fit = gather_lanes_for(h_flags[3]);
   {
     // the choices of build_levels (the kernel kind once the levels are known)
     setup_sweep_grid(ctx, h_flags[1]);
@@ -4647,15 +5066,49 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
 #undef MFG_FLUX
     count_launch();
   }
+  if (ctx->gather_lanes == 4 || ctx->gather_lanes == 8) {
+    const int gl = gather_blocks(ctx);
+#define MFG_LANES(L_, F_, D_, G_, M_)                                                          \
+  k_face_gather_lanes<L_, F_, D_, G_, M_><<<gl, kBlock, 0, st>>>(                              \
+      ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,    \
+      ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux)
+#define MFG_LANES_L(F_, D_, G_, M_)                                                            \
+  if (ctx->gather_lanes == 4)                                                                 \
+    MFG_LANES(4, F_, D_, G_, M_);                                                             \
+  else                                                                                        \
+    MFG_LANES(8, F_, D_, G_, M_)
+    if (flux && dtp && diag) {
+      if (ctx->gather_minb == 2) {
+        MFG_LANES_L(true, true, true, 2);
+      } else if (ctx->gather_minb == 4) {
+        MFG_LANES_L(true, true, true, 4);
+      } else {
+        MFG_LANES_L(true, true, true, 3);
+      }
+    } else if (flux && !dtp && !diag) {
+      MFG_LANES_L(true, false, false, MFG_GATHER_MINB);
+    } else if (!flux && dtp && !diag) {
+      MFG_LANES_L(false, true, false, MFG_GATHER_MINB);
+    } else if (!flux && !dtp && diag) {
+      MFG_LANES_L(false, false, true, MFG_GATHER_MINB);
+    } else {
+      return MFG_ERR_INVALID;
+    }
+#undef MFG_LANES_L
+#undef MFG_LANES
+    count_launch();
+    if (flux) ctx->res_zero = false;
+    return check_kernel();
+  }
 #define MFG_FACE_M(F_, D_, G_, M_)                                                            \
   if (mx)                                                                                     \
     k_face_gather_mx<F_, D_, G_, F_, M_><<<g, kBlock, 0, st>>>(                               \
-        ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
+        ctx->C, ctx->cptr, ctx->sslots, ctx->sptr32, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
         ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
         ctx->F);                                                                              \
   else                                                                                        \
     k_face_gather<F_, D_, G_, F_, M_><<<g, kBlock, 0, st>>>(                                  \
-        ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
+        ctx->C, ctx->cptr, ctx->sslots, ctx->sptr32, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
         ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
         ctx->F)
 #define MFG_FACE(F_, D_, G_) MFG_FACE_M(F_, D_, G_, MFG_GATHER_MINB)
@@ -4898,13 +5351,35 @@ static void launch_node_values(mfg_ctx *ctx, cudaStream_t st) {
 
 static void launch_grad_faces(mfg_ctx *ctx, cudaStream_t st) {
   const int gb = ctx->grad_block;
+  const bool mx = ctx->precision == MFG_PREC_MIXED;
+  const int L = ctx->gather_lanes;
+  if (L == 4 || L == 8) {
+    const int g = grid_for((int64_t)ctx->C * L, gb);
+    const double *q = ctx->q8[ctx->cur];
+#define MFG_GRAD_LANES(L_, MX_)                                                                \
+  k_grad_faces_lanes<L_, MX_><<<g, gb, 0, st>>>(ctx->C, ctx->n, ctx->cptr, ctx->slots,           \
+                                                ctx->fnptr, ctx->fnodes, ctx->qn8, ctx->qn4, q,  \
+                                                ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz,       \
+                                                ctx->P, cases_of(ctx))
+    if (L == 4 && mx)
+      MFG_GRAD_LANES(4, true);
+    else if (L == 4)
+      MFG_GRAD_LANES(4, false);
+    else if (mx)
+      MFG_GRAD_LANES(8, true);
+    else
+      MFG_GRAD_LANES(8, false);
+#undef MFG_GRAD_LANES
+    count_launch();
+    return;
+  }
   if (ctx->precision == MFG_PREC_MIXED)
     k_grad_faces_mx<<<grid_for(ctx->C, gb), gb, 0, st>>>(
-        ctx->C, ctx->n, ctx->cptr, ctx->slots, ctx->fnptr, ctx->fnodes, ctx->qn4,
+        ctx->C, ctx->n, ctx->cptr, ctx->sslots, ctx->sptr32, ctx->fnptr, ctx->fnodes, ctx->qn4,
         ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->P, cases_of(ctx));
   else
     k_grad_faces<<<grid_for(ctx->C, gb), gb, 0, st>>>(
-        ctx->C, ctx->n, ctx->cptr, ctx->slots, ctx->fnptr, ctx->fnodes, ctx->qn8,
+        ctx->C, ctx->n, ctx->cptr, ctx->sslots, ctx->sptr32, ctx->fnptr, ctx->fnodes, ctx->qn8,
         ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
   count_launch();
 }
@@ -4927,7 +5402,7 @@ int mfg_calculate_gradient(mfg_ctx *ctx) {
 // batch reduces each case's cell range.
 static int launch_norm_tail(mfg_ctx *ctx, cudaStream_t st) {
   if (ctx->ncase == 1) {
-    k_norm_final<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, ctx->norm_out,
+    k_norm_final<<<1, kNormThreads, 0, st>>>(gather_blocks(ctx), ctx->norm_part, ctx->norm_out,
                                     ctx->iter_counter, ctx->norm_hist);
     count_launch();
   } else {
@@ -5304,6 +5779,7 @@ int mfg_autotune(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, int32_t flags
   knobs.push_back({MFG_KNOB_FLUX_BLOCKS, {3, 2, 4}});
   knobs.push_back({MFG_KNOB_NODE_BLOCK, {512, 256, 128}});
   knobs.push_back({MFG_KNOB_GRAD_BLOCK, {128, 64, 256}});
+  if (ctx->gather_lanes_fit) knobs.push_back({MFG_KNOB_GATHER_LANES, {0, ctx->gather_lanes_fit}});
   auto current = [&](int id) {
     switch (id) {
       case MFG_KNOB_SWEEP_KERNEL: return ctx->sweep_kind;
@@ -5313,6 +5789,7 @@ int mfg_autotune(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, int32_t flags
       case MFG_KNOB_GATHER_BLOCKS: return ctx->gather_minb;
       case MFG_KNOB_FLUX_BLOCKS: return ctx->flux_minb;
       case MFG_KNOB_NODE_BLOCK: return ctx->node_block;
+      case MFG_KNOB_GATHER_LANES: return ctx->gather_lanes;
       default: return ctx->grad_block;
     }
   };
@@ -5326,6 +5803,7 @@ int mfg_autotune(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, int32_t flags
       case MFG_KNOB_GATHER_BLOCKS: ctx->gather_minb = v; break;
       case MFG_KNOB_FLUX_BLOCKS: ctx->flux_minb = v; break;
       case MFG_KNOB_NODE_BLOCK: ctx->node_block = v; break;
+      case MFG_KNOB_GATHER_LANES: ctx->gather_lanes = v; break;
       default: ctx->grad_block = v; break;
     }
     drop_graphs(ctx);
@@ -5552,7 +6030,7 @@ int mfg_residual_norm(mfg_ctx *ctx, double out[5]) {
     return MFG_OK;
   }
   k_norm_partial<<<kNormBlocks, kBlock, 0, st>>>(ctx->C, ctx->res, ctx->norm_part);
-  k_norm_final<<<1, 160, 0, st>>>(kNormBlocks, ctx->norm_part, ctx->norm_out, nullptr, nullptr);
+  k_norm_final<<<1, kNormThreads, 0, st>>>(kNormBlocks, ctx->norm_part, ctx->norm_out, nullptr, nullptr);
   count_launch(2);
   MFG_CUDA(cudaGetLastError());
   MFG_CUDA(cudaMemcpyAsync(ctx->h_pinned, ctx->norm_out, 5 * sizeof(double),
@@ -5810,7 +6288,7 @@ int mfg_halo_phase(mfg_ctx *ctx, int32_t phase, int32_t iter_done) {
       ctx->res_zero = true;
       rc = launch_face(ctx, true, true, true, cfl_for(ctx->hp, iter_done), false, !second);
       if (rc) return rc;
-      k_norm_sums<<<1, 160, 0, st>>>(grid_for(ctx->C), ctx->norm_part, h.norm_sq);
+      k_norm_sums<<<1, kNormThreads, 0, st>>>(gather_blocks(ctx), ctx->norm_part, h.norm_sq);
       count_launch();
       MFG_CUDA(cudaMemcpyAsync(h.ext, ctx->dt_ext, 2 * sizeof(int64_t), cudaMemcpyDeviceToDevice,
                                st));
@@ -6056,7 +6534,7 @@ extern "C" int mfg_residual_norm_static(const double *res, int32_t n_cell, doubl
   // every partial that k_norm_final reads is written first, so nothing in
   // the scratch needs clearing between calls
   k_norm_partial<<<nblocks, kBlock, 0, st>>>(n_cell, res, scratch);
-  k_norm_final<<<1, 160, 0, st>>>(nblocks, scratch, norms, nullptr, nullptr);
+  k_norm_final<<<1, kNormThreads, 0, st>>>(nblocks, scratch, norms, nullptr, nullptr);
   count_launch(2);
   MFG_CUDA(cudaGetLastError());
   return MFG_OK;
