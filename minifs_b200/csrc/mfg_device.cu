@@ -274,6 +274,11 @@ __device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double d
 constexpr int kFluxRow = 6;
 // Cells per slice of the sliced slot records (one warp).
 constexpr int kSlice = 32;
+// One entry of a node's list (a cell, or a boundary face), with its weight.
+struct __align__(16) NodeEnt {
+  int32_t src, pad;
+  double w;
+};
 static_assert(kBlock % kSlice == 0, "blocks hold whole slices");
 
 // Per-cell face gather: Roe flux into the residual, local time step with
@@ -2066,7 +2071,7 @@ __device__ __forceinline__ void node_finish(int32_t nd, int32_t info,
 // the symmetry-plane projection of the velocity.
 __global__ void __launch_bounds__(kNodeBlock)
 k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
-              const int32_t *__restrict__ nsrc, const double *__restrict__ nw,
+              const NodeEnt *__restrict__ nsl, const int32_t *__restrict__ nsptr32,
               const int32_t *__restrict__ ninfo, const double *__restrict__ wnode,
               const double *__restrict__ nsym, const int32_t *__restrict__ bface_c1,
               const double *__restrict__ q8, double *__restrict__ qn8) {
@@ -2074,11 +2079,13 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
   if (nd >= N) return;
   const int32_t info = ninfo[nd];
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  const int32_t e1 = nptr[nd + 1];
+  const int32_t ne = nptr[nd + 1] - nptr[nd];
+  const NodeEnt *el = nsl + nsptr32[nd / kSlice] + nd % kSlice;  // sliced
   if (info & 1) {
-    for (int32_t e = nptr[nd]; e < e1; e++) {
-      const int32_t k = nsrc[e];
-      const double w = nw[e];
+    for (int32_t j = 0; j < ne; j++) {
+      const NodeEnt en = el[(int64_t)j * kSlice];
+      const int32_t k = en.src;
+      const double w = en.w;
       double qa[Q_STRIDE], qb[Q_STRIDE];
       load_q(q8, bface_c1[k], qa);
       load_q(q8, (int64_t)C + k, qb);
@@ -2089,10 +2096,11 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
       }
     }
   } else {
-    for (int32_t e = nptr[nd]; e < e1; e++) {
+    for (int32_t j = 0; j < ne; j++) {
+      const NodeEnt en = el[(int64_t)j * kSlice];
       double qa[Q_STRIDE];
-      load_q(q8, nsrc[e], qa);
-      const double w = nw[e];
+      load_q(q8, en.src, qa);
+      const double w = en.w;
       for (int v = 0; v < 5; v++) acc[v] += qa[v] * w;
     }
   }
@@ -2212,7 +2220,7 @@ __device__ __forceinline__ void node_finish_mx(int32_t nd, int32_t info,
 // the deviations instead of with the values.  Gradients stored in FP64.
 __global__ void __launch_bounds__(kNodeBlock)
 k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
-                 const int32_t *__restrict__ nsrc, const double *__restrict__ nw,
+                 const NodeEnt *__restrict__ nsl, const int32_t *__restrict__ nsptr32,
                  const int32_t *__restrict__ ninfo, const double *__restrict__ wnode,
                  const double *__restrict__ nsym, const int32_t *__restrict__ bface_c1,
                  const double *__restrict__ q8, float *__restrict__ qn4, Params P0, Cases cs) {
@@ -2220,14 +2228,15 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
   if (nd >= N) return;
   const int32_t info = ninfo[nd];
   float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-  const int32_t e0 = nptr[nd], e1 = nptr[nd + 1];
+  const int32_t ne = nptr[nd + 1] - nptr[nd];
+  const NodeEnt *el = nsl + nsptr32[nd / kSlice] + nd % kSlice;  // sliced
   // the case of a node is that of any cell it touches
-  const Params P =
-      e1 > e0 ? params_of(P0, cs, (info & 1) ? bface_c1[nsrc[e0]] : nsrc[e0]) : P0;
+  const Params P = ne > 0 ? params_of(P0, cs, (info & 1) ? bface_c1[el[0].src] : el[0].src) : P0;
   if (info & 1) {
-    for (int32_t e = e0; e < e1; e++) {
-      const int32_t k = nsrc[e];
-      const float w = (float)nw[e];
+    for (int32_t j = 0; j < ne; j++) {
+      const NodeEnt en = el[(int64_t)j * kSlice];
+      const int32_t k = en.src;
+      const float w = (float)en.w;
       double qa[Q_STRIDE], qb[Q_STRIDE];
       load_q(q8, bface_c1[k], qa);
       load_q(q8, (int64_t)C + k, qb);
@@ -2235,10 +2244,11 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
         acc[v] += (float)(0.5 * ((qa[v] - P.ref[v]) + (qb[v] - P.ref[v]))) * w;
     }
   } else {
-    for (int32_t e = e0; e < e1; e++) {
+    for (int32_t j = 0; j < ne; j++) {
+      const NodeEnt en = el[(int64_t)j * kSlice];
       double qa[Q_STRIDE];
-      load_q(q8, nsrc[e], qa);
-      const float w = (float)nw[e];
+      load_q(q8, en.src, qa);
+      const float w = (float)en.w;
       for (int v = 0; v < 5; v++) acc[v] += (float)(qa[v] - P.ref[v]) * w;
     }
   }
@@ -2931,6 +2941,10 @@ struct mfg_ctx {
   double *phi = nullptr;                 // limiter [5][C]
   int32_t *fnptr = nullptr, *fnodes = nullptr;
   int32_t *nptr = nullptr, *nsrc = nullptr, *ninfo = nullptr, *bface_c1 = nullptr;
+  // the node lists again, sliced like the slot records (entry j of the
+  // slice's lane t at nsptr32[slice] + j kSlice + t)
+  NodeEnt *nsl = nullptr;
+  int32_t *nsptr32 = nullptr;
   double *nw = nullptr, *wnode = nullptr, *nsym = nullptr;
   int32_t *fw_cells = nullptr, *fw_sptr = nullptr, *fw_nb = nullptr;
   SweepRec *fw_recs = nullptr;
@@ -4516,8 +4530,18 @@ __global__ void k_slice_fill(int32_t C, const int32_t *__restrict__ cptr,
   for (int32_t j = 0; j < ns; j++) o[(int64_t)j * kSlice] = slots[s0 + j];
 }
 
-// The sliced copy of the slot records (see mfg_ctx::sslots), from cptr and
-// slots on the device.
+__global__ void k_node_slice_fill(int32_t N, const int32_t *__restrict__ nptr,
+                                  const int32_t *__restrict__ nsrc, const double *__restrict__ nw,
+                                  const int32_t *__restrict__ nsptr32, NodeEnt *__restrict__ nsl) {
+  const int32_t nd = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nd >= N) return;
+  NodeEnt *o = nsl + nsptr32[nd / kSlice] + nd % kSlice;
+  const int32_t e0 = nptr[nd], ne = nptr[nd + 1] - e0;
+  for (int32_t j = 0; j < ne; j++) o[(int64_t)j * kSlice] = NodeEnt{nsrc[e0 + j], 0, nw[e0 + j]};
+}
+
+// The sliced copies of the slot records and of the node lists (see
+// mfg_ctx::sslots, nsl), from the plain ones on the device.
 int build_sliced_slots(mfg_ctx *ctx) {
   const int32_t C = ctx->C, nsl = (C + kSlice - 1) / kSlice;
   cudaStream_t st = ctx->stream;
@@ -4533,6 +4557,18 @@ int build_sliced_slots(mfg_ctx *ctx) {
   if ((rc = dalloc(ctx, &ctx->sslots, (size_t)std::max(total, 1)))) return rc;
   k_slice_fill<<<grid_for(C), kBlock, 0, st>>>(C, ctx->cptr, ctx->slots, ctx->sptr32,
                                                  ctx->sslots);
+  // the node lists
+  const int32_t N = ctx->N, nsn = (N + kSlice - 1) / kSlice;
+  int32_t *nwidth = nullptr;
+  if ((rc = sc.get(&nwidth, (int64_t)nsn + 1))) return rc;
+  if ((rc = dalloc(ctx, &ctx->nsptr32, (size_t)nsn + 1))) return rc;
+  k_slice_width<<<grid_for((int64_t)nsn + 1), kBlock, 0, st>>>(N, ctx->nptr, nwidth);
+  if ((rc = dev_scan(sc, nwidth, ctx->nsptr32, nsn + 1, st))) return rc;
+  int32_t ntotal = 0;
+  if ((rc = dev_read_i32(ctx->nsptr32 + nsn, &ntotal, st))) return rc;
+  if ((rc = dalloc(ctx, &ctx->nsl, (size_t)std::max(ntotal, 1)))) return rc;
+  k_node_slice_fill<<<grid_for(N), kBlock, 0, st>>>(N, ctx->nptr, ctx->nsrc, ctx->nw,
+                                                      ctx->nsptr32, ctx->nsl);
   MFG_CUDA(cudaGetLastError());
   MFG_CUDA(cudaStreamSynchronize(st));
   return MFG_OK;
@@ -5340,11 +5376,11 @@ static void launch_node_values(mfg_ctx *ctx, cudaStream_t st) {
   const int nb = ctx->node_block;
   if (ctx->precision == MFG_PREC_MIXED)
     k_node_values_mx<<<grid_for(ctx->N, nb), nb, 0, st>>>(
-        ctx->N, ctx->C, ctx->nptr, ctx->nsrc, ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
+        ctx->N, ctx->C, ctx->nptr, ctx->nsl, ctx->nsptr32, ctx->ninfo, ctx->wnode, ctx->nsym,
         ctx->bface_c1, ctx->q8[ctx->cur], ctx->qn4, ctx->P, cases_of(ctx));
   else
     k_node_values<<<grid_for(ctx->N, nb), nb, 0, st>>>(
-        ctx->N, ctx->C, ctx->nptr, ctx->nsrc, ctx->nw, ctx->ninfo, ctx->wnode, ctx->nsym,
+        ctx->N, ctx->C, ctx->nptr, ctx->nsl, ctx->nsptr32, ctx->ninfo, ctx->wnode, ctx->nsym,
         ctx->bface_c1, ctx->q8[ctx->cur], ctx->qn8);
   count_launch();
 }
