@@ -274,6 +274,8 @@ __device__ __forceinline__ void gather_epilogue(bool live, int32_t cse, double d
 constexpr int kFluxRow = 6;
 // Cells per slice of the sliced slot records (one warp).
 constexpr int kSlice = 32;
+// RN(1/3), folded by the compiler: the reciprocal of a triangle's node count.
+constexpr double kRcp3 = 1.0 / 3.0;
 // One entry of a node's list (a cell, or a boundary face), with its weight.
 struct __align__(16) NodeEnt {
   int32_t src, pad;
@@ -2156,8 +2158,17 @@ __device__ __forceinline__ void grad_faces_cell(
         for (int32_t j = j0; j < j1; j++) add(fnodes[j]);
         nn = j1 - j0;
       }
+      // the mean: a triangle's sums times RN(1/3) with Markstein's
+      // correction (the quotient's bits), else the divisions
       const double cnt = (double)nn;
-      for (int v = 0; v < 5; v++) qs[v] /= cnt;
+      bool ok = nn == 3;
+      double t[5];
+      for (int v = 0; v < 5; v++) t[v] = quot_pos(qs[v], 3.0, kRcp3, ok);
+      if (ok) {
+        for (int v = 0; v < 5; v++) qs[v] = t[v];
+      } else {
+        for (int v = 0; v < 5; v++) qs[v] /= cnt;
+      }
     }
     const bool minus = (sr.flags & SLOT_IS_C2) != 0;
     for (int v = 0; v < 5; v++) {
@@ -2174,11 +2185,29 @@ __device__ __forceinline__ void grad_faces_cell(
       }
     }
   }
+  // the 15 quotients by the volume from one reciprocal (the divisions when
+  // an operand is outside the window)
   const double vc = vol[c];
+  bool ok;
+  const double y = rcp_rn_fast(vc, ok);
+  double tx[5], ty[5], tz[5];
   for (int v = 0; v < 5; v++) {
-    dqdx[v * n + c] = gx[v] / vc;
-    dqdy[v * n + c] = gy[v] / vc;
-    dqdz[v * n + c] = gz[v] / vc;
+    tx[v] = quot_pos(gx[v], vc, y, ok);
+    ty[v] = quot_pos(gy[v], vc, y, ok);
+    tz[v] = quot_pos(gz[v], vc, y, ok);
+  }
+  if (!(vc > 0.0)) ok = false;
+  if (!ok) {
+    for (int v = 0; v < 5; v++) {
+      tx[v] = gx[v] / vc;
+      ty[v] = gy[v] / vc;
+      tz[v] = gz[v] / vc;
+    }
+  }
+  for (int v = 0; v < 5; v++) {
+    dqdx[v * n + c] = tx[v];
+    dqdy[v * n + c] = ty[v];
+    dqdz[v * n + c] = tz[v];
   }
 }
 

@@ -336,6 +336,17 @@ __device__ __forceinline__ double div_recip_fast(double a, double b, double y, b
   return __fma_rn(r1, y, q1);
 }
 
+// a / b for b > 0 with y = rcp_rn_fast(b): a zero a is its own quotient
+// (with its sign); otherwise div_recip_fast, which clears ok outside its
+// window (the caller then divides).
+__device__ __forceinline__ double quot_pos(double a, double b, double y, bool &ok) {
+  bool okq;
+  const double q = div_recip_fast(a, b, y, okq);
+  if (a == 0.0) return a;
+  ok = ok && okq;
+  return q;
+}
+
 // FluxLUSGS3D (forward_lusgs.cpp:1271-1324) with the neighbour's sound speed
 // and conserved energy taken from its record (same expressions), in two
 // parts: what the neighbour's state and the face give, which an LU-SGS sweep
