@@ -170,6 +170,12 @@ int mfg_info_get(mfg_ctx *ctx, mfg_info *info);
  * waits, with a bounded spin, for that neighbour's ready flag.  Both modes
  * give identical results. */
 int mfg_set_sweep_mode(mfg_ctx *ctx, int32_t mode);
+/* Face gather and gradient face sums: lanes = 0, one thread per cell (the
+ * default), or one lane per face of a cell with the per-cell sums passed
+ * from lane to lane in ascending face order (lanes = 4 where every cell has
+ * at most 4 faces, 8 where at most 8; other values MFG_ERR_UNSUPPORTED).
+ * Identical results, norms included; the autotuner times both. */
+int mfg_set_gather_lanes(mfg_ctx *ctx, int32_t lanes);
 /* Persistent sweeps: lanes per cell; the record slots per cell W is the
  * only value the current kernels take (others: MFG_ERR_UNSUPPORTED). */
 int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes);

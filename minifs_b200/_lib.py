@@ -156,6 +156,7 @@ def load(build_if_missing: bool = True):
         "mfg_info_get": (ct.c_int, [ctxp, ct.POINTER(Info)]),
         "mfg_set_sweep_mode": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_sweep_lanes": (ct.c_int, [ctxp, ct.c_int32]),
+        "mfg_set_gather_lanes": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_chunking": (ct.c_int, [ct.c_int32]),
         "mfg_set_sweep_kernel": (ct.c_int, [ct.c_int32]),
         "mfg_autotune_sweeps": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),

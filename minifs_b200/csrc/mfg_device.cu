@@ -4196,13 +4196,10 @@ namespace {
 int build_sliced_slots(mfg_ctx *ctx);  // defined with the device-build helpers
 }  // namespace
 
-// Blocks of the face gather, each leaving one partial of the residual norm.
-static int gather_blocks(const mfg_ctx *ctx) {
-  return grid_for((int64_t)ctx->C * std::max(ctx->gather_lanes, 1));
-}
-static int gather_blocks_max(const mfg_ctx *ctx) {
-  return grid_for((int64_t)ctx->C * std::max(ctx->gather_lanes_fit, 1));
-}
+// Partials of the residual norm a face gather leaves: one per 256 cells in
+// either gather form (the lane-per-face form has them formed by
+// k_norm_partial from res, in the one-thread gather's order).
+static int gather_blocks(const mfg_ctx *ctx) { return grid_for(ctx->C); }
 
 // Buffers of the iteration, their initial contents and the initial state:
 // the end of every context creation.
@@ -4229,7 +4226,7 @@ static int ctx_finish(mfg_ctx *ctx, const double *q0, const CaseLayout &cl) {
   if ((rc = dalloc(ctx, &ctx->qn8, (size_t)ctx->N * Q_STRIDE))) return rc;
   if ((rc = dalloc(ctx, &ctx->staging, (size_t)5 * n))) return rc;
   if ((rc = dalloc(ctx, &ctx->dt_ext, (size_t)2 * cl.ncase))) return rc;
-  const int nparts = std::max(gather_blocks_max(ctx), kNormBlocks);
+  const int nparts = std::max(gather_blocks(ctx), kNormBlocks);
   if ((rc = dalloc(ctx, &ctx->norm_part, (size_t)5 * nparts))) return rc;
   if ((rc = dalloc(ctx, &ctx->norm_out, (size_t)5 * cl.ncase))) return rc;
   if ((rc = dalloc(ctx, &ctx->iter_counter, 1))) return rc;
@@ -4989,6 +4986,15 @@ static void drop_graphs(mfg_ctx *ctx) {
     }
 }
 
+int mfg_set_gather_lanes(mfg_ctx *ctx, int32_t lanes) {
+  if (!ctx || lanes < 0) return MFG_ERR_INVALID;
+  if (lanes != 0 && lanes != ctx->gather_lanes_fit) return MFG_ERR_UNSUPPORTED;
+  ctx->gather_lanes = lanes;
+  drop_graphs(ctx);
+  return MFG_OK;
+}
+
+
 static int launch_ghost_bc(mfg_ctx *ctx, cudaStream_t st) {
   if (ctx->G == 0) return MFG_OK;
   const bool mx = ctx->precision == MFG_PREC_MIXED;
@@ -5132,11 +5138,11 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
     count_launch();
   }
   if (ctx->gather_lanes == 4 || ctx->gather_lanes == 8) {
-    const int gl = gather_blocks(ctx);
+    const int gl = grid_for((int64_t)ctx->C * ctx->gather_lanes);
 #define MFG_LANES(L_, F_, D_, G_, M_)                                                          \
   k_face_gather_lanes<L_, F_, D_, G_, M_><<<gl, kBlock, 0, st>>>(                              \
       ctx->C, ctx->cptr, ctx->slots, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,    \
-      ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux)
+      ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, nullptr, cs, ctx->fflux)
 #define MFG_LANES_L(F_, D_, G_, M_)                                                            \
   if (ctx->gather_lanes == 4)                                                                 \
     MFG_LANES(4, F_, D_, G_, M_);                                                             \
@@ -5162,6 +5168,10 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
 #undef MFG_LANES_L
 #undef MFG_LANES
     count_launch();
+    if (np) {  // the norm partials, from res in the one-thread gather's order
+      k_norm_partial<<<gather_blocks(ctx), kBlock, 0, st>>>(ctx->C, ctx->res, np);
+      count_launch();
+    }
     if (flux) ctx->res_zero = false;
     return check_kernel();
   }

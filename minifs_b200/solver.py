@@ -169,6 +169,11 @@ class Solver:
         """Persistent sweeps: lanes per cell (the record slots per cell W)."""
         self._call("mfg_set_sweep_lanes", int(lanes))
 
+    def set_gather_lanes(self, lanes: int):
+        """Face gather and gradient sums: 0 = one thread per cell, 4 or 8 = one
+        lane per face (as the grid's cells allow); identical results."""
+        self._call("mfg_set_gather_lanes", int(lanes))
+
     def autotune_sweeps(self, n_trial: int = 3) -> dict:
         """Time both lane counts on this grid and keep the faster; the state
         is left as it was.  Returns the choice and the ms per iteration."""

@@ -70,3 +70,30 @@ def test_wide_and_deep_sweep_kernels_same_bits(cube24, mixed):
         s.close()
     for f in out[0]:
         assert_bitwise(out[1][f], out[0][f], f"wide vs deep kernels: {f}")
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_lane_per_face_gathers_same_bits(cube24, mixed):
+    """The face gather and gradient sums with one lane per face (the sums
+    passed from lane to lane in face order) against one thread per cell:
+    every field and every iteration's residual norms bit for bit, fused and
+    per routine."""
+    from minifs_b200 import _lib
+    from minifs_b200.solver import Solver
+    p, pg = cube24
+    prec = "mixed" if mixed else "fp64"
+    a, b = Solver(pg, p, precision=prec), Solver(pg, p, precision=prec)
+    b.set_gather_lanes(4)
+    with pytest.raises(_lib.MfgError):
+        b.set_gather_lanes(8)  # tetrahedra: four faces per cell
+    for s in (a, b):
+        s.calculate_gradient()
+    na, nb = a.iterate(4), b.iterate(4)
+    assert_bitwise(nb.reshape(-1), na.reshape(-1), f"{prec} norms")
+    for s in (a, b):
+        s.step()
+    for f in ("q", "res", "dt", "diag", "dq", "dqdx", "dqdy", "dqdz"):
+        assert_bitwise(b.download(f), a.download(f), f"{prec} lanes per face: {f}")
+    assert_bitwise(b.residual_norm(), a.residual_norm(), f"{prec} routine norm")
+    a.close()
+    b.close()
