@@ -2546,7 +2546,7 @@ __global__ void k_norm_partial(int32_t C, const double *__restrict__ res,
 // The sums over b < nparts of part[b][k] (k < 5) in a fixed order: thread t
 // of the block (kNormThreads) adds b = t, t + kNormThreads, ... in turn, then
 // a tree over the threads halves them in fixed pairs.  sh[k][0] holds sum k.
-constexpr int kNormThreads = 256;
+constexpr int kNormThreads = 1024;
 __device__ __forceinline__ void norm_parts_sum(int32_t nparts, const double *__restrict__ part,
                                                double (*sh)[kNormThreads]) {
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
