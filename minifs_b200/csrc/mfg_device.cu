@@ -316,6 +316,10 @@ __device__ __forceinline__ void face_gather_cell(
     const SlotRec *sl = sslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
     double dtl = kBig;
     int det = 1;
+    // Diag's terms 0.5 area eig lhs_omga of the first four faces, formed with
+    // the time step's eigenvalue (the same expression), so that Diag's pass
+    // reads no slot record again for them
+    double dg0 = 0.0, dg1 = 0.0, dg2 = 0.0, dg3 = 0.0;
     for (int32_t j = 0; j < ns; j++) {
       const SlotRec sr = sl[(int64_t)j * kSlice];
       if (FLUX || DT) {
@@ -347,6 +351,13 @@ __device__ __forceinline__ void face_gather_cell(
           vn = fabs(vn);
           const double eigv = vn + qc[Q_A];
           dtl = smin(dtl, sr.dn / eigv);
+          if (DIAG) {
+            const double t = 0.5 * sr.area * eigv * P.lhs_omga;
+            dg0 = j == 0 ? t : dg0;
+            dg1 = j == 1 ? t : dg1;
+            dg2 = j == 2 ? t : dg2;
+            dg3 = j == 3 ? t : dg3;
+          }
           // CellIsMG: |p2-p1| and p2+p1 are symmetric in the two sides.
           if (PRE) {
             if (mgf != 0.0) det = 0;
@@ -367,7 +378,15 @@ __device__ __forceinline__ void face_gather_cell(
     if (DIAG) {
       const double dtv = DT ? dtc : dt[c];
       double d = vol[c] / dtv;
-      for (int32_t j = 0; j < ns; j++) {
+      int32_t j0 = 0;
+      if (DT) {
+        if (ns > 0) d += dg0;
+        if (ns > 1) d += dg1;
+        if (ns > 2) d += dg2;
+        if (ns > 3) d += dg3;
+        j0 = ns < 4 ? ns : 4;
+      }
+      for (int32_t j = j0; j < ns; j++) {
         const SlotRec sr = sl[(int64_t)j * kSlice];
         double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
         vn = fabs(vn);
@@ -427,6 +446,7 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
     const SlotRec *sl = sslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
     double dtl = kBig;
     int det = 1;
+    double dg0 = 0.0, dg1 = 0.0, dg2 = 0.0, dg3 = 0.0;  // as in face_gather_cell
     for (int32_t j = 0; j < ns; j++) {
       const SlotRec sr = sl[(int64_t)j * kSlice];
       if (FLUX || DT) {
@@ -456,6 +476,13 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
           vn = fabs(vn);
           const double eigv = vn + qd[Q_A];
           dtl = smin(dtl, sr.dn / eigv);
+          if (DIAG) {
+            const double t = 0.5 * sr.area * eigv * P.lhs_omga;
+            dg0 = j == 0 ? t : dg0;
+            dg1 = j == 1 ? t : dg1;
+            dg2 = j == 2 ? t : dg2;
+            dg3 = j == 3 ? t : dg3;
+          }
           if (PRE) {
             if (mgf != 0.0) det = 0;
           } else {
@@ -474,7 +501,15 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
     if (DIAG) {
       const double dtv = DT ? dtc : dt[c];
       double d = vol[c] / dtv;
-      for (int32_t j = 0; j < ns; j++) {
+      int32_t j0 = 0;
+      if (DT) {
+        if (ns > 0) d += dg0;
+        if (ns > 1) d += dg1;
+        if (ns > 2) d += dg2;
+        if (ns > 3) d += dg3;
+        j0 = ns < 4 ? ns : 4;
+      }
+      for (int32_t j = j0; j < ns; j++) {
         const SlotRec sr = sl[(int64_t)j * kSlice];
         double vn = qd[1] * sr.nx + qd[2] * sr.ny + qd[3] * sr.nz;
         vn = fabs(vn);
