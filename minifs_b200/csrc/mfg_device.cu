@@ -276,6 +276,24 @@ constexpr int kFluxRow = 6;
 constexpr int kSlice = 32;
 // RN(1/3), folded by the compiler: the reciprocal of a triangle's node count.
 constexpr double kRcp3 = 1.0 / 3.0;
+// The sliced slot records of the one-thread-per-cell kernels, each holding
+// what its kernel reads (48 bytes, so that a warp reads 1.5 KB per face
+// position).  The face gathers': the normal, area, dn, the neighbour, and
+// the face with the side in bit 31 (set where the cell is the face's second
+// cell).
+struct __align__(16) GatherSlot {
+  double nx, ny, nz, area, dn;
+  int32_t nb;
+  uint32_t face_c2;
+};
+// The gradient's: the normal, area, flags and n0..n2 = a triangle's nodes
+// (SLOT_TRI), else n0 = the ghost (a boundary face averaged with its ghost)
+// or the face (its nodes through the face -> node lists).
+struct __align__(16) GradSlot {
+  double nx, ny, nz, area;
+  int32_t n0, n1, n2, flags;
+};
+static_assert(sizeof(GatherSlot) == 48 && sizeof(GradSlot) == 48, "sliced slot records");
 // One entry of a node's list (a cell, or a boundary face), with its weight.
 struct __align__(16) NodeEnt {
   int32_t src, pad;
@@ -296,7 +314,7 @@ static_assert(kBlock % kSlice == 0, "blocks hold whole slices");
 
 template <bool FLUX, bool DT, bool DIAG, bool PRE>
 __device__ __forceinline__ void face_gather_cell(
-    int32_t c, int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ sslots,
+    int32_t c, int32_t C, const int32_t *__restrict__ cptr, const GatherSlot *__restrict__ gslots,
     const int32_t *__restrict__ sptr32, const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ res,
     int res_zero, double *__restrict__ dt, double *__restrict__ diag,
     const double *__restrict__ cfl_tab, const int32_t *__restrict__ iter_counter, double cfl_arg,
@@ -313,7 +331,7 @@ __device__ __forceinline__ void face_gather_cell(
     if (FLUX && !res_zero)
       for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
     const int32_t ns = __ldg(cptr + c + 1) - __ldg(cptr + c);
-    const SlotRec *sl = sslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
+    const GatherSlot *sl = gslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
     double dtl = kBig;
     int det = 1;
     // Diag's terms 0.5 area eig lhs_omga of the first four faces, formed with
@@ -321,7 +339,7 @@ __device__ __forceinline__ void face_gather_cell(
     // reads no slot record again for them
     double dg0 = 0.0, dg1 = 0.0, dg2 = 0.0, dg3 = 0.0;
     for (int32_t j = 0; j < ns; j++) {
-      const SlotRec sr = sl[(int64_t)j * kSlice];
+      const GatherSlot sr = sl[(int64_t)j * kSlice];
       if (FLUX || DT) {
         // the neighbour's state: its pressure for CellIsMG and, without the
         // per-face rows, the flux; with them (PRE) the row holds both
@@ -331,16 +349,16 @@ __device__ __forceinline__ void face_gather_cell(
           double f[5];
           if (PRE) {  // the face's flux, computed once by k_face_flux
             const double2 *row =
-                reinterpret_cast<const double2 *>(fflux + (int64_t)sr.face * kFluxRow);
+                reinterpret_cast<const double2 *>(fflux + (int64_t)(sr.face_c2 & 0x7FFFFFFFu) * kFluxRow);
             const double2 a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2);
             f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y; f[4] = e.x;
             mgf = e.y;
-          } else if (sr.flags & SLOT_IS_C2) {
+          } else if (sr.face_c2 >> 31) {
             roe_flux(qn, qc, sr.nx, sr.ny, sr.nz, sr.area, P, f);
           } else {
             roe_flux(qc, qn, sr.nx, sr.ny, sr.nz, sr.area, P, f);
           }
-          if (sr.flags & SLOT_IS_C2) {
+          if (sr.face_c2 >> 31) {
             for (int k = 0; k < 5; k++) r[k] += f[k];
           } else {
             for (int k = 0; k < 5; k++) r[k] -= f[k];
@@ -387,7 +405,7 @@ __device__ __forceinline__ void face_gather_cell(
         j0 = ns < 4 ? ns : 4;
       }
       for (int32_t j = j0; j < ns; j++) {
-        const SlotRec sr = sl[(int64_t)j * kSlice];
+        const GatherSlot sr = sl[(int64_t)j * kSlice];
         double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
         vn = fabs(vn);
         const double eig = vn + qc[Q_A];
@@ -403,7 +421,7 @@ __device__ __forceinline__ void face_gather_cell(
 
 template <bool FLUX, bool DT, bool DIAG, bool PRE, int MINB = MFG_GATHER_MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
-k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__restrict__ sslots,
+k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const GatherSlot *__restrict__ gslots,
               const int32_t *__restrict__ sptr32, const double *__restrict__ q8,
               const double *__restrict__ vol,
               double *__restrict__ res, int res_zero, double *__restrict__ dt,
@@ -411,7 +429,7 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
               const int32_t *__restrict__ iter_counter, double cfl_arg, Params P0,
               unsigned long long *__restrict__ dt_ext, double *__restrict__ norm_part, Cases cs,
               const double *__restrict__ fflux, int32_t F) {
-  face_gather_cell<FLUX, DT, DIAG, PRE>(blockIdx.x * blockDim.x + threadIdx.x, C, cptr, sslots,
+  face_gather_cell<FLUX, DT, DIAG, PRE>(blockIdx.x * blockDim.x + threadIdx.x, C, cptr, gslots,
                                         sptr32, q8, vol, res, res_zero, dt, diag, cfl_tab, iter_counter,
                                         cfl_arg, P0, dt_ext, norm_part, cs, fflux, F);
 }
@@ -423,7 +441,7 @@ k_face_gather(int32_t C, const int32_t *__restrict__ cptr, const SlotRec *__rest
 template <bool FLUX, bool DT, bool DIAG, bool PRE, int MINB = MFG_GATHER_MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
 k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
-                 const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+                 const GatherSlot *__restrict__ gslots, const int32_t *__restrict__ sptr32,
                  const double *__restrict__ q8, const double *__restrict__ vol,
                  double *__restrict__ res, int res_zero, double *__restrict__ dt,
                  double *__restrict__ diag, const double *__restrict__ cfl_tab,
@@ -443,12 +461,12 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
     if (FLUX && !res_zero)
       for (int k = 0; k < 5; k++) r[k] = res[(int64_t)k * C + c];
     const int32_t ns = __ldg(cptr + c + 1) - __ldg(cptr + c);
-    const SlotRec *sl = sslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
+    const GatherSlot *sl = gslots + __ldg(sptr32 + c / kSlice) + c % kSlice;  // sliced
     double dtl = kBig;
     int det = 1;
     double dg0 = 0.0, dg1 = 0.0, dg2 = 0.0, dg3 = 0.0;  // as in face_gather_cell
     for (int32_t j = 0; j < ns; j++) {
-      const SlotRec sr = sl[(int64_t)j * kSlice];
+      const GatherSlot sr = sl[(int64_t)j * kSlice];
       if (FLUX || DT) {
         double qn[Q_STRIDE], mgf = 0.0;
         if (!PRE) load_q(q8, sr.nb, qn);
@@ -456,16 +474,16 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
           double f[5];
           if (PRE) {  // the face's flux, computed once by k_face_flux
             const double2 *row =
-                reinterpret_cast<const double2 *>(fflux + (int64_t)sr.face * kFluxRow);
+                reinterpret_cast<const double2 *>(fflux + (int64_t)(sr.face_c2 & 0x7FFFFFFFu) * kFluxRow);
             const double2 a = __ldg(row), b = __ldg(row + 1), e = __ldg(row + 2);
             f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y; f[4] = e.x;
             mgf = e.y;
-          } else if (sr.flags & SLOT_IS_C2) {
+          } else if (sr.face_c2 >> 31) {
             roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
           } else {
             roe_flux_mx(qd, qn, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
           }
-          if (sr.flags & SLOT_IS_C2) {
+          if (sr.face_c2 >> 31) {
             for (int k = 0; k < 5; k++) r[k] += f[k];
           } else {
             for (int k = 0; k < 5; k++) r[k] -= f[k];
@@ -510,7 +528,7 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
         j0 = ns < 4 ? ns : 4;
       }
       for (int32_t j = j0; j < ns; j++) {
-        const SlotRec sr = sl[(int64_t)j * kSlice];
+        const GatherSlot sr = sl[(int64_t)j * kSlice];
         double vn = qd[1] * sr.nx + qd[2] * sr.ny + qd[3] * sr.nz;
         vn = fabs(vn);
         d += 0.5 * sr.area * (vn + qd[Q_A]) * P.lhs_omga;
@@ -2161,7 +2179,7 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
 // cal_gradient.cpp:1740-1897), divided by the volume.
 __device__ __forceinline__ void grad_faces_cell(
     int32_t c, int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-    const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+    const GradSlot *__restrict__ rslots, const int32_t *__restrict__ sptr32,
     const int32_t *__restrict__ fnptr,
     const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
     const double *__restrict__ q8, const double *__restrict__ vol, double *__restrict__ dqdx,
@@ -2170,14 +2188,14 @@ __device__ __forceinline__ void grad_faces_cell(
   double gx[5] = {0., 0., 0., 0., 0.}, gy[5] = {0., 0., 0., 0., 0.},
          gz[5] = {0., 0., 0., 0., 0.};
   const int32_t ns = cptr[c + 1] - cptr[c];
-  const SlotRec *sl = sslots + sptr32[c / kSlice] + c % kSlice;  // sliced
+  const GradSlot *sl = rslots + sptr32[c / kSlice] + c % kSlice;  // sliced
   for (int32_t j = 0; j < ns; j++) {
-    const SlotRec sr = sl[(int64_t)j * kSlice];
+    const GradSlot sr = sl[(int64_t)j * kSlice];
     double qs[5];
     if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
       double qc[Q_STRIDE], qg[Q_STRIDE];
       load_q(q8, c, qc);
-      load_q(q8, sr.nb, qg);
+      load_q(q8, sr.n0, qg);
       for (int v = 0; v < 5; v++) qs[v] = 0.5 * (qc[v] + qg[v]);
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.0;
@@ -2192,11 +2210,11 @@ __device__ __forceinline__ void grad_faces_cell(
       };
       int32_t nn = 3;
       if (sr.flags & SLOT_TRI) {
-        add(sr.tri[0]);
-        add(sr.tri[1]);
-        add(sr.tri[2]);
+        add(sr.n0);
+        add(sr.n1);
+        add(sr.n2);
       } else {
-        const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+        const int32_t j0 = fnptr[sr.n0], j1 = fnptr[sr.n0 + 1];
         for (int32_t j = j0; j < j1; j++) add(fnodes[j]);
         nn = j1 - j0;
       }
@@ -2255,12 +2273,12 @@ __device__ __forceinline__ void grad_faces_cell(
 
 __global__ void __launch_bounds__(kGradBlockMax)
 k_grad_faces(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-             const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+             const GradSlot *__restrict__ rslots, const int32_t *__restrict__ sptr32,
              const int32_t *__restrict__ fnptr,
              const int32_t *__restrict__ fnodes, const double *__restrict__ qn8,
              const double *__restrict__ q8, const double *__restrict__ vol,
              double *__restrict__ dqdx, double *__restrict__ dqdy, double *__restrict__ dqdz) {
-  grad_faces_cell(blockIdx.x * blockDim.x + threadIdx.x, C, n, cptr, sslots, sptr32, fnptr,
+  grad_faces_cell(blockIdx.x * blockDim.x + threadIdx.x, C, n, cptr, rslots, sptr32, fnptr,
                   fnodes, qn8, q8, vol, dqdx, dqdy, dqdz);
 }
 
@@ -2332,7 +2350,7 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
 
 __global__ void __launch_bounds__(kGradBlockMax)
 k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
-                const SlotRec *__restrict__ sslots, const int32_t *__restrict__ sptr32,
+                const GradSlot *__restrict__ rslots, const int32_t *__restrict__ sptr32,
                 const int32_t *__restrict__ fnptr,
                 const int32_t *__restrict__ fnodes, const float *__restrict__ qn4,
                 const double *__restrict__ q8, const double *__restrict__ vol,
@@ -2344,14 +2362,14 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
   float gx[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, gy[5] = {0.f, 0.f, 0.f, 0.f, 0.f},
         gz[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   const int32_t ns = cptr[c + 1] - cptr[c];
-  const SlotRec *sl = sslots + sptr32[c / kSlice] + c % kSlice;  // sliced
+  const GradSlot *sl = rslots + sptr32[c / kSlice] + c % kSlice;  // sliced
   for (int32_t j = 0; j < ns; j++) {
-    const SlotRec sr = sl[(int64_t)j * kSlice];
+    const GradSlot sr = sl[(int64_t)j * kSlice];
     float qs[5];
     if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG)) {
       double qc[Q_STRIDE], qg[Q_STRIDE];
       load_q(q8, c, qc);
-      load_q(q8, sr.nb, qg);
+      load_q(q8, sr.n0, qg);
       for (int v = 0; v < 5; v++) qs[v] = (float)(0.5 * ((qc[v] - P.ref[v]) + (qg[v] - P.ref[v])));
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.f;
@@ -2366,11 +2384,11 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
       };
       int32_t nn = 3;
       if (sr.flags & SLOT_TRI) {
-        add(sr.tri[0]);
-        add(sr.tri[1]);
-        add(sr.tri[2]);
+        add(sr.n0);
+        add(sr.n1);
+        add(sr.n2);
       } else {
-        const int32_t j0 = fnptr[sr.face], j1 = fnptr[sr.face + 1];
+        const int32_t j0 = fnptr[sr.n0], j1 = fnptr[sr.n0 + 1];
         for (int32_t j = j0; j < j1; j++) add(fnodes[j]);
         nn = j1 - j0;
       }
@@ -2997,7 +3015,8 @@ struct mfg_ctx {
   // the slots again, sliced: the cells in slices of kSlice (a warp), slot j
   // of the slice's lane t at sptr32[slice] + j kSlice + t, so that a warp's
   // one-thread-per-cell gathers read consecutive records
-  SlotRec *sslots = nullptr;
+  GatherSlot *gslots = nullptr;
+  GradSlot *rslots = nullptr;
   int32_t *sptr32 = nullptr;
   FaceRec *faces = nullptr;  // per-face flux: normal, area, cells
   double *fflux = nullptr;   // per-face flux rows [F][kFluxRow]
@@ -4590,12 +4609,23 @@ __global__ void k_slice_width(int32_t C, const int32_t *__restrict__ cptr,
 
 __global__ void k_slice_fill(int32_t C, const int32_t *__restrict__ cptr,
                              const SlotRec *__restrict__ slots, const int32_t *__restrict__ sptr32,
-                             SlotRec *__restrict__ sslots) {
+                             GatherSlot *__restrict__ gslots, GradSlot *__restrict__ rslots) {
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= C) return;
-  SlotRec *o = sslots + sptr32[c / kSlice] + c % kSlice;
+  const int64_t o = sptr32[c / kSlice] + c % kSlice;
   const int32_t s0 = cptr[c], ns = cptr[c + 1] - s0;
-  for (int32_t j = 0; j < ns; j++) o[(int64_t)j * kSlice] = slots[s0 + j];
+  for (int32_t j = 0; j < ns; j++) {
+    const SlotRec sr = slots[s0 + j];
+    const int64_t k = o + (int64_t)j * kSlice;
+    gslots[k] = GatherSlot{sr.nx, sr.ny, sr.nz, sr.area, sr.dn, sr.nb,
+                           (uint32_t)sr.face | ((sr.flags & SLOT_IS_C2) ? 0x80000000u : 0u)};
+    GradSlot g{sr.nx, sr.ny, sr.nz, sr.area, sr.tri[0], sr.tri[1], sr.tri[2], sr.flags};
+    if ((sr.flags & SLOT_BOUNDARY) && !(sr.flags & SLOT_NODE_AVG))
+      g.n0 = sr.nb;  // averaged with the ghost
+    else if (!(sr.flags & SLOT_TRI))
+      g.n0 = sr.face;  // nodes through the face -> node lists
+    rslots[k] = g;
+  }
 }
 
 __global__ void k_node_slice_fill(int32_t N, const int32_t *__restrict__ nptr,
@@ -4609,7 +4639,7 @@ __global__ void k_node_slice_fill(int32_t N, const int32_t *__restrict__ nptr,
 }
 
 // The sliced copies of the slot records and of the node lists (see
-// mfg_ctx::sslots, nsl), from the plain ones on the device.
+// mfg_ctx::gslots, rslots, nsl), from the plain ones on the device.
 int build_sliced_slots(mfg_ctx *ctx) {
   const int32_t C = ctx->C, nsl = (C + kSlice - 1) / kSlice;
   cudaStream_t st = ctx->stream;
@@ -4622,9 +4652,11 @@ int build_sliced_slots(mfg_ctx *ctx) {
   if ((rc = dev_scan(sc, width, ctx->sptr32, nsl + 1, st))) return rc;
   int32_t total = 0;
   if ((rc = dev_read_i32(ctx->sptr32 + nsl, &total, st))) return rc;
-  if ((rc = dalloc(ctx, &ctx->sslots, (size_t)std::max(total, 1)))) return rc;
+  if ((rc = dalloc(ctx, &ctx->gslots, (size_t)std::max(total, 1))) ||
+      (rc = dalloc(ctx, &ctx->rslots, (size_t)std::max(total, 1))))
+    return rc;
   k_slice_fill<<<grid_for(C), kBlock, 0, st>>>(C, ctx->cptr, ctx->slots, ctx->sptr32,
-                                                 ctx->sslots);
+                                                 ctx->gslots, ctx->rslots);
   // the node lists
   const int32_t N = ctx->N, nsn = (N + kSlice - 1) / kSlice;
   int32_t *nwidth = nullptr;
@@ -5220,12 +5252,12 @@ static int launch_face(mfg_ctx *ctx, bool flux, bool dtp, bool diag, double cfl,
 #define MFG_FACE_M(F_, D_, G_, M_)                                                            \
   if (mx)                                                                                     \
     k_face_gather_mx<F_, D_, G_, F_, M_><<<g, kBlock, 0, st>>>(                               \
-        ctx->C, ctx->cptr, ctx->sslots, ctx->sptr32, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
+        ctx->C, ctx->cptr, ctx->gslots, ctx->sptr32, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
         ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
         ctx->F);                                                                              \
   else                                                                                        \
     k_face_gather<F_, D_, G_, F_, M_><<<g, kBlock, 0, st>>>(                                  \
-        ctx->C, ctx->cptr, ctx->sslots, ctx->sptr32, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
+        ctx->C, ctx->cptr, ctx->gslots, ctx->sptr32, q, ctx->vol, ctx->res, ctx->res_zero ? 1 : 0, ctx->dt,  \
         ctx->diag, tab, ctx->iter_counter, cfl, ctx->P, ctx->dt_ext, np, cs, ctx->fflux,       \
         ctx->F)
 #define MFG_FACE(F_, D_, G_) MFG_FACE_M(F_, D_, G_, MFG_GATHER_MINB)
@@ -5502,11 +5534,11 @@ static void launch_grad_faces(mfg_ctx *ctx, cudaStream_t st) {
   }
   if (ctx->precision == MFG_PREC_MIXED)
     k_grad_faces_mx<<<grid_for(ctx->C, gb), gb, 0, st>>>(
-        ctx->C, ctx->n, ctx->cptr, ctx->sslots, ctx->sptr32, ctx->fnptr, ctx->fnodes, ctx->qn4,
+        ctx->C, ctx->n, ctx->cptr, ctx->rslots, ctx->sptr32, ctx->fnptr, ctx->fnodes, ctx->qn4,
         ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz, ctx->P, cases_of(ctx));
   else
     k_grad_faces<<<grid_for(ctx->C, gb), gb, 0, st>>>(
-        ctx->C, ctx->n, ctx->cptr, ctx->sslots, ctx->sptr32, ctx->fnptr, ctx->fnodes, ctx->qn8,
+        ctx->C, ctx->n, ctx->cptr, ctx->rslots, ctx->sptr32, ctx->fnptr, ctx->fnodes, ctx->qn8,
         ctx->q8[ctx->cur], ctx->vol, ctx->dqdx, ctx->dqdy, ctx->dqdz);
   count_launch();
 }
