@@ -97,3 +97,30 @@ def test_lane_per_face_gathers_same_bits(cube24, mixed):
     assert_bitwise(b.residual_norm(), a.residual_norm(), f"{prec} routine norm")
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_lane_per_face_gathers_hexahedra_and_prisms(mixed):
+    """Eight lanes per cell (hexahedra and prisms, 5 and 6 faces, walls,
+    symmetry and far field): the same bits as one thread per cell."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from minifs_b200 import _lib, grid as gr, meshgen
+    from minifs_b200.solver import Solver
+    m = meshgen.hexprism_mesh(10, 9, 8, jitter=0.15, seed=5, bc_types=(6, 6, 4, 6, 3, 6))
+    p = gr.make_params(mach=0.6, alpha=2.0, cfl_start=10.0, cfl_end=10.0)
+    pg = gr.prepare(m, p, bump_amp=0.05, bump_sigma=0.15)
+    prec = "mixed" if mixed else "fp64"
+    a, b = Solver(pg, p, precision=prec), Solver(pg, p, precision=prec)
+    with pytest.raises(_lib.MfgError):
+        b.set_gather_lanes(4)  # cells of six faces
+    b.set_gather_lanes(8)
+    for s in (a, b):
+        s.calculate_gradient()
+    na, nb = a.iterate(4), b.iterate(4)
+    assert_bitwise(nb.reshape(-1), na.reshape(-1), f"{prec} norms")
+    for f in ("q", "res", "dt", "diag", "dq", "dqdx", "dqdy", "dqdz"):
+        assert_bitwise(b.download(f), a.download(f), f"{prec} eight lanes: {f}")
+    a.close()
+    b.close()
