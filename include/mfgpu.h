@@ -207,9 +207,11 @@ int mfg_set_chunking(int32_t kind);
 #define MFG_SWEEP_DEEP 0
 #define MFG_SWEEP_WIDE 1
 int mfg_set_sweep_kernel(int32_t kind);
-/* Times n_trial fused iterations with each lane count on this context's own
- * grid and keeps the faster (ms_out[2], optional, receives the ms per
- * iteration of W and W / 2 lanes).  The state and the dt extrema are
+/* Times n_trial fused iterations with each lane count the persistent
+ * sweeps take on this context's own grid and keeps the faster (ms_out[2],
+ * optional, receives the ms per iteration of W and W / 2 lanes; the
+ * current kernels take W only, so ms_out[1] is -1).  mfg_autotune covers
+ * this and the other launch parameters.  The state and the dt extrema are
  * restored afterwards; res, dt, Diag, DQ and the gradient hold the last
  * trial iteration's values.  iter_done: the CFL ramp position to time at. */
 int mfg_autotune_sweeps(mfg_ctx *ctx, int32_t n_trial, int32_t iter_done, double *ms_out);
