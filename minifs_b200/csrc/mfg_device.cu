@@ -322,7 +322,11 @@ __device__ __forceinline__ void face_gather_cell(
     const Cases &cs, const double *__restrict__ fflux, int32_t F) {
   const bool live = c < C;
   const int32_t cse = live ? case_of(cs, c) : 0;
-  const Params P = live ? params_of(P0, cs, c) : P0;
+  // the parameters the gather reads, field by field: a batch's case table
+  // or the kernel argument
+  const Params *Pc = (live && cs.P) ? cs.P + cse : nullptr;
+  const double p_bar = Pc ? Pc->p_bar : P0.p_bar;
+  const double lhs_omga = Pc ? Pc->lhs_omga : P0.lhs_omga;
   double qc[Q_STRIDE];
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   double dtc = 0.0;
@@ -354,9 +358,9 @@ __device__ __forceinline__ void face_gather_cell(
             f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y; f[4] = e.x;
             mgf = e.y;
           } else if (sr.face_c2 >> 31) {
-            roe_flux(qn, qc, sr.nx, sr.ny, sr.nz, sr.area, P, f);
+            roe_flux(qn, qc, sr.nx, sr.ny, sr.nz, sr.area, params_of(P0, cs, c), f);
           } else {
-            roe_flux(qc, qn, sr.nx, sr.ny, sr.nz, sr.area, P, f);
+            roe_flux(qc, qn, sr.nx, sr.ny, sr.nz, sr.area, params_of(P0, cs, c), f);
           }
           if (sr.face_c2 >> 31) {
             for (int k = 0; k < 5; k++) r[k] += f[k];
@@ -370,7 +374,7 @@ __device__ __forceinline__ void face_gather_cell(
           const double eigv = vn + qc[Q_A];
           dtl = smin(dtl, sr.dn / eigv);
           if (DIAG) {
-            const double t = 0.5 * sr.area * eigv * P.lhs_omga;
+            const double t = 0.5 * sr.area * eigv * lhs_omga;
             dg0 = j == 0 ? t : dg0;
             dg1 = j == 1 ? t : dg1;
             dg2 = j == 2 ? t : dg2;
@@ -380,7 +384,7 @@ __device__ __forceinline__ void face_gather_cell(
           if (PRE) {
             if (mgf != 0.0) det = 0;
           } else {
-            const double dp = fabs(qn[4] - qc[4]) / (qn[4] + qc[4] + P.p_bar + P.p_bar);
+            const double dp = fabs(qn[4] - qc[4]) / (qn[4] + qc[4] + p_bar + p_bar);
             if (dp > 0.1) det = 0;
           }
         }
@@ -390,7 +394,8 @@ __device__ __forceinline__ void face_gather_cell(
       const double cfl =
           cfl_tab ? cfl_tab[(int64_t)(*iter_counter) * max(cs.ncase, 1) + cse] : cfl_arg;
       const double cfl_min = 0.5 * cfl;
-      dtc = dtl * local_cfl(qc[4], det, cfl, cfl_min, P);
+      dtc = dtl * local_cfl_pb(qc[4], det, cfl, cfl_min, Pc ? Pc->p_break : P0.p_break,
+                               Pc ? Pc->p_min : P0.p_min);
       dt[c] = dtc;
     }
     if (DIAG) {
@@ -409,7 +414,7 @@ __device__ __forceinline__ void face_gather_cell(
         double vn = qc[1] * sr.nx + qc[2] * sr.ny + qc[3] * sr.nz;
         vn = fabs(vn);
         const double eig = vn + qc[Q_A];
-        d += 0.5 * sr.area * eig * P.lhs_omga;
+        d += 0.5 * sr.area * eig * lhs_omga;
       }
       diag[c] = d;
     }
@@ -451,8 +456,9 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = c < C;
   const int32_t cse = live ? case_of(cs, c) : 0;
-  const Params P = live ? params_of(P0, cs, c) : P0;
-  const FluxP<float> FP = flux_params<float>(P);
+  const Params *Pc = (live && cs.P) ? cs.P + cse : nullptr;  // as in face_gather_cell
+  const double p_bar = Pc ? Pc->p_bar : P0.p_bar;
+  const double lhs_omga = Pc ? Pc->lhs_omga : P0.lhs_omga;
   double qd[Q_STRIDE];
   double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   double dtc = 0.0;
@@ -479,9 +485,11 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
             f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y; f[4] = e.x;
             mgf = e.y;
           } else if (sr.face_c2 >> 31) {
-            roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
+            const Params P = params_of(P0, cs, c);
+            roe_flux_mx(qn, qd, sr.nx, sr.ny, sr.nz, sr.area, P, flux_params<float>(P), f);
           } else {
-            roe_flux_mx(qd, qn, sr.nx, sr.ny, sr.nz, sr.area, P, FP, f);
+            const Params P = params_of(P0, cs, c);
+            roe_flux_mx(qd, qn, sr.nx, sr.ny, sr.nz, sr.area, P, flux_params<float>(P), f);
           }
           if (sr.face_c2 >> 31) {
             for (int k = 0; k < 5; k++) r[k] += f[k];
@@ -495,7 +503,7 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
           const double eigv = vn + qd[Q_A];
           dtl = smin(dtl, sr.dn / eigv);
           if (DIAG) {
-            const double t = 0.5 * sr.area * eigv * P.lhs_omga;
+            const double t = 0.5 * sr.area * eigv * lhs_omga;
             dg0 = j == 0 ? t : dg0;
             dg1 = j == 1 ? t : dg1;
             dg2 = j == 2 ? t : dg2;
@@ -504,7 +512,7 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
           if (PRE) {
             if (mgf != 0.0) det = 0;
           } else {
-            const double dp = fabs(qn[4] - qd[4]) / (qn[4] + qd[4] + P.p_bar + P.p_bar);
+            const double dp = fabs(qn[4] - qd[4]) / (qn[4] + qd[4] + p_bar + p_bar);
             if (dp > 0.1) det = 0;
           }
         }
@@ -513,7 +521,8 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
     if (DT) {
       const double cfl =
           cfl_tab ? cfl_tab[(int64_t)(*iter_counter) * max(cs.ncase, 1) + cse] : cfl_arg;
-      dtc = dtl * local_cfl(qd[4], det, cfl, 0.5 * cfl, P);
+      dtc = dtl * local_cfl_pb(qd[4], det, cfl, 0.5 * cfl, Pc ? Pc->p_break : P0.p_break,
+                               Pc ? Pc->p_min : P0.p_min);
       dt[c] = dtc;
     }
     if (DIAG) {
@@ -531,7 +540,7 @@ k_face_gather_mx(int32_t C, const int32_t *__restrict__ cptr,
         const GatherSlot sr = sl[(int64_t)j * kSlice];
         double vn = qd[1] * sr.nx + qd[2] * sr.ny + qd[3] * sr.nz;
         vn = fabs(vn);
-        d += 0.5 * sr.area * (vn + qd[Q_A]) * P.lhs_omga;
+        d += 0.5 * sr.area * (vn + qd[Q_A]) * lhs_omga;
       }
       diag[c] = d;
     }

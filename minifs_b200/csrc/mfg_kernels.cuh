@@ -622,17 +622,21 @@ __device__ __forceinline__ void update_cell(double *q, const double *DQ, const P
 }
 
 // LimitTimeStep's local CFL (compute_timestep.cpp:881-906).
-__device__ __forceinline__ double local_cfl(double p, int det, double cfl, double cfl_min,
-                                            const Params &P) {
+__device__ __forceinline__ double local_cfl_pb(double p, int det, double cfl, double cfl_min,
+                                               double p_break, double p_min) {
   double cfl_tmp;
-  if (p > P.p_break)
+  if (p > p_break)
     cfl_tmp = cfl;
-  else if (p < P.p_min)
+  else if (p < p_min)
     cfl_tmp = cfl_min;
   else
-    cfl_tmp = (p - P.p_min) / (P.p_break - P.p_min) * (cfl - cfl_min) + cfl_min;
+    cfl_tmp = (p - p_min) / (p_break - p_min) * (cfl - cfl_min) + cfl_min;
   if (!det) cfl_tmp = cfl_min;
   return cfl_tmp;
+}
+__device__ __forceinline__ double local_cfl(double p, int det, double cfl, double cfl_min,
+                                            const Params &P) {
+  return local_cfl_pb(p, det, cfl, cfl_min, P.p_break, P.p_min);
 }
 
 // Order-preserving bit pattern of a non-negative double for atomic max/min.
