@@ -733,8 +733,8 @@ k_face_flux(int32_t F, const FaceRec *__restrict__ faces, const double *__restri
   const FaceRec fr = faces[f];
   const Params P = params_of(P0, cs, fr.c1);
   double ql[Q_STRIDE], qr[Q_STRIDE], fl[5];
-  load_q(q8, fr.c1, ql);
-  load_q(q8, fr.c2, qr);
+  load_q_w(q8, fr.c1, ql);
+  load_q_w(q8, fr.c2, qr);
   // CellIsMG's test of the two cells' states (first order, as the gathers)
   const double dp = fabs(qr[4] - ql[4]) / (qr[4] + ql[4] + P.p_bar + P.p_bar);
   const double mg = dp > 0.1 ? 1.0 : 0.0;
@@ -2158,8 +2158,8 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
       const int32_t k = en.src;
       const double w = en.w;
       double qa[Q_STRIDE], qb[Q_STRIDE];
-      load_q(q8, bface_c1[k], qa);
-      load_q(q8, (int64_t)C + k, qb);
+      load_q5_w(q8, bface_c1[k], qa);
+      load_q5_w(q8, (int64_t)C + k, qb);
       for (int v = 0; v < 5; v++) {
         double facq = qa[v] + qb[v];
         facq *= 0.5;
@@ -2170,7 +2170,7 @@ k_node_values(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
     for (int32_t j = 0; j < ne; j++) {
       const NodeEnt en = el[(int64_t)j * kSlice];
       double qa[Q_STRIDE];
-      load_q(q8, en.src, qa);
+      load_q5_w(q8, en.src, qa);
       const double w = en.w;
       for (int v = 0; v < 5; v++) acc[v] += qa[v] * w;
     }
@@ -2209,8 +2209,10 @@ __device__ __forceinline__ void grad_faces_cell(
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.0;
       auto add = [&](int32_t node) {
-        const double2 *p = reinterpret_cast<const double2 *>(qn8 + (int64_t)node * Q_STRIDE);
-        const double2 a = __ldg(p), b = __ldg(p + 1), e = __ldg(p + 2);
+        const double *pn = qn8 + (int64_t)node * Q_STRIDE;
+        double2 a, b, e;
+        ldg_v4(pn, a.x, a.y, b.x, b.y);
+        e.x = __ldg(pn + 4);
         qs[0] += a.x;
         qs[1] += a.y;
         qs[2] += b.x;
@@ -2336,8 +2338,8 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
       const int32_t k = en.src;
       const float w = (float)en.w;
       double qa[Q_STRIDE], qb[Q_STRIDE];
-      load_q(q8, bface_c1[k], qa);
-      load_q(q8, (int64_t)C + k, qb);
+      load_q5_w(q8, bface_c1[k], qa);
+      load_q5_w(q8, (int64_t)C + k, qb);
       for (int v = 0; v < 5; v++)
         acc[v] += (float)(0.5 * ((qa[v] - P.ref[v]) + (qb[v] - P.ref[v]))) * w;
     }
@@ -2345,7 +2347,7 @@ k_node_values_mx(int32_t N, int32_t C, const int32_t *__restrict__ nptr,
     for (int32_t j = 0; j < ne; j++) {
       const NodeEnt en = el[(int64_t)j * kSlice];
       double qa[Q_STRIDE];
-      load_q(q8, en.src, qa);
+      load_q5_w(q8, en.src, qa);
       const float w = (float)en.w;
       for (int v = 0; v < 5; v++) acc[v] += (float)(qa[v] - P.ref[v]) * w;
     }
@@ -2383,8 +2385,10 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.f;
       auto add = [&](int32_t node) {
-        const float4 *p = reinterpret_cast<const float4 *>(qn4 + (int64_t)node * Q_STRIDE);
-        const float4 a = __ldg(p), b = __ldg(p + 1);
+        float t8[8];
+        ldg_v8f(qn4 + (int64_t)node * Q_STRIDE, t8);
+        const float4 a = make_float4(t8[0], t8[1], t8[2], t8[3]),
+                     b = make_float4(t8[4], t8[5], t8[6], t8[7]);
         qs[0] += a.x;
         qs[1] += a.y;
         qs[2] += a.z;
