@@ -2209,15 +2209,13 @@ __device__ __forceinline__ void grad_faces_cell(
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.0;
       auto add = [&](int32_t node) {
-        const double *pn = qn8 + (int64_t)node * Q_STRIDE;
-        double2 a, b, e;
-        ldg_v4(pn, a.x, a.y, b.x, b.y);
-        e.x = __ldg(pn + 4);
-        qs[0] += a.x;
-        qs[1] += a.y;
-        qs[2] += b.x;
-        qs[3] += b.y;
-        qs[4] += e.x;
+        double r[5];
+        load_q5_w(qn8, node, r);
+        qs[0] += r[0];
+        qs[1] += r[1];
+        qs[2] += r[2];
+        qs[3] += r[3];
+        qs[4] += r[4];
       };
       int32_t nn = 3;
       if (sr.flags & SLOT_TRI) {
@@ -2385,15 +2383,13 @@ k_grad_faces_mx(int32_t C, int64_t n, const int32_t *__restrict__ cptr,
     } else {
       for (int v = 0; v < 5; v++) qs[v] = 0.f;
       auto add = [&](int32_t node) {
-        float t8[8];
-        ldg_v8f(qn4 + (int64_t)node * Q_STRIDE, t8);
-        const float4 a = make_float4(t8[0], t8[1], t8[2], t8[3]),
-                     b = make_float4(t8[4], t8[5], t8[6], t8[7]);
-        qs[0] += a.x;
-        qs[1] += a.y;
-        qs[2] += a.z;
-        qs[3] += a.w;
-        qs[4] += b.x;
+        float r[8];
+        ldg_v8f(qn4 + (int64_t)node * Q_STRIDE, r);
+        qs[0] += r[0];
+        qs[1] += r[1];
+        qs[2] += r[2];
+        qs[3] += r[3];
+        qs[4] += r[4];
       };
       int32_t nn = 3;
       if (sr.flags & SLOT_TRI) {
