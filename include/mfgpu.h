@@ -158,10 +158,17 @@ int mfg_batch_layout(mfg_ctx *ctx, int32_t *cell0, int32_t *bface0);
 int mfg_batch_dt_extrema(mfg_ctx *ctx, double *ext);
 /* Residual L2 norms per case: out[5k + v]. */
 int mfg_batch_residual_norm(mfg_ctx *ctx, double *out);
+/* Frees the context's device and pinned host memory, streams, events and
+ * graphs. */
 int mfg_destroy(mfg_ctx *ctx);
 /* Issue all further work on this cudaStream_t (NULL = the context's own). */
 int mfg_set_stream(mfg_ctx *ctx, void *cuda_stream);
+/* New flow parameters (e.g. another CFL ramp) for the following calls;
+ * the captured iteration graphs are rebuilt on the next mfg_iterate.
+ * MFG_ERR_UNSUPPORTED for a batch (its cases fix theirs at creation). */
 int mfg_set_params(mfg_ctx *ctx, const mfg_params *params);
+/* Sizes, level counts, precision, device bytes, and the sweep choices and
+ * their record counts (mfg_info above); host-side only. */
 int mfg_info_get(mfg_ctx *ctx, mfg_info *info);
 /* Sweep strategy: 0 = one kernel per LU-SGS level; 1 (default when the
  * device supports cooperative launch) = one persistent kernel per sweep: the
@@ -503,6 +510,7 @@ int mfg_halo_phase(mfg_ctx *ctx, int32_t phase, int32_t iter_done);
 /* ---- data movement ----------------------------------------------------- */
 int mfg_download(mfg_ctx *ctx, int32_t field, double *host);
 int mfg_upload(mfg_ctx *ctx, int32_t field, const double *host);
+/* Waits for the work issued on the context's stream. */
 int mfg_sync(mfg_ctx *ctx);
 
 /* ---- diagnostics ------------------------------------------------------- */
