@@ -783,7 +783,34 @@ def _cpu_sample(mesh, wl, iters, tdtree):
                       f"{time.perf_counter() - t0:.1f} s"}
 
 
-def form_batched(args, local, stream):
+def cpu_sample_batched(bw, ncase=8, iters=5, seed=7):
+    """The reference's threaded build on all host cores over a seeded subset
+    of the batch's cases, one case after another (its per-case runs), capped
+    at `iters` iterations each: cell-updates over the summed iteration times
+    (each case's set-up stated apart)."""
+    from minifs_b200 import meshgen
+    rng = np.random.default_rng(seed)
+    pick = sorted(int(i) for i in rng.choice(len(bw["cases"]), size=min(ncase, len(bw["cases"])),
+                                             replace=False))
+    t0 = time.perf_counter()
+    updates, t, r, cells = 0, 0.0, None, 0
+    for i in pick:
+        c = bw["cases"][i]
+        mesh = meshgen.cube_mesh(c["n"], jitter=c["jitter"], seed=c["seed"])
+        r = cpu_reference_run(mesh, c, iters, tdtree=True)
+        if r is None:
+            return None
+        updates += mesh.n_cell * len(r["iter_times"])
+        t += sum(r["iter_times"])
+        cells += mesh.n_cell
+    return {"value": float(updates / t), "unit": UNIT, "cores": r["threads"], "kind": r["kind"],
+            "sample": f"{bw['name']}: cases {pick} ({cells} cells) one after another, "
+                      f"{iters} full iterations each (iteration-capped) after set-up, "
+                      f"{r['desc']}, {t:.2f} s; run with its set-ups "
+                      f"{time.perf_counter() - t0:.1f} s"}
+
+
+def form_batched(args, local, stream, with_cpu=False):
     """Configuration 4: 64 cube cases (n uniform in 8..48, Mach U(0.3, 0.8),
     alpha U(-5, 5) deg, jitter U(0, 0.2)h) in one context against the same
     cases one after another in their own contexts, FP64 and mixed, each over
@@ -840,6 +867,11 @@ def form_batched(args, local, stream):
                          "sweep_chunking": info["sweep_chunking"],
                          "sweep_model_us": info["sweep_model_us"]}
     out["clocks"] = clk.summary()
+    if with_cpu:
+        try:
+            out["cpu_baseline"] = cpu_sample_batched(bw)
+        except Exception as e:  # reported beside the GPU figures
+            out["cpu_baseline"] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
     return out
 
 
@@ -848,7 +880,7 @@ def run_forms(args, local, stream, with_cpu):
     forms = {}
     for name, fn in (("mixed", lambda: form_mixed(args, local, stream, with_cpu)),
                      ("channel", lambda: form_channel(args, local, stream, with_cpu)),
-                     ("batched", lambda: form_batched(args, local, stream))):
+                     ("batched", lambda: form_batched(args, local, stream, with_cpu))):
         t0 = time.perf_counter()
         try:
             forms[name] = fn()
@@ -1121,6 +1153,12 @@ def run_batched(args, rank, world, local, stream, dist):
     norms = b.residual_norm()
     info = r["info"]
     seq_value = total_cells * args.steps / (seq_ms / 1e3)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_sample_batched(bw)
+        except Exception as e:  # reported beside the GPU figures
+            cpu = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
     if rank == 0:
         ns = [c["n"] for c in bw["cases"]]
         line = {
@@ -1151,7 +1189,7 @@ def run_batched(args, rank, world, local, stream, dist):
             "roofline": r["roofline"],
             "flux_plus_gradient": r["flux_plus_gradient"],
             "phases": r["phases"],
-            "cpu_baseline": None,
+            "cpu_baseline": cpu,
             "e2e": r["e2e"],
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
