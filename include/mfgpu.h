@@ -202,6 +202,22 @@ int mfg_set_sweep_lanes(mfg_ctx *ctx, int32_t lanes);
 #define MFG_CHUNK_TRANSVERSE_YZ 3
 #define MFG_CHUNK_TRANSVERSE_ANY 4 /* the best transverse grid over any axis pair */
 int mfg_set_chunking(int32_t kind);
+/* The chunk assignment a context makes for one sweep, on the host (no
+ * device; for inspection and tests).  The sweep: L levels over C cells,
+ * lptr [L + 1] the level bounds in cells [C] (cells in level order, a
+ * permutation of 0..C-1), and the dependencies of the cell at position i
+ * in nbs[sptr[i] .. sptr[i + 1]) (cell ids; ids >= C, ghosts, are not
+ * dependencies).  xc, yc, zc: cell centroids [C] for the transverse
+ * assignments (NULL: the vote only).  P chunks of G lane groups each;
+ * force: -1 (the model's choice, as a context makes it) or MFG_CHUNK_*.
+ * assign [C]: each cell's chunk; grid (optional, [2]): the transverse
+ * grid Pa, Pb (a cell's chunk is la + Pa * lb), 0, 0 for the vote;
+ * est_us (optional): the modelled sweep duration.  Returns the assignment
+ * made (MFG_CHUNK_*), MFG_ERR_INVALID for inconsistent tables. */
+int mfg_plan_chunks(int32_t C, int32_t L, const int32_t *lptr, const int32_t *cells,
+                    const int32_t *sptr, const int32_t *nbs, const double *xc,
+                    const double *yc, const double *zc, int32_t P, int32_t G, int32_t force,
+                    int32_t *assign, int32_t *grid, double *est_us);
 /* The persistent sweep kernels.  MFG_SWEEP_DEEP: one block per SM, producer
  * warps staging each cell's static terms ahead for consumer lane pairs that
  * run only the dependent chain -- short per-level latency, for levels of up

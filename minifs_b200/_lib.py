@@ -158,6 +158,9 @@ def load(build_if_missing: bool = True):
         "mfg_set_sweep_lanes": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_gather_lanes": (ct.c_int, [ctxp, ct.c_int32]),
         "mfg_set_chunking": (ct.c_int, [ct.c_int32]),
+        "mfg_plan_chunks": (ct.c_int, [ct.c_int32, ct.c_int32, i32p, i32p, i32p, i32p, f64p, f64p,
+                                       f64p, ct.c_int32, ct.c_int32, ct.c_int32, i32p, i32p,
+                                       f64p]),
         "mfg_set_sweep_kernel": (ct.c_int, [ct.c_int32]),
         "mfg_autotune_sweeps": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, f64p]),
         "mfg_autotune": (ct.c_int, [ctxp, ct.c_int32, ct.c_int32, ct.c_int32,

@@ -3793,15 +3793,17 @@ static int32_t max_chunk_level(int32_t P, const std::vector<int32_t> &lptr, cons
 // first (else the fewest cells per chunk and level); among those the
 // shortest modelled sweep is kept.  Returns the choice (MFG_CHUNK_VOTE or
 // MFG_CHUNK_TRANSVERSE_*) and its modelled duration in microseconds at
-// 1.9 GHz.
+// 1.9 GHz; grid (optional) receives the transverse grid Pa, Pb (0, 0 for
+// the vote).
 static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int32_t> &lptr,
                          const int32_t *cells, const int32_t *sptr, const int32_t *nbs,
                          const double *const xyz[3], int force, std::vector<int32_t> &assign,
-                         double *est_us) {
+                         double *est_us, int32_t *grid = nullptr) {
   std::vector<int32_t> best, cand;
   double tbest = 1e300;
   int32_t lbest = INT32_MAX;
   int choice = MFG_CHUNK_VOTE;
+  int32_t pa_best = 0;
   // MFG_CHUNK_TRANSVERSE_ANY: the transverse grids of every axis pair, no vote
   const bool any_t = force == MFG_CHUNK_TRANSVERSE_ANY;
   if (any_t) force = -1;
@@ -3830,6 +3832,7 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
     struct Best {
       int32_t load = INT32_MAX;
       double t = 1e300;
+      int32_t pa = 0;
       std::vector<int32_t> assign;
     } pb[3];
     auto pair_search = [&](int kind) {
@@ -3857,6 +3860,7 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
         if (load < b.load || t < b.t) {
           b.load = load;
           b.t = t;
+          b.pa = Pa;
           b.assign.swap(a);
         }
       }
@@ -3871,6 +3875,7 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
       lbest = b.load;
       tbest = b.t;
       choice = kind;
+      pa_best = b.pa;
       best.swap(b.assign);
     }
   }
@@ -3878,10 +3883,15 @@ static int choose_chunks(int32_t C, int32_t P, int32_t G, const std::vector<int3
     assign_chunks(C, P, lptr, cells, sptr, nbs, best);
     tbest = model_sweep_cycles(C, P, G, lptr, cells, sptr, nbs, best);
     choice = MFG_CHUNK_VOTE;
+    pa_best = 0;
   }
   (void)lbest;
   assign.swap(best);
   if (est_us) *est_us = tbest / 1900.0;
+  if (grid) {
+    grid[0] = choice == MFG_CHUNK_VOTE ? 0 : pa_best;
+    grid[1] = choice == MFG_CHUNK_VOTE ? 0 : P / pa_best;
+  }
   return choice;
 }
 
@@ -5053,6 +5063,42 @@ int mfg_set_chunking(int32_t kind) {
   if (kind < -1 || kind > MFG_CHUNK_TRANSVERSE_ANY) return MFG_ERR_INVALID;
   g_chunking.store(kind);
   return MFG_OK;
+}
+
+int mfg_plan_chunks(int32_t C, int32_t L, const int32_t *lptr, const int32_t *cells,
+                    const int32_t *sptr, const int32_t *nbs, const double *xc,
+                    const double *yc, const double *zc, int32_t P, int32_t G, int32_t force,
+                    int32_t *assign, int32_t *grid, double *est_us) {
+  if (C < 0 || L < 0 || P < 1 || G < 1 || !lptr || (C > 0 && (!cells || !sptr || !nbs || !assign)))
+    return MFG_ERR_INVALID;
+  if (force < -1 || force > MFG_CHUNK_TRANSVERSE_ANY) return MFG_ERR_INVALID;
+  // the tables are indexed by what they hold: check them all first
+  if (lptr[0] != 0 || lptr[L] != C) return MFG_ERR_INVALID;
+  for (int32_t l = 0; l < L; l++)
+    if (lptr[l + 1] < lptr[l]) return MFG_ERR_INVALID;
+  std::vector<char> seen(C, 0);
+  for (int32_t i = 0; i < C; i++) {
+    if (cells[i] < 0 || cells[i] >= C || seen[cells[i]]) return MFG_ERR_INVALID;
+    seen[cells[i]] = 1;
+  }
+  if (C > 0 && sptr[0] != 0) return MFG_ERR_INVALID;
+  for (int32_t i = 0; i < C; i++)
+    if (sptr[i + 1] < sptr[i]) return MFG_ERR_INVALID;
+  for (int32_t s0 = 0; C > 0 && s0 < sptr[C]; s0++)
+    if (nbs[s0] < 0) return MFG_ERR_INVALID;
+  const std::vector<int32_t> lp(lptr, lptr + L + 1);
+  const double *const xyz[3] = {xc, yc, zc};
+  std::vector<int32_t> a;
+  int32_t g[2] = {0, 0};
+  double us = 0.0;
+  const int choice = choose_chunks(C, P, G, lp, cells, sptr, nbs, xyz, force, a, &us, g);
+  if (C > 0) std::copy(a.begin(), a.end(), assign);
+  if (grid) {
+    grid[0] = g[0];
+    grid[1] = g[1];
+  }
+  if (est_us) *est_us = us;
+  return choice;
 }
 
 int mfg_set_sweep_kernel(int32_t kind) {
